@@ -1,0 +1,147 @@
+/*
+ * pbbfmm3d_b200 — C ABI of the B200-native black-box FMM matvec.
+ *
+ * This is the drop-in boundary for PBBFMM3D's matvec hot path
+ * (H2_3D_Compute<T>, include/compute.hpp:67-149 of the reference).  Plain
+ * pointers and sizes only; every call returns a status code (never exits)
+ * and pbbfmm_last_error() describes the most recent failure on this thread.
+ *
+ * Object model, one-to-one with the reference:
+ *   pbbfmm_tree_create   <- H2_3D_Tree(L, tree_level, order, eps, use_chebyshev)
+ *                           + SetKernelProperty()   (src/H2_3D_Tree.cpp:12-38,
+ *                           src/kernel_Types.cpp)
+ *   pbbfmm_tree_build    <- buildFMMTree()          (src/H2_3D_Tree.cpp:40-66)
+ *   pbbfmm_compute       <- H2_3D_Compute<T>(tree, target, source, weight,
+ *                           nCols, output)           (include/compute.hpp:67)
+ * A tree is built once and can then serve any number of computes (the
+ * reference cannot be reused; here geometry and operators are cached on the
+ * device and points are re-binned on every call).
+ *
+ * Layouts (as in the reference): points are xyz AoS float64 (vector3,
+ * include/bbfmm.h:29-39); weight is column-major Ns x nCols
+ * (weight[col*Ns + i]); output is column-major Nf x nCols and is ACCUMULATED
+ * into (include/compute.hpp:747).  Sources and targets may differ.
+ */
+#ifndef PBBFMM3D_B200_H
+#define PBBFMM3D_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ---- */
+#define PBBFMM_OK 0
+#define PBBFMM_ERR_ARG 1         /* bad argument (size, order, level, pointer) */
+#define PBBFMM_ERR_CUDA 2        /* CUDA runtime / launch error                */
+#define PBBFMM_ERR_ALLOC 3       /* device or host allocation failed           */
+#define PBBFMM_ERR_STATE 4       /* call out of order (e.g. compute before build) */
+#define PBBFMM_ERR_IO 5          /* operator cache file unreadable / malformed */
+#define PBBFMM_ERR_UNSUPPORTED 6 /* combination not implemented                */
+#define PBBFMM_ERR_NUMERIC 7     /* non-finite input detected                  */
+
+/* ---- built-in kernels (src/kernel_Types.cpp; the last three are the user
+ * kernels of the reference's examples and python binding) ---- */
+#define PBBFMM_KERNEL_LAPLACIAN 0       /* 1/r            homogen -1 */
+#define PBBFMM_KERNEL_ONEOVERR2 1       /* 1/r^2          homogen -2 */
+#define PBBFMM_KERNEL_ONEOVERR4 2       /* 1/r^4          homogen -4 */
+#define PBBFMM_KERNEL_GAUSSIAN 3        /* exp(-r^2)                 */
+#define PBBFMM_KERNEL_LOGARITHM 4       /* 0.5 log(r^2)              */
+#define PBBFMM_KERNEL_QUADRIC 5         /* 1 + r^2                   */
+#define PBBFMM_KERNEL_INVQUADRIC 6      /* 1 / (1 + r^2)             */
+#define PBBFMM_KERNEL_THINPLATESPLINE 7 /* 0.5 r^2 log(r^2)          */
+#define PBBFMM_KERNEL_EXPCOV 8          /* exp(-r / p0)              */
+#define PBBFMM_KERNEL_GAUSSSIGMA 9      /* exp(-r^2 / (2 p0^2))      */
+#define PBBFMM_KERNEL_ANISOEXP 10       /* 0.75 exp(-sqrt(dx^2/100 + dy^2/100 + dz^2/2.25)) */
+#define PBBFMM_KERNEL_COUNT 11
+
+/* ---- precision modes ---- */
+#define PBBFMM_PREC_FP64 0  /* every phase in float64 (the plain GPU path)  */
+#define PBBFMM_PREC_MIXED 1 /* tensor-core split-precision M2L, FP32 Kahan
+                               interpolation and near field                  */
+
+typedef struct pbbfmm_tree pbbfmm_tree;
+
+typedef struct {
+  double L;                /* side of the cubic computational box           */
+  int tree_level;          /* number of levels below the root               */
+  int interpolation_order; /* n, nodes per dimension (2..10)                */
+  double epsilon;          /* SVD truncation tolerance (Chebyshev)          */
+  int use_chebyshev;       /* 1: Chebyshev + SVD M2L, 0: uniform + FFT M2L  */
+  int kernel;              /* PBBFMM_KERNEL_*                               */
+  double kernel_param[4];  /* kernel parameters (p0 = length scale)         */
+} pbbfmm_tree_params;
+
+/* H2_3D_Tree constructor + SetKernelProperty (src/H2_3D_Tree.cpp:12-38).
+ * Selects the CUDA device; nothing is computed yet.  device = -1 makes a
+ * host-only tree: buildFMMTree's float64 precompute and the operator
+ * accessors work without a GPU, computes return PBBFMM_ERR_STATE. */
+int pbbfmm_tree_create(const pbbfmm_tree_params *params, int device, pbbfmm_tree **tree);
+
+/* buildFMMTree (src/H2_3D_Tree.cpp:40-66): computes the interpolation
+ * weights and the M2L operators in float64 on the host and uploads them.
+ * If cache_dir is non-NULL, operator files in the reference's format and
+ * naming (<cache_dir>/<kernelType>{Cheb,Unif}{K,U,V}<n>.bin,
+ * src/H2_3D_Tree.cpp:84-91) are read when present and valid
+ * (PrecomputeAvailable, :102-132) and written otherwise. */
+int pbbfmm_tree_build(pbbfmm_tree *tree, const char *cache_dir);
+
+/* Install M2L operators directly, in the layout FMMReadMatrices returns
+ * (src/H2_3D_Tree.cpp:186-239): Chebyshev K = nlev x 316 x (rf x rs),
+ * U = nlev x (n^3 x rf), VT = nlev x (rs x n^3), all column-major; uniform
+ * K = nlev x 316 x (2n-1)^3 FFTW halfcomplex spectra, U/VT ignored.
+ * nlev = 1 for homogeneous kernels, tree_level - 1 otherwise.  Replaces
+ * pbbfmm_tree_build's precompute (the weights are still computed). */
+int pbbfmm_tree_set_operators(pbbfmm_tree *tree, int rf, int rs, int nlev, const double *K,
+                              const double *U, const double *VT);
+
+/* Copy the tree's operators out in the same layout (NULL pointers query the
+ * sizes: *rf, *rs, *nlev are always written). */
+int pbbfmm_tree_get_operators(const pbbfmm_tree *tree, int *rf, int *rs, int *nlev, double *K,
+                              double *U, double *VT);
+
+int pbbfmm_tree_destroy(pbbfmm_tree *tree);
+
+/* H2_3D_Compute<T>(tree, target, source, weight, nCols, output)
+ * (include/compute.hpp:67-149).  HOST buffers; copies in, runs on the tree's
+ * device, copies out and synchronises.  output += K * weight. */
+int pbbfmm_compute(pbbfmm_tree *tree, const double *target, int64_t Nf, const double *source,
+                   int64_t Ns, const double *weight, int nCols, double *output);
+
+/* Same, on DEVICE buffers, asynchronous on `stream` (a cudaStream_t; NULL =
+ * legacy default stream).  precision: PBBFMM_PREC_*. */
+int pbbfmm_compute_device(pbbfmm_tree *tree, const double *d_target, int64_t Nf,
+                          const double *d_source, int64_t Ns, const double *d_weight, int nCols,
+                          double *d_output, int precision, void *stream);
+
+/* Precision used by pbbfmm_compute (default PBBFMM_PREC_FP64). */
+int pbbfmm_set_precision(pbbfmm_tree *tree, int precision);
+
+/* Per-phase device times (ms) of the last compute, when timing is enabled
+ * with pbbfmm_set_timing(tree, 1).  names: comma-separated phase names. */
+int pbbfmm_set_timing(pbbfmm_tree *tree, int enable);
+int pbbfmm_get_phase_times(const pbbfmm_tree *tree, float *ms, int max_phases, int *nphases,
+                           const char **names);
+
+/* Debug/test access to device arrays of the last compute (all as float64):
+ * what = 0 moments S of `level` (8^level x nCols x n^3, cell-major; only
+ * nonempty source cells are defined), 1 locals F after L2L (nonempty target
+ * cells), 2 target leaf offsets (8^L + 1), 3 target sort permutation (Nf),
+ * 4 source leaf offsets, 5 source sort permutation (Ns).
+ * Writes at most `count` doubles; *written gets the full size. */
+int pbbfmm_debug_copy(pbbfmm_tree *tree, int what, int level, double *host, int64_t count,
+                      int64_t *written);
+
+/* Interpolation weights of the tree (ComputeWeights, src/H2_3D_Tree.cpp:715-826):
+ * Tkz n*n, Kweights n^3, Cweights 2n^2, Ktable 343 (any pointer may be NULL). */
+int pbbfmm_tree_get_weights(const pbbfmm_tree *tree, double *Tkz, double *Kweights,
+                            double *Cweights, int *Ktable);
+
+const char *pbbfmm_last_error(void);
+const char *pbbfmm_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* PBBFMM3D_B200_H */

@@ -1,0 +1,624 @@
+// C ABI (include/pbbfmm3d_b200.h): tree lifecycle, operator upload, the
+// per-call workspace and the phase sequence of one matvec.
+//
+// Phase order follows H2_3D_Compute (include/compute.hpp:140-222):
+// distribute (binning) -> upward (P2M, M2M) -> far field (M2L with its pre-
+// and post-transforms) -> downward (L2L) -> near field (L2P, P2P, scatter).
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "fmm.cuh"
+
+namespace pbbfmm {
+
+static thread_local std::string g_err;
+
+void set_error(const std::string& msg) { g_err = msg; }
+
+int cuda_status(cudaError_t e, const char* what) {
+  g_err = std::string(what) + ": " + cudaGetErrorString(e);
+  if (e == cudaErrorMemoryAllocation) return PBBFMM_ERR_ALLOC;
+  return PBBFMM_ERR_CUDA;
+}
+
+int grow(DevBuf& b, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  if (b.p && b.cap >= bytes) return PBBFMM_OK;
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.cap = 0;
+  cudaError_t e = cudaMalloc(&b.p, bytes);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    b.p = nullptr;
+    set_error("device allocation of " + std::to_string(bytes) + " bytes failed: " +
+              cudaGetErrorString(e));
+    return PBBFMM_ERR_ALLOC;
+  }
+  b.cap = bytes;
+  return PBBFMM_OK;
+}
+
+void release(DevBuf& b) {
+  if (b.p) cudaFree(b.p);
+  b.p = nullptr;
+  b.cap = 0;
+}
+
+static int upload(double** dst, const double* src, size_t count) {
+  if (*dst) cudaFree(*dst);
+  *dst = nullptr;
+  if (count == 0) return PBBFMM_OK;
+  PB_CUDA(cudaMalloc(dst, count * sizeof(double)));
+  PB_CUDA(cudaMemcpy(*dst, src, count * sizeof(double), cudaMemcpyHostToDevice));
+  return PBBFMM_OK;
+}
+
+// conj(DFT3(stencil)) for k3 < n, stored [lvl][k][lex 343] complex; the 27
+// inner (near-field) slots stay zero.  k = (k1*m + k2)*n + k3.
+void unif_spectra(int n, const std::vector<double>& stencil, int nlev, std::vector<double>* op) {
+  const int m = 2 * n - 1, P = m * m * m, nk = m * m * n;
+  op->assign((size_t)nlev * nk * 343 * 2, 0.0);
+  std::vector<int> lex;
+  for (int a = -3; a < 4; ++a)
+    for (int b = -3; b < 4; ++b)
+      for (int c = -3; c < 4; ++c)
+        if (abs(a) > 1 || abs(b) > 1 || abs(c) > 1) lex.push_back(49 * (a + 3) + 7 * (b + 3) + (c + 3));
+  std::vector<double> cs(m), sn(m);
+  for (int j = 0; j < m; ++j) {
+    cs[j] = cos(2.0 * M_PI * j / m);
+    sn[j] = sin(2.0 * M_PI * j / m);
+  }
+  parallel_for((int64_t)nlev * 316, [&](int64_t b0, int64_t b1) {
+    std::vector<double> zr((size_t)m * m * n), zi((size_t)m * m * n), yr((size_t)m * m * n),
+        yi((size_t)m * m * n);
+    for (int64_t b = b0; b < b1; ++b) {
+      const int lvl = (int)(b / 316), i = (int)(b % 316);
+      const double* A = &stencil[((size_t)lvl * 316 + i) * P];
+      // along d3 (real input), keep k3 < n
+      for (int d1 = 0; d1 < m; ++d1)
+        for (int d2 = 0; d2 < m; ++d2)
+          for (int k3 = 0; k3 < n; ++k3) {
+            double re = 0, im = 0;
+            for (int d3 = 0; d3 < m; ++d3) {
+              const int e = (k3 * d3) % m;
+              const double v = A[(d1 * m + d2) * m + d3];
+              re += v * cs[e];
+              im -= v * sn[e];
+            }
+            zr[(d1 * m + d2) * n + k3] = re;
+            zi[(d1 * m + d2) * n + k3] = im;
+          }
+      // along d2
+      for (int d1 = 0; d1 < m; ++d1)
+        for (int k2 = 0; k2 < m; ++k2)
+          for (int k3 = 0; k3 < n; ++k3) {
+            double re = 0, im = 0;
+            for (int d2 = 0; d2 < m; ++d2) {
+              const int e = (k2 * d2) % m;
+              const double xr = zr[(d1 * m + d2) * n + k3], xi = zi[(d1 * m + d2) * n + k3];
+              re += xr * cs[e] + xi * sn[e];
+              im += xi * cs[e] - xr * sn[e];
+            }
+            yr[(d1 * m + k2) * n + k3] = re;
+            yi[(d1 * m + k2) * n + k3] = im;
+          }
+      // along d1, conjugate, store
+      for (int k1 = 0; k1 < m; ++k1)
+        for (int k2 = 0; k2 < m; ++k2)
+          for (int k3 = 0; k3 < n; ++k3) {
+            double re = 0, im = 0;
+            for (int d1 = 0; d1 < m; ++d1) {
+              const int e = (k1 * d1) % m;
+              const double xr = yr[(d1 * m + k2) * n + k3], xi = yi[(d1 * m + k2) * n + k3];
+              re += xr * cs[e] + xi * sn[e];
+              im += xi * cs[e] - xr * sn[e];
+            }
+            const size_t k = ((size_t)k1 * m + k2) * n + k3;
+            double* dst = &(*op)[(((size_t)lvl * nk + k) * 343 + lex[i]) * 2];
+            dst[0] = re;
+            dst[1] = -im;
+          }
+    }
+  });
+}
+
+// 189 interaction offsets per child type, in the order InteractionList
+// visits them (parent-neighbour slot 9(x+1)+3(y+1)+(z+1), then child j;
+// include/compute.hpp:1062-1106), with their operator index (Ktable).
+static std::vector<int> m2l_offsets(const int* Ktable) {
+  std::vector<int> offs;
+  for (int t = 0; t < 8; ++t) {
+    const int tx = (t >> 2) & 1, ty = (t >> 1) & 1, tz = t & 1;
+    int cnt = 0;
+    for (int px = -1; px <= 1; ++px)
+      for (int py = -1; py <= 1; ++py)
+        for (int pz = -1; pz <= 1; ++pz)
+          for (int j = 0; j < 8; ++j) {
+            const int ox = 2 * px + ((j >> 2) & 1) - tx, oy = 2 * py + ((j >> 1) & 1) - ty,
+                      oz = 2 * pz + (j & 1) - tz;
+            if (abs(ox) <= 1 && abs(oy) <= 1 && abs(oz) <= 1) continue;
+            offs.push_back(ox);
+            offs.push_back(oy);
+            offs.push_back(oz);
+            offs.push_back(Ktable[49 * (ox + 3) + 7 * (oy + 3) + (oz + 3)]);
+            ++cnt;
+          }
+    (void)cnt;
+  }
+  return offs;
+}
+
+static int upload_operators(pbbfmm_tree* t) {
+  if (t->device < 0) {
+    t->ops_ready = true;
+    return PBBFMM_OK;
+  }
+  PB_CUDA(cudaSetDevice(t->device));
+  int rc;
+  if (t->p.use_chebyshev) {
+    if ((rc = upload(&t->d_E, t->ops.K.data(), t->ops.K.size()))) return rc;
+    if ((rc = upload(&t->d_U, t->ops.U.data(), t->ops.U.size()))) return rc;
+    if ((rc = upload(&t->d_VT, t->ops.VT.data(), t->ops.VT.size()))) return rc;
+  } else {
+    std::vector<double> op;
+    unif_spectra(t->n, t->ops.stencil, t->ops.nlev, &op);
+    if ((rc = upload(&t->d_op, op.data(), op.size()))) return rc;
+  }
+  t->ops_ready = true;
+  return PBBFMM_OK;
+}
+
+static void free_tree_device(pbbfmm_tree* t) {
+  double** bufs[] = {&t->d_Tkz, &t->d_Kw, &t->d_Cw, &t->d_E,  &t->d_U,
+                     &t->d_VT,  &t->d_op, &t->d_twid, &t->d_kparam};
+  for (double** b : bufs) {
+    if (*b) cudaFree(*b);
+    *b = nullptr;
+  }
+  if (t->d_offs) cudaFree(t->d_offs);
+  t->d_offs = nullptr;
+  Workspace& ws = t->ws;
+  DevBuf* all[] = {&ws.bbox_part, &ws.ctr,   &ws.key,     &ws.key_sorted, &ws.idx,
+                   &ws.tperm,     &ws.sperm, &ws.tstart,  &ws.sstart,     &ws.tpos,
+                   &ws.spos,      &ws.wsorted, &ws.cub_temp, &ws.lists,    &ws.dcounts,
+                   &ws.S,         &ws.F,     &ws.proxy,   &ws.pf,         &ws.io_tgt,
+                   &ws.io_src,    &ws.io_w,  &ws.io_out};
+  for (DevBuf* b : all) release(*b);
+  for (int i = 0; i < 16; ++i)
+    if (t->ev[i]) {
+      cudaEventDestroy(t->ev[i]);
+      t->ev[i] = nullptr;
+    }
+}
+
+static const char* kPhaseNames = "binning,upward,far_field,downward,near_field";
+constexpr int kNumPhases = 5;
+
+static int compute_chunk(pbbfmm_tree* t, const double* d_tgt, int64_t Nf, const double* d_src,
+                         int64_t Ns, const double* d_w, int C, double* d_out, int precision,
+                         cudaStream_t st) {
+  const int L = t->p.tree_level, n3 = t->n3;
+  Workspace& ws = t->ws;
+  int rc;
+  if (t->timing) PB_CUDA(cudaEventRecord(t->ev[0], st));
+  t->last_Nf = Nf;
+  t->last_Ns = Ns;
+  t->last_C = C;
+  if ((rc = run_binning(t, d_tgt, Nf, d_src, Ns, d_w, C, st))) return rc;
+  if (t->timing) PB_CUDA(cudaEventRecord(t->ev[1], st));
+  const int64_t perS = (int64_t)C * n3;
+  if ((rc = grow(ws.S, sizeof(double) * level_total(L, perS)))) return rc;
+  if ((rc = grow(ws.F, sizeof(double) * level_total(L, perS)))) return rc;
+  if (t->p.use_chebyshev) {
+    if ((rc = grow(ws.proxy, sizeof(double) * level_total(L, (int64_t)C * t->ops.rs)))) return rc;
+    if ((rc = grow(ws.pf, sizeof(double) * level_total(L, (int64_t)C * t->ops.rf)))) return rc;
+  } else {
+    if ((rc = grow(ws.proxy, 2 * sizeof(double) * level_total(L, (int64_t)C * t->nk)))) return rc;
+    if ((rc = grow(ws.pf, 2 * sizeof(double) * level_total(L, (int64_t)C * t->nk)))) return rc;
+  }
+  (void)precision;
+  if ((rc = run_upward(t, C, st))) return rc;
+  if (t->timing) PB_CUDA(cudaEventRecord(t->ev[2], st));
+  if (t->p.use_chebyshev)
+    rc = run_m2l_cheb(t, C, st);
+  else
+    rc = run_m2l_unif(t, C, st);
+  if (rc) return rc;
+  if (t->timing) PB_CUDA(cudaEventRecord(t->ev[3], st));
+  if ((rc = run_downward(t, C, st))) return rc;
+  if (t->timing) PB_CUDA(cudaEventRecord(t->ev[4], st));
+  if ((rc = run_leaves(t, Nf, Ns, C, d_out, st))) return rc;
+  if (t->timing) PB_CUDA(cudaEventRecord(t->ev[5], st));
+  t->have_last = true;
+  return PBBFMM_OK;
+}
+
+}  // namespace pbbfmm
+
+using namespace pbbfmm;
+
+extern "C" {
+
+const char* pbbfmm_last_error(void) { return g_err.c_str(); }
+const char* pbbfmm_version(void) { return "pbbfmm3d_b200 0.1 (sm_100a)"; }
+
+int pbbfmm_tree_create(const pbbfmm_tree_params* params, int device, pbbfmm_tree** out) {
+  if (!params || !out) {
+    set_error("null argument");
+    return PBBFMM_ERR_ARG;
+  }
+  *out = nullptr;
+  const pbbfmm_tree_params& p = *params;
+  if (!(p.L > 0) || !std::isfinite(p.L)) {
+    set_error("box length L must be positive");
+    return PBBFMM_ERR_ARG;
+  }
+  if (p.tree_level < 2 || p.tree_level > kMaxLevel) {
+    set_error("tree_level must be in [2, 10]");
+    return PBBFMM_ERR_ARG;
+  }
+  if (p.interpolation_order < 2 || p.interpolation_order > kMaxOrder) {
+    set_error("interpolation_order must be in [2, 10]");
+    return PBBFMM_ERR_ARG;
+  }
+  if (p.kernel < 0 || p.kernel >= PBBFMM_KERNEL_COUNT) {
+    set_error("unknown kernel id");
+    return PBBFMM_ERR_ARG;
+  }
+  if (p.use_chebyshev && !(p.epsilon > 0)) {
+    set_error("epsilon must be positive");
+    return PBBFMM_ERR_ARG;
+  }
+  if ((p.kernel == PBBFMM_KERNEL_EXPCOV || p.kernel == PBBFMM_KERNEL_GAUSSSIGMA) &&
+      !(p.kernel_param[0] > 0)) {
+    set_error("kernel_param[0] (length scale) must be positive");
+    return PBBFMM_ERR_ARG;
+  }
+  if (device >= 0) {
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) {
+      cudaGetLastError();
+      set_error("no CUDA device available");
+      return PBBFMM_ERR_CUDA;
+    }
+    if (device >= ndev) {
+      set_error("device index out of range");
+      return PBBFMM_ERR_ARG;
+    }
+    PB_CUDA(cudaSetDevice(device));
+  }
+  pbbfmm_tree* t = new pbbfmm_tree();
+  t->p = p;
+  t->device = device;
+  t->kspec = kernel_spec(p.kernel, p.kernel_param);
+  t->n = p.interpolation_order;
+  t->n3 = t->n * t->n * t->n;
+  t->m = 2 * t->n - 1;
+  t->nk = t->m * t->m * t->n;
+  t->homog = is_homogeneous(t->kspec.homogen);
+  t->homogen_neg = -t->kspec.homogen;  // src/H2_3D_Tree.cpp:45
+  t->w = compute_weights(t->n, p.use_chebyshev);
+  t->weights_ready = true;
+  if (device < 0) {  // host-only tree: precompute and operator access, no compute
+    *out = t;
+    return PBBFMM_OK;
+  }
+  int rc;
+  if ((rc = upload(&t->d_Tkz, t->w.Tkz.data(), t->w.Tkz.size())) ||
+      (rc = upload(&t->d_Kw, t->w.Kweights.data(), t->w.Kweights.size())) ||
+      (rc = upload(&t->d_Cw, t->w.Cweights.data(), t->w.Cweights.size())) ||
+      (rc = upload(&t->d_kparam, t->kspec.param, 4))) {
+    free_tree_device(t);
+    delete t;
+    return rc;
+  }
+  {
+    std::vector<double> tw(2 * t->m);
+    for (int j = 0; j < t->m; ++j) {
+      tw[j] = cos(2.0 * M_PI * j / t->m);
+      tw[t->m + j] = sin(2.0 * M_PI * j / t->m);
+    }
+    if ((rc = upload(&t->d_twid, tw.data(), tw.size()))) {
+      free_tree_device(t);
+      delete t;
+      return rc;
+    }
+    std::vector<int> offs = m2l_offsets(t->w.Ktable);
+    cudaError_t e = cudaMalloc(&t->d_offs, offs.size() * sizeof(int));
+    if (e == cudaSuccess)
+      e = cudaMemcpy(t->d_offs, offs.data(), offs.size() * sizeof(int), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) {
+      rc = cuda_status(e, "upload offsets");
+      free_tree_device(t);
+      delete t;
+      return rc;
+    }
+  }
+  *out = t;
+  return PBBFMM_OK;
+}
+
+int pbbfmm_tree_build(pbbfmm_tree* t, const char* cache_dir) {
+  if (!t) {
+    set_error("null tree");
+    return PBBFMM_ERR_ARG;
+  }
+  std::string err;
+  const pbbfmm_tree_params& p = t->p;
+  bool have = false;
+  if (cache_dir) {
+    int r = read_cache(cache_dir, t->kspec, t->n, p.use_chebyshev, p.L, p.tree_level, &t->ops, &err);
+    if (r < 0) {
+      set_error(err);
+      return PBBFMM_ERR_IO;
+    }
+    have = (r == 0);
+  }
+  if (!have) {
+    if (precompute_operators(t->kspec, t->n, p.use_chebyshev, p.L, p.tree_level, p.epsilon, t->w,
+                             &t->ops, &err)) {
+      set_error(err);
+      return PBBFMM_ERR_ARG;
+    }
+    if (cache_dir && write_cache(cache_dir, t->kspec, t->n, p.use_chebyshev, p.L, p.tree_level,
+                                 t->ops, &err)) {
+      set_error(err);
+      return PBBFMM_ERR_IO;
+    }
+  }
+  return upload_operators(t);
+}
+
+int pbbfmm_tree_set_operators(pbbfmm_tree* t, int rf, int rs, int nlev, const double* K,
+                              const double* U, const double* VT) {
+  if (!t || !K) {
+    set_error("null argument");
+    return PBBFMM_ERR_ARG;
+  }
+  const int n3 = t->n3;
+  const int want = t->homog ? 1 : t->p.tree_level - 1;
+  if (nlev != want) {
+    set_error("nlev must be " + std::to_string(want) + " for this kernel and tree_level");
+    return PBBFMM_ERR_ARG;
+  }
+  t->ops.cheb = t->p.use_chebyshev;
+  t->ops.n = t->n;
+  t->ops.nlev = nlev;
+  if (t->p.use_chebyshev) {
+    if (!U || !VT || rf < 1 || rf > n3 || rs < 1 || rs > n3) {
+      set_error("Chebyshev operators need U, VT and 1 <= rf, rs <= n^3");
+      return PBBFMM_ERR_ARG;
+    }
+    t->ops.rf = rf;
+    t->ops.rs = rs;
+    t->ops.K.assign(K, K + (size_t)nlev * 316 * rf * rs);
+    t->ops.U.assign(U, U + (size_t)nlev * n3 * rf);
+    t->ops.VT.assign(VT, VT + (size_t)nlev * rs * n3);
+  } else {
+    const int P = t->m * t->m * t->m;
+    t->ops.rf = t->ops.rs = n3;
+    std::vector<double> hc(K, K + (size_t)nlev * 316 * P);
+    halfcomplex_to_stencils(hc, P, &t->ops.stencil);
+  }
+  return upload_operators(t);
+}
+
+int pbbfmm_tree_get_operators(const pbbfmm_tree* t, int* rf, int* rs, int* nlev, double* K,
+                              double* U, double* VT) {
+  if (!t || !t->ops_ready) {
+    set_error("tree has no operators (call pbbfmm_tree_build)");
+    return PBBFMM_ERR_STATE;
+  }
+  if (rf) *rf = t->ops.rf;
+  if (rs) *rs = t->ops.rs;
+  if (nlev) *nlev = t->ops.nlev;
+  if (t->p.use_chebyshev) {
+    if (K) memcpy(K, t->ops.K.data(), t->ops.K.size() * sizeof(double));
+    if (U) memcpy(U, t->ops.U.data(), t->ops.U.size() * sizeof(double));
+    if (VT) memcpy(VT, t->ops.VT.data(), t->ops.VT.size() * sizeof(double));
+  } else if (K) {
+    std::vector<double> hc;
+    stencils_to_halfcomplex(t->ops.stencil, t->m * t->m * t->m, &hc);
+    memcpy(K, hc.data(), hc.size() * sizeof(double));
+  }
+  return PBBFMM_OK;
+}
+
+int pbbfmm_tree_get_weights(const pbbfmm_tree* t, double* Tkz, double* Kweights, double* Cweights,
+                            int* Ktable) {
+  if (!t) {
+    set_error("null tree");
+    return PBBFMM_ERR_ARG;
+  }
+  if (Tkz) memcpy(Tkz, t->w.Tkz.data(), t->w.Tkz.size() * sizeof(double));
+  if (Kweights) memcpy(Kweights, t->w.Kweights.data(), t->w.Kweights.size() * sizeof(double));
+  if (Cweights) memcpy(Cweights, t->w.Cweights.data(), t->w.Cweights.size() * sizeof(double));
+  if (Ktable) memcpy(Ktable, t->w.Ktable, sizeof(int) * 343);
+  return PBBFMM_OK;
+}
+
+int pbbfmm_tree_destroy(pbbfmm_tree* t) {
+  if (!t) return PBBFMM_OK;
+  if (t->device >= 0) {
+    cudaSetDevice(t->device);
+    free_tree_device(t);
+  }
+  delete t;
+  return PBBFMM_OK;
+}
+
+int pbbfmm_set_precision(pbbfmm_tree* t, int precision) {
+  if (!t || (precision != PBBFMM_PREC_FP64 && precision != PBBFMM_PREC_MIXED)) {
+    set_error("bad precision mode");
+    return PBBFMM_ERR_ARG;
+  }
+  t->precision = precision;
+  return PBBFMM_OK;
+}
+
+int pbbfmm_set_timing(pbbfmm_tree* t, int enable) {
+  if (!t || t->device < 0) return PBBFMM_ERR_ARG;
+  PB_CUDA(cudaSetDevice(t->device));
+  if (enable && !t->ev[0])
+    for (int i = 0; i <= kNumPhases; ++i) PB_CUDA(cudaEventCreate(&t->ev[i]));
+  t->timing = enable != 0;
+  return PBBFMM_OK;
+}
+
+int pbbfmm_get_phase_times(const pbbfmm_tree* t, float* ms, int max_phases, int* nphases,
+                           const char** names) {
+  if (!t) return PBBFMM_ERR_ARG;
+  if (names) *names = kPhaseNames;
+  if (nphases) *nphases = kNumPhases;
+  if (!t->timing || !t->have_last) {
+    set_error("timing not enabled or no compute yet");
+    return PBBFMM_ERR_STATE;
+  }
+  for (int i = 0; i < kNumPhases && i < max_phases; ++i) {
+    PB_CUDA(cudaEventSynchronize(t->ev[i + 1]));
+    PB_CUDA(cudaEventElapsedTime(&ms[i], t->ev[i], t->ev[i + 1]));
+  }
+  return PBBFMM_OK;
+}
+
+int pbbfmm_compute_device(pbbfmm_tree* t, const double* d_target, int64_t Nf,
+                          const double* d_source, int64_t Ns, const double* d_weight, int nCols,
+                          double* d_output, int precision, void* stream) {
+  if (!t) {
+    set_error("null tree");
+    return PBBFMM_ERR_ARG;
+  }
+  if (!t->ops_ready) {
+    set_error("tree operators missing: call pbbfmm_tree_build first");
+    return PBBFMM_ERR_STATE;
+  }
+  if (t->device < 0) {
+    set_error("host-only tree (device -1) cannot compute");
+    return PBBFMM_ERR_STATE;
+  }
+  if (Nf < 0 || Ns < 0 || nCols < 1 || Nf > INT32_MAX || Ns > INT32_MAX) {
+    set_error("bad sizes (0 <= Nf, Ns < 2^31, nCols >= 1)");
+    return PBBFMM_ERR_ARG;
+  }
+  if ((Nf > 0 && (!d_target || !d_output)) || (Ns > 0 && (!d_source || !d_weight))) {
+    set_error("null data pointer");
+    return PBBFMM_ERR_ARG;
+  }
+  if (precision != PBBFMM_PREC_FP64 && precision != PBBFMM_PREC_MIXED) {
+    set_error("bad precision mode");
+    return PBBFMM_ERR_ARG;
+  }
+  if (Nf == 0) return PBBFMM_OK;
+  PB_CUDA(cudaSetDevice(t->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  // Right-hand sides run in blocks of at most 64 columns (the Chebyshev M2L
+  // tile width; it also bounds the per-CTA shared memory of P2M); weights
+  // and outputs are column-major, so a block is a contiguous slice of each.
+  const int cmax = 64;
+  for (int c0 = 0; c0 < nCols; c0 += cmax) {
+    const int cc = nCols - c0 < cmax ? nCols - c0 : cmax;
+    int rc = compute_chunk(t, d_target, Nf, d_source, Ns, d_weight + (int64_t)c0 * Ns, cc,
+                           d_output + (int64_t)c0 * Nf, precision, st);
+    if (rc) return rc;
+  }
+  return PBBFMM_OK;
+}
+
+int pbbfmm_compute(pbbfmm_tree* t, const double* target, int64_t Nf, const double* source,
+                   int64_t Ns, const double* weight, int nCols, double* output) {
+  if (!t) {
+    set_error("null tree");
+    return PBBFMM_ERR_ARG;
+  }
+  if (Nf < 0 || Ns < 0 || nCols < 1) {
+    set_error("bad sizes");
+    return PBBFMM_ERR_ARG;
+  }
+  if ((Nf > 0 && (!target || !output)) || (Ns > 0 && (!source || !weight))) {
+    set_error("null data pointer");
+    return PBBFMM_ERR_ARG;
+  }
+  if (Nf == 0) return PBBFMM_OK;
+  if (t->device < 0 || !t->ops_ready) {
+    set_error("tree cannot compute: host-only or operators missing");
+    return PBBFMM_ERR_STATE;
+  }
+  PB_CUDA(cudaSetDevice(t->device));
+  Workspace& ws = t->ws;
+  int rc;
+  const bool same = (source == target && Ns == Nf);
+  if ((rc = grow(ws.io_tgt, sizeof(double) * 3 * Nf))) return rc;
+  if (!same && (rc = grow(ws.io_src, sizeof(double) * 3 * (Ns ? Ns : 1)))) return rc;
+  if ((rc = grow(ws.io_w, sizeof(double) * (size_t)(Ns ? Ns : 1) * nCols))) return rc;
+  if ((rc = grow(ws.io_out, sizeof(double) * (size_t)Nf * nCols))) return rc;
+  double* dt = ws.io_tgt.as<double>();
+  double* ds = same ? dt : ws.io_src.as<double>();
+  PB_CUDA(cudaMemcpy(dt, target, sizeof(double) * 3 * Nf, cudaMemcpyHostToDevice));
+  if (!same && Ns > 0) PB_CUDA(cudaMemcpy(ds, source, sizeof(double) * 3 * Ns, cudaMemcpyHostToDevice));
+  if (Ns > 0)
+    PB_CUDA(cudaMemcpy(ws.io_w.p, weight, sizeof(double) * Ns * nCols, cudaMemcpyHostToDevice));
+  PB_CUDA(cudaMemcpy(ws.io_out.p, output, sizeof(double) * Nf * nCols, cudaMemcpyHostToDevice));
+  rc = pbbfmm_compute_device(t, dt, Nf, ds, Ns, ws.io_w.as<double>(), nCols,
+                             ws.io_out.as<double>(), t->precision, nullptr);
+  if (rc) return rc;
+  PB_CUDA(cudaMemcpy(output, ws.io_out.p, sizeof(double) * Nf * nCols, cudaMemcpyDeviceToHost));
+  return PBBFMM_OK;
+}
+
+int pbbfmm_debug_copy(pbbfmm_tree* t, int what, int level, double* host, int64_t count,
+                      int64_t* written) {
+  if (!t || !t->have_last || t->device < 0) {
+    set_error("no compute to inspect");
+    return PBBFMM_ERR_STATE;
+  }
+  PB_CUDA(cudaSetDevice(t->device));
+  PB_CUDA(cudaDeviceSynchronize());
+  const int L = t->p.tree_level;
+  const int C = t->last_C;
+  std::vector<int> tmp;
+  const double* src = nullptr;
+  int64_t total = 0;
+  if (what == 0 || what == 1) {
+    if (level < 2 || level > L) {
+      set_error("level must be in [2, tree_level]");
+      return PBBFMM_ERR_ARG;
+    }
+    const int64_t per = (int64_t)C * t->n3;
+    total = cells_at(level) * per;
+    src = (what == 0 ? t->ws.S.as<double>() : t->ws.F.as<double>()) + level_offset(level, per);
+  } else if (what >= 2 && what <= 5) {
+    const int* p = nullptr;
+    if (what == 2) {
+      p = t->ws.tstart.as<int>();
+      total = cells_at(L) + 1;
+    } else if (what == 3) {
+      p = t->ws.tperm.as<int>();
+      total = t->last_Nf;
+    } else if (what == 4) {
+      p = t->ws.sstart.as<int>();
+      total = cells_at(L) + 1;
+    } else {
+      p = t->ws.sperm.as<int>();
+      total = t->last_Ns;
+    }
+    tmp.resize(total);
+    PB_CUDA(cudaMemcpy(tmp.data(), p, sizeof(int) * total, cudaMemcpyDeviceToHost));
+    int64_t nc = count < total ? count : total;
+    for (int64_t i = 0; i < nc; ++i) host[i] = tmp[i];
+    if (written) *written = total;
+    return PBBFMM_OK;
+  } else {
+    set_error("unknown debug array");
+    return PBBFMM_ERR_ARG;
+  }
+  if (written) *written = total;
+  int64_t nc = count < total ? count : total;
+  if (host && nc > 0) PB_CUDA(cudaMemcpy(host, src, sizeof(double) * nc, cudaMemcpyDeviceToHost));
+  return PBBFMM_OK;
+}
+
+}  // extern "C"

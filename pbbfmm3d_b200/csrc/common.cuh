@@ -1,0 +1,180 @@
+// Shared device utilities: kernel functors, interpolation basis, Morton codes.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "../../include/pbbfmm3d_b200.h"
+
+namespace pbbfmm {
+
+constexpr int kMaxOrder = 10;
+
+// ------------------------------------------------------------ Morton codes
+// Leaf index of the reference: sum_l j_l 8^(L-1-l), j = 4 bx + 2 by + bz
+// (src/H2_3D_Tree.cpp:939-971) -- x in the most significant bit of each
+// octal digit.  Coordinate bit k sits at bit 3k+2 (x), 3k+1 (y), 3k (z).
+__host__ __device__ inline uint32_t spread3(uint32_t v) {
+  v &= 0x3ff;
+  v = (v | (v << 16)) & 0x030000ff;
+  v = (v | (v << 8)) & 0x0300f00f;
+  v = (v | (v << 4)) & 0x030c30c3;
+  v = (v | (v << 2)) & 0x09249249;
+  return v;
+}
+__host__ __device__ inline uint32_t compact3(uint32_t v) {
+  v &= 0x09249249;
+  v = (v | (v >> 2)) & 0x030c30c3;
+  v = (v | (v >> 4)) & 0x0300f00f;
+  v = (v | (v >> 8)) & 0x030000ff;
+  v = (v | (v >> 16)) & 0x000003ff;
+  return v;
+}
+__host__ __device__ inline uint32_t morton_encode(int x, int y, int z) {
+  return (spread3((uint32_t)x) << 2) | (spread3((uint32_t)y) << 1) | spread3((uint32_t)z);
+}
+__host__ __device__ inline void morton_decode(uint32_t m, int* x, int* y, int* z) {
+  *x = (int)compact3(m >> 2);
+  *y = (int)compact3(m >> 1);
+  *z = (int)compact3(m);
+}
+
+// ------------------------------------------------------------ kernels
+// K(t, s) with d = s - t, exactly the arithmetic of src/kernel_Types.cpp.
+template <int KID>
+struct Kern;
+
+template <>
+struct Kern<PBBFMM_KERNEL_LAPLACIAN> {
+  template <typename T>
+  __device__ static T eval(T dx, T dy, T dz, const double*) {
+    return T(1) / sqrt(dx * dx + dy * dy + dz * dz);
+  }
+};
+template <>
+struct Kern<PBBFMM_KERNEL_ONEOVERR2> {
+  template <typename T>
+  __device__ static T eval(T dx, T dy, T dz, const double*) {
+    T ri = T(1) / sqrt(dx * dx + dy * dy + dz * dz);
+    return ri * ri;
+  }
+};
+template <>
+struct Kern<PBBFMM_KERNEL_ONEOVERR4> {
+  template <typename T>
+  __device__ static T eval(T dx, T dy, T dz, const double*) {
+    T ri = T(1) / sqrt(dx * dx + dy * dy + dz * dz);
+    return ri * ri * ri * ri;
+  }
+};
+template <>
+struct Kern<PBBFMM_KERNEL_GAUSSIAN> {
+  template <typename T>
+  __device__ static T eval(T dx, T dy, T dz, const double*) {
+    T r = sqrt(dx * dx + dy * dy + dz * dz);
+    return exp(-r * r);
+  }
+};
+template <>
+struct Kern<PBBFMM_KERNEL_LOGARITHM> {
+  template <typename T>
+  __device__ static T eval(T dx, T dy, T dz, const double*) {
+    T r2 = dx * dx + dy * dy + dz * dz;
+    return r2 == T(0) ? T(0) : T(0.5) * log(r2);
+  }
+};
+template <>
+struct Kern<PBBFMM_KERNEL_QUADRIC> {
+  template <typename T>
+  __device__ static T eval(T dx, T dy, T dz, const double*) {
+    return T(1) + (dx * dx + dy * dy + dz * dz);
+  }
+};
+template <>
+struct Kern<PBBFMM_KERNEL_INVQUADRIC> {
+  template <typename T>
+  __device__ static T eval(T dx, T dy, T dz, const double*) {
+    return T(1) / (T(1) + (dx * dx + dy * dy + dz * dz));
+  }
+};
+template <>
+struct Kern<PBBFMM_KERNEL_THINPLATESPLINE> {
+  template <typename T>
+  __device__ static T eval(T dx, T dy, T dz, const double*) {
+    T r2 = dx * dx + dy * dy + dz * dz;
+    return r2 == T(0) ? T(0) : T(0.5) * r2 * log(r2);
+  }
+};
+template <>
+struct Kern<PBBFMM_KERNEL_EXPCOV> {
+  template <typename T>
+  __device__ static T eval(T dx, T dy, T dz, const double* p) {
+    return exp(-sqrt(dx * dx + dy * dy + dz * dz) / T(p[0]));
+  }
+};
+template <>
+struct Kern<PBBFMM_KERNEL_GAUSSSIGMA> {
+  template <typename T>
+  __device__ static T eval(T dx, T dy, T dz, const double* p) {
+    return exp(-(dx * dx + dy * dy + dz * dz) / (T(2) * T(p[0]) * T(p[0])));
+  }
+};
+template <>
+struct Kern<PBBFMM_KERNEL_ANISOEXP> {
+  template <typename T>
+  __device__ static T eval(T dx, T dy, T dz, const double*) {
+    return T(0.75) * exp(-sqrt(dx * dx / T(100) + dy * dy / T(100) + dz * dz / T(2.25)));
+  }
+};
+
+// Run `f.template operator()<Kern<K>>()` for the runtime kernel id.
+template <typename F>
+inline int dispatch_kernel(int kid, F&& f) {
+  switch (kid) {
+    case PBBFMM_KERNEL_LAPLACIAN: return f.template run<Kern<PBBFMM_KERNEL_LAPLACIAN>>();
+    case PBBFMM_KERNEL_ONEOVERR2: return f.template run<Kern<PBBFMM_KERNEL_ONEOVERR2>>();
+    case PBBFMM_KERNEL_ONEOVERR4: return f.template run<Kern<PBBFMM_KERNEL_ONEOVERR4>>();
+    case PBBFMM_KERNEL_GAUSSIAN: return f.template run<Kern<PBBFMM_KERNEL_GAUSSIAN>>();
+    case PBBFMM_KERNEL_LOGARITHM: return f.template run<Kern<PBBFMM_KERNEL_LOGARITHM>>();
+    case PBBFMM_KERNEL_QUADRIC: return f.template run<Kern<PBBFMM_KERNEL_QUADRIC>>();
+    case PBBFMM_KERNEL_INVQUADRIC: return f.template run<Kern<PBBFMM_KERNEL_INVQUADRIC>>();
+    case PBBFMM_KERNEL_THINPLATESPLINE:
+      return f.template run<Kern<PBBFMM_KERNEL_THINPLATESPLINE>>();
+    case PBBFMM_KERNEL_EXPCOV: return f.template run<Kern<PBBFMM_KERNEL_EXPCOV>>();
+    case PBBFMM_KERNEL_GAUSSSIGMA: return f.template run<Kern<PBBFMM_KERNEL_GAUSSSIGMA>>();
+    case PBBFMM_KERNEL_ANISOEXP: return f.template run<Kern<PBBFMM_KERNEL_ANISOEXP>>();
+    default: return PBBFMM_ERR_ARG;
+  }
+}
+
+// ------------------------------------------------------------ basis
+// S_m(x) per coordinate (ComputeSn, src/H2_3D_Tree.cpp:830-892).
+// Chebyshev: (2/n) * Clenshaw sum of T_k(node_m) T_k(x); uniform: Lagrange.
+template <typename T>
+__device__ __forceinline__ T basis_one(int n, int cheb, T x, const T* Tkz, int m) {
+  if (cheb) {
+    const T* Tk = Tkz + m * n;
+    T d0 = 0, d1 = 0, d2;
+    for (int j = n - 1; j > 0; j--) {
+      d2 = d0;
+      d0 = T(2) * x * d0 - d1 + Tk[j];
+      d1 = d2;
+    }
+    return (T(2) / T(n)) * (x * d0 - d1 + T(0.5) * Tk[0]);
+  }
+  T num = 1, den = 1;
+  for (int j = 0; j < n; j++)
+    if (m != j) {
+      num *= x - (T(1) - T(2) * T(j) / T(n - 1));
+      den *= T(-2) * (T(m) - T(j)) / T(n - 1);
+    }
+  return num / den;
+}
+
+// out[m * stride] = S_m(x), m < n
+template <typename T>
+__device__ __forceinline__ void basis_all(int n, int cheb, T x, const T* Tkz, T* out,
+                                          int stride = 1) {
+  for (int m = 0; m < n; ++m) out[m * stride] = basis_one<T>(n, cheb, x, Tkz, m);
+}
+
+}  // namespace pbbfmm

@@ -1,0 +1,234 @@
+// Downward pass (L2L) and the leaf phase (L2P + P2P + scatter to output).
+//
+// Reference: DownwardPass / Local2Local (include/compute.hpp:552-587,
+// 799-878) and NearFieldInteractions (include/compute.hpp:591-749) with
+// EvaluateField / EvaluateField_self (:761-785).  The reference's P2P uses
+// the kernel's symmetry to update both leaves of a pair under an OpenMP
+// critical section; here each target point gathers from its 27 neighbour
+// leaves (no atomics, no symmetry assumption, sources may differ from
+// targets), and the far-field interpolation, the near-field sum and the
+// scatter to the caller's output are one kernel.
+#include "fmm.cuh"
+
+namespace pbbfmm {
+
+__device__ __forceinline__ void cell_center_d(uint32_t m, int l, double box, double* c) {
+  int x, y, z;
+  morton_decode(m, &x, &y, &z);
+  double cx = 0, cy = 0, cz = 0, len = box;
+  for (int i = l - 1; i >= 0; --i) {
+    const double q = 0.25 * len;
+    cx = ((x >> i) & 1) ? __dadd_rn(cx, q) : __dsub_rn(cx, q);
+    cy = ((y >> i) & 1) ? __dadd_rn(cy, q) : __dsub_rn(cy, q);
+    cz = ((z >> i) & 1) ? __dadd_rn(cz, q) : __dsub_rn(cz, q);
+    len = 0.5 * len;
+  }
+  c[0] = cx;
+  c[1] = cy;
+  c[2] = cz;
+}
+
+constexpr int kL2LThreads = 128;
+constexpr int kL2LGroup = 1024;
+
+// One CTA per nonempty target cell at level l: F_child += L2L(F_parent).
+__global__ void __launch_bounds__(kL2LThreads)
+    k_l2l(const int* __restrict__ cells, const double* __restrict__ Fpar,
+          double* __restrict__ Fch, int C, int n, const double* __restrict__ Cw_g) {
+  __shared__ double sCw[2 * kMaxOrder * kMaxOrder];
+  __shared__ double b0[kL2LGroup], b1[kL2LGroup];
+  const int n2 = n * n, n3 = n2 * n;
+  for (int i = threadIdx.x; i < 2 * n2; i += blockDim.x) sCw[i] = Cw_g[i];
+  const int cell = cells[blockIdx.x];
+  const int par = cell >> 3, ch = cell & 7;
+  const double* wx = sCw + (((ch >> 2) & 1) ? n2 : 0);
+  const double* wy = sCw + (((ch >> 1) & 1) ? n2 : 0);
+  const double* wz = sCw + ((ch & 1) ? n2 : 0);
+  const int CG = max(1, min(C, kL2LGroup / n3));
+  for (int c0 = 0; c0 < C; c0 += CG) {
+    const int cg = min(CG, C - c0), tot = cg * n3;
+    __syncthreads();
+    for (int i = threadIdx.x; i < tot; i += blockDim.x)
+      b0[i] = Fpar[((int64_t)par * C + c0) * n3 + i];
+    __syncthreads();
+    // x: Fx[l1 n2 + l2 n + l3] = sum_k F[k n2 + l2 n + l3] wx[l1 + k n]
+    for (int i = threadIdx.x; i < tot; i += blockDim.x) {
+      const int cc = i / n3, r = i % n3, l1 = r / n2, rem = r % n2;
+      const double* s = b0 + cc * n3 + rem;
+      double v = 0;
+      for (int k = 0; k < n; ++k) v += s[k * n2] * wx[l1 + k * n];
+      b1[i] = v;
+    }
+    __syncthreads();
+    // y: Fy[l1 n2 + l2 n + l3] = sum_k Fx[l1 n2 + k n + l3] wy[l2 + k n]
+    for (int i = threadIdx.x; i < tot; i += blockDim.x) {
+      const int cc = i / n3, r = i % n3, l1 = r / n2, l2 = (r / n) % n, l3 = r % n;
+      const double* s = b1 + cc * n3 + l1 * n2 + l3;
+      double v = 0;
+      for (int k = 0; k < n; ++k) v += s[k * n] * wy[l2 + k * n];
+      b0[i] = v;
+    }
+    __syncthreads();
+    // z: Fchild[l1 n + l3] += sum_k Fy[l1 n + k] wz[l3 + k n]   (l1 over n^2)
+    for (int i = threadIdx.x; i < tot; i += blockDim.x) {
+      const int cc = i / n3, r = i % n3, l1 = r / n, l3 = r % n;
+      const double* s = b0 + cc * n3 + l1 * n;
+      double v = 0;
+      for (int k = 0; k < n; ++k) v += s[k] * wz[l3 + k * n];
+      Fch[((int64_t)cell * C + c0) * n3 + i] += v;
+    }
+  }
+}
+
+// Leaf phase: one warp per nonempty target leaf, lanes over the sources of
+// the 27 neighbour leaves (and over the n^3 local coefficients for L2P);
+// warp-reduced per target point, then scattered to out[col*Nf + index].
+constexpr int kLeafWarps = 4;
+constexpr int kLeafCols = 8;  // columns per pass (registers)
+
+template <class KF>
+__global__ void __launch_bounds__(32 * kLeafWarps)
+    k_leaf(const int* __restrict__ leaves, int nleaves, const int* __restrict__ tstart,
+           const int* __restrict__ sstart, const int* __restrict__ tperm,
+           const double* __restrict__ tpos, const double* __restrict__ spos,
+           const double* __restrict__ wsorted, int Nf, int Ns, int C,
+           const double* __restrict__ F_L, int n, int cheb, const double* __restrict__ Tkz_g,
+           double box, int L, const double* __restrict__ kparam_g, double* __restrict__ out) {
+  __shared__ double sTkz[kMaxOrder * kMaxOrder];
+  __shared__ double kp[4];
+  __shared__ int s_nb[kLeafWarps][27][2];           // neighbour source ranges
+  __shared__ double s_b[kLeafWarps][3][kMaxOrder];  // basis values of the current target
+  for (int i = threadIdx.x; i < n * n; i += blockDim.x) sTkz[i] = Tkz_g[i];
+  if (threadIdx.x < 4) kp[threadIdx.x] = kparam_g[threadIdx.x];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+  const int wid = blockIdx.x * kLeafWarps + wl;
+  if (wid >= nleaves) return;
+  const int leaf = leaves[wid];
+  const int ta = tstart[leaf], te = tstart[leaf + 1];
+  const int n3 = n * n * n;
+  double c[3];
+  cell_center_d((uint32_t)leaf, L, box, c);
+  double len = box;
+  for (int i = 0; i < L; ++i) len = 0.5 * len;
+  const double ihalfL = 2. / len;
+  int ax, ay, az;
+  morton_decode((uint32_t)leaf, &ax, &ay, &az);
+  const int nside = 1 << L;
+  // neighbour source ranges, slot 9(x+1)+3(y+1)+(z+1)
+  if (lane < 27) {
+    const int q = lane;
+    const int bx = ax + q / 9 - 1, by = ay + (q / 3) % 3 - 1, bz = az + q % 3 - 1;
+    int a = 0, e = 0;
+    if (bx >= 0 && by >= 0 && bz >= 0 && bx < nside && by < nside && bz < nside) {
+      const uint32_t bm = morton_encode(bx, by, bz);
+      a = sstart[bm];
+      e = sstart[bm + 1];
+    }
+    s_nb[wl][q][0] = a;
+    s_nb[wl][q][1] = e;
+  }
+  __syncwarp();
+  for (int c0 = 0; c0 < C; c0 += kLeafCols) {
+    const int cg = min(kLeafCols, C - c0);
+    for (int i = ta; i < te; ++i) {
+      const double x = tpos[i], y = tpos[(int64_t)Nf + i], z = tpos[2 * (int64_t)Nf + i];
+      double acc[kLeafCols];
+#pragma unroll
+      for (int cc = 0; cc < kLeafCols; ++cc) acc[cc] = 0;
+      // far field: phi += sum_l F[l] Sx[l1] Sy[l2] Sz[l3]
+      {
+        __syncwarp();
+        if (lane < 3 * n) {
+          const int d = lane / n, mm = lane % n;
+          const double q = ihalfL * ((d == 0 ? x : d == 1 ? y : z) - c[d]);
+          s_b[wl][d][mm] = basis_one<double>(n, cheb, q, sTkz, mm);
+        }
+        __syncwarp();
+        const double* Fl = F_L + ((int64_t)leaf * C + c0) * n3;
+        for (int l = lane; l < n3; l += 32) {
+          const int l1 = l / (n * n), l2 = (l / n) % n, l3 = l % n;
+          const double tmp2 = s_b[wl][0][l1] * s_b[wl][1][l2];
+          const double bz3 = s_b[wl][2][l3];
+#pragma unroll
+          for (int cc = 0; cc < kLeafCols; ++cc)
+            if (cc < cg) acc[cc] += Fl[cc * n3 + l] * tmp2 * bz3;
+        }
+      }
+      // near field over the 27 neighbour leaves
+      for (int q = 0; q < 27; ++q) {
+        const int qa = s_nb[wl][q][0], qe = s_nb[wl][q][1];
+        for (int j = qa + lane; j < qe; j += 32) {
+          const double dx = spos[j] - x, dy = spos[(int64_t)Ns + j] - y,
+                       dz = spos[2 * (int64_t)Ns + j] - z;
+          double kv = KF::template eval<double>(dx, dy, dz, kp);
+          if (isinf(kv)) kv = 0;
+          const double* wj = wsorted + (int64_t)j * C + c0;
+#pragma unroll
+          for (int cc = 0; cc < kLeafCols; ++cc)
+            if (cc < cg) acc[cc] += kv * wj[cc];
+        }
+      }
+#pragma unroll
+      for (int cc = 0; cc < kLeafCols; ++cc) {
+        double v = acc[cc];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+        acc[cc] = v;
+      }
+      if (lane == 0) {
+        const int64_t oi = tperm[i];
+#pragma unroll
+        for (int cc = 0; cc < kLeafCols; ++cc)
+          if (cc < cg) out[(int64_t)(c0 + cc) * Nf + oi] += acc[cc];
+      }
+    }
+  }
+}
+
+struct LeafLaunch {
+  pbbfmm_tree* t;
+  int64_t Nf, Ns;
+  int C;
+  double* out;
+  cudaStream_t st;
+  const double* kparam;
+  template <class KF>
+  int run() {
+    const int L = t->p.tree_level;
+    const int nl = t->lists.ntgt[L];
+    if (nl == 0) return PBBFMM_OK;
+    Workspace& ws = t->ws;
+    const int64_t perS = (int64_t)C * t->n3;
+    k_leaf<KF><<<(nl + kLeafWarps - 1) / kLeafWarps, 32 * kLeafWarps, 0, st>>>(
+        ws.lists.as<int>() + t->lists.tgt_off[L], nl, ws.tstart.as<int>(), ws.sstart.as<int>(),
+        ws.tperm.as<int>(), ws.tpos.as<double>(), ws.spos.as<double>(), ws.wsorted.as<double>(),
+        (int)Nf, (int)Ns, C, ws.F.as<double>() + level_offset(L, perS), t->n,
+        t->p.use_chebyshev, t->d_Tkz, t->p.L, L, kparam, out);
+    PB_LAUNCH("leaf");
+    return PBBFMM_OK;
+  }
+};
+
+int run_downward(pbbfmm_tree* t, int C, cudaStream_t st) {
+  const int L = t->p.tree_level, n3 = t->n3;
+  Workspace& ws = t->ws;
+  const int* lists = ws.lists.as<int>();
+  double* F = ws.F.as<double>();
+  const int64_t per = (int64_t)C * n3;
+  for (int l = 3; l <= L; ++l) {
+    if (t->lists.ntgt[l] == 0) continue;
+    k_l2l<<<t->lists.ntgt[l], kL2LThreads, 0, st>>>(lists + t->lists.tgt_off[l],
+                                                     F + level_offset(l - 1, per),
+                                                     F + level_offset(l, per), C, t->n, t->d_Cw);
+    PB_LAUNCH("l2l");
+  }
+  return PBBFMM_OK;
+}
+
+int run_leaves(pbbfmm_tree* t, int64_t Nf, int64_t Ns, int C, double* d_out, cudaStream_t st) {
+  LeafLaunch ll{t, Nf, Ns, C, d_out, st, t->d_kparam};
+  return dispatch_kernel(t->p.kernel, ll);
+}
+
+}  // namespace pbbfmm

@@ -1,0 +1,136 @@
+// Internal state of a tree (the C-ABI's opaque pbbfmm_tree) and the launch
+// entry points of each phase.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "precompute.h"
+
+namespace pbbfmm {
+
+constexpr int kMaxLevel = 10;
+
+// Grow-only device buffer.
+struct DevBuf {
+  void* p = nullptr;
+  size_t cap = 0;
+  template <typename T>
+  T* as() const {
+    return static_cast<T*>(p);
+  }
+};
+int grow(DevBuf& b, size_t bytes);  // PBBFMM_OK or PBBFMM_ERR_ALLOC
+void release(DevBuf& b);
+
+// Device arrays of one compute, grown on demand and kept by the tree.
+struct Workspace {
+  // binning
+  DevBuf bbox_part;  // 6 doubles per reduction block
+  DevBuf ctr;        // 3 doubles: recentring shift
+  DevBuf key, key_sorted, idx;  // max(Nf, Ns)
+  DevBuf tperm, sperm;          // sorted position -> original index
+  DevBuf tstart, sstart;        // nleaf + 1 leaf offsets
+  DevBuf tpos, spos;            // SoA 3 x N, recentred, sorted
+  DevBuf wsorted;               // Ns x C, point-major
+  DevBuf cub_temp;
+  DevBuf lists;    // nonempty-cell lists, back to back
+  DevBuf dcounts;  // device-side counts of the lists
+  // per-level coefficient arrays (levels 2..L)
+  DevBuf S;      // moments      sum_l 8^l * C * n3
+  DevBuf F;      // locals       sum_l 8^l * C * n3
+  DevBuf proxy;  // Cheb: sum_l 8^l * C * rs ;  Unif: spectra sum_l 8^l * nk * C (complex)
+  DevBuf pf;     // Cheb: sum_l 8^l * C * rf ;  Unif: accumulated spectra
+  // staging for the host-pointer entry point
+  DevBuf io_tgt, io_src, io_w, io_out;
+};
+
+struct LevelLists {
+  // offsets into Workspace::lists and counts (host copies after binning)
+  int64_t src_off[kMaxLevel + 1];   // nonempty source cells, Morton order
+  int64_t tgt_off[kMaxLevel + 1];   // nonempty target cells, Morton order
+  int64_t typ_off[kMaxLevel + 1];   // nonempty target cells ordered (child type, parent)
+  int nsrc[kMaxLevel + 1];
+  int ntgt[kMaxLevel + 1];
+  int ntyp[kMaxLevel + 1][9];       // type boundaries within the typed list
+};
+
+}  // namespace pbbfmm
+
+struct pbbfmm_tree {
+  pbbfmm_tree_params p{};
+  pbbfmm::KernelSpec kspec;
+  pbbfmm::Weights w;
+  pbbfmm::Operators ops;
+  int device = 0;
+  bool weights_ready = false;
+  bool ops_ready = false;
+  int precision = PBBFMM_PREC_FP64;
+  int n = 0, n3 = 0, m = 0, nk = 0;  // order, n^3, 2n-1, complex spectrum size m*m*n
+  bool homog = false;
+  double homogen_neg = 0;
+  // device operators
+  double* d_Tkz = nullptr;
+  double* d_Kw = nullptr;
+  double* d_Cw = nullptr;
+  double* d_E = nullptr;   // Cheb: nlev x 316 x rf x rs (col-major blocks)
+  double* d_U = nullptr;   // Cheb: nlev x n3 x rf
+  double* d_VT = nullptr;  // Cheb: nlev x rs x n3
+  double* d_op = nullptr;  // Unif: nlev x 343 x nk complex (lex-indexed, inner 27 zero)
+  int* d_offs = nullptr;   // Cheb M2L: 8 types x 189 x 4 (ox, oy, oz, op index)
+  double* d_twid = nullptr;  // Unif: cos/sin of 2 pi j / m, j < m
+  double* d_kparam = nullptr;  // 4 kernel parameters
+  pbbfmm::Workspace ws;
+  pbbfmm::LevelLists lists;
+  // last compute (debug access)
+  int last_C = 0;
+  int64_t last_Nf = 0, last_Ns = 0;
+  bool have_last = false;
+  // timing
+  bool timing = false;
+  cudaEvent_t ev[16] = {};
+  int nev = 0;
+  float phase_ms[16] = {};
+  int nphase = 0;
+};
+
+namespace pbbfmm {
+
+// level geometry
+inline int64_t cells_at(int l) { return (int64_t)1 << (3 * l); }
+// element offset of level l in an array holding `per_cell` values per cell for levels 2..L
+inline int64_t level_offset(int l, int64_t per_cell) {
+  int64_t off = 0;
+  for (int j = 2; j < l; ++j) off += cells_at(j) * per_cell;
+  return off;
+}
+inline int64_t level_total(int L, int64_t per_cell) { return level_offset(L + 1, per_cell); }
+
+// ---- phase launchers (return PBBFMM_* status; errors via last_error) ----
+int run_binning(pbbfmm_tree* t, const double* d_tgt, int64_t Nf, const double* d_src, int64_t Ns,
+                const double* d_w, int C, cudaStream_t st);
+int run_upward(pbbfmm_tree* t, int C, cudaStream_t st);
+int run_m2l_cheb(pbbfmm_tree* t, int C, cudaStream_t st);
+int run_m2l_unif(pbbfmm_tree* t, int C, cudaStream_t st);
+int run_downward(pbbfmm_tree* t, int C, cudaStream_t st);
+int run_leaves(pbbfmm_tree* t, int64_t Nf, int64_t Ns, int C, double* d_out, cudaStream_t st);
+// operator spectra for the uniform path (host, float64) from the stencils
+void unif_spectra(int n, const std::vector<double>& stencil, int nlev, std::vector<double>* op);
+
+void set_error(const std::string& msg);
+int cuda_status(cudaError_t e, const char* what);
+
+#define PB_CUDA(call)                                              \
+  do {                                                             \
+    cudaError_t e_ = (call);                                       \
+    if (e_ != cudaSuccess) return ::pbbfmm::cuda_status(e_, #call); \
+  } while (0)
+#define PB_LAUNCH(what)                                                    \
+  do {                                                                     \
+    cudaError_t e_ = cudaGetLastError();                                   \
+    if (e_ != cudaSuccess) return ::pbbfmm::cuda_status(e_, what);         \
+  } while (0)
+
+}  // namespace pbbfmm

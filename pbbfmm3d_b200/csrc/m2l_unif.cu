@@ -1,0 +1,372 @@
+// Uniform-grid far field in float64: FFT of the padded moments, the
+// frequency-domain M2L, and the inverse FFT to local coefficients.
+//
+// Reference: UpwardPass padding + R2HC (include/compute.hpp:337-372),
+// FarFieldInteractions / FrequencyProduct / HC2R (include/compute.hpp:
+// 488-544, 930-943) and the stencils of ComputeKernelUnif
+// (src/H2_3D_Tree.cpp:585-648).
+//
+// The reference embeds the n^3 moments in a length-(2n-1)^3 vector at offset
+// (P-1)/2 and uses a 1-D circular correlation of length P; because the offset
+// digits never carry, that equals the 3-D Toeplitz product
+//     y[a] = sum_b A[n-1+b-a] x[b],   a, b in [0,n)^3,  A the (2n-1)^3 stencil,
+// which is what runs here, as a 3-D real DFT on the m^3 grid (m = 2n-1):
+// x placed at grid position b, y read at grid position (a + n) mod m, and
+// the operator spectra stored as conj(DFT3(A)).  Only the k3 < n half of each
+// spectrum is kept (Hermitian symmetry), nk = m*m*n complex values per cell
+// and column.  Same sums as the reference, different rounding.
+#include "fmm.cuh"
+
+namespace pbbfmm {
+
+// ----------------------------------------------------------------- FFT
+// twid[j] = cos(2 pi j / m), twid[m + j] = sin(2 pi j / m)
+
+// Forward: one CTA per nonempty source cell; columns in groups of CG.
+__global__ void k_fft_fwd(const int* __restrict__ cells, const double* __restrict__ S_l,
+                          double2* __restrict__ X_l, int C, int CG, int n, int m,
+                          const double* __restrict__ twid) {
+  extern __shared__ double sm[];
+  const int n2 = n * n, n3 = n2 * n, nk = m * m * n;
+  double* sc = sm;               // m
+  double* ss = sc + m;           // m
+  double* sin_ = ss + m;         // CG * n3 real moments
+  double2* Z = (double2*)(sin_ + ((CG * n3 + 1) & ~1));  // CG * n * n * n   (l1, l2, k3)
+  double2* Y = Z + CG * n3;                              // CG * n * m * n   (l1, k2, k3)
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    sc[i] = twid[i];
+    ss[i] = twid[m + i];
+  }
+  const int cell = cells[blockIdx.x];
+  for (int c0 = 0; c0 < C; c0 += CG) {
+    const int cg = min(CG, C - c0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < cg * n3; i += blockDim.x)
+      sin_[i] = S_l[((int64_t)cell * C + c0) * n3 + i];
+    __syncthreads();
+    // z: Z[c][l1][l2][k3] = sum_l3 S[c][l1][l2][l3] w^(k3 l3),  w = e^{-2 pi i / m}
+    for (int i = threadIdx.x; i < cg * n3; i += blockDim.x) {
+      const int cc = i / n3, r = i % n3, l12 = r / n, k3 = r % n;
+      const double* s = sin_ + cc * n3 + l12 * n;
+      double re = 0, im = 0;
+      int e = 0;
+      for (int l3 = 0; l3 < n; ++l3) {
+        re += s[l3] * sc[e];
+        im -= s[l3] * ss[e];
+        e += k3;
+        if (e >= m) e -= m;
+      }
+      Z[i] = make_double2(re, im);
+    }
+    __syncthreads();
+    // y: Y[c][l1][k2][k3] = sum_l2 Z[c][l1][l2][k3] w^(k2 l2)
+    const int ny = n * m * n;
+    for (int i = threadIdx.x; i < cg * ny; i += blockDim.x) {
+      const int cc = i / ny, r = i % ny, l1 = r / (m * n), k2 = (r / n) % m, k3 = r % n;
+      const double2* z = Z + cc * n3 + l1 * n2 + k3;
+      double re = 0, im = 0;
+      int e = 0;
+      for (int l2 = 0; l2 < n; ++l2) {
+        const double2 v = z[l2 * n];
+        const double c = sc[e], s = ss[e];
+        re += v.x * c + v.y * s;
+        im += v.y * c - v.x * s;
+        e += k2;
+        if (e >= m) e -= m;
+      }
+      Y[i] = make_double2(re, im);
+    }
+    __syncthreads();
+    // x: X[k1][k2][k3][c] = sum_l1 Y[c][l1][k2][k3] w^(k1 l1)
+    for (int i = threadIdx.x; i < cg * nk; i += blockDim.x) {
+      const int k = i / cg, cc = i % cg;
+      const int k1 = k / (m * n), k23 = k % (m * n);
+      const double2* y = Y + cc * ny + k23;
+      double re = 0, im = 0;
+      int e = 0;
+      for (int l1 = 0; l1 < n; ++l1) {
+        const double2 v = y[l1 * m * n];
+        const double c = sc[e], s = ss[e];
+        re += v.x * c + v.y * s;
+        im += v.y * c - v.x * s;
+        e += k1;
+        if (e >= m) e -= m;
+      }
+      X_l[((int64_t)cell * nk + k) * C + c0 + cc] = make_double2(re, im);
+    }
+  }
+}
+
+// Inverse: one CTA per nonempty target cell.  F = scale * IDFT(Y)/P at
+// grid positions (a + n) mod m.
+__global__ void k_fft_inv(const int* __restrict__ cells, const double2* __restrict__ Y_l,
+                          double* __restrict__ F_l, int C, int CG, int n, int m,
+                          const double* __restrict__ twid, double invP, double scale) {
+  extern __shared__ double sm[];
+  const int n2 = n * n, n3 = n2 * n, nk = m * m * n;
+  double* sc = sm;
+  double* ss = sc + m;
+  double2* Yh = (double2*)(sm + 2 * m);                     // CG * nk   (k1, k2, k3)
+  double2* G = Yh + CG * nk;                                // CG * n*m*n (a1, k2, k3)
+  double2* H = G + CG * n * m * n;                          // CG * n3    (a1, a2, k3)
+  for (int i = threadIdx.x; i < m; i += blockDim.x) {
+    sc[i] = twid[i];
+    ss[i] = twid[m + i];
+  }
+  const int cell = cells[blockIdx.x];
+  for (int c0 = 0; c0 < C; c0 += CG) {
+    const int cg = min(CG, C - c0);
+    __syncthreads();
+    for (int i = threadIdx.x; i < cg * nk; i += blockDim.x) {
+      const int k = i / cg, cc = i % cg;
+      Yh[cc * nk + k] = Y_l[((int64_t)cell * nk + k) * C + c0 + cc];
+    }
+    __syncthreads();
+    // x: G[c][a1][k2][k3] = sum_k1 Yh[c][k1][k2][k3] e^{+2 pi i k1 t1 / m}
+    const int ng = n * m * n;
+    for (int i = threadIdx.x; i < cg * ng; i += blockDim.x) {
+      const int cc = i / ng, r = i % ng, a1 = r / (m * n), k23 = r % (m * n);
+      const int t1 = (a1 + n) % m;
+      const double2* y = Yh + cc * nk + k23;
+      double re = 0, im = 0;
+      int e = 0;
+      for (int k1 = 0; k1 < m; ++k1) {
+        const double2 v = y[k1 * m * n];
+        const double c = sc[e], s = ss[e];
+        re += v.x * c - v.y * s;
+        im += v.y * c + v.x * s;
+        e += t1;
+        if (e >= m) e -= m;
+      }
+      G[i] = make_double2(re, im);
+    }
+    __syncthreads();
+    // y: H[c][a1][a2][k3] = sum_k2 G[c][a1][k2][k3] e^{+2 pi i k2 t2 / m}
+    for (int i = threadIdx.x; i < cg * n3; i += blockDim.x) {
+      const int cc = i / n3, r = i % n3, a1 = r / n2, a2 = (r / n) % n, k3 = r % n;
+      const int t2 = (a2 + n) % m;
+      const double2* g = G + cc * ng + a1 * m * n + k3;
+      double re = 0, im = 0;
+      int e = 0;
+      for (int k2 = 0; k2 < m; ++k2) {
+        const double2 v = g[k2 * n];
+        const double c = sc[e], s = ss[e];
+        re += v.x * c - v.y * s;
+        im += v.y * c + v.x * s;
+        e += t2;
+        if (e >= m) e -= m;
+      }
+      H[i] = make_double2(re, im);
+    }
+    __syncthreads();
+    // z (complex to real over the Hermitian half):
+    // out = Re H[..][0] + 2 sum_{k3>=1} Re(H[..][k3] e^{+2 pi i k3 t3 / m})
+    for (int i = threadIdx.x; i < cg * n3; i += blockDim.x) {
+      const int cc = i / n3, r = i % n3, a12 = r / n, a3 = r % n;
+      const int t3 = (a3 + n) % m;
+      const double2* h = H + cc * n3 + a12 * n;
+      double acc = h[0].x;
+      int e = t3;
+      for (int k3 = 1; k3 < n; ++k3) {
+        const double2 v = h[k3];
+        acc += 2.0 * (v.x * sc[e] - v.y * ss[e]);
+        e += t3;
+        if (e >= m) e -= m;
+      }
+      F_l[((int64_t)cell * C + c0 + cc) * n3 + r] = scale * (acc * invP);
+    }
+  }
+}
+
+// ----------------------------------------------------------------- MAC
+// One CTA per block of 2x2x2 parents (4x4x4 targets) and per chunk of
+// frequencies.  Threads = (parent, kc, col); each thread accumulates the 8
+// children of its parent for one frequency and one column, sweeping the
+// 6x6x6 children of the parent's neighbours (the source halo, staged in
+// shared memory for the whole block: 8x8x8 cells).  The (child, source)
+// interaction pattern and operator index are compile-time constants.
+
+__host__ __device__ constexpr int lexidx(int ox, int oy, int oz) {
+  return 49 * (ox + 3) + 7 * (oy + 3) + (oz + 3);
+}
+
+template <int KC, int CG>
+__global__ void __launch_bounds__(8 * KC * CG)
+    k_m2l_unif_mac(const double2* __restrict__ X_l, double2* __restrict__ Y_l,
+                   const double2* __restrict__ op,  // nk x 343 for this level
+                   const int* __restrict__ sstart, const int* __restrict__ tstart, int span,
+                   int lev, int C, int nk, int ksteps) {
+  constexpr int NT = 8 * KC * CG;
+  constexpr int RC = 512;  // region cells (8 x 8 x 8)
+  extern __shared__ double2 smc[];
+  double2* reg = smc;                 // RC x KC x CG
+  double2* sop = reg + RC * KC * CG;  // KC x 343
+  const int tid = threadIdx.x;
+  const int cc = tid % CG, kc = (tid / CG) % KC, p = tid / (CG * KC);
+  const int px = (p >> 2) & 1, py = (p >> 1) & 1, pz = p & 1;
+  const int nb = 1 << (lev - 2);  // parent blocks per dimension
+  const int bidx = blockIdx.x;
+  const int bx = bidx / (nb * nb), by = (bidx / nb) % nb, bz = bidx % nb;
+  const int ox0 = 4 * bx - 2, oy0 = 4 * by - 2, oz0 = 4 * bz - 2;  // region origin (child coords)
+  const int c0 = blockIdx.z * CG;
+  const int nside = 1 << lev;
+  // does this block have any target?
+  int mine = 0;
+  {
+    const int qx = 2 * bx + px, qy = 2 * by + py, qz = 2 * bz + pz;  // parent coords
+    const uint32_t pm = morton_encode(qx, qy, qz);
+    const int64_t a = (int64_t)pm * 8 * span, b = (int64_t)(pm + 1) * 8 * span;
+    mine = tstart[b] > tstart[a];
+  }
+  if (!__syncthreads_or(mine)) return;
+  const int kbeg = blockIdx.y * ksteps * KC;
+  for (int step = 0; step < ksteps; ++step) {
+    const int k0 = kbeg + step * KC;
+    if (k0 >= nk) break;
+    __syncthreads();
+    // stage the source halo for frequencies k0..k0+KC-1 and columns c0..c0+CG-1
+    for (int i = tid; i < RC * KC * CG; i += NT) {
+      const int r = i / (KC * CG), q = i % (KC * CG), kk = q / CG, c = q % CG;
+      const int rx = r >> 6, ry = (r >> 3) & 7, rz = r & 7;
+      const int x = ox0 + rx, y = oy0 + ry, z = oz0 + rz;
+      double2 v = make_double2(0.0, 0.0);
+      if (x >= 0 && y >= 0 && z >= 0 && x < nside && y < nside && z < nside && k0 + kk < nk &&
+          c0 + c < C) {
+        const uint32_t cm = morton_encode(x, y, z);
+        if (sstart[(int64_t)(cm + 1) * span] > sstart[(int64_t)cm * span])
+          v = X_l[((int64_t)cm * nk + k0 + kk) * C + c0 + c];
+      }
+      reg[i] = v;
+    }
+    for (int i = tid; i < KC * 343; i += NT) {
+      const int kk = i / 343, e = i % 343;
+      sop[i] = (k0 + kk < nk) ? op[(int64_t)(k0 + kk) * 343 + e] : make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    double2 acc[8];
+#pragma unroll
+    for (int t = 0; t < 8; ++t) acc[t] = make_double2(0.0, 0.0);
+    const double2* myop = sop + kc * 343;
+    // sx runs as a loop (keeps the unrolled body and its registers small);
+    // for each (sy, sz, t) the y/z offsets are compile-time constants, so the
+    // interaction test reduces to |ox| > 1 unless |oy| or |oz| already is > 1.
+#pragma unroll 1
+    for (int sx = 0; sx < 6; ++sx) {
+      const double2* rrow = reg + (((2 * px + sx) << 6) * KC + kc) * CG + cc;
+      const double2* orow = myop + 49 * (sx + 1);  // lex of ox + 3 = sx + 1 - tx
+#pragma unroll
+      for (int sy = 0; sy < 6; ++sy)
+#pragma unroll
+        for (int sz = 0; sz < 6; ++sz) {
+          const int r = ((2 * py + sy) << 3) | (2 * pz + sz);
+          const double2 xv = rrow[r * KC * CG];
+#pragma unroll
+          for (int t = 0; t < 8; ++t) {
+            const int tx = (t >> 2) & 1;
+            const int oy = sy - 2 - ((t >> 1) & 1);
+            const int oz = sz - 2 - (t & 1);
+            const int ox = sx - 2 - tx;
+            const bool far_yz = oy > 1 || oy < -1 || oz > 1 || oz < -1;
+            if (far_yz || ox > 1 || ox < -1) {
+              const double2 a = orow[-49 * tx + 7 * (oy + 3) + (oz + 3)];
+              acc[t].x = fma(a.x, xv.x, acc[t].x);
+              acc[t].x = fma(-a.y, xv.y, acc[t].x);
+              acc[t].y = fma(a.x, xv.y, acc[t].y);
+              acc[t].y = fma(a.y, xv.x, acc[t].y);
+            }
+          }
+        }
+    }
+    if (k0 + kc < nk && c0 + cc < C) {
+#pragma unroll
+      for (int t = 0; t < 8; ++t) {
+        const int x = 2 * (2 * bx + px) + ((t >> 2) & 1);
+        const int y = 2 * (2 * by + py) + ((t >> 1) & 1);
+        const int z = 2 * (2 * bz + pz) + (t & 1);
+        const uint32_t cm = morton_encode(x, y, z);
+        if (tstart[(int64_t)(cm + 1) * span] > tstart[(int64_t)cm * span])
+          Y_l[((int64_t)cm * nk + k0 + kc) * C + c0 + cc] = acc[t];
+      }
+    }
+  }
+}
+
+template <int KC, int CG>
+static int launch_mac(const double2* X, double2* Y, const double2* op, const int* sstart,
+                      const int* tstart, int span, int lev, int C, int nk, cudaStream_t st) {
+  const int nb = 1 << (lev - 2);
+  const int ksteps = 4;
+  const int kchunks = (nk + KC * ksteps - 1) / (KC * ksteps);
+  dim3 g((unsigned)(nb * nb * nb), (unsigned)kchunks, (unsigned)((C + CG - 1) / CG));
+  const size_t smem = sizeof(double2) * (512 * KC * CG + KC * 343);
+  PB_CUDA(cudaFuncSetAttribute(k_m2l_unif_mac<KC, CG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)smem));
+  k_m2l_unif_mac<KC, CG><<<g, 8 * KC * CG, smem, st>>>(X, Y, op, sstart, tstart, span, lev, C,
+                                                       nk, ksteps);
+  PB_LAUNCH("m2l_unif_mac");
+  return PBBFMM_OK;
+}
+
+int run_m2l_unif(pbbfmm_tree* t, int C, cudaStream_t st) {
+  const int L = t->p.tree_level, n = t->n, m = t->m, n3 = t->n3, nk = t->nk;
+  Workspace& ws = t->ws;
+  const int* lists = ws.lists.as<int>();
+  const double* S = ws.S.as<double>();
+  double* F = ws.F.as<double>();
+  double2* X = ws.proxy.as<double2>();
+  double2* Y = ws.pf.as<double2>();
+  const int* sstart = ws.sstart.as<int>();
+  const int* tstart = ws.tstart.as<int>();
+  const int64_t perS = (int64_t)C * n3, perX = (int64_t)nk * C;
+  const double invP = 1.0 / (double)(m * m * m);
+  // forward transforms of all nonempty source cells, levels 2..L
+  const int fwd_col = n3 * 8 + n3 * 16 + n * m * n * 16;
+  const int CGf = max(1, min(C, 45000 / fwd_col));
+  const size_t smem_f = sizeof(double) * (2 * m + ((CGf * n3 + 1) & ~1)) +
+                        sizeof(double2) * (CGf * n3 + CGf * n * m * n);
+  const int inv_col = nk * 16 + n * m * n * 16 + n3 * 16;
+  const int CGi = max(1, min(C, 45000 / inv_col));
+  const size_t smem_i =
+      sizeof(double) * (2 * m) + sizeof(double2) * (CGi * nk + CGi * n * m * n + CGi * n3);
+  PB_CUDA(cudaFuncSetAttribute(k_fft_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_f));
+  PB_CUDA(cudaFuncSetAttribute(k_fft_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_i));
+  for (int l = 2; l <= L; ++l) {
+    if (t->lists.nsrc[l] == 0) continue;
+    k_fft_fwd<<<t->lists.nsrc[l], 128, smem_f, st>>>(lists + t->lists.src_off[l],
+                                                     S + level_offset(l, perS),
+                                                     X + level_offset(l, perX), C, CGf, n, m,
+                                                     t->d_twid);
+    PB_LAUNCH("fft_fwd");
+  }
+  for (int l = 2; l <= L; ++l) {
+    if (t->lists.ntgt[l] == 0) continue;
+    const int lvl = t->homog ? 0 : l - 2;
+    const double2* op = (const double2*)t->d_op + (int64_t)lvl * nk * 343;
+    const int span = (int)cells_at(L - l);
+    int rc;
+    if (C >= 8)
+      rc = launch_mac<1, 8>(X + level_offset(l, perX), Y + level_offset(l, perX), op, sstart,
+                            tstart, span, l, C, nk, st);
+    else if (C >= 4)
+      rc = launch_mac<2, 4>(X + level_offset(l, perX), Y + level_offset(l, perX), op, sstart,
+                            tstart, span, l, C, nk, st);
+    else if (C >= 2)
+      rc = launch_mac<4, 2>(X + level_offset(l, perX), Y + level_offset(l, perX), op, sstart,
+                            tstart, span, l, C, nk, st);
+    else
+      rc = launch_mac<8, 1>(X + level_offset(l, perX), Y + level_offset(l, perX), op, sstart,
+                            tstart, span, l, C, nk, st);
+    if (rc) return rc;
+    double len = t->p.L;
+    for (int i = 0; i < l; ++i) len = 0.5 * len;
+    const double scale = pow(1.0 / len, t->homogen_neg);
+    k_fft_inv<<<t->lists.ntgt[l], 128, smem_i, st>>>(lists + t->lists.tgt_off[l],
+                                                     Y + level_offset(l, perX),
+                                                     F + level_offset(l, perS), C, CGi, n, m,
+                                                     t->d_twid, invP, scale);
+    PB_LAUNCH("fft_inv");
+  }
+  return PBBFMM_OK;
+}
+
+}  // namespace pbbfmm

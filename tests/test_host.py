@@ -1,0 +1,133 @@
+"""Host-side logic of the product (no GPU): the C-ABI library loads and exports
+every declared symbol, the float64 operator precompute reproduces the
+reference's, the reference cache format round-trips, and bad arguments are
+rejected with status codes instead of crashing."""
+import os
+import re
+
+import numpy as np
+import pytest
+
+import oracle
+import pbbfmm3d_b200 as fmm
+from pbbfmm3d_b200 import _lib
+from helpers import load_case, make_tree, rel
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    src = open(os.path.join(ROOT, "include", "pbbfmm3d_b200.h")).read()
+    return sorted(set(re.findall(r"^\s*(?:const\s+)?\w+\s*\*?\s*(pbbfmm_\w+)\s*\(", src, re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    L = _lib.lib()
+    names = declared_functions()
+    assert len(names) >= 14
+    for n in names:
+        assert hasattr(L, n), n
+    assert set(names) <= set(_lib.EXPORTS), set(names) - set(_lib.EXPORTS)
+    assert b"sm_100a" in L.pbbfmm_version()
+
+
+def test_weights_match_oracle():
+    for n in (3, 4, 5, 6):
+        for cheb in (0, 1):
+            t = fmm.kernel_Laplacian(1.0, 3, n, 1e-5, cheb, device=-1)
+            a = t.get_weights()
+            b = oracle.compute_weights(n, cheb)
+            for x, y in zip(a, b):
+                if cheb == 0 and x is a[1]:
+                    continue  # Kweights unused for uniform grids
+                assert np.array_equal(x, y)
+            t.close()
+
+
+def test_uniform_precompute_matches_reference_operators():
+    case = load_case("expcov_unif4")
+    m = case["meta"]
+    t = make_tree(m["kernel"], m["param"], m["box"], m["level"], m["order"], m["eps"], 0, device=-1)
+    t.buildFMMTree()
+    ops = t.get_operators()
+    assert ops["nlev_ops"] == m["nlev_ops"] == 2
+    assert rel(ops["K"], case["K"]) < 1e-12
+
+
+@pytest.mark.parametrize("name", ["lap_cheb3", "gauss_cheb3", "tps_cheb3_outside"])
+def test_chebyshev_precompute_cutoffs_and_operator_range(name):
+    """Same SVD cutoffs as the reference; the compressed operators U E_i V^T
+    agree up to the truncation level (the kept subspace is only defined up to
+    degenerate singular values, so bitwise agreement is not expected)."""
+    case = load_case(name)
+    m = case["meta"]
+    t = make_tree(m["kernel"], m["param"], m["box"], m["level"], m["order"], m["eps"], 1, device=-1)
+    t.buildFMMTree()
+    ops = t.get_operators()
+    assert (ops["rf"], ops["rs"], ops["nlev_ops"]) == (m["rf"], m["rs"], m["nlev_ops"])
+    n3 = m["order"] ** 3
+
+    def recon(o, lvl):
+        rf, rs = o["rf"], o["rs"]
+        U = o["U"][lvl * n3 * rf:(lvl + 1) * n3 * rf].reshape(rf, n3).T
+        VT = o["VT"][lvl * rs * n3:(lvl + 1) * rs * n3].reshape(n3, rs).T
+        E = o["K"][lvl * 316 * rf * rs:(lvl + 1) * 316 * rf * rs].reshape(316, rs, rf).transpose(0, 2, 1)
+        return np.einsum("ia,kab,bj->kij", U, E, VT)
+
+    ref = {"rf": m["rf"], "rs": m["rs"], "U": case["U"], "VT": case["VT"], "K": case["K"]}
+    for lvl in range(m["nlev_ops"]):
+        assert rel(recon(ops, lvl), recon(ref, lvl)) < 10 * m["eps"]
+
+
+def test_cache_roundtrip_reference_format(tmp_path):
+    t = fmm.kernel_Laplacian(1.0, 3, 3, 1e-4, 1, device=-1)
+    t.buildFMMTree(str(tmp_path))
+    files = sorted(os.listdir(tmp_path))
+    assert files == ["LaplacianChebK3.bin", "LaplacianChebU3.bin", "LaplacianChebV3.bin"]
+    a = t.get_operators()
+    # the oracle's reader (reference layout) reads what we wrote
+    b = oracle.read_reference_cache(str(tmp_path), "Laplacian", 3, 1, 3, True)
+    assert a["rf"] == b["rf"] and np.array_equal(a["K"], b["K"]) and np.array_equal(a["U"], b["U"])
+    # a second tree reads the cache instead of recomputing
+    t2 = fmm.kernel_Laplacian(1.0, 3, 3, 1e-4, 1, device=-1)
+    t2.buildFMMTree(str(tmp_path))
+    c = t2.get_operators()
+    assert np.array_equal(a["K"], c["K"]) and np.array_equal(a["VT"], c["VT"])
+
+
+def test_nonhomogeneous_cache_is_keyed_on_box_and_level(tmp_path):
+    t = fmm.kernel_ExpCov(1.0, 3, 3, 1e-5, 0, ell=0.3, device=-1)
+    t.buildFMMTree(str(tmp_path))
+    t2 = fmm.kernel_ExpCov(2.0, 3, 3, 1e-5, 0, ell=0.3, device=-1)  # different box: stale
+    t2.buildFMMTree(str(tmp_path))
+    t3 = fmm.kernel_ExpCov(2.0, 3, 3, 1e-5, 0, ell=0.3, device=-1)
+    t3.buildFMMTree()
+    assert rel(t2.get_operators()["K"], t3.get_operators()["K"]) < 1e-14
+
+
+def test_bad_arguments_return_status():
+    with pytest.raises(fmm.FMMError) as e:
+        fmm.kernel_Laplacian(1.0, 1, 4, 1e-5, 1, device=-1)
+    assert e.value.code == _lib.ERR_ARG
+    with pytest.raises(fmm.FMMError):
+        fmm.kernel_Laplacian(-1.0, 3, 4, 1e-5, 1, device=-1)
+    with pytest.raises(fmm.FMMError):
+        fmm.kernel_Laplacian(1.0, 3, 11, 1e-5, 1, device=-1)
+    with pytest.raises(fmm.FMMError):
+        fmm.kernel_ExpCov(1.0, 3, 4, 1e-5, 0, ell=0.0, device=-1)
+    t = fmm.kernel_Laplacian(1.0, 3, 3, 1e-4, 1, device=-1)
+    with pytest.raises(fmm.FMMError) as e:  # compute before build
+        fmm.H2_3D_Compute(t, np.zeros((4, 3)), np.zeros((4, 3)), np.zeros(4), 1, np.zeros(4))
+    assert e.value.code == _lib.ERR_STATE
+    t.buildFMMTree()
+    with pytest.raises(fmm.FMMError) as e:  # host-only tree cannot compute
+        fmm.H2_3D_Compute(t, np.zeros((4, 3)), np.zeros((4, 3)), np.zeros(4), 1, np.zeros(4))
+    assert e.value.code == _lib.ERR_STATE
+    with pytest.raises(ValueError):
+        fmm.H2_3D_Compute(t, np.zeros((4, 3)), np.zeros((4, 3)), np.zeros(3), 1, np.zeros(4))
+    # wrong operator level count (homogeneous kernel: one level)
+    z = np.zeros(5 * 316 * 27 * 27)
+    with pytest.raises(fmm.FMMError) as e:
+        _lib.check(
+            _lib.lib().pbbfmm_tree_set_operators(t._h, 27, 27, 5, fmm._dp(z), fmm._dp(z), fmm._dp(z)))
+    assert e.value.code == _lib.ERR_ARG
