@@ -124,6 +124,18 @@ int pbbfmm_set_timing(pbbfmm_tree *tree, int enable);
 int pbbfmm_get_phase_times(const pbbfmm_tree *tree, float *ms, int max_phases, int *nphases,
                            const char **names);
 
+/* Per-kernel device times: with timing enabled, every launch of a compute
+ * is bracketed by CUDA events on its stream.  Slots (names, comma-separated):
+ * binning, p2m, m2m, m2l_pre, m2l, m2l_post, fft_fwd, m2l_mac, fft_inv,
+ * l2l, leaf.  ms / launches are summed since the last reset. */
+int pbbfmm_reset_kernel_times(pbbfmm_tree *tree);
+int pbbfmm_get_kernel_times(pbbfmm_tree *tree, float *ms, int *launches, int max_slots,
+                            int *nslots, const char **names);
+
+/* Measured float64 (precision 0) or float32 (1) FMA throughput of `device`
+ * in TFLOP/s (2 flops per FMA): the peak the CUDA-core kernels are held to. */
+int pbbfmm_measure_fma_peak(int device, int precision, double *tflops);
+
 /* Debug/test access to device arrays of the last compute (all as float64):
  * what = 0 moments S of `level` (8^level x nCols x n^3, cell-major; only
  * nonempty source cells are defined), 1 locals F after L2L (nonempty target
@@ -140,6 +152,10 @@ int pbbfmm_tree_get_weights(const pbbfmm_tree *tree, double *Tkz, double *Kweigh
 
 const char *pbbfmm_last_error(void);
 const char *pbbfmm_version(void);
+
+/* Number of CUDA kernel launches this library has issued in this process
+ * (including the kernels of the CUB sort/select calls it makes). */
+long long pbbfmm_launch_count(void);
 
 #ifdef __cplusplus
 }

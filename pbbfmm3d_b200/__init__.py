@@ -143,6 +143,20 @@ class H2_3D_Tree:
                                                      ctypes.byref(names)))
         return dict(zip(names.value.decode().split(","), [ms[i] for i in range(nph.value)]))
 
+    def reset_kernel_times(self) -> None:
+        _lib.check(_lib.lib().pbbfmm_reset_kernel_times(self._h))
+
+    def kernel_times(self) -> dict:
+        """{slot: (ms, launches)} summed since the last reset (timing on)."""
+        ms = (ctypes.c_float * 32)()
+        cnt = (ctypes.c_int * 32)()
+        ns = ctypes.c_int()
+        names = ctypes.c_char_p()
+        _lib.check(_lib.lib().pbbfmm_get_kernel_times(self._h, ms, cnt, 32, ctypes.byref(ns),
+                                                      ctypes.byref(names)))
+        keys = names.value.decode().split(",")
+        return {k: (ms[i], cnt[i]) for i, k in enumerate(keys[:ns.value])}
+
     def debug_copy(self, what: int, level: int = 0) -> np.ndarray:
         n = ctypes.c_int64()
         L = _lib.lib()
@@ -219,6 +233,18 @@ def H2_3D_Compute(tree: H2_3D_Tree, target, source, weight, nCols: int, output) 
     _lib.check(_lib.lib().pbbfmm_compute(tree._h, _dp(t), Nf, _dp(s), Ns, _dp(w), int(nCols),
                                          _dp(output)))
     return output
+
+
+def launch_count() -> int:
+    """Kernel launches issued by the library so far in this process."""
+    return int(_lib.lib().pbbfmm_launch_count())
+
+
+def measure_fma_peak(device: int = 0, precision: int = PREC_FP64) -> float:
+    """Measured FMA throughput (TFLOP/s) of the FP64 or FP32 pipes."""
+    v = ctypes.c_double()
+    _lib.check(_lib.lib().pbbfmm_measure_fma_peak(int(device), int(precision), ctypes.byref(v)))
+    return v.value
 
 
 def compute_device(tree: H2_3D_Tree, target, source, weight, nCols: int, output,

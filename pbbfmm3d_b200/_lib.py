@@ -59,6 +59,11 @@ EXPORTS = {
     "pbbfmm_tree_get_weights": ([_vp, _dp, _dp, _dp, _ip], ctypes.c_int),
     "pbbfmm_last_error": ([], ctypes.c_char_p),
     "pbbfmm_version": ([], ctypes.c_char_p),
+    "pbbfmm_launch_count": ([], ctypes.c_longlong),
+    "pbbfmm_reset_kernel_times": ([_vp], ctypes.c_int),
+    "pbbfmm_get_kernel_times": ([_vp, ctypes.POINTER(ctypes.c_float), _ip, ctypes.c_int, _ip,
+                                 ctypes.POINTER(ctypes.c_char_p)], ctypes.c_int),
+    "pbbfmm_measure_fma_peak": ([ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
 }
 
 

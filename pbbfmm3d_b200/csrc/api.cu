@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
 #include <string>
 
 #include "fmm.cuh"
@@ -14,6 +15,35 @@
 namespace pbbfmm {
 
 static thread_local std::string g_err;
+static std::atomic<long long> g_launches{0};
+
+void count_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+const char* const kSlotNames =
+    "binning,p2m,m2m,m2l_pre,m2l,m2l_post,fft_fwd,m2l_mac,fft_inv,l2l,leaf";
+
+int kt_begin(pbbfmm_tree* t, int slot, cudaStream_t st) {
+  if (!t->timing) return PBBFMM_OK;
+  if (t->kused + 2 > t->kev.size()) {
+    for (int i = 0; i < 64; ++i) {
+      cudaEvent_t e;
+      PB_CUDA(cudaEventCreate(&e));
+      t->kev.push_back(e);
+    }
+    t->kslot.resize(t->kev.size() / 2 + 1);
+  }
+  t->kslot[t->kused / 2] = slot;
+  PB_CUDA(cudaEventRecord(t->kev[t->kused], st));
+  t->kused += 1;
+  return PBBFMM_OK;
+}
+
+int kt_end(pbbfmm_tree* t, cudaStream_t st) {
+  if (!t->timing) return PBBFMM_OK;
+  PB_CUDA(cudaEventRecord(t->kev[t->kused], st));
+  t->kused += 1;
+  return PBBFMM_OK;
+}
 
 void set_error(const std::string& msg) { g_err = msg; }
 
@@ -185,13 +215,16 @@ static void free_tree_device(pbbfmm_tree* t) {
                    &ws.tperm,     &ws.sperm, &ws.tstart,  &ws.sstart,     &ws.tpos,
                    &ws.spos,      &ws.wsorted, &ws.cub_temp, &ws.lists,    &ws.dcounts,
                    &ws.S,         &ws.F,     &ws.proxy,   &ws.pf,         &ws.io_tgt,
-                   &ws.io_src,    &ws.io_w,  &ws.io_out};
+                   &ws.io_src,    &ws.io_w,  &ws.io_out, &ws.halo};
   for (DevBuf* b : all) release(*b);
   for (int i = 0; i < 16; ++i)
     if (t->ev[i]) {
       cudaEventDestroy(t->ev[i]);
       t->ev[i] = nullptr;
     }
+  for (cudaEvent_t e : t->kev) cudaEventDestroy(e);
+  t->kev.clear();
+  t->kused = 0;
 }
 
 static const char* kPhaseNames = "binning,upward,far_field,downward,near_field";
@@ -207,7 +240,9 @@ static int compute_chunk(pbbfmm_tree* t, const double* d_tgt, int64_t Nf, const 
   t->last_Nf = Nf;
   t->last_Ns = Ns;
   t->last_C = C;
+  if ((rc = kt_begin(t, KS_BINNING, st))) return rc;
   if ((rc = run_binning(t, d_tgt, Nf, d_src, Ns, d_w, C, st))) return rc;
+  if ((rc = kt_end(t, st))) return rc;
   if (t->timing) PB_CUDA(cudaEventRecord(t->ev[1], st));
   const int64_t perS = (int64_t)C * n3;
   if ((rc = grow(ws.S, sizeof(double) * level_total(L, perS)))) return rc;
@@ -218,6 +253,7 @@ static int compute_chunk(pbbfmm_tree* t, const double* d_tgt, int64_t Nf, const 
   } else {
     if ((rc = grow(ws.proxy, 2 * sizeof(double) * level_total(L, (int64_t)C * t->nk)))) return rc;
     if ((rc = grow(ws.pf, 2 * sizeof(double) * level_total(L, (int64_t)C * t->nk)))) return rc;
+    if ((rc = grow(ws.halo, sizeof(int) * 576 * cells_at(L - 2)))) return rc;
   }
   (void)precision;
   if ((rc = run_upward(t, C, st))) return rc;
@@ -244,6 +280,8 @@ extern "C" {
 
 const char* pbbfmm_last_error(void) { return g_err.c_str(); }
 const char* pbbfmm_version(void) { return "pbbfmm3d_b200 0.1 (sm_100a)"; }
+
+long long pbbfmm_launch_count(void) { return g_launches.load(); }
 
 int pbbfmm_tree_create(const pbbfmm_tree_params* params, int device, pbbfmm_tree** out) {
   if (!params || !out) {
@@ -466,6 +504,35 @@ int pbbfmm_set_timing(pbbfmm_tree* t, int enable) {
   if (enable && !t->ev[0])
     for (int i = 0; i <= kNumPhases; ++i) PB_CUDA(cudaEventCreate(&t->ev[i]));
   t->timing = enable != 0;
+  return PBBFMM_OK;
+}
+
+int pbbfmm_reset_kernel_times(pbbfmm_tree* t) {
+  if (!t) return PBBFMM_ERR_ARG;
+  t->kused = 0;
+  return PBBFMM_OK;
+}
+
+int pbbfmm_get_kernel_times(pbbfmm_tree* t, float* ms, int* launches, int max_slots, int* nslots,
+                            const char** names) {
+  if (!t || t->device < 0) return PBBFMM_ERR_ARG;
+  if (names) *names = kSlotNames;
+  if (nslots) *nslots = KS_COUNT;
+  for (int i = 0; i < max_slots && i < KS_COUNT; ++i) {
+    if (ms) ms[i] = 0;
+    if (launches) launches[i] = 0;
+  }
+  PB_CUDA(cudaSetDevice(t->device));
+  for (size_t k = 0; k + 1 < t->kused; k += 2) {
+    float v = 0;
+    PB_CUDA(cudaEventSynchronize(t->kev[k + 1]));
+    PB_CUDA(cudaEventElapsedTime(&v, t->kev[k], t->kev[k + 1]));
+    const int slot = t->kslot[k / 2];
+    if (slot < max_slots) {
+      if (ms) ms[slot] += v;
+      if (launches) launches[slot] += 1;
+    }
+  }
   return PBBFMM_OK;
 }
 

@@ -146,6 +146,40 @@ inline int dispatch_kernel(int kid, F&& f) {
   }
 }
 
+// ------------------------------------------------------------ async copies
+// 16-byte global -> shared copy that bypasses registers (cp.async, L2 only);
+// src_bytes = 0 zero-fills the destination without reading `src` (which must
+// still be a valid address).
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* src, int src_bytes) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(d), "l"(src),
+               "r"(src_bytes)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() {
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
+}
+
+// Run `f.template run<N>()` for the runtime interpolation order N (2..10).
+template <typename F>
+inline int dispatch_order(int n, F&& f) {
+  switch (n) {
+    case 2: return f.template run<2>();
+    case 3: return f.template run<3>();
+    case 4: return f.template run<4>();
+    case 5: return f.template run<5>();
+    case 6: return f.template run<6>();
+    case 7: return f.template run<7>();
+    case 8: return f.template run<8>();
+    case 9: return f.template run<9>();
+    case 10: return f.template run<10>();
+    default: return PBBFMM_ERR_ARG;
+  }
+}
+
 // ------------------------------------------------------------ basis
 // S_m(x) per coordinate (ComputeSn, src/H2_3D_Tree.cpp:830-892).
 // Chebyshev: (2/n) * Clenshaw sum of T_k(node_m) T_k(x); uniform: Lagrange.

@@ -97,6 +97,7 @@ __global__ void __launch_bounds__(32 * kLeafWarps)
   __shared__ double sTkz[kMaxOrder * kMaxOrder];
   __shared__ double kp[4];
   __shared__ int s_nb[kLeafWarps][27][2];           // neighbour source ranges
+  __shared__ int s_pre[kLeafWarps][28];             // exclusive prefix of their lengths
   __shared__ double s_b[kLeafWarps][3][kMaxOrder];  // basis values of the current target
   for (int i = threadIdx.x; i < n * n; i += blockDim.x) sTkz[i] = Tkz_g[i];
   if (threadIdx.x < 4) kp[threadIdx.x] = kparam_g[threadIdx.x];
@@ -129,6 +130,16 @@ __global__ void __launch_bounds__(32 * kLeafWarps)
     s_nb[wl][q][1] = e;
   }
   __syncwarp();
+  if (lane == 0) {
+    int acc = 0;
+    for (int q = 0; q < 27; ++q) {
+      s_pre[wl][q] = acc;
+      acc += s_nb[wl][q][1] - s_nb[wl][q][0];
+    }
+    s_pre[wl][27] = acc;
+  }
+  __syncwarp();
+  const int nsrc_total = s_pre[wl][27];
   for (int c0 = 0; c0 < C; c0 += kLeafCols) {
     const int cg = min(kLeafCols, C - c0);
     for (int i = ta; i < te; ++i) {
@@ -155,10 +166,13 @@ __global__ void __launch_bounds__(32 * kLeafWarps)
             if (cc < cg) acc[cc] += Fl[cc * n3 + l] * tmp2 * bz3;
         }
       }
-      // near field over the 27 neighbour leaves
-      for (int q = 0; q < 27; ++q) {
-        const int qa = s_nb[wl][q][0], qe = s_nb[wl][q][1];
-        for (int j = qa + lane; j < qe; j += 32) {
+      // near field over the 27 neighbour leaves, their source ranges
+      // concatenated so that the lanes stay busy when leaves are small
+      {
+        int q = 0;
+        for (int v = lane; v < nsrc_total; v += 32) {
+          while (v >= s_pre[wl][q + 1]) ++q;
+          const int j = s_nb[wl][q][0] + (v - s_pre[wl][q]);
           const double dx = spos[j] - x, dy = spos[(int64_t)Ns + j] - y,
                        dz = spos[2 * (int64_t)Ns + j] - z;
           double kv = KF::template eval<double>(dx, dy, dz, kp);
@@ -200,12 +214,14 @@ struct LeafLaunch {
     if (nl == 0) return PBBFMM_OK;
     Workspace& ws = t->ws;
     const int64_t perS = (int64_t)C * t->n3;
+    if (int rc_ = kt_begin(t, KS_LEAF, st)) return rc_;
     k_leaf<KF><<<(nl + kLeafWarps - 1) / kLeafWarps, 32 * kLeafWarps, 0, st>>>(
         ws.lists.as<int>() + t->lists.tgt_off[L], nl, ws.tstart.as<int>(), ws.sstart.as<int>(),
         ws.tperm.as<int>(), ws.tpos.as<double>(), ws.spos.as<double>(), ws.wsorted.as<double>(),
         (int)Nf, (int)Ns, C, ws.F.as<double>() + level_offset(L, perS), t->n,
         t->p.use_chebyshev, t->d_Tkz, t->p.L, L, kparam, out);
     PB_LAUNCH("leaf");
+    if (int rc_ = kt_end(t, st)) return rc_;
     return PBBFMM_OK;
   }
 };
@@ -218,10 +234,12 @@ int run_downward(pbbfmm_tree* t, int C, cudaStream_t st) {
   const int64_t per = (int64_t)C * n3;
   for (int l = 3; l <= L; ++l) {
     if (t->lists.ntgt[l] == 0) continue;
+    if (int rc_ = kt_begin(t, KS_L2L, st)) return rc_;
     k_l2l<<<t->lists.ntgt[l], kL2LThreads, 0, st>>>(lists + t->lists.tgt_off[l],
                                                      F + level_offset(l - 1, per),
                                                      F + level_offset(l, per), C, t->n, t->d_Cw);
     PB_LAUNCH("l2l");
+    if (int rc_ = kt_end(t, st)) return rc_;
   }
   return PBBFMM_OK;
 }

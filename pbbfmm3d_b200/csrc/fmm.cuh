@@ -43,6 +43,7 @@ struct Workspace {
   DevBuf F;      // locals       sum_l 8^l * C * n3
   DevBuf proxy;  // Cheb: sum_l 8^l * C * rs ;  Unif: spectra sum_l 8^l * nk * C (complex)
   DevBuf pf;     // Cheb: sum_l 8^l * C * rf ;  Unif: accumulated spectra
+  DevBuf halo;   // Unif M2L: per parent block 512 halo + 64 target cells
   // staging for the host-pointer entry point
   DevBuf io_tgt, io_src, io_w, io_out;
 };
@@ -94,6 +95,10 @@ struct pbbfmm_tree {
   int nev = 0;
   float phase_ms[16] = {};
   int nphase = 0;
+  // per-kernel event pairs of the computes since the last reset (timing on)
+  std::vector<cudaEvent_t> kev;
+  std::vector<int> kslot;  // slot of each event pair
+  size_t kused = 0;
 };
 
 namespace pbbfmm {
@@ -119,6 +124,16 @@ int run_leaves(pbbfmm_tree* t, int64_t Nf, int64_t Ns, int C, double* d_out, cud
 // operator spectra for the uniform path (host, float64) from the stencils
 void unif_spectra(int n, const std::vector<double>& stencil, int nlev, std::vector<double>* op);
 
+// Kernel timer slots (pbbfmm_get_kernel_times).
+enum KSlot {
+  KS_BINNING = 0, KS_P2M, KS_M2M, KS_M2L_PRE, KS_M2L, KS_M2L_POST, KS_FFT_FWD, KS_MAC, KS_FFT_INV,
+  KS_L2L, KS_LEAF, KS_COUNT
+};
+extern const char* const kSlotNames;
+// Record an event before / after a launch when timing is enabled.
+int kt_begin(pbbfmm_tree* t, int slot, cudaStream_t st);
+int kt_end(pbbfmm_tree* t, cudaStream_t st);
+
 void set_error(const std::string& msg);
 int cuda_status(cudaError_t e, const char* what);
 
@@ -127,10 +142,15 @@ int cuda_status(cudaError_t e, const char* what);
     cudaError_t e_ = (call);                                       \
     if (e_ != cudaSuccess) return ::pbbfmm::cuda_status(e_, #call); \
   } while (0)
-#define PB_LAUNCH(what)                                                    \
+// Kernel launches issued by this library (CUB calls count their internal
+// launches: see count_launches at the CUB call sites).
+void count_launches(int n);
+#define PB_LAUNCH_N(what, n)                                               \
   do {                                                                     \
+    ::pbbfmm::count_launches(n);                                           \
     cudaError_t e_ = cudaGetLastError();                                   \
     if (e_ != cudaSuccess) return ::pbbfmm::cuda_status(e_, what);         \
   } while (0)
+#define PB_LAUNCH(what) PB_LAUNCH_N(what, 1)
 
 }  // namespace pbbfmm

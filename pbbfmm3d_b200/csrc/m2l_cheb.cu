@@ -218,11 +218,13 @@ int run_m2l_cheb(pbbfmm_tree* t, int C, cudaStream_t st) {
     const int ns = t->lists.nsrc[l];
     if (ns > 0) {
       dim3 g((unsigned)((ns * (int64_t)C + GBN - 1) / GBN), (unsigned)((rs + GBM - 1) / GBM));
+      if (int rc_ = kt_begin(t, KS_M2L_PRE, st)) return rc_;
       k_colgemm<<<g, kGemmThreads, 0, st>>>(rs, n3, t->d_VT + (int64_t)lvl * rs * n3,
                                             lists + t->lists.src_off[l], ns * C, C,
                                             S + level_offset(l, (int64_t)C * n3), t->d_Kw,
                                             proxy + level_offset(l, (int64_t)C * rs), nullptr, 1.0);
       PB_LAUNCH("m2l_pre");
+      if (int rc_ = kt_end(t, st)) return rc_;
     }
   }
   for (int l = 2; l <= L; ++l) {
@@ -241,22 +243,26 @@ int run_m2l_cheb(pbbfmm_tree* t, int C, cudaStream_t st) {
     tt.start[8] = tiles;
     if (tiles > 0) {
       dim3 g((unsigned)tiles, (unsigned)((rf + GBM - 1) / GBM));
+      if (int rc_ = kt_begin(t, KS_M2L, st)) return rc_;
       k_m2l_cheb<<<g, kGemmThreads, 0, st>>>(
           rf, rs, t->d_E + (int64_t)lvl * 316 * rf * rs, lists + t->lists.typ_off[l], tt, C, l,
           sstart, (int)cells_at(L - l), t->d_offs, proxy + level_offset(l, (int64_t)C * rs),
           pf + level_offset(l, (int64_t)C * rf));
       PB_LAUNCH("m2l_cheb");
+      if (int rc_ = kt_end(t, st)) return rc_;
     }
     // F = scale * Kw o (U_lvl * Pf)
     double len = t->p.L;
     for (int i = 0; i < l; ++i) len = 0.5 * len;
     const double scale = pow(1.0 / len, t->homogen_neg);
     dim3 g2((unsigned)((nt * (int64_t)C + GBN - 1) / GBN), (unsigned)((n3 + GBM - 1) / GBM));
+    if (int rc_ = kt_begin(t, KS_M2L_POST, st)) return rc_;
     k_colgemm<<<g2, kGemmThreads, 0, st>>>(n3, rf, t->d_U + (int64_t)lvl * n3 * rf,
                                            lists + t->lists.tgt_off[l], nt * C, C,
                                            pf + level_offset(l, (int64_t)C * rf), nullptr,
                                            F + level_offset(l, (int64_t)C * n3), t->d_Kw, scale);
     PB_LAUNCH("m2l_post");
+    if (int rc_ = kt_end(t, st)) return rc_;
   }
   return PBBFMM_OK;
 }

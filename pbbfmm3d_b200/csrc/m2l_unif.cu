@@ -22,12 +22,17 @@ namespace pbbfmm {
 // ----------------------------------------------------------------- FFT
 // twid[j] = cos(2 pi j / m), twid[m + j] = sin(2 pi j / m)
 
+// Spectra of a level are stored frequency-major: X[(k * ncells + cell) * C + col]
+// (ncells = 8^level), so that one frequency plane of a level is contiguous.
+
 // Forward: one CTA per nonempty source cell; columns in groups of CG.
+// Templated on the order so that all index arithmetic is by constants.
+template <int n>
 __global__ void k_fft_fwd(const int* __restrict__ cells, const double* __restrict__ S_l,
-                          double2* __restrict__ X_l, int C, int CG, int n, int m,
+                          double2* __restrict__ X_l, int64_t ncells, int C, int CG,
                           const double* __restrict__ twid) {
   extern __shared__ double sm[];
-  const int n2 = n * n, n3 = n2 * n, nk = m * m * n;
+  constexpr int m = 2 * n - 1, n2 = n * n, n3 = n2 * n, nk = m * m * n;
   double* sc = sm;               // m
   double* ss = sc + m;           // m
   double* sin_ = ss + m;         // CG * n3 real moments
@@ -50,6 +55,7 @@ __global__ void k_fft_fwd(const int* __restrict__ cells, const double* __restric
       const double* s = sin_ + cc * n3 + l12 * n;
       double re = 0, im = 0;
       int e = 0;
+#pragma unroll
       for (int l3 = 0; l3 < n; ++l3) {
         re += s[l3] * sc[e];
         im -= s[l3] * ss[e];
@@ -60,12 +66,13 @@ __global__ void k_fft_fwd(const int* __restrict__ cells, const double* __restric
     }
     __syncthreads();
     // y: Y[c][l1][k2][k3] = sum_l2 Z[c][l1][l2][k3] w^(k2 l2)
-    const int ny = n * m * n;
+    constexpr int ny = n * m * n;
     for (int i = threadIdx.x; i < cg * ny; i += blockDim.x) {
       const int cc = i / ny, r = i % ny, l1 = r / (m * n), k2 = (r / n) % m, k3 = r % n;
       const double2* z = Z + cc * n3 + l1 * n2 + k3;
       double re = 0, im = 0;
       int e = 0;
+#pragma unroll
       for (int l2 = 0; l2 < n; ++l2) {
         const double2 v = z[l2 * n];
         const double c = sc[e], s = ss[e];
@@ -84,6 +91,7 @@ __global__ void k_fft_fwd(const int* __restrict__ cells, const double* __restric
       const double2* y = Y + cc * ny + k23;
       double re = 0, im = 0;
       int e = 0;
+#pragma unroll
       for (int l1 = 0; l1 < n; ++l1) {
         const double2 v = y[l1 * m * n];
         const double c = sc[e], s = ss[e];
@@ -92,18 +100,19 @@ __global__ void k_fft_fwd(const int* __restrict__ cells, const double* __restric
         e += k1;
         if (e >= m) e -= m;
       }
-      X_l[((int64_t)cell * nk + k) * C + c0 + cc] = make_double2(re, im);
+      X_l[((int64_t)k * ncells + cell) * C + c0 + cc] = make_double2(re, im);
     }
   }
 }
 
 // Inverse: one CTA per nonempty target cell.  F = scale * IDFT(Y)/P at
 // grid positions (a + n) mod m.
+template <int n>
 __global__ void k_fft_inv(const int* __restrict__ cells, const double2* __restrict__ Y_l,
-                          double* __restrict__ F_l, int C, int CG, int n, int m,
+                          double* __restrict__ F_l, int64_t ncells, int C, int CG,
                           const double* __restrict__ twid, double invP, double scale) {
   extern __shared__ double sm[];
-  const int n2 = n * n, n3 = n2 * n, nk = m * m * n;
+  constexpr int m = 2 * n - 1, n2 = n * n, n3 = n2 * n, nk = m * m * n;
   double* sc = sm;
   double* ss = sc + m;
   double2* Yh = (double2*)(sm + 2 * m);                     // CG * nk   (k1, k2, k3)
@@ -119,17 +128,18 @@ __global__ void k_fft_inv(const int* __restrict__ cells, const double2* __restri
     __syncthreads();
     for (int i = threadIdx.x; i < cg * nk; i += blockDim.x) {
       const int k = i / cg, cc = i % cg;
-      Yh[cc * nk + k] = Y_l[((int64_t)cell * nk + k) * C + c0 + cc];
+      Yh[cc * nk + k] = Y_l[((int64_t)k * ncells + cell) * C + c0 + cc];
     }
     __syncthreads();
     // x: G[c][a1][k2][k3] = sum_k1 Yh[c][k1][k2][k3] e^{+2 pi i k1 t1 / m}
-    const int ng = n * m * n;
+    constexpr int ng = n * m * n;
     for (int i = threadIdx.x; i < cg * ng; i += blockDim.x) {
       const int cc = i / ng, r = i % ng, a1 = r / (m * n), k23 = r % (m * n);
       const int t1 = (a1 + n) % m;
       const double2* y = Yh + cc * nk + k23;
       double re = 0, im = 0;
       int e = 0;
+#pragma unroll
       for (int k1 = 0; k1 < m; ++k1) {
         const double2 v = y[k1 * m * n];
         const double c = sc[e], s = ss[e];
@@ -148,6 +158,7 @@ __global__ void k_fft_inv(const int* __restrict__ cells, const double2* __restri
       const double2* g = G + cc * ng + a1 * m * n + k3;
       double re = 0, im = 0;
       int e = 0;
+#pragma unroll
       for (int k2 = 0; k2 < m; ++k2) {
         const double2 v = g[k2 * n];
         const double c = sc[e], s = ss[e];
@@ -167,6 +178,7 @@ __global__ void k_fft_inv(const int* __restrict__ cells, const double2* __restri
       const double2* h = H + cc * n3 + a12 * n;
       double acc = h[0].x;
       int e = t3;
+#pragma unroll
       for (int k3 = 1; k3 < n; ++k3) {
         const double2 v = h[k3];
         acc += 2.0 * (v.x * sc[e] - v.y * ss[e]);
@@ -179,133 +191,178 @@ __global__ void k_fft_inv(const int* __restrict__ cells, const double2* __restri
 }
 
 // ----------------------------------------------------------------- MAC
-// One CTA per block of 2x2x2 parents (4x4x4 targets) and per chunk of
-// frequencies.  Threads = (parent, kc, col); each thread accumulates the 8
-// children of its parent for one frequency and one column, sweeping the
-// 6x6x6 children of the parent's neighbours (the source halo, staged in
-// shared memory for the whole block: 8x8x8 cells).  The (child, source)
+// One CTA per (block of 2x2x2 parents = 4x4x4 targets, frequency chunk),
+// the frequency chunk varying slowest in the grid so that resident CTAs work
+// on the same frequency plane (one plane of level 6 is 33.5 MB and stays in
+// L2 while its ~8x halo reuse is served).  Threads = (parent, kc, col); each
+// thread accumulates the 8 children of its parent for one frequency and one
+// column, sweeping the 6x6x6 children of the parent's neighbours staged in
+// shared memory for the whole block (8x8x8 cells).  The (child, source)
 // interaction pattern and operator index are compile-time constants.
+//
+// Per level, halo[b*576 + r] (r < 512) holds the source cell of region slot r
+// of parent block b (or -1: outside the domain or no sources) and
+// halo[b*576 + 512 + q] the target cell of block slot q (or -1).
 
-__host__ __device__ constexpr int lexidx(int ox, int oy, int oz) {
-  return 49 * (ox + 3) + 7 * (oy + 3) + (oz + 3);
+__global__ void k_halo_tables(const int* __restrict__ sstart, const int* __restrict__ tstart,
+                              int span, int lev, int* __restrict__ halo) {
+  const int nb = 1 << (lev - 2);
+  const int b = blockIdx.x;
+  const int bx = b / (nb * nb), by = (b / nb) % nb, bz = b % nb;
+  const int nside = 1 << lev;
+  for (int r = threadIdx.x; r < 576; r += blockDim.x) {
+    int v = -1;
+    if (r < 512) {
+      const int x = 4 * bx - 2 + (r >> 6), y = 4 * by - 2 + ((r >> 3) & 7), z = 4 * bz - 2 + (r & 7);
+      if (x >= 0 && y >= 0 && z >= 0 && x < nside && y < nside && z < nside) {
+        const uint32_t cm = morton_encode(x, y, z);
+        if (sstart[(int64_t)(cm + 1) * span] > sstart[(int64_t)cm * span]) v = (int)cm;
+      }
+    } else {
+      const int q = r - 512;
+      const uint32_t cm = morton_encode(4 * bx + (q >> 4), 4 * by + ((q >> 2) & 3), 4 * bz + (q & 3));
+      if (tstart[(int64_t)(cm + 1) * span] > tstart[(int64_t)cm * span]) v = (int)cm;
+    }
+    halo[(int64_t)b * 576 + r] = v;
+  }
 }
 
 template <int KC, int CG>
 __global__ void __launch_bounds__(8 * KC * CG)
     k_m2l_unif_mac(const double2* __restrict__ X_l, double2* __restrict__ Y_l,
                    const double2* __restrict__ op,  // nk x 343 for this level
-                   const int* __restrict__ sstart, const int* __restrict__ tstart, int span,
-                   int lev, int C, int nk, int ksteps) {
+                   const int* __restrict__ halo, int64_t ncells, int C, int nk) {
   constexpr int NT = 8 * KC * CG;
   constexpr int RC = 512;  // region cells (8 x 8 x 8)
   extern __shared__ double2 smc[];
-  double2* reg = smc;                 // RC x KC x CG
-  double2* sop = reg + RC * KC * CG;  // KC x 343
+  double2* reg = smc;                   // RC x KC x CG
+  double2* sop = reg + RC * KC * CG;    // KC x 343
+  int* s_src = (int*)(sop + KC * 343);  // RC source cells, then 64 target cells
+  int* s_tgt = s_src + RC;
   const int tid = threadIdx.x;
   const int cc = tid % CG, kc = (tid / CG) % KC, p = tid / (CG * KC);
   const int px = (p >> 2) & 1, py = (p >> 1) & 1, pz = p & 1;
-  const int nb = 1 << (lev - 2);  // parent blocks per dimension
-  const int bidx = blockIdx.x;
-  const int bx = bidx / (nb * nb), by = (bidx / nb) % nb, bz = bidx % nb;
-  const int ox0 = 4 * bx - 2, oy0 = 4 * by - 2, oz0 = 4 * bz - 2;  // region origin (child coords)
-  const int c0 = blockIdx.z * CG;
-  const int nside = 1 << lev;
-  // does this block have any target?
+  const int* hb = halo + (int64_t)blockIdx.x * 576;
   int mine = 0;
-  {
-    const int qx = 2 * bx + px, qy = 2 * by + py, qz = 2 * bz + pz;  // parent coords
-    const uint32_t pm = morton_encode(qx, qy, qz);
-    const int64_t a = (int64_t)pm * 8 * span, b = (int64_t)(pm + 1) * 8 * span;
-    mine = tstart[b] > tstart[a];
+  for (int r = tid; r < 576; r += NT) {
+    const int v = hb[r];
+    s_src[r] = v;
+    if (r >= RC) mine |= v >= 0;
   }
   if (!__syncthreads_or(mine)) return;
-  const int kbeg = blockIdx.y * ksteps * KC;
-  for (int step = 0; step < ksteps; ++step) {
-    const int k0 = kbeg + step * KC;
-    if (k0 >= nk) break;
-    __syncthreads();
-    // stage the source halo for frequencies k0..k0+KC-1 and columns c0..c0+CG-1
-    for (int i = tid; i < RC * KC * CG; i += NT) {
-      const int r = i / (KC * CG), q = i % (KC * CG), kk = q / CG, c = q % CG;
-      const int rx = r >> 6, ry = (r >> 3) & 7, rz = r & 7;
-      const int x = ox0 + rx, y = oy0 + ry, z = oz0 + rz;
-      double2 v = make_double2(0.0, 0.0);
-      if (x >= 0 && y >= 0 && z >= 0 && x < nside && y < nside && z < nside && k0 + kk < nk &&
-          c0 + c < C) {
-        const uint32_t cm = morton_encode(x, y, z);
-        if (sstart[(int64_t)(cm + 1) * span] > sstart[(int64_t)cm * span])
-          v = X_l[((int64_t)cm * nk + k0 + kk) * C + c0 + c];
-      }
-      reg[i] = v;
-    }
-    for (int i = tid; i < KC * 343; i += NT) {
-      const int kk = i / 343, e = i % 343;
-      sop[i] = (k0 + kk < nk) ? op[(int64_t)(k0 + kk) * 343 + e] : make_double2(0.0, 0.0);
-    }
-    __syncthreads();
-    double2 acc[8];
+  const int k0 = blockIdx.y * KC;
+  const int c0 = blockIdx.z * CG;
+  // stage the source halo for frequencies k0..k0+KC-1 and columns
+  // c0..c0+CG-1 with asynchronous copies (all in flight at once; empty or
+  // out-of-domain cells are zero-filled)
+  for (int i = tid; i < RC * KC * CG; i += NT) {
+    const int r = i / (KC * CG), q = i % (KC * CG), kk = q / CG, c = q % CG;
+    const int src = s_src[r];
+    const bool ok = src >= 0 && k0 + kk < nk && c0 + c < C;
+    const double2* g = ok ? &X_l[((int64_t)(k0 + kk) * ncells + src) * C + c0 + c] : X_l;
+    cp_async16(&reg[i], g, ok ? 16 : 0);
+  }
+  for (int i = tid; i < KC * 343; i += NT) {
+    const int kk = i / 343, e = i % 343;
+    const bool ok = k0 + kk < nk;
+    cp_async16(&sop[i], ok ? &op[(int64_t)(k0 + kk) * 343 + e] : op, ok ? 16 : 0);
+  }
+  cp_async_commit();
+  cp_async_wait_all();
+  __syncthreads();
+  double2 acc[8];
 #pragma unroll
-    for (int t = 0; t < 8; ++t) acc[t] = make_double2(0.0, 0.0);
-    const double2* myop = sop + kc * 343;
-    // sx runs as a loop (keeps the unrolled body and its registers small);
-    // for each (sy, sz, t) the y/z offsets are compile-time constants, so the
-    // interaction test reduces to |ox| > 1 unless |oy| or |oz| already is > 1.
+  for (int t = 0; t < 8; ++t) acc[t] = make_double2(0.0, 0.0);
+  const double2* myop = sop + kc * 343;
+  // sx runs as a loop (keeps the unrolled body and its registers small);
+  // for each (sy, sz, t) the y/z offsets are compile-time constants, so the
+  // interaction test reduces to |ox| > 1 unless |oy| or |oz| already is > 1.
 #pragma unroll 1
-    for (int sx = 0; sx < 6; ++sx) {
-      const double2* rrow = reg + (((2 * px + sx) << 6) * KC + kc) * CG + cc;
-      const double2* orow = myop + 49 * (sx + 1);  // lex of ox + 3 = sx + 1 - tx
+  for (int sx = 0; sx < 6; ++sx) {
+    const double2* rrow = reg + (((2 * px + sx) << 6) * KC + kc) * CG + cc;
+    const double2* orow = myop + 49 * (sx + 1);  // lex of ox + 3 = sx + 1 - tx
 #pragma unroll
-      for (int sy = 0; sy < 6; ++sy)
+    for (int sy = 0; sy < 6; ++sy)
 #pragma unroll
-        for (int sz = 0; sz < 6; ++sz) {
-          const int r = ((2 * py + sy) << 3) | (2 * pz + sz);
-          const double2 xv = rrow[r * KC * CG];
+      for (int sz = 0; sz < 6; ++sz) {
+        const int r = ((2 * py + sy) << 3) | (2 * pz + sz);
+        const double2 xv = rrow[r * KC * CG];
 #pragma unroll
-          for (int t = 0; t < 8; ++t) {
-            const int tx = (t >> 2) & 1;
-            const int oy = sy - 2 - ((t >> 1) & 1);
-            const int oz = sz - 2 - (t & 1);
-            const int ox = sx - 2 - tx;
-            const bool far_yz = oy > 1 || oy < -1 || oz > 1 || oz < -1;
-            if (far_yz || ox > 1 || ox < -1) {
-              const double2 a = orow[-49 * tx + 7 * (oy + 3) + (oz + 3)];
-              acc[t].x = fma(a.x, xv.x, acc[t].x);
-              acc[t].x = fma(-a.y, xv.y, acc[t].x);
-              acc[t].y = fma(a.x, xv.y, acc[t].y);
-              acc[t].y = fma(a.y, xv.x, acc[t].y);
-            }
+        for (int t = 0; t < 8; ++t) {
+          const int tx = (t >> 2) & 1;
+          const int oy = sy - 2 - ((t >> 1) & 1);
+          const int oz = sz - 2 - (t & 1);
+          const int ox = sx - 2 - tx;
+          const bool far_yz = oy > 1 || oy < -1 || oz > 1 || oz < -1;
+          if (far_yz || ox > 1 || ox < -1) {
+            const double2 a = orow[-49 * tx + 7 * (oy + 3) + (oz + 3)];
+            acc[t].x = fma(a.x, xv.x, acc[t].x);
+            acc[t].x = fma(-a.y, xv.y, acc[t].x);
+            acc[t].y = fma(a.x, xv.y, acc[t].y);
+            acc[t].y = fma(a.y, xv.x, acc[t].y);
           }
         }
-    }
-    if (k0 + kc < nk && c0 + cc < C) {
-#pragma unroll
-      for (int t = 0; t < 8; ++t) {
-        const int x = 2 * (2 * bx + px) + ((t >> 2) & 1);
-        const int y = 2 * (2 * by + py) + ((t >> 1) & 1);
-        const int z = 2 * (2 * bz + pz) + (t & 1);
-        const uint32_t cm = morton_encode(x, y, z);
-        if (tstart[(int64_t)(cm + 1) * span] > tstart[(int64_t)cm * span])
-          Y_l[((int64_t)cm * nk + k0 + kc) * C + c0 + cc] = acc[t];
       }
+  }
+  if (k0 + kc < nk && c0 + cc < C) {
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+      const int q = ((2 * px + ((t >> 2) & 1)) << 4) | ((2 * py + ((t >> 1) & 1)) << 2) |
+                    (2 * pz + (t & 1));
+      const int cm = s_tgt[q];
+      if (cm >= 0) Y_l[((int64_t)(k0 + kc) * ncells + cm) * C + c0 + cc] = acc[t];
     }
   }
 }
 
 template <int KC, int CG>
-static int launch_mac(const double2* X, double2* Y, const double2* op, const int* sstart,
-                      const int* tstart, int span, int lev, int C, int nk, cudaStream_t st) {
+static int launch_mac(const double2* X, double2* Y, const double2* op, const int* halo,
+                      int lev, int C, int nk, cudaStream_t st) {
   const int nb = 1 << (lev - 2);
-  const int ksteps = 4;
-  const int kchunks = (nk + KC * ksteps - 1) / (KC * ksteps);
-  dim3 g((unsigned)(nb * nb * nb), (unsigned)kchunks, (unsigned)((C + CG - 1) / CG));
-  const size_t smem = sizeof(double2) * (512 * KC * CG + KC * 343);
+  dim3 g((unsigned)(nb * nb * nb), (unsigned)((nk + KC - 1) / KC), (unsigned)((C + CG - 1) / CG));
+  const size_t smem = sizeof(double2) * (512 * KC * CG + KC * 343) + sizeof(int) * 576;
   PB_CUDA(cudaFuncSetAttribute(k_m2l_unif_mac<KC, CG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                (int)smem));
-  k_m2l_unif_mac<KC, CG><<<g, 8 * KC * CG, smem, st>>>(X, Y, op, sstart, tstart, span, lev, C,
-                                                       nk, ksteps);
+  k_m2l_unif_mac<KC, CG><<<g, 8 * KC * CG, smem, st>>>(X, Y, op, halo, cells_at(lev), C, nk);
   PB_LAUNCH("m2l_unif_mac");
   return PBBFMM_OK;
 }
+
+struct FftLaunch {
+  pbbfmm_tree* t;
+  int C, CGf, CGi;
+  size_t smem_f, smem_i;
+  double invP;
+  cudaStream_t st;
+  int level = 2;
+  bool inverse = false;
+  double scale = 1.0;
+  template <int N>
+  int run() {
+    const int L = t->p.tree_level, n3 = N * N * N, nk = (2 * N - 1) * (2 * N - 1) * N;
+    Workspace& ws = t->ws;
+    const int* lists = ws.lists.as<int>();
+    const int64_t perS = (int64_t)C * n3, perX = (int64_t)nk * C;
+    const int l = level;
+    if (!inverse) {
+      PB_CUDA(cudaFuncSetAttribute(k_fft_fwd<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem_f));
+      k_fft_fwd<N><<<t->lists.nsrc[l], 128, smem_f, st>>>(
+          lists + t->lists.src_off[l], ws.S.as<double>() + level_offset(l, perS),
+          ws.proxy.as<double2>() + level_offset(l, perX), cells_at(l), C, CGf, t->d_twid);
+      PB_LAUNCH("fft_fwd");
+    } else {
+      PB_CUDA(cudaFuncSetAttribute(k_fft_inv<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)smem_i));
+      k_fft_inv<N><<<t->lists.ntgt[l], 128, smem_i, st>>>(
+          lists + t->lists.tgt_off[l], ws.pf.as<double2>() + level_offset(l, perX),
+          ws.F.as<double>() + level_offset(l, perS), cells_at(l), C, CGi, t->d_twid, invP,
+          scale);
+      PB_LAUNCH("fft_inv");
+    }
+    return PBBFMM_OK;
+  }
+};
 
 int run_m2l_unif(pbbfmm_tree* t, int C, cudaStream_t st) {
   const int L = t->p.tree_level, n = t->n, m = t->m, n3 = t->n3, nk = t->nk;
@@ -321,50 +378,54 @@ int run_m2l_unif(pbbfmm_tree* t, int C, cudaStream_t st) {
   const double invP = 1.0 / (double)(m * m * m);
   // forward transforms of all nonempty source cells, levels 2..L
   const int fwd_col = n3 * 8 + n3 * 16 + n * m * n * 16;
-  const int CGf = max(1, min(C, 45000 / fwd_col));
+  const int CGf = max(1, min(C, 60000 / fwd_col));
   const size_t smem_f = sizeof(double) * (2 * m + ((CGf * n3 + 1) & ~1)) +
                         sizeof(double2) * (CGf * n3 + CGf * n * m * n);
   const int inv_col = nk * 16 + n * m * n * 16 + n3 * 16;
-  const int CGi = max(1, min(C, 45000 / inv_col));
+  const int CGi = max(1, min(C, 60000 / inv_col));
   const size_t smem_i =
       sizeof(double) * (2 * m) + sizeof(double2) * (CGi * nk + CGi * n * m * n + CGi * n3);
-  PB_CUDA(cudaFuncSetAttribute(k_fft_fwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_f));
-  PB_CUDA(cudaFuncSetAttribute(k_fft_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_i));
+  FftLaunch fl{t, C, CGf, CGi, smem_f, smem_i, invP, st};
   for (int l = 2; l <= L; ++l) {
     if (t->lists.nsrc[l] == 0) continue;
-    k_fft_fwd<<<t->lists.nsrc[l], 128, smem_f, st>>>(lists + t->lists.src_off[l],
-                                                     S + level_offset(l, perS),
-                                                     X + level_offset(l, perX), C, CGf, n, m,
-                                                     t->d_twid);
-    PB_LAUNCH("fft_fwd");
+    if (int rc_ = kt_begin(t, KS_FFT_FWD, st)) return rc_;
+    fl.level = l;
+    fl.inverse = false;
+    if (int rc_ = dispatch_order(n, fl)) return rc_;
+    if (int rc_ = kt_end(t, st)) return rc_;
   }
+  int* halo = ws.halo.as<int>();
   for (int l = 2; l <= L; ++l) {
     if (t->lists.ntgt[l] == 0) continue;
     const int lvl = t->homog ? 0 : l - 2;
     const double2* op = (const double2*)t->d_op + (int64_t)lvl * nk * 343;
     const int span = (int)cells_at(L - l);
+    const int nblk = 1 << (3 * (l - 2));
     int rc;
+    if ((rc = kt_begin(t, KS_MAC, st))) return rc;
+    k_halo_tables<<<nblk, 256, 0, st>>>(sstart, tstart, span, l, halo);
+    PB_LAUNCH("halo_tables");
+    const double2* Xl = X + level_offset(l, perX);
+    double2* Yl = Y + level_offset(l, perX);
     if (C >= 8)
-      rc = launch_mac<1, 8>(X + level_offset(l, perX), Y + level_offset(l, perX), op, sstart,
-                            tstart, span, l, C, nk, st);
+      rc = launch_mac<1, 8>(Xl, Yl, op, halo, l, C, nk, st);
     else if (C >= 4)
-      rc = launch_mac<2, 4>(X + level_offset(l, perX), Y + level_offset(l, perX), op, sstart,
-                            tstart, span, l, C, nk, st);
+      rc = launch_mac<2, 4>(Xl, Yl, op, halo, l, C, nk, st);
     else if (C >= 2)
-      rc = launch_mac<4, 2>(X + level_offset(l, perX), Y + level_offset(l, perX), op, sstart,
-                            tstart, span, l, C, nk, st);
+      rc = launch_mac<4, 2>(Xl, Yl, op, halo, l, C, nk, st);
     else
-      rc = launch_mac<8, 1>(X + level_offset(l, perX), Y + level_offset(l, perX), op, sstart,
-                            tstart, span, l, C, nk, st);
+      rc = launch_mac<8, 1>(Xl, Yl, op, halo, l, C, nk, st);
     if (rc) return rc;
+    if ((rc = kt_end(t, st))) return rc;
     double len = t->p.L;
     for (int i = 0; i < l; ++i) len = 0.5 * len;
     const double scale = pow(1.0 / len, t->homogen_neg);
-    k_fft_inv<<<t->lists.ntgt[l], 128, smem_i, st>>>(lists + t->lists.tgt_off[l],
-                                                     Y + level_offset(l, perX),
-                                                     F + level_offset(l, perS), C, CGi, n, m,
-                                                     t->d_twid, invP, scale);
-    PB_LAUNCH("fft_inv");
+    if (int rc_ = kt_begin(t, KS_FFT_INV, st)) return rc_;
+    fl.level = l;
+    fl.inverse = true;
+    fl.scale = scale;
+    if (int rc_ = dispatch_order(n, fl)) return rc_;
+    if (int rc_ = kt_end(t, st)) return rc_;
   }
   return PBBFMM_OK;
 }

@@ -214,7 +214,7 @@ int run_binning(pbbfmm_tree* t, const double* d_tgt, int64_t Nf, const double* d
   // recentre on the target bounding box
   k_bbox_partial<<<kBBoxBlocks, kBBoxThreads, 0, st>>>(d_tgt, Nf, ws.bbox_part.as<double>());
   k_bbox_final<<<1, 32, 0, st>>>(ws.bbox_part.as<double>(), kBBoxBlocks, ctr);
-  PB_LAUNCH("bbox");
+  PB_LAUNCH_N("bbox", 2);
 
   auto bin_set = [&](const double* pts, int64_t N, int* perm, int* start) -> int {
     if (N > 0) {
@@ -223,6 +223,8 @@ int run_binning(pbbfmm_tree* t, const double* d_tgt, int64_t Nf, const double* d
       size_t bytes = ws.cub_temp.cap;
       PB_CUDA(cub::DeviceRadixSort::SortPairs(ws.cub_temp.p, bytes, key, key_sorted, idx, perm,
                                               (int)N, 0, 3 * L, st));
+      // onesweep: one histogram pass plus one pass per 8-bit digit
+      count_launches(1 + (3 * L + 7) / 8);
     }
     k_leaf_start<<<(unsigned)((nleaf + 1 + 255) / 256), 256, 0, st>>>(key_sorted, (int)N, nleaf,
                                                                       start);
@@ -242,7 +244,7 @@ int run_binning(pbbfmm_tree* t, const double* d_tgt, int64_t Nf, const double* d
     int64_t tot = Ns * (int64_t)C;
     k_gather_w<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(d_w, ws.sperm.as<int>(), (int)Ns, C,
                                                               ws.wsorted.as<double>());
-    PB_LAUNCH("gather_src");
+    PB_LAUNCH_N("gather_src", 2);
   }
 
   // nonempty-cell lists for levels 2..L
@@ -269,6 +271,7 @@ int run_binning(pbbfmm_tree* t, const double* d_tgt, int64_t Nf, const double* d
     auto tit = thrust::make_transform_iterator(it, TypedCell{(int)(nc / 8)});
     PB_CUDA(cub::DeviceSelect::If(ws.cub_temp.p, bytes, tit, lists + off, cnt + 12 * l + 2,
                                   (int)nc, NonEmpty{ws.tstart.as<int>(), shift}, st));
+    count_launches(3 * 2);  // three DeviceSelect calls: init + scan kernels each
     k_type_bounds<<<1, 32, 0, st>>>(lists + off, cnt + 12 * l + 2, cnt + 12 * l + 3);
     PB_LAUNCH("type_bounds");
     off += (nc < Nf ? nc : Nf);

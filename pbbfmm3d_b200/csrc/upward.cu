@@ -170,18 +170,22 @@ int run_upward(pbbfmm_tree* t, int C, cudaStream_t st) {
   const int64_t per = (int64_t)C * n3;
   if (t->lists.nsrc[L] > 0) {
     size_t smem = sizeof(double) * (n * n + 3 * n * kP2MChunk + kP2MChunk * C);
+    if (int rc_ = kt_begin(t, KS_P2M, st)) return rc_;
     k_p2m<<<t->lists.nsrc[L], kP2MThreads, smem, st>>>(
         lists + t->lists.src_off[L], sstart, ws.spos.as<double>(), (int)t->last_Ns,
         ws.wsorted.as<double>(), C, n, t->p.use_chebyshev, t->d_Tkz, t->p.L, L,
         S + level_offset(L, per));
     PB_LAUNCH("p2m");
+    if (int rc_ = kt_end(t, st)) return rc_;
   }
   for (int l = L - 1; l >= 2; --l) {
     if (t->lists.nsrc[l] == 0) continue;
+    if (int rc_ = kt_begin(t, KS_M2M, st)) return rc_;
     k_m2m<<<t->lists.nsrc[l], kM2MThreads, 0, st>>>(
         lists + t->lists.src_off[l], sstart, (int)cells_at(L - l - 1), S + level_offset(l + 1, per),
         S + level_offset(l, per), C, n, t->d_Cw);
     PB_LAUNCH("m2m");
+    if (int rc_ = kt_end(t, st)) return rc_;
   }
   return PBBFMM_OK;
 }
