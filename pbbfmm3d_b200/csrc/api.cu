@@ -253,6 +253,7 @@ static int compute_chunk(pbbfmm_tree* t, const double* d_tgt, int64_t Nf, const 
   } else {
     if ((rc = grow(ws.proxy, 2 * sizeof(double) * level_total(L, (int64_t)C * t->nk)))) return rc;
     if ((rc = grow(ws.pf, 2 * sizeof(double) * level_total(L, (int64_t)C * t->nk)))) return rc;
+    // halo tables: at most 8^(L-2) parent blocks x (region + target) entries
     if ((rc = grow(ws.halo, sizeof(int) * 576 * cells_at(L - 2)))) return rc;
   }
   (void)precision;

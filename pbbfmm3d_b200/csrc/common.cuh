@@ -156,6 +156,11 @@ __device__ __forceinline__ void cp_async16(void* smem_dst, const void* src, int 
                "r"(src_bytes)
                : "memory");
 }
+// 8-byte variant (through L1), for arrays without 16-byte alignment.
+__device__ __forceinline__ void cp_async8(void* smem_dst, const void* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() {
   asm volatile("cp.async.commit_group;\n" ::: "memory");
 }

@@ -28,57 +28,99 @@ __device__ __forceinline__ void cell_center_d(uint32_t m, int l, double box, dou
   c[2] = cz;
 }
 
-constexpr int kL2LThreads = 128;
-constexpr int kL2LGroup = 1024;
+// L2L, one warp per nonempty target parent and column: the parent's local
+// coefficients are staged once and pushed through the x, y and z passes for
+// each nonempty child, which is updated in place (F_child += ...).
+template <int N>
+struct L2LCfg {
+  static constexpr int n3 = N * N * N;
+  static constexpr int per_warp = 3 * n3;  // parent + two pass buffers (doubles)
+  static constexpr int warps = 8;
+};
 
-// One CTA per nonempty target cell at level l: F_child += L2L(F_parent).
-__global__ void __launch_bounds__(kL2LThreads)
-    k_l2l(const int* __restrict__ cells, const double* __restrict__ Fpar,
-          double* __restrict__ Fch, int C, int n, const double* __restrict__ Cw_g) {
-  __shared__ double sCw[2 * kMaxOrder * kMaxOrder];
-  __shared__ double b0[kL2LGroup], b1[kL2LGroup];
-  const int n2 = n * n, n3 = n2 * n;
+template <int N>
+__global__ void __launch_bounds__(32 * L2LCfg<N>::warps)
+    k_l2l(const int* __restrict__ parents, int npar, const int* __restrict__ tstart,
+          int span_child, const double* __restrict__ Fpar, double* __restrict__ Fch, int C,
+          const double* __restrict__ Cw_g) {
+  using G = L2LCfg<N>;
+  constexpr int n2 = N * N, n3 = G::n3;
+  extern __shared__ double smd[];
+  __shared__ double sCw[2 * N * N];
   for (int i = threadIdx.x; i < 2 * n2; i += blockDim.x) sCw[i] = Cw_g[i];
-  const int cell = cells[blockIdx.x];
-  const int par = cell >> 3, ch = cell & 7;
-  const double* wx = sCw + (((ch >> 2) & 1) ? n2 : 0);
-  const double* wy = sCw + (((ch >> 1) & 1) ? n2 : 0);
-  const double* wz = sCw + ((ch & 1) ? n2 : 0);
-  const int CG = max(1, min(C, kL2LGroup / n3));
-  for (int c0 = 0; c0 < C; c0 += CG) {
-    const int cg = min(CG, C - c0), tot = cg * n3;
-    __syncthreads();
-    for (int i = threadIdx.x; i < tot; i += blockDim.x)
-      b0[i] = Fpar[((int64_t)par * C + c0) * n3 + i];
-    __syncthreads();
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+  const int task = blockIdx.x * G::warps + wl;
+  if (task >= npar * C) return;
+  const int par = parents[task / C], col = task % C;
+  double* sp = smd + wl * G::per_warp;
+  double* b0 = sp + n3;
+  double* b1 = b0 + n3;
+  const double* src = Fpar + ((int64_t)par * C + col) * n3;
+  for (int i = lane; i < n3; i += 32) cp_async8(&sp[i], &src[i]);
+  cp_async_commit();
+  cp_async_wait_all();
+  __syncwarp();
+  for (int ch = 0; ch < 8; ++ch) {
+    const int cell = par * 8 + ch;
+    const int64_t a = (int64_t)cell * span_child, b = (int64_t)(cell + 1) * span_child;
+    if (tstart[b] == tstart[a]) continue;  // child without targets
+    const double* wx = sCw + (((ch >> 2) & 1) ? n2 : 0);
+    const double* wy = sCw + (((ch >> 1) & 1) ? n2 : 0);
+    const double* wz = sCw + ((ch & 1) ? n2 : 0);
     // x: Fx[l1 n2 + l2 n + l3] = sum_k F[k n2 + l2 n + l3] wx[l1 + k n]
-    for (int i = threadIdx.x; i < tot; i += blockDim.x) {
-      const int cc = i / n3, r = i % n3, l1 = r / n2, rem = r % n2;
-      const double* s = b0 + cc * n3 + rem;
+    for (int i = lane; i < n3; i += 32) {
+      const int l1 = i / n2, rem = i % n2;
       double v = 0;
-      for (int k = 0; k < n; ++k) v += s[k * n2] * wx[l1 + k * n];
-      b1[i] = v;
-    }
-    __syncthreads();
-    // y: Fy[l1 n2 + l2 n + l3] = sum_k Fx[l1 n2 + k n + l3] wy[l2 + k n]
-    for (int i = threadIdx.x; i < tot; i += blockDim.x) {
-      const int cc = i / n3, r = i % n3, l1 = r / n2, l2 = (r / n) % n, l3 = r % n;
-      const double* s = b1 + cc * n3 + l1 * n2 + l3;
-      double v = 0;
-      for (int k = 0; k < n; ++k) v += s[k * n] * wy[l2 + k * n];
+#pragma unroll
+      for (int k = 0; k < N; ++k) v += sp[k * n2 + rem] * wx[l1 + k * N];
       b0[i] = v;
     }
-    __syncthreads();
-    // z: Fchild[l1 n + l3] += sum_k Fy[l1 n + k] wz[l3 + k n]   (l1 over n^2)
-    for (int i = threadIdx.x; i < tot; i += blockDim.x) {
-      const int cc = i / n3, r = i % n3, l1 = r / n, l3 = r % n;
-      const double* s = b0 + cc * n3 + l1 * n;
+    __syncwarp();
+    // y: Fy[l1 n2 + l2 n + l3] = sum_k Fx[l1 n2 + k n + l3] wy[l2 + k n]
+    for (int i = lane; i < n3; i += 32) {
+      const int l1 = i / n2, l2 = (i / N) % N, l3 = i % N;
       double v = 0;
-      for (int k = 0; k < n; ++k) v += s[k] * wz[l3 + k * n];
-      Fch[((int64_t)cell * C + c0) * n3 + i] += v;
+#pragma unroll
+      for (int k = 0; k < N; ++k) v += b0[l1 * n2 + k * N + l3] * wy[l2 + k * N];
+      b1[i] = v;
     }
+    __syncwarp();
+    // z: Fchild[l1 n + l3] += sum_k Fy[l1 n + k] wz[l3 + k n]   (l1 over n^2)
+    double* dst = Fch + ((int64_t)cell * C + col) * n3;
+    for (int i = lane; i < n3; i += 32) {
+      const int l1 = i / N, l3 = i % N;
+      double v = 0;
+#pragma unroll
+      for (int k = 0; k < N; ++k) v += b1[l1 * N + k] * wz[l3 + k * N];
+      dst[i] += v;
+    }
+    __syncwarp();
   }
 }
+
+struct L2LLaunch {
+  pbbfmm_tree* t;
+  int C, l;  // child level
+  cudaStream_t st;
+  template <int N>
+  int run() {
+    using G = L2LCfg<N>;
+    const int L = t->p.tree_level;
+    Workspace& ws = t->ws;
+    const int64_t per = (int64_t)C * G::n3;
+    const int np = t->lists.ntgt[l - 1];
+    const int64_t tasks = (int64_t)np * C;
+    const size_t smem = sizeof(double) * G::per_warp * G::warps;
+    PB_CUDA(cudaFuncSetAttribute(k_l2l<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_l2l<N><<<(unsigned)((tasks + G::warps - 1) / G::warps), 32 * G::warps, smem, st>>>(
+        ws.lists.as<int>() + t->lists.tgt_off[l - 1], np, ws.tstart.as<int>(),
+        (int)cells_at(L - l), ws.F.as<double>() + level_offset(l - 1, per),
+        ws.F.as<double>() + level_offset(l, per), C, t->d_Cw);
+    PB_LAUNCH("l2l");
+    return PBBFMM_OK;
+  }
+};
 
 // Leaf phase: one warp per nonempty target leaf, lanes over the sources of
 // the 27 neighbour leaves (and over the n^3 local coefficients for L2P);
@@ -227,18 +269,13 @@ struct LeafLaunch {
 };
 
 int run_downward(pbbfmm_tree* t, int C, cudaStream_t st) {
-  const int L = t->p.tree_level, n3 = t->n3;
-  Workspace& ws = t->ws;
-  const int* lists = ws.lists.as<int>();
-  double* F = ws.F.as<double>();
-  const int64_t per = (int64_t)C * n3;
+  const int L = t->p.tree_level;
+  // level-2 locals have no parent contribution (levels 0 and 1 carry none)
   for (int l = 3; l <= L; ++l) {
-    if (t->lists.ntgt[l] == 0) continue;
+    if (t->lists.ntgt[l - 1] == 0) continue;
     if (int rc_ = kt_begin(t, KS_L2L, st)) return rc_;
-    k_l2l<<<t->lists.ntgt[l], kL2LThreads, 0, st>>>(lists + t->lists.tgt_off[l],
-                                                     F + level_offset(l - 1, per),
-                                                     F + level_offset(l, per), C, t->n, t->d_Cw);
-    PB_LAUNCH("l2l");
+    L2LLaunch ll{t, C, l, st};
+    if (int rc_ = dispatch_order(t->n, ll)) return rc_;
     if (int rc_ = kt_end(t, st)) return rc_;
   }
   return PBBFMM_OK;

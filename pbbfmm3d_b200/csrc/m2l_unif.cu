@@ -47,7 +47,9 @@ __global__ void k_fft_fwd(const int* __restrict__ cells, const double* __restric
     const int cg = min(CG, C - c0);
     __syncthreads();
     for (int i = threadIdx.x; i < cg * n3; i += blockDim.x)
-      sin_[i] = S_l[((int64_t)cell * C + c0) * n3 + i];
+      cp_async8(&sin_[i], &S_l[((int64_t)cell * C + c0) * n3 + i]);
+    cp_async_commit();
+    cp_async_wait_all();
     __syncthreads();
     // z: Z[c][l1][l2][k3] = sum_l3 S[c][l1][l2][l3] w^(k3 l3),  w = e^{-2 pi i / m}
     for (int i = threadIdx.x; i < cg * n3; i += blockDim.x) {
@@ -128,8 +130,10 @@ __global__ void k_fft_inv(const int* __restrict__ cells, const double2* __restri
     __syncthreads();
     for (int i = threadIdx.x; i < cg * nk; i += blockDim.x) {
       const int k = i / cg, cc = i % cg;
-      Yh[cc * nk + k] = Y_l[((int64_t)k * ncells + cell) * C + c0 + cc];
+      cp_async16(&Yh[cc * nk + k], &Y_l[((int64_t)k * ncells + cell) * C + c0 + cc], 16);
     }
+    cp_async_commit();
+    cp_async_wait_all();
     __syncthreads();
     // x: G[c][a1][k2][k3] = sum_k1 Yh[c][k1][k2][k3] e^{+2 pi i k1 t1 / m}
     constexpr int ng = n * m * n;
@@ -191,60 +195,77 @@ __global__ void k_fft_inv(const int* __restrict__ cells, const double2* __restri
 }
 
 // ----------------------------------------------------------------- MAC
-// One CTA per (block of 2x2x2 parents = 4x4x4 targets, frequency chunk),
-// the frequency chunk varying slowest in the grid so that resident CTAs work
-// on the same frequency plane (one plane of level 6 is 33.5 MB and stays in
-// L2 while its ~8x halo reuse is served).  Threads = (parent, kc, col); each
-// thread accumulates the 8 children of its parent for one frequency and one
-// column, sweeping the 6x6x6 children of the parent's neighbours staged in
-// shared memory for the whole block (8x8x8 cells).  The (child, source)
-// interaction pattern and operator index are compile-time constants.
+// One CTA per (block of PBX x 2 x 2 parents = 2PBX x 4 x 4 targets,
+// frequency chunk), the frequency chunk varying slowest in the grid so that
+// resident CTAs work on the same frequency plane (one plane of level 6 is
+// 33.5 MB and stays in L2 while its halo reuse is served).  Threads =
+// (parent, kc, col); each thread accumulates the 8 children of its parent for
+// one frequency and one column, sweeping the 6x6x6 children of the parent's
+// neighbours, staged in shared memory for the whole block ((2PBX+4) x 8 x 8
+// cells).  The (child, source) interaction pattern and the operator index are
+// compile-time constants; each complex accumulator is split over four
+// independent FMA chains.
 //
-// Per level, halo[b*576 + r] (r < 512) holds the source cell of region slot r
-// of parent block b (or -1: outside the domain or no sources) and
-// halo[b*576 + 512 + q] the target cell of block slot q (or -1).
+// Per level, halo[b*stride + r] holds the source cell of region slot r of
+// parent block b (or -1: outside the domain or no sources), followed by the
+// target cell of each block slot (or -1).
 
+template <int PBX>
+struct MacGeom {
+  static constexpr int RX = 2 * PBX + 4;       // region extent in x (y, z: 8)
+  static constexpr int RC = RX * 64;           // region cells
+  static constexpr int TC = 2 * PBX * 16;      // target cells of a block
+  static constexpr int STRIDE = RC + TC;       // halo table entries per block
+  static constexpr int NPAR = PBX * 4;         // parents per block
+};
+
+template <int PBX>
 __global__ void k_halo_tables(const int* __restrict__ sstart, const int* __restrict__ tstart,
                               int span, int lev, int* __restrict__ halo) {
-  const int nb = 1 << (lev - 2);
+  using G = MacGeom<PBX>;
+  const int nby = 1 << (lev - 2), nbx = (1 << (lev - 1)) / PBX;  // blocks per dim
   const int b = blockIdx.x;
-  const int bx = b / (nb * nb), by = (b / nb) % nb, bz = b % nb;
+  const int bx = b / (nby * nby), by = (b / nby) % nby, bz = b % nby;
   const int nside = 1 << lev;
-  for (int r = threadIdx.x; r < 576; r += blockDim.x) {
+  for (int r = threadIdx.x; r < G::STRIDE; r += blockDim.x) {
     int v = -1;
-    if (r < 512) {
-      const int x = 4 * bx - 2 + (r >> 6), y = 4 * by - 2 + ((r >> 3) & 7), z = 4 * bz - 2 + (r & 7);
+    if (r < G::RC) {
+      const int x = 2 * PBX * bx - 2 + (r >> 6), y = 4 * by - 2 + ((r >> 3) & 7),
+                z = 4 * bz - 2 + (r & 7);
       if (x >= 0 && y >= 0 && z >= 0 && x < nside && y < nside && z < nside) {
         const uint32_t cm = morton_encode(x, y, z);
         if (sstart[(int64_t)(cm + 1) * span] > sstart[(int64_t)cm * span]) v = (int)cm;
       }
     } else {
-      const int q = r - 512;
-      const uint32_t cm = morton_encode(4 * bx + (q >> 4), 4 * by + ((q >> 2) & 3), 4 * bz + (q & 3));
+      const int q = r - G::RC;
+      const uint32_t cm =
+          morton_encode(2 * PBX * bx + (q >> 4), 4 * by + ((q >> 2) & 3), 4 * bz + (q & 3));
       if (tstart[(int64_t)(cm + 1) * span] > tstart[(int64_t)cm * span]) v = (int)cm;
     }
-    halo[(int64_t)b * 576 + r] = v;
+    halo[(int64_t)b * G::STRIDE + r] = v;
   }
+  (void)nbx;
 }
 
-template <int KC, int CG>
-__global__ void __launch_bounds__(8 * KC * CG)
+template <int PBX, int KC, int CG>
+__global__ void __launch_bounds__(4 * PBX * KC * CG)
     k_m2l_unif_mac(const double2* __restrict__ X_l, double2* __restrict__ Y_l,
                    const double2* __restrict__ op,  // nk x 343 for this level
                    const int* __restrict__ halo, int64_t ncells, int C, int nk) {
-  constexpr int NT = 8 * KC * CG;
-  constexpr int RC = 512;  // region cells (8 x 8 x 8)
+  using G = MacGeom<PBX>;
+  constexpr int NT = G::NPAR * KC * CG;
+  constexpr int RC = G::RC;
   extern __shared__ double2 smc[];
   double2* reg = smc;                   // RC x KC x CG
   double2* sop = reg + RC * KC * CG;    // KC x 343
-  int* s_src = (int*)(sop + KC * 343);  // RC source cells, then 64 target cells
+  int* s_src = (int*)(sop + KC * 343);  // RC source cells, then TC target cells
   int* s_tgt = s_src + RC;
   const int tid = threadIdx.x;
   const int cc = tid % CG, kc = (tid / CG) % KC, p = tid / (CG * KC);
-  const int px = (p >> 2) & 1, py = (p >> 1) & 1, pz = p & 1;
-  const int* hb = halo + (int64_t)blockIdx.x * 576;
+  const int px = p >> 2, py = (p >> 1) & 1, pz = p & 1;
+  const int* hb = halo + (int64_t)blockIdx.x * G::STRIDE;
   int mine = 0;
-  for (int r = tid; r < 576; r += NT) {
+  for (int r = tid; r < G::STRIDE; r += NT) {
     const int v = hb[r];
     s_src[r] = v;
     if (r >= RC) mine |= v >= 0;
@@ -270,9 +291,9 @@ __global__ void __launch_bounds__(8 * KC * CG)
   cp_async_commit();
   cp_async_wait_all();
   __syncthreads();
-  double2 acc[8];
+  double ar[8], br[8], ai[8], bi[8];  // re = ar + br, im = ai + bi
 #pragma unroll
-  for (int t = 0; t < 8; ++t) acc[t] = make_double2(0.0, 0.0);
+  for (int t = 0; t < 8; ++t) ar[t] = br[t] = ai[t] = bi[t] = 0.0;
   const double2* myop = sop + kc * 343;
   // sx runs as a loop (keeps the unrolled body and its registers small);
   // for each (sy, sz, t) the y/z offsets are compile-time constants, so the
@@ -296,10 +317,10 @@ __global__ void __launch_bounds__(8 * KC * CG)
           const bool far_yz = oy > 1 || oy < -1 || oz > 1 || oz < -1;
           if (far_yz || ox > 1 || ox < -1) {
             const double2 a = orow[-49 * tx + 7 * (oy + 3) + (oz + 3)];
-            acc[t].x = fma(a.x, xv.x, acc[t].x);
-            acc[t].x = fma(-a.y, xv.y, acc[t].x);
-            acc[t].y = fma(a.x, xv.y, acc[t].y);
-            acc[t].y = fma(a.y, xv.x, acc[t].y);
+            ar[t] = fma(a.x, xv.x, ar[t]);
+            br[t] = fma(-a.y, xv.y, br[t]);
+            ai[t] = fma(a.x, xv.y, ai[t]);
+            bi[t] = fma(a.y, xv.x, bi[t]);
           }
         }
       }
@@ -310,22 +331,40 @@ __global__ void __launch_bounds__(8 * KC * CG)
       const int q = ((2 * px + ((t >> 2) & 1)) << 4) | ((2 * py + ((t >> 1) & 1)) << 2) |
                     (2 * pz + (t & 1));
       const int cm = s_tgt[q];
-      if (cm >= 0) Y_l[((int64_t)(k0 + kc) * ncells + cm) * C + c0 + cc] = acc[t];
+      if (cm >= 0)
+        Y_l[((int64_t)(k0 + kc) * ncells + cm) * C + c0 + cc] =
+            make_double2(ar[t] + br[t], ai[t] + bi[t]);
     }
   }
 }
 
-template <int KC, int CG>
-static int launch_mac(const double2* X, double2* Y, const double2* op, const int* halo,
-                      int lev, int C, int nk, cudaStream_t st) {
-  const int nb = 1 << (lev - 2);
-  dim3 g((unsigned)(nb * nb * nb), (unsigned)((nk + KC - 1) / KC), (unsigned)((C + CG - 1) / CG));
-  const size_t smem = sizeof(double2) * (512 * KC * CG + KC * 343) + sizeof(int) * 576;
-  PB_CUDA(cudaFuncSetAttribute(k_m2l_unif_mac<KC, CG>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                               (int)smem));
-  k_m2l_unif_mac<KC, CG><<<g, 8 * KC * CG, smem, st>>>(X, Y, op, halo, cells_at(lev), C, nk);
+template <int PBX, int KC, int CG>
+static int launch_mac(const double2* X, double2* Y, const double2* op, int* halo,
+                      const int* sstart, const int* tstart, int span, int lev, int C, int nk,
+                      cudaStream_t st) {
+  using G = MacGeom<PBX>;
+  const int nby = 1 << (lev - 2), nbx = (1 << (lev - 1)) / PBX;
+  const int nblk = nbx * nby * nby;
+  k_halo_tables<PBX><<<nblk, 256, 0, st>>>(sstart, tstart, span, lev, halo);
+  PB_LAUNCH("halo_tables");
+  dim3 g((unsigned)nblk, (unsigned)((nk + KC - 1) / KC), (unsigned)((C + CG - 1) / CG));
+  const size_t smem = sizeof(double2) * (G::RC * KC * CG + KC * 343) + sizeof(int) * G::STRIDE;
+  PB_CUDA(cudaFuncSetAttribute(k_m2l_unif_mac<PBX, KC, CG>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k_m2l_unif_mac<PBX, KC, CG><<<g, G::NPAR * KC * CG, smem, st>>>(X, Y, op, halo, cells_at(lev),
+                                                                  C, nk);
   PB_LAUNCH("m2l_unif_mac");
   return PBBFMM_OK;
+}
+
+template <int PBX>
+static int launch_mac_cols(const double2* X, double2* Y, const double2* op, int* halo,
+                           const int* sstart, const int* tstart, int span, int lev, int C, int nk,
+                           cudaStream_t st) {
+  if (C >= 8) return launch_mac<PBX, 1, 8>(X, Y, op, halo, sstart, tstart, span, lev, C, nk, st);
+  if (C >= 4) return launch_mac<PBX, 2, 4>(X, Y, op, halo, sstart, tstart, span, lev, C, nk, st);
+  if (C >= 2) return launch_mac<PBX, 4, 2>(X, Y, op, halo, sstart, tstart, span, lev, C, nk, st);
+  return launch_mac<PBX, 8, 1>(X, Y, op, halo, sstart, tstart, span, lev, C, nk, st);
 }
 
 struct FftLaunch {
@@ -400,21 +439,15 @@ int run_m2l_unif(pbbfmm_tree* t, int C, cudaStream_t st) {
     const int lvl = t->homog ? 0 : l - 2;
     const double2* op = (const double2*)t->d_op + (int64_t)lvl * nk * 343;
     const int span = (int)cells_at(L - l);
-    const int nblk = 1 << (3 * (l - 2));
     int rc;
     if ((rc = kt_begin(t, KS_MAC, st))) return rc;
-    k_halo_tables<<<nblk, 256, 0, st>>>(sstart, tstart, span, l, halo);
-    PB_LAUNCH("halo_tables");
     const double2* Xl = X + level_offset(l, perX);
     double2* Yl = Y + level_offset(l, perX);
-    if (C >= 8)
-      rc = launch_mac<1, 8>(Xl, Yl, op, halo, l, C, nk, st);
-    else if (C >= 4)
-      rc = launch_mac<2, 4>(Xl, Yl, op, halo, l, C, nk, st);
-    else if (C >= 2)
-      rc = launch_mac<4, 2>(Xl, Yl, op, halo, l, C, nk, st);
+    // 4x2x2 parent blocks from level 3 up (level 2 has 2 parents per side)
+    if (l >= 3)
+      rc = launch_mac_cols<4>(Xl, Yl, op, halo, sstart, tstart, span, l, C, nk, st);
     else
-      rc = launch_mac<8, 1>(Xl, Yl, op, halo, l, C, nk, st);
+      rc = launch_mac_cols<2>(Xl, Yl, op, halo, sstart, tstart, span, l, C, nk, st);
     if (rc) return rc;
     if ((rc = kt_end(t, st))) return rc;
     double len = t->p.L;

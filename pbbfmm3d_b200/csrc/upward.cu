@@ -30,161 +30,215 @@ __device__ __forceinline__ void cell_center(uint32_t m, int l, double box, doubl
   c[2] = cz;
 }
 
-constexpr int kP2MThreads = 256;
-constexpr int kP2MChunk = 32;
-constexpr int kMaxOut = 4;  // outputs per thread per column group (<= 1024 / 256)
+constexpr int kP2MChunk = 32;  // points per pass (one per lane)
+constexpr int kP2MCols = 8;    // columns per pass
+// warps per CTA: static shared memory (basis + weights) stays under 48 KB
+template <int N>
+constexpr int p2m_warps() {
+  return (3 * N * kP2MChunk + kP2MChunk * kP2MCols) * 8 * 8 <= 40 * 1024 ? 8 : 4;
+}
 
-// One CTA per nonempty source leaf.
-__global__ void __launch_bounds__(kP2MThreads)
-    k_p2m(const int* __restrict__ leaves, const int* __restrict__ sstart,
+// One warp per nonempty source leaf.  Lanes first evaluate the basis of up to
+// 32 points (one point each) and stage their weights, then each lane owns
+// outputs o = lane + 32 r of the (column, l1, l2, l3) block and sums over the
+// staged points in point order.  Leaves with more than 32 points accumulate
+// chunk by chunk in the output array (each output has a single owner lane).
+template <int N, int kP2MWarps = p2m_warps<N>()>
+__global__ void __launch_bounds__(32 * kP2MWarps)
+    k_p2m(const int* __restrict__ leaves, int nleaves, const int* __restrict__ sstart,
           const double* __restrict__ spos, int Ns, const double* __restrict__ wsorted, int C,
-          int n, int cheb, const double* __restrict__ Tkz_g, double box, int L,
+          int cheb, const double* __restrict__ Tkz_g, double box, int L,
           double* __restrict__ S_L) {
-  extern __shared__ double sm[];
-  double* sTkz = sm;                               // n*n
-  double* sB = sTkz + n * n;                       // 3 x n x chunk basis values
-  double* sW = sB + 3 * n * kP2MChunk;             // chunk x C weights
-  const int leaf = leaves[blockIdx.x];
+  constexpr int n3 = N * N * N;
+  __shared__ double sTkz[N * N];
+  __shared__ double sB[kP2MWarps][3][N][kP2MChunk];
+  __shared__ double sW[kP2MWarps][kP2MChunk][kP2MCols];
+  for (int i = threadIdx.x; i < N * N; i += blockDim.x) sTkz[i] = Tkz_g[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+  const int wid = blockIdx.x * kP2MWarps + wl;
+  if (wid >= nleaves) return;
+  const int leaf = leaves[wid];
   const int a = sstart[leaf], e = sstart[leaf + 1];
-  const int n3 = n * n * n;
-  for (int i = threadIdx.x; i < n * n; i += blockDim.x) sTkz[i] = Tkz_g[i];
   double c[3];
   cell_center((uint32_t)leaf, L, box, c);
   double len = box;
   for (int i = 0; i < L; ++i) len = 0.5 * len;
   const double ihalfL = 2. / len;
-  const int CG = max(1, min(C, (kP2MThreads * kMaxOut) / n3));
-  for (int c0 = 0; c0 < C; c0 += CG) {
-    const int cg = min(CG, C - c0);
-    double acc[kMaxOut];
-#pragma unroll
-    for (int r = 0; r < kMaxOut; ++r) acc[r] = 0;
+  for (int c0 = 0; c0 < C; c0 += kP2MCols) {
+    const int cg = min(kP2MCols, C - c0);
+    double* Sout = S_L + ((int64_t)leaf * C + c0) * n3;
     for (int p0 = a; p0 < e; p0 += kP2MChunk) {
       const int cnt = min(kP2MChunk, e - p0);
-      __syncthreads();
-      if (threadIdx.x < 3 * cnt) {
-        const int j = threadIdx.x % cnt, d = threadIdx.x / cnt;
-        const double q = ihalfL * (spos[(int64_t)d * Ns + p0 + j] - c[d]);
-        basis_all<double>(n, cheb, q, sTkz, sB + (d * n) * kP2MChunk + j, kP2MChunk);
-      }
-      for (int i = threadIdx.x; i < cnt * cg; i += blockDim.x) {
-        const int j = i / cg, cc = i % cg;
-        sW[j * CG + cc] = wsorted[(int64_t)(p0 + j) * C + c0 + cc];
-      }
-      __syncthreads();
+      __syncwarp();
+      if (lane < cnt) {
 #pragma unroll
-      for (int r = 0; r < kMaxOut; ++r) {
-        const int o = threadIdx.x + r * kP2MThreads;
-        if (o < cg * n3) {
-          const int cc = o / n3, l = o % n3;
-          const int l1 = l / (n * n), l2 = (l / n) % n, l3 = l % n;
-          const double* bx = sB + (0 * n + l1) * kP2MChunk;
-          const double* by = sB + (1 * n + l2) * kP2MChunk;
-          const double* bz = sB + (2 * n + l3) * kP2MChunk;
-          double s = acc[r];
-          for (int j = 0; j < cnt; ++j) s += sW[j * CG + cc] * bx[j] * by[j] * bz[j];
-          acc[r] = s;
+        for (int d = 0; d < 3; ++d) {
+          const double q = ihalfL * (spos[(int64_t)d * Ns + p0 + lane] - c[d]);
+#pragma unroll
+          for (int m = 0; m < N; ++m) sB[wl][d][m][lane] = basis_one<double>(N, cheb, q, sTkz, m);
         }
+        for (int cc = 0; cc < cg; ++cc) sW[wl][lane][cc] = wsorted[(int64_t)(p0 + lane) * C + c0 + cc];
       }
-    }
-#pragma unroll
-    for (int r = 0; r < kMaxOut; ++r) {
-      const int o = threadIdx.x + r * kP2MThreads;
-      if (o < cg * n3) {
+      __syncwarp();
+      for (int o = lane; o < cg * n3; o += 32) {
         const int cc = o / n3, l = o % n3;
-        S_L[((int64_t)leaf * C + c0 + cc) * n3 + l] = acc[r];
+        const int l1 = l / (N * N), l2 = (l / N) % N, l3 = l % N;
+        double sum = p0 == a ? 0.0 : Sout[o];
+        for (int j = 0; j < cnt; ++j)
+          sum += sW[wl][j][cc] * sB[wl][0][l1][j] * sB[wl][1][l2][j] * sB[wl][2][l3][j];
+        Sout[o] = sum;
       }
     }
   }
 }
 
-constexpr int kM2MThreads = 128;
-constexpr int kM2MGroup = 1024;  // values per smem buffer
+struct P2MLaunch {
+  pbbfmm_tree* t;
+  int C;
+  cudaStream_t st;
+  template <int N>
+  int run() {
+    const int L = t->p.tree_level;
+    Workspace& ws = t->ws;
+    const int nl = t->lists.nsrc[L];
+    constexpr int W = p2m_warps<N>();
+    k_p2m<N><<<(nl + W - 1) / W, 32 * W, 0, st>>>(
+        ws.lists.as<int>() + t->lists.src_off[L], nl, ws.sstart.as<int>(), ws.spos.as<double>(),
+        (int)t->last_Ns, ws.wsorted.as<double>(), C, t->p.use_chebyshev, t->d_Tkz, t->p.L, L,
+        ws.S.as<double>() + level_offset(L, (int64_t)C * N * N * N));
+    PB_LAUNCH("p2m");
+    return PBBFMM_OK;
+  }
+};
 
-// One CTA per nonempty parent at level l; children at level l+1.
-__global__ void __launch_bounds__(kM2MThreads)
-    k_m2m(const int* __restrict__ parents, const int* __restrict__ sstart, int span_child,
-          const double* __restrict__ Schild, double* __restrict__ Spar, int C, int n,
+// M2M, one warp per nonempty parent and column: the column's moments of all
+// nonempty children are staged in the warp's shared slice (cp.async), then
+// each child goes through the z, y and x passes and is added to the parent
+// (children in order 0..7, as the reference accumulates them).
+template <int N>
+struct M2MCfg {
+  static constexpr int n3 = N * N * N;
+  static constexpr int per_warp = 8 * n3 + 2 * n3;  // children + two pass buffers (doubles)
+  static constexpr int warps = (per_warp * 8 * 4 <= 96 * 1024) ? 4 : 1;
+};
+
+template <int N>
+__global__ void __launch_bounds__(32 * M2MCfg<N>::warps)
+    k_m2m(const int* __restrict__ parents, int npar, const int* __restrict__ sstart,
+          int span_child, const double* __restrict__ Schild, double* __restrict__ Spar, int C,
           const double* __restrict__ Cw_g) {
-  __shared__ double sCw[2 * kMaxOrder * kMaxOrder];
-  __shared__ double b0[kM2MGroup], b1[kM2MGroup], acc[kM2MGroup];
-  const int n2 = n * n, n3 = n2 * n;
+  using G = M2MCfg<N>;
+  constexpr int n2 = N * N, n3 = G::n3;
+  extern __shared__ double smd[];
+  __shared__ double sCw[2 * N * N];
   for (int i = threadIdx.x; i < 2 * n2; i += blockDim.x) sCw[i] = Cw_g[i];
-  const int par = parents[blockIdx.x];
-  const int CG = max(1, min(C, kM2MGroup / n3));
-  for (int c0 = 0; c0 < C; c0 += CG) {
-    const int cg = min(CG, C - c0);
-    const int tot = cg * n3;
-    __syncthreads();
-    for (int i = threadIdx.x; i < tot; i += blockDim.x) acc[i] = 0;
-    for (int ch = 0; ch < 8; ++ch) {
-      const int cell = par * 8 + ch;
-      const int64_t a = (int64_t)cell * span_child, b = (int64_t)(cell + 1) * span_child;
-      if (sstart[b] == sstart[a]) continue;  // empty child: no moments
-      const double* wx = sCw + (((ch >> 2) & 1) ? n2 : 0);
-      const double* wy = sCw + (((ch >> 1) & 1) ? n2 : 0);
-      const double* wz = sCw + ((ch & 1) ? n2 : 0);
-      __syncthreads();
-      for (int i = threadIdx.x; i < tot; i += blockDim.x)
-        b0[i] = Schild[((int64_t)cell * C + c0) * n3 + i];
-      __syncthreads();
-      // z: Sz[l1*n + l3] = sum_k S[l1*n + k] wz[l3*n + k]   (l1 over n^2)
-      for (int i = threadIdx.x; i < tot; i += blockDim.x) {
-        const int cc = i / n3, r = i % n3, l1 = r / n, l3 = r % n;
-        const double* s = b0 + cc * n3 + l1 * n;
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+  const int task = blockIdx.x * G::warps + wl;  // (parent, column)
+  if (task >= npar * C) return;
+  const int par = parents[task / C], col = task % C;
+  double* sch = smd + wl * G::per_warp;  // 8 x n3
+  double* b0 = sch + 8 * n3;
+  double* b1 = b0 + n3;
+  unsigned present = 0;
+  for (int ch = 0; ch < 8; ++ch) {
+    const int cell = par * 8 + ch;
+    const int64_t a = (int64_t)cell * span_child, b = (int64_t)(cell + 1) * span_child;
+    if (sstart[b] == sstart[a]) continue;  // empty child: no moments
+    present |= 1u << ch;
+    const double* src = Schild + ((int64_t)cell * C + col) * n3;
+    for (int i = lane; i < n3; i += 32) cp_async8(&sch[ch * n3 + i], &src[i]);
+  }
+  cp_async_commit();
+  cp_async_wait_all();
+  __syncwarp();
+  constexpr int PER = (n3 + 31) / 32;
+  double acc[PER];
+#pragma unroll
+  for (int r = 0; r < PER; ++r) acc[r] = 0;
+  for (int ch = 0; ch < 8; ++ch) {
+    if (!((present >> ch) & 1)) continue;
+    const double* wx = sCw + (((ch >> 2) & 1) ? n2 : 0);
+    const double* wy = sCw + (((ch >> 1) & 1) ? n2 : 0);
+    const double* wz = sCw + ((ch & 1) ? n2 : 0);
+    const double* sc = sch + ch * n3;
+    // z: Sz[l1*n + l3] = sum_k S[l1*n + k] wz[l3*n + k]   (l1 over n^2)
+    for (int i = lane; i < n3; i += 32) {
+      const int l1 = i / N, l3 = i % N;
+      double v = 0;
+#pragma unroll
+      for (int k = 0; k < N; ++k) v += sc[l1 * N + k] * wz[l3 * N + k];
+      b0[i] = v;
+    }
+    __syncwarp();
+    // y: Sy[l1 n2 + l2 n + l3] = sum_k Sz[l1 n2 + k n + l3] wy[l2 n + k]
+    for (int i = lane; i < n3; i += 32) {
+      const int l1 = i / n2, l2 = (i / N) % N, l3 = i % N;
+      double v = 0;
+#pragma unroll
+      for (int k = 0; k < N; ++k) v += b0[l1 * n2 + k * N + l3] * wy[l2 * N + k];
+      b1[i] = v;
+    }
+    __syncwarp();
+    // x: SS[l1 n2 + l2 n + l3] = sum_k Sy[k n2 + l2 n + l3] wx[l1 n + k]
+#pragma unroll
+    for (int r = 0; r < PER; ++r) {
+      const int i = lane + 32 * r;
+      if (i < n3) {
+        const int l1 = i / n2, rem = i % n2;
         double v = 0;
-        for (int k = 0; k < n; ++k) v += s[k] * wz[l3 * n + k];
-        b1[i] = v;
-      }
-      __syncthreads();
-      // y: Sy[l1 n2 + l2 n + l3] = sum_k Sz[l1 n2 + k n + l3] wy[l2 n + k]
-      for (int i = threadIdx.x; i < tot; i += blockDim.x) {
-        const int cc = i / n3, r = i % n3, l1 = r / n2, l2 = (r / n) % n, l3 = r % n;
-        const double* s = b1 + cc * n3 + l1 * n2 + l3;
-        double v = 0;
-        for (int k = 0; k < n; ++k) v += s[k * n] * wy[l2 * n + k];
-        b0[i] = v;
-      }
-      __syncthreads();
-      // x: SS[l1 n2 + l2 n + l3] = sum_k Sy[k n2 + l2 n + l3] wx[l1 n + k]
-      for (int i = threadIdx.x; i < tot; i += blockDim.x) {
-        const int cc = i / n3, r = i % n3, l1 = r / n2, rem = r % n2;
-        const double* s = b0 + cc * n3 + rem;
-        double v = 0;
-        for (int k = 0; k < n; ++k) v += s[k * n2] * wx[l1 * n + k];
-        acc[i] += v;
+#pragma unroll
+        for (int k = 0; k < N; ++k) v += b1[k * n2 + rem] * wx[l1 * N + k];
+        acc[r] += v;
       }
     }
-    __syncthreads();
-    for (int i = threadIdx.x; i < tot; i += blockDim.x)
-      Spar[((int64_t)par * C + c0) * n3 + i] = acc[i];
+    __syncwarp();
+  }
+  double* dst = Spar + ((int64_t)par * C + col) * n3;
+#pragma unroll
+  for (int r = 0; r < PER; ++r) {
+    const int i = lane + 32 * r;
+    if (i < n3) dst[i] = acc[r];
   }
 }
+
+struct M2MLaunch {
+  pbbfmm_tree* t;
+  int C, l;
+  cudaStream_t st;
+  template <int N>
+  int run() {
+    using G = M2MCfg<N>;
+    const int L = t->p.tree_level;
+    Workspace& ws = t->ws;
+    const int64_t per = (int64_t)C * G::n3;
+    const int np = t->lists.nsrc[l];
+    const int64_t tasks = (int64_t)np * C;
+    const size_t smem = sizeof(double) * G::per_warp * G::warps;
+    PB_CUDA(cudaFuncSetAttribute(k_m2m<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_m2m<N><<<(unsigned)((tasks + G::warps - 1) / G::warps), 32 * G::warps, smem, st>>>(
+        ws.lists.as<int>() + t->lists.src_off[l], np, ws.sstart.as<int>(), (int)cells_at(L - l - 1),
+        ws.S.as<double>() + level_offset(l + 1, per), ws.S.as<double>() + level_offset(l, per), C,
+        t->d_Cw);
+    PB_LAUNCH("m2m");
+    return PBBFMM_OK;
+  }
+};
 
 int run_upward(pbbfmm_tree* t, int C, cudaStream_t st) {
-  const int L = t->p.tree_level, n = t->n, n3 = t->n3;
-  Workspace& ws = t->ws;
-  const int* lists = ws.lists.as<int>();
-  double* S = ws.S.as<double>();
-  const int* sstart = ws.sstart.as<int>();
-  const int64_t per = (int64_t)C * n3;
+  const int L = t->p.tree_level, n = t->n;
   if (t->lists.nsrc[L] > 0) {
-    size_t smem = sizeof(double) * (n * n + 3 * n * kP2MChunk + kP2MChunk * C);
     if (int rc_ = kt_begin(t, KS_P2M, st)) return rc_;
-    k_p2m<<<t->lists.nsrc[L], kP2MThreads, smem, st>>>(
-        lists + t->lists.src_off[L], sstart, ws.spos.as<double>(), (int)t->last_Ns,
-        ws.wsorted.as<double>(), C, n, t->p.use_chebyshev, t->d_Tkz, t->p.L, L,
-        S + level_offset(L, per));
-    PB_LAUNCH("p2m");
+    P2MLaunch pl{t, C, st};
+    if (int rc_ = dispatch_order(n, pl)) return rc_;
     if (int rc_ = kt_end(t, st)) return rc_;
   }
   for (int l = L - 1; l >= 2; --l) {
     if (t->lists.nsrc[l] == 0) continue;
     if (int rc_ = kt_begin(t, KS_M2M, st)) return rc_;
-    k_m2m<<<t->lists.nsrc[l], kM2MThreads, 0, st>>>(
-        lists + t->lists.src_off[l], sstart, (int)cells_at(L - l - 1), S + level_offset(l + 1, per),
-        S + level_offset(l, per), C, n, t->d_Cw);
-    PB_LAUNCH("m2m");
+    M2MLaunch ml{t, C, l, st};
+    if (int rc_ = dispatch_order(n, ml)) return rc_;
     if (int rc_ = kt_end(t, st)) return rc_;
   }
   return PBBFMM_OK;
