@@ -150,6 +150,30 @@ int pbbfmm_debug_copy(pbbfmm_tree *tree, int what, int level, double *host, int6
 int pbbfmm_tree_get_weights(const pbbfmm_tree *tree, double *Tkz, double *Kweights,
                             double *Cweights, int *Ktable);
 
+/* Leaf binning that allocates nothing.  No counterpart in the reference: it
+ * exists for callers that cannot call cudaMalloc, e.g. a process whose device
+ * memory is reserved up front by another allocator, or a deployment that
+ * forbids allocation after start-up to keep its footprint fixed.
+ *
+ * For the N points at d_points (xyz AoS float64, device) it does the binning
+ * step of the matvec: recentring on the points' bounding box (*d_center gets
+ * the shift if non-NULL), the reference's leaf assignment on a tree of
+ * `tree_level` levels and side `box`, and a stable sort by leaf: d_perm[i] is
+ * the original index of the i-th point in leaf order (N ints), d_leaf_start
+ * the first sorted position of every leaf (8^tree_level + 1 ints).  Same
+ * results as the binning inside pbbfmm_compute_device.
+ *
+ * All scratch lives in one fixed device array inside this library (about
+ * 18 MB, held on every GPU that loads the library until the process exits),
+ * so N may not exceed PBBFMM_NOALLOC_MAX_POINTS (larger N returns
+ * PBBFMM_ERR_ARG).  The first call on each device looks up the array's device
+ * address; make that first call before any stream capture.  Calls share the
+ * array: calls that overlap on the GPU (other streams, other host threads)
+ * race on it.  Runs on the current device, asynchronously on `stream`. */
+#define PBBFMM_NOALLOC_MAX_POINTS 524288
+int pbbfmm_bin_points_noalloc(const double *d_points, int64_t N, double box, int tree_level,
+                              int *d_perm, int *d_leaf_start, double *d_center, void *stream);
+
 const char *pbbfmm_last_error(void);
 const char *pbbfmm_version(void);
 

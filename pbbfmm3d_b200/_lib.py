@@ -63,6 +63,8 @@ EXPORTS = {
     "pbbfmm_reset_kernel_times": ([_vp], ctypes.c_int),
     "pbbfmm_get_kernel_times": ([_vp, ctypes.POINTER(ctypes.c_float), _ip, ctypes.c_int, _ip,
                                  ctypes.POINTER(ctypes.c_char_p)], ctypes.c_int),
+    "pbbfmm_bin_points_noalloc": ([_vp, _i64, ctypes.c_double, ctypes.c_int, _vp, _vp, _vp, _vp],
+                                  ctypes.c_int),
     "pbbfmm_measure_fma_peak": ([ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
 }
 
