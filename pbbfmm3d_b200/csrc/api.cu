@@ -86,6 +86,17 @@ static int upload(double** dst, const double* src, size_t count) {
   return PBBFMM_OK;
 }
 
+// float32 copy (rounded once from the float64 tables) for the mixed path
+static int upload_f32(float** dst, const double* src, size_t count) {
+  if (*dst) cudaFree(*dst);
+  *dst = nullptr;
+  if (count == 0) return PBBFMM_OK;
+  std::vector<float> h(src, src + count);
+  PB_CUDA(cudaMalloc(dst, count * sizeof(float)));
+  PB_CUDA(cudaMemcpy(*dst, h.data(), count * sizeof(float), cudaMemcpyHostToDevice));
+  return PBBFMM_OK;
+}
+
 // conj(DFT3(stencil)) for k3 < n, stored [lvl][k][lex 343] complex; the 27
 // inner (near-field) slots stay zero.  k = (k1*m + k2)*n + k3.
 void unif_spectra(int n, const std::vector<double>& stencil, int nlev, std::vector<double>* op) {
@@ -192,10 +203,14 @@ static int upload_operators(pbbfmm_tree* t) {
     if ((rc = upload(&t->d_E, t->ops.K.data(), t->ops.K.size()))) return rc;
     if ((rc = upload(&t->d_U, t->ops.U.data(), t->ops.U.size()))) return rc;
     if ((rc = upload(&t->d_VT, t->ops.VT.data(), t->ops.VT.size()))) return rc;
+    if ((rc = upload_f32(&t->f_E, t->ops.K.data(), t->ops.K.size()))) return rc;
+    if ((rc = upload_f32(&t->f_U, t->ops.U.data(), t->ops.U.size()))) return rc;
+    if ((rc = upload_f32(&t->f_VT, t->ops.VT.data(), t->ops.VT.size()))) return rc;
   } else {
     std::vector<double> op;
     unif_spectra(t->n, t->ops.stencil, t->ops.nlev, &op);
     if ((rc = upload(&t->d_op, op.data(), op.size()))) return rc;
+    if ((rc = upload_f32(&t->f_op, op.data(), op.size()))) return rc;
   }
   t->ops_ready = true;
   return PBBFMM_OK;
@@ -205,6 +220,11 @@ static void free_tree_device(pbbfmm_tree* t) {
   double** bufs[] = {&t->d_Tkz, &t->d_Kw, &t->d_Cw, &t->d_E,  &t->d_U,
                      &t->d_VT,  &t->d_op, &t->d_twid, &t->d_kparam};
   for (double** b : bufs) {
+    if (*b) cudaFree(*b);
+    *b = nullptr;
+  }
+  float** fbufs[] = {&t->f_Tkz, &t->f_Kw, &t->f_Cw, &t->f_E, &t->f_U, &t->f_VT, &t->f_op, &t->f_twid};
+  for (float** b : fbufs) {
     if (*b) cudaFree(*b);
     *b = nullptr;
   }
@@ -240,6 +260,7 @@ static int compute_chunk(pbbfmm_tree* t, const double* d_tgt, int64_t Nf, const 
   t->last_Nf = Nf;
   t->last_Ns = Ns;
   t->last_C = C;
+  t->cur_prec = precision;
   if ((rc = kt_begin(t, KS_BINNING, st))) return rc;
   if ((rc = run_binning(t, d_tgt, Nf, d_src, Ns, d_w, C, st))) return rc;
   if ((rc = kt_end(t, st))) return rc;
@@ -256,7 +277,6 @@ static int compute_chunk(pbbfmm_tree* t, const double* d_tgt, int64_t Nf, const 
     // halo tables: at most 8^(L-2) parent blocks x (region + target) entries
     if ((rc = grow(ws.halo, sizeof(int) * 576 * cells_at(L - 2)))) return rc;
   }
-  (void)precision;
   if ((rc = run_upward(t, C, st))) return rc;
   if (t->timing) PB_CUDA(cudaEventRecord(t->ev[2], st));
   if (t->p.use_chebyshev)
@@ -350,7 +370,10 @@ int pbbfmm_tree_create(const pbbfmm_tree_params* params, int device, pbbfmm_tree
   if ((rc = upload(&t->d_Tkz, t->w.Tkz.data(), t->w.Tkz.size())) ||
       (rc = upload(&t->d_Kw, t->w.Kweights.data(), t->w.Kweights.size())) ||
       (rc = upload(&t->d_Cw, t->w.Cweights.data(), t->w.Cweights.size())) ||
-      (rc = upload(&t->d_kparam, t->kspec.param, 4))) {
+      (rc = upload(&t->d_kparam, t->kspec.param, 4)) ||
+      (rc = upload_f32(&t->f_Tkz, t->w.Tkz.data(), t->w.Tkz.size())) ||
+      (rc = upload_f32(&t->f_Kw, t->w.Kweights.data(), t->w.Kweights.size())) ||
+      (rc = upload_f32(&t->f_Cw, t->w.Cweights.data(), t->w.Cweights.size()))) {
     free_tree_device(t);
     delete t;
     return rc;
@@ -361,7 +384,8 @@ int pbbfmm_tree_create(const pbbfmm_tree_params* params, int device, pbbfmm_tree
       tw[j] = cos(2.0 * M_PI * j / t->m);
       tw[t->m + j] = sin(2.0 * M_PI * j / t->m);
     }
-    if ((rc = upload(&t->d_twid, tw.data(), tw.size()))) {
+    if ((rc = upload(&t->d_twid, tw.data(), tw.size())) ||
+        (rc = upload_f32(&t->f_twid, tw.data(), tw.size()))) {
       free_tree_device(t);
       delete t;
       return rc;
@@ -657,6 +681,18 @@ int pbbfmm_debug_copy(pbbfmm_tree* t, int what, int level, double* host, int64_t
     }
     const int64_t per = (int64_t)C * t->n3;
     total = cells_at(level) * per;
+    if (t->cur_prec != PBBFMM_PREC_FP64) {  // mixed path: float32 arrays, widened here
+      const float* fs =
+          (what == 0 ? t->ws.S.as<float>() : t->ws.F.as<float>()) + level_offset(level, per);
+      const int64_t nc = count < total ? count : total;
+      std::vector<float> tmpf(nc > 0 ? nc : 1);
+      if (host && nc > 0) {
+        PB_CUDA(cudaMemcpy(tmpf.data(), fs, sizeof(float) * nc, cudaMemcpyDeviceToHost));
+        for (int64_t i = 0; i < nc; ++i) host[i] = tmpf[i];
+      }
+      if (written) *written = total;
+      return PBBFMM_OK;
+    }
     src = (what == 0 ? t->ws.S.as<double>() : t->ws.F.as<double>()) + level_offset(level, per);
   } else if (what >= 2 && what <= 5) {
     const int* p = nullptr;

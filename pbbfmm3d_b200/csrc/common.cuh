@@ -146,6 +146,41 @@ inline int dispatch_kernel(int kid, F&& f) {
   }
 }
 
+// ------------------------------------------------------------ real types
+// Every phase runs in float64 (PBBFMM_PREC_FP64) or float32 (the mixed path).
+template <typename T>
+struct Cplx;
+template <>
+struct Cplx<double> {
+  using type = double2;
+};
+template <>
+struct Cplx<float> {
+  using type = float2;
+};
+template <typename T>
+using cplx_t = typename Cplx<T>::type;
+template <typename T>
+__host__ __device__ __forceinline__ cplx_t<T> make_cplx(T re, T im) {
+  cplx_t<T> v;
+  v.x = re;
+  v.y = im;
+  return v;
+}
+
+// Compensated (Kahan) sum: s holds the sum, c the running low-order error.
+template <typename T>
+struct Kahan {
+  T s = 0, c = 0;
+  __device__ __forceinline__ void add(T x) {
+    const T y = x - c;
+    const T t = s + y;
+    c = (t - s) - y;
+    s = t;
+  }
+  __device__ __forceinline__ double value() const { return (double)s - (double)c; }
+};
+
 // ------------------------------------------------------------ async copies
 // 16-byte global -> shared copy that bypasses registers (cp.async, L2 only);
 // src_bytes = 0 zero-fills the destination without reading `src` (which must
@@ -156,6 +191,23 @@ __device__ __forceinline__ void cp_async16(void* smem_dst, const void* src, int 
                "r"(src_bytes)
                : "memory");
 }
+// 8-byte copy with zero-fill (src_bytes 0 or 8), through L1.
+__device__ __forceinline__ void cp_async8z(void* smem_dst, const void* src, int src_bytes) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8, %2;\n" ::"r"(d), "l"(src),
+               "r"(src_bytes)
+               : "memory");
+}
+// Copy one complex value (double2: 16 bytes, float2: 8 bytes), zero-filled
+// when `ok` is false.
+template <typename C2>
+__device__ __forceinline__ void cp_async_cplx(C2* smem_dst, const C2* src, bool ok) {
+  if (sizeof(C2) == 16)
+    cp_async16(smem_dst, src, ok ? 16 : 0);
+  else
+    cp_async8z(smem_dst, src, ok ? 8 : 0);
+}
+
 // 8-byte variant (through L1), for arrays without 16-byte alignment.
 __device__ __forceinline__ void cp_async8(void* smem_dst, const void* src) {
   const unsigned d = (unsigned)__cvta_generic_to_shared(smem_dst);

@@ -34,44 +34,43 @@ __device__ __forceinline__ void cell_center_d(uint32_t m, int l, double box, dou
 template <int N>
 struct L2LCfg {
   static constexpr int n3 = N * N * N;
-  static constexpr int per_warp = 3 * n3;  // parent + two pass buffers (doubles)
+  static constexpr int per_warp = 3 * n3;  // parent + two pass buffers (elements)
   static constexpr int warps = 8;
 };
 
-template <int N>
+template <int N, typename T>
 __global__ void __launch_bounds__(32 * L2LCfg<N>::warps)
     k_l2l(const int* __restrict__ parents, int npar, const int* __restrict__ tstart,
-          int span_child, const double* __restrict__ Fpar, double* __restrict__ Fch, int C,
-          const double* __restrict__ Cw_g) {
+          int span_child, const T* __restrict__ Fpar, T* __restrict__ Fch, int C,
+          const T* __restrict__ Cw_g) {
   using G = L2LCfg<N>;
   constexpr int n2 = N * N, n3 = G::n3;
-  extern __shared__ double smd[];
-  __shared__ double sCw[2 * N * N];
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* smd = reinterpret_cast<T*>(smraw);
+  __shared__ T sCw[2 * N * N];
   for (int i = threadIdx.x; i < 2 * n2; i += blockDim.x) sCw[i] = Cw_g[i];
   __syncthreads();
   const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
   const int task = blockIdx.x * G::warps + wl;
   if (task >= npar * C) return;
   const int par = parents[task / C], col = task % C;
-  double* sp = smd + wl * G::per_warp;
-  double* b0 = sp + n3;
-  double* b1 = b0 + n3;
-  const double* src = Fpar + ((int64_t)par * C + col) * n3;
-  for (int i = lane; i < n3; i += 32) cp_async8(&sp[i], &src[i]);
-  cp_async_commit();
-  cp_async_wait_all();
+  T* sp = smd + wl * G::per_warp;
+  T* b0 = sp + n3;
+  T* b1 = b0 + n3;
+  const T* src = Fpar + ((int64_t)par * C + col) * n3;
+  for (int i = lane; i < n3; i += 32) sp[i] = src[i];
   __syncwarp();
   for (int ch = 0; ch < 8; ++ch) {
     const int cell = par * 8 + ch;
     const int64_t a = (int64_t)cell * span_child, b = (int64_t)(cell + 1) * span_child;
     if (tstart[b] == tstart[a]) continue;  // child without targets
-    const double* wx = sCw + (((ch >> 2) & 1) ? n2 : 0);
-    const double* wy = sCw + (((ch >> 1) & 1) ? n2 : 0);
-    const double* wz = sCw + ((ch & 1) ? n2 : 0);
+    const T* wx = sCw + (((ch >> 2) & 1) ? n2 : 0);
+    const T* wy = sCw + (((ch >> 1) & 1) ? n2 : 0);
+    const T* wz = sCw + ((ch & 1) ? n2 : 0);
     // x: Fx[l1 n2 + l2 n + l3] = sum_k F[k n2 + l2 n + l3] wx[l1 + k n]
     for (int i = lane; i < n3; i += 32) {
       const int l1 = i / n2, rem = i % n2;
-      double v = 0;
+      T v = 0;
 #pragma unroll
       for (int k = 0; k < N; ++k) v += sp[k * n2 + rem] * wx[l1 + k * N];
       b0[i] = v;
@@ -80,17 +79,17 @@ __global__ void __launch_bounds__(32 * L2LCfg<N>::warps)
     // y: Fy[l1 n2 + l2 n + l3] = sum_k Fx[l1 n2 + k n + l3] wy[l2 + k n]
     for (int i = lane; i < n3; i += 32) {
       const int l1 = i / n2, l2 = (i / N) % N, l3 = i % N;
-      double v = 0;
+      T v = 0;
 #pragma unroll
       for (int k = 0; k < N; ++k) v += b0[l1 * n2 + k * N + l3] * wy[l2 + k * N];
       b1[i] = v;
     }
     __syncwarp();
     // z: Fchild[l1 n + l3] += sum_k Fy[l1 n + k] wz[l3 + k n]   (l1 over n^2)
-    double* dst = Fch + ((int64_t)cell * C + col) * n3;
+    T* dst = Fch + ((int64_t)cell * C + col) * n3;
     for (int i = lane; i < n3; i += 32) {
       const int l1 = i / N, l3 = i % N;
-      double v = 0;
+      T v = 0;
 #pragma unroll
       for (int k = 0; k < N; ++k) v += b1[l1 * N + k] * wz[l3 + k * N];
       dst[i] += v;
@@ -99,6 +98,7 @@ __global__ void __launch_bounds__(32 * L2LCfg<N>::warps)
   }
 }
 
+template <typename T>
 struct L2LLaunch {
   pbbfmm_tree* t;
   int C, l;  // child level
@@ -111,12 +111,12 @@ struct L2LLaunch {
     const int64_t per = (int64_t)C * G::n3;
     const int np = t->lists.ntgt[l - 1];
     const int64_t tasks = (int64_t)np * C;
-    const size_t smem = sizeof(double) * G::per_warp * G::warps;
-    PB_CUDA(cudaFuncSetAttribute(k_l2l<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_l2l<N><<<(unsigned)((tasks + G::warps - 1) / G::warps), 32 * G::warps, smem, st>>>(
+    const size_t smem = sizeof(T) * G::per_warp * G::warps;
+    PB_CUDA(cudaFuncSetAttribute(k_l2l<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_l2l<N, T><<<(unsigned)((tasks + G::warps - 1) / G::warps), 32 * G::warps, smem, st>>>(
         ws.lists.as<int>() + t->lists.tgt_off[l - 1], np, ws.tstart.as<int>(),
-        (int)cells_at(L - l), ws.F.as<double>() + level_offset(l - 1, per),
-        ws.F.as<double>() + level_offset(l, per), C, t->d_Cw);
+        (int)cells_at(L - l), ws.F.as<T>() + level_offset(l - 1, per),
+        ws.F.as<T>() + level_offset(l, per), C, ops_view<T>(t).Cw);
     PB_LAUNCH("l2l");
     return PBBFMM_OK;
   }
@@ -128,19 +128,24 @@ struct L2LLaunch {
 constexpr int kLeafWarps = 4;
 constexpr int kLeafCols = 8;  // columns per pass (registers)
 
-template <class KF>
+// T = float (mixed path): the kernel is evaluated in float32 on differences
+// formed in float64, the far-field interpolation runs in float32, and every
+// lane's partial sums are compensated (Kahan); the warp reduction and the
+// output update are float64.
+template <class KF, typename T>
 __global__ void __launch_bounds__(32 * kLeafWarps)
     k_leaf(const int* __restrict__ leaves, int nleaves, const int* __restrict__ tstart,
            const int* __restrict__ sstart, const int* __restrict__ tperm,
            const double* __restrict__ tpos, const double* __restrict__ spos,
            const double* __restrict__ wsorted, int Nf, int Ns, int C,
-           const double* __restrict__ F_L, int n, int cheb, const double* __restrict__ Tkz_g,
+           const T* __restrict__ F_L, int n, int cheb, const T* __restrict__ Tkz_g,
            double box, int L, const double* __restrict__ kparam_g, double* __restrict__ out) {
-  __shared__ double sTkz[kMaxOrder * kMaxOrder];
+  constexpr bool kKahan = sizeof(T) == 4;
+  __shared__ T sTkz[kMaxOrder * kMaxOrder];
   __shared__ double kp[4];
-  __shared__ int s_nb[kLeafWarps][27][2];           // neighbour source ranges
-  __shared__ int s_pre[kLeafWarps][28];             // exclusive prefix of their lengths
-  __shared__ double s_b[kLeafWarps][3][kMaxOrder];  // basis values of the current target
+  __shared__ int s_nb[kLeafWarps][27][2];      // neighbour source ranges
+  __shared__ int s_pre[kLeafWarps][28];        // exclusive prefix of their lengths
+  __shared__ T s_b[kLeafWarps][3][kMaxOrder];  // basis values of the current target
   for (int i = threadIdx.x; i < n * n; i += blockDim.x) sTkz[i] = Tkz_g[i];
   if (threadIdx.x < 4) kp[threadIdx.x] = kparam_g[threadIdx.x];
   __syncthreads();
@@ -186,26 +191,29 @@ __global__ void __launch_bounds__(32 * kLeafWarps)
     const int cg = min(kLeafCols, C - c0);
     for (int i = ta; i < te; ++i) {
       const double x = tpos[i], y = tpos[(int64_t)Nf + i], z = tpos[2 * (int64_t)Nf + i];
-      double acc[kLeafCols];
-#pragma unroll
-      for (int cc = 0; cc < kLeafCols; ++cc) acc[cc] = 0;
+      Kahan<T> acc[kLeafCols];
       // far field: phi += sum_l F[l] Sx[l1] Sy[l2] Sz[l3]
       {
         __syncwarp();
         if (lane < 3 * n) {
           const int d = lane / n, mm = lane % n;
-          const double q = ihalfL * ((d == 0 ? x : d == 1 ? y : z) - c[d]);
-          s_b[wl][d][mm] = basis_one<double>(n, cheb, q, sTkz, mm);
+          const T q = (T)(ihalfL * ((d == 0 ? x : d == 1 ? y : z) - c[d]));
+          s_b[wl][d][mm] = basis_one<T>(n, cheb, q, sTkz, mm);
         }
         __syncwarp();
-        const double* Fl = F_L + ((int64_t)leaf * C + c0) * n3;
+        const T* Fl = F_L + ((int64_t)leaf * C + c0) * n3;
         for (int l = lane; l < n3; l += 32) {
           const int l1 = l / (n * n), l2 = (l / n) % n, l3 = l % n;
-          const double tmp2 = s_b[wl][0][l1] * s_b[wl][1][l2];
-          const double bz3 = s_b[wl][2][l3];
+          const T tmp2 = s_b[wl][0][l1] * s_b[wl][1][l2];
+          const T bz3 = s_b[wl][2][l3];
 #pragma unroll
           for (int cc = 0; cc < kLeafCols; ++cc)
-            if (cc < cg) acc[cc] += Fl[cc * n3 + l] * tmp2 * bz3;
+            if (cc < cg) {
+              if (kKahan)
+                acc[cc].add(Fl[cc * n3 + l] * tmp2 * bz3);
+              else
+                acc[cc].s += Fl[cc * n3 + l] * tmp2 * bz3;
+            }
         }
       }
       // near field over the 27 neighbour leaves, their source ranges
@@ -215,33 +223,40 @@ __global__ void __launch_bounds__(32 * kLeafWarps)
         for (int v = lane; v < nsrc_total; v += 32) {
           while (v >= s_pre[wl][q + 1]) ++q;
           const int j = s_nb[wl][q][0] + (v - s_pre[wl][q]);
-          const double dx = spos[j] - x, dy = spos[(int64_t)Ns + j] - y,
-                       dz = spos[2 * (int64_t)Ns + j] - z;
-          double kv = KF::template eval<double>(dx, dy, dz, kp);
+          const T dx = (T)(spos[j] - x), dy = (T)(spos[(int64_t)Ns + j] - y),
+                  dz = (T)(spos[2 * (int64_t)Ns + j] - z);
+          T kv = KF::template eval<T>(dx, dy, dz, kp);
           if (isinf(kv)) kv = 0;
           const double* wj = wsorted + (int64_t)j * C + c0;
 #pragma unroll
           for (int cc = 0; cc < kLeafCols; ++cc)
-            if (cc < cg) acc[cc] += kv * wj[cc];
+            if (cc < cg) {
+              if (kKahan)
+                acc[cc].add(kv * (T)wj[cc]);
+              else
+                acc[cc].s += kv * wj[cc];
+            }
         }
       }
+      double tot[kLeafCols];
 #pragma unroll
       for (int cc = 0; cc < kLeafCols; ++cc) {
-        double v = acc[cc];
+        double v = kKahan ? acc[cc].value() : (double)acc[cc].s;
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        acc[cc] = v;
+        tot[cc] = v;
       }
       if (lane == 0) {
         const int64_t oi = tperm[i];
 #pragma unroll
         for (int cc = 0; cc < kLeafCols; ++cc)
-          if (cc < cg) out[(int64_t)(c0 + cc) * Nf + oi] += acc[cc];
+          if (cc < cg) out[(int64_t)(c0 + cc) * Nf + oi] += tot[cc];
       }
     }
   }
 }
 
+template <typename T>
 struct LeafLaunch {
   pbbfmm_tree* t;
   int64_t Nf, Ns;
@@ -257,32 +272,42 @@ struct LeafLaunch {
     Workspace& ws = t->ws;
     const int64_t perS = (int64_t)C * t->n3;
     if (int rc_ = kt_begin(t, KS_LEAF, st)) return rc_;
-    k_leaf<KF><<<(nl + kLeafWarps - 1) / kLeafWarps, 32 * kLeafWarps, 0, st>>>(
+    k_leaf<KF, T><<<(nl + kLeafWarps - 1) / kLeafWarps, 32 * kLeafWarps, 0, st>>>(
         ws.lists.as<int>() + t->lists.tgt_off[L], nl, ws.tstart.as<int>(), ws.sstart.as<int>(),
         ws.tperm.as<int>(), ws.tpos.as<double>(), ws.spos.as<double>(), ws.wsorted.as<double>(),
-        (int)Nf, (int)Ns, C, ws.F.as<double>() + level_offset(L, perS), t->n,
-        t->p.use_chebyshev, t->d_Tkz, t->p.L, L, kparam, out);
+        (int)Nf, (int)Ns, C, ws.F.as<T>() + level_offset(L, perS), t->n, t->p.use_chebyshev,
+        ops_view<T>(t).Tkz, t->p.L, L, kparam, out);
     PB_LAUNCH("leaf");
     if (int rc_ = kt_end(t, st)) return rc_;
     return PBBFMM_OK;
   }
 };
 
-int run_downward(pbbfmm_tree* t, int C, cudaStream_t st) {
+template <typename T>
+static int run_downward_t(pbbfmm_tree* t, int C, cudaStream_t st) {
   const int L = t->p.tree_level;
   // level-2 locals have no parent contribution (levels 0 and 1 carry none)
   for (int l = 3; l <= L; ++l) {
     if (t->lists.ntgt[l - 1] == 0) continue;
     if (int rc_ = kt_begin(t, KS_L2L, st)) return rc_;
-    L2LLaunch ll{t, C, l, st};
+    L2LLaunch<T> ll{t, C, l, st};
     if (int rc_ = dispatch_order(t->n, ll)) return rc_;
     if (int rc_ = kt_end(t, st)) return rc_;
   }
   return PBBFMM_OK;
 }
 
+int run_downward(pbbfmm_tree* t, int C, cudaStream_t st) {
+  return t->cur_prec == PBBFMM_PREC_FP64 ? run_downward_t<double>(t, C, st)
+                                         : run_downward_t<float>(t, C, st);
+}
+
 int run_leaves(pbbfmm_tree* t, int64_t Nf, int64_t Ns, int C, double* d_out, cudaStream_t st) {
-  LeafLaunch ll{t, Nf, Ns, C, d_out, st, t->d_kparam};
+  if (t->cur_prec == PBBFMM_PREC_FP64) {
+    LeafLaunch<double> ll{t, Nf, Ns, C, d_out, st, t->d_kparam};
+    return dispatch_kernel(t->p.kernel, ll);
+  }
+  LeafLaunch<float> ll{t, Nf, Ns, C, d_out, st, t->d_kparam};
   return dispatch_kernel(t->p.kernel, ll);
 }
 

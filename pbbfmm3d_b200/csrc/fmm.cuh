@@ -83,6 +83,16 @@ struct pbbfmm_tree {
   int* d_offs = nullptr;   // Cheb M2L: 8 types x 189 x 4 (ox, oy, oz, op index)
   double* d_twid = nullptr;  // Unif: cos/sin of 2 pi j / m, j < m
   double* d_kparam = nullptr;  // 4 kernel parameters
+  // float32 copies of the weights and operators for the mixed path
+  float* f_Tkz = nullptr;
+  float* f_Kw = nullptr;
+  float* f_Cw = nullptr;
+  float* f_E = nullptr;
+  float* f_U = nullptr;
+  float* f_VT = nullptr;
+  float* f_op = nullptr;  // nlev x nk x 343 complex (float2)
+  float* f_twid = nullptr;
+  int cur_prec = PBBFMM_PREC_FP64;  // precision of the compute in flight
   pbbfmm::Workspace ws;
   pbbfmm::LevelLists lists;
   // last compute (debug access)
@@ -102,6 +112,28 @@ struct pbbfmm_tree {
 };
 
 namespace pbbfmm {
+
+// Device operators in the precision of a compute.
+template <typename T>
+struct OpsView {
+  const T* Tkz;
+  const T* Kw;
+  const T* Cw;
+  const T* E;
+  const T* U;
+  const T* VT;
+  const cplx_t<T>* op;
+};
+template <typename T>
+inline OpsView<T> ops_view(const pbbfmm_tree* t);
+template <>
+inline OpsView<double> ops_view<double>(const pbbfmm_tree* t) {
+  return {t->d_Tkz, t->d_Kw, t->d_Cw, t->d_E, t->d_U, t->d_VT, (const double2*)t->d_op};
+}
+template <>
+inline OpsView<float> ops_view<float>(const pbbfmm_tree* t) {
+  return {t->f_Tkz, t->f_Kw, t->f_Cw, t->f_E, t->f_U, t->f_VT, (const float2*)t->f_op};
+}
 
 // level geometry
 inline int64_t cells_at(int l) { return (int64_t)1 << (3 * l); }

@@ -19,12 +19,13 @@ constexpr int kGemmThreads = (GBM / GTM) * (GBN / GTN);  // 256
 // Out(:, j) = alpha * oscale o (A * (bscale o B(:, j))), A col-major M x K,
 // column j = (cells[j / C], j % C); B columns are K-contiguous, Out columns
 // M-contiguous, both indexed by (cell * C + col).
+template <typename T>
 __global__ void __launch_bounds__(kGemmThreads)
-    k_colgemm(int M, int K, const double* __restrict__ A, const int* __restrict__ cells,
-              int ncols, int C, const double* __restrict__ B, const double* __restrict__ bscale,
-              double* __restrict__ Out, const double* __restrict__ oscale, double alpha) {
-  __shared__ double As[GBK][GBM];
-  __shared__ double Bs[GBK][GBN];
+    k_colgemm(int M, int K, const T* __restrict__ A, const int* __restrict__ cells, int ncols,
+              int C, const T* __restrict__ B, const T* __restrict__ bscale, T* __restrict__ Out,
+              const T* __restrict__ oscale, T alpha) {
+  __shared__ T As[GBK][GBM];
+  __shared__ T Bs[GBK][GBN];
   __shared__ int64_t colbase[GBN];
   const int tid = threadIdx.x;
   const int tx = tid % (GBN / GTN), ty = tid / (GBN / GTN);
@@ -33,7 +34,7 @@ __global__ void __launch_bounds__(kGemmThreads)
     int j = j0 + tid;
     colbase[tid] = j < ncols ? (int64_t)cells[j / C] * C + j % C : -1;
   }
-  double acc[GTM][GTN];
+  T acc[GTM][GTN];
 #pragma unroll
   for (int i = 0; i < GTM; ++i)
 #pragma unroll
@@ -44,14 +45,14 @@ __global__ void __launch_bounds__(kGemmThreads)
     for (int r = 0; r < (GBM * GBK) / kGemmThreads; ++r) {
       const int e = tid + r * kGemmThreads, mm = e % GBM, kk = e / GBM;
       const int gm = m0 + mm, gk = k0 + kk;
-      As[kk][mm] = (gm < M && gk < K) ? A[gm + (int64_t)M * gk] : 0.0;
+      As[kk][mm] = (gm < M && gk < K) ? A[gm + (int64_t)M * gk] : T(0);
     }
 #pragma unroll
     for (int r = 0; r < (GBN * GBK) / kGemmThreads; ++r) {
       const int e = tid + r * kGemmThreads, kk = e % GBK, jj = e / GBK;
       const int gk = k0 + kk;
       const int64_t cb = colbase[jj];
-      double v = 0;
+      T v = 0;
       if (cb >= 0 && gk < K) {
         v = B[cb * K + gk];
         if (bscale) v = v * bscale[gk];
@@ -61,7 +62,7 @@ __global__ void __launch_bounds__(kGemmThreads)
     __syncthreads();
 #pragma unroll
     for (int kk = 0; kk < GBK; ++kk) {
-      double a[GTM], b[GTN];
+      T a[GTM], b[GTN];
 #pragma unroll
       for (int i = 0; i < GTM; ++i) a[i] = As[kk][ty * GTM + i];
 #pragma unroll
@@ -81,7 +82,7 @@ __global__ void __launch_bounds__(kGemmThreads)
     for (int i = 0; i < GTM; ++i) {
       const int gm = m0 + ty * GTM + i;
       if (gm >= M) continue;
-      double v = alpha * acc[i][j];
+      T v = alpha * acc[i][j];
       if (oscale) v = v * oscale[gm];
       Out[cb * M + gm] = v;
     }
@@ -96,13 +97,13 @@ struct TypeTiles {
 
 // M2L for one level.  Grid: (tiles over all types, M-tiles).  A tile holds
 // up to GBN / C targets of one child type; columns are (target, col).
+template <typename T>
 __global__ void __launch_bounds__(kGemmThreads)
-    k_m2l_cheb(int rf, int rs, const double* __restrict__ E, const int* __restrict__ typed,
+    k_m2l_cheb(int rf, int rs, const T* __restrict__ E, const int* __restrict__ typed,
                TypeTiles tt, int C, int lev, const int* __restrict__ sstart, int span,
-               const int* __restrict__ offs, const double* __restrict__ proxy,
-               double* __restrict__ pf) {
-  __shared__ double As[GBK][GBM];
-  __shared__ double Bs[GBK][GBN];
+               const int* __restrict__ offs, const T* __restrict__ proxy, T* __restrict__ pf) {
+  __shared__ T As[GBK][GBM];
+  __shared__ T Bs[GBK][GBN];
   __shared__ int s_tx[GBN], s_ty[GBN], s_tz[GBN];
   __shared__ int64_t s_src[GBN];  // proxy column base of the source, or -1
   __shared__ int s_tcell[GBN];
@@ -129,7 +130,7 @@ __global__ void __launch_bounds__(kGemmThreads)
     }
   }
   const int nside = 1 << lev;
-  double acc[GTM][GTN];
+  T acc[GTM][GTN];
 #pragma unroll
   for (int i = 0; i < GTM; ++i)
 #pragma unroll
@@ -154,25 +155,25 @@ __global__ void __launch_bounds__(kGemmThreads)
       any = src >= 0;
     }
     if (!__syncthreads_or(any)) continue;
-    const double* Eo = E + (int64_t)opi * rf * rs;
+    const T* Eo = E + (int64_t)opi * rf * rs;
     for (int k0 = 0; k0 < rs; k0 += GBK) {
 #pragma unroll
       for (int r = 0; r < (GBM * GBK) / kGemmThreads; ++r) {
         const int e = tid + r * kGemmThreads, mm = e % GBM, kk = e / GBM;
         const int gm = m0 + mm, gk = k0 + kk;
-        As[kk][mm] = (gm < rf && gk < rs) ? Eo[gm + (int64_t)rf * gk] : 0.0;
+        As[kk][mm] = (gm < rf && gk < rs) ? Eo[gm + (int64_t)rf * gk] : T(0);
       }
 #pragma unroll
       for (int r = 0; r < (GBN * GBK) / kGemmThreads; ++r) {
         const int e = tid + r * kGemmThreads, kk = e % GBK, jj = e / GBK;
         const int gk = k0 + kk;
         const int64_t sb = s_src[jj];
-        Bs[kk][jj] = (sb >= 0 && gk < rs) ? proxy[sb + gk] : 0.0;
+        Bs[kk][jj] = (sb >= 0 && gk < rs) ? proxy[sb + gk] : T(0);
       }
       __syncthreads();
 #pragma unroll
       for (int kk = 0; kk < GBK; ++kk) {
-        double a[GTM], b[GTN];
+        T a[GTM], b[GTN];
 #pragma unroll
         for (int i = 0; i < GTM; ++i) a[i] = As[kk][ty * GTM + i];
 #pragma unroll
@@ -198,15 +199,17 @@ __global__ void __launch_bounds__(kGemmThreads)
   }
 }
 
-int run_m2l_cheb(pbbfmm_tree* t, int C, cudaStream_t st) {
+template <typename T>
+static int run_m2l_cheb_t(pbbfmm_tree* t, int C, cudaStream_t st) {
   const int L = t->p.tree_level, n3 = t->n3;
   const int rf = t->ops.rf, rs = t->ops.rs;
   Workspace& ws = t->ws;
   const int* lists = ws.lists.as<int>();
-  const double* S = ws.S.as<double>();
-  double* F = ws.F.as<double>();
-  double* proxy = ws.proxy.as<double>();
-  double* pf = ws.pf.as<double>();
+  const T* S = ws.S.as<T>();
+  T* F = ws.F.as<T>();
+  T* proxy = ws.proxy.as<T>();
+  T* pf = ws.pf.as<T>();
+  const OpsView<T> ov = ops_view<T>(t);
   const int* sstart = ws.sstart.as<int>();
   if (C > GBN) {
     set_error("nCols above 64 must be split by the caller");
@@ -219,10 +222,11 @@ int run_m2l_cheb(pbbfmm_tree* t, int C, cudaStream_t st) {
     if (ns > 0) {
       dim3 g((unsigned)((ns * (int64_t)C + GBN - 1) / GBN), (unsigned)((rs + GBM - 1) / GBM));
       if (int rc_ = kt_begin(t, KS_M2L_PRE, st)) return rc_;
-      k_colgemm<<<g, kGemmThreads, 0, st>>>(rs, n3, t->d_VT + (int64_t)lvl * rs * n3,
+      k_colgemm<T><<<g, kGemmThreads, 0, st>>>(rs, n3, ov.VT + (int64_t)lvl * rs * n3,
                                             lists + t->lists.src_off[l], ns * C, C,
-                                            S + level_offset(l, (int64_t)C * n3), t->d_Kw,
-                                            proxy + level_offset(l, (int64_t)C * rs), nullptr, 1.0);
+                                            S + level_offset(l, (int64_t)C * n3), ov.Kw,
+                                            proxy + level_offset(l, (int64_t)C * rs), nullptr,
+                                            T(1));
       PB_LAUNCH("m2l_pre");
       if (int rc_ = kt_end(t, st)) return rc_;
     }
@@ -244,8 +248,8 @@ int run_m2l_cheb(pbbfmm_tree* t, int C, cudaStream_t st) {
     if (tiles > 0) {
       dim3 g((unsigned)tiles, (unsigned)((rf + GBM - 1) / GBM));
       if (int rc_ = kt_begin(t, KS_M2L, st)) return rc_;
-      k_m2l_cheb<<<g, kGemmThreads, 0, st>>>(
-          rf, rs, t->d_E + (int64_t)lvl * 316 * rf * rs, lists + t->lists.typ_off[l], tt, C, l,
+      k_m2l_cheb<T><<<g, kGemmThreads, 0, st>>>(
+          rf, rs, ov.E + (int64_t)lvl * 316 * rf * rs, lists + t->lists.typ_off[l], tt, C, l,
           sstart, (int)cells_at(L - l), t->d_offs, proxy + level_offset(l, (int64_t)C * rs),
           pf + level_offset(l, (int64_t)C * rf));
       PB_LAUNCH("m2l_cheb");
@@ -257,14 +261,20 @@ int run_m2l_cheb(pbbfmm_tree* t, int C, cudaStream_t st) {
     const double scale = pow(1.0 / len, t->homogen_neg);
     dim3 g2((unsigned)((nt * (int64_t)C + GBN - 1) / GBN), (unsigned)((n3 + GBM - 1) / GBM));
     if (int rc_ = kt_begin(t, KS_M2L_POST, st)) return rc_;
-    k_colgemm<<<g2, kGemmThreads, 0, st>>>(n3, rf, t->d_U + (int64_t)lvl * n3 * rf,
+    k_colgemm<T><<<g2, kGemmThreads, 0, st>>>(n3, rf, ov.U + (int64_t)lvl * n3 * rf,
                                            lists + t->lists.tgt_off[l], nt * C, C,
                                            pf + level_offset(l, (int64_t)C * rf), nullptr,
-                                           F + level_offset(l, (int64_t)C * n3), t->d_Kw, scale);
+                                           F + level_offset(l, (int64_t)C * n3), ov.Kw,
+                                           (T)scale);
     PB_LAUNCH("m2l_post");
     if (int rc_ = kt_end(t, st)) return rc_;
   }
   return PBBFMM_OK;
+}
+
+int run_m2l_cheb(pbbfmm_tree* t, int C, cudaStream_t st) {
+  return t->cur_prec == PBBFMM_PREC_FP64 ? run_m2l_cheb_t<double>(t, C, st)
+                                         : run_m2l_cheb_t<float>(t, C, st);
 }
 
 }  // namespace pbbfmm

@@ -27,17 +27,19 @@ namespace pbbfmm {
 
 // Forward: one CTA per nonempty source cell; columns in groups of CG.
 // Templated on the order so that all index arithmetic is by constants.
-template <int n>
-__global__ void k_fft_fwd(const int* __restrict__ cells, const double* __restrict__ S_l,
-                          double2* __restrict__ X_l, int64_t ncells, int C, int CG,
-                          const double* __restrict__ twid) {
-  extern __shared__ double sm[];
+template <int n, typename T>
+__global__ void k_fft_fwd(const int* __restrict__ cells, const T* __restrict__ S_l,
+                          cplx_t<T>* __restrict__ X_l, int64_t ncells, int C, int CG,
+                          const T* __restrict__ twid) {
+  using C2 = cplx_t<T>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* sm = reinterpret_cast<T*>(smraw);
   constexpr int m = 2 * n - 1, n2 = n * n, n3 = n2 * n, nk = m * m * n;
-  double* sc = sm;               // m
-  double* ss = sc + m;           // m
-  double* sin_ = ss + m;         // CG * n3 real moments
-  double2* Z = (double2*)(sin_ + ((CG * n3 + 1) & ~1));  // CG * n * n * n   (l1, l2, k3)
-  double2* Y = Z + CG * n3;                              // CG * n * m * n   (l1, k2, k3)
+  T* sc = sm;        // m
+  T* ss = sc + m;    // m
+  T* sin_ = ss + m;  // CG * n3 real moments
+  C2* Z = (C2*)(sin_ + ((CG * n3 + 3) & ~3));  // CG * n * n * n   (l1, l2, k3)
+  C2* Y = Z + CG * n3;                         // CG * n * m * n   (l1, k2, k3)
   for (int i = threadIdx.x; i < m; i += blockDim.x) {
     sc[i] = twid[i];
     ss[i] = twid[m + i];
@@ -47,15 +49,13 @@ __global__ void k_fft_fwd(const int* __restrict__ cells, const double* __restric
     const int cg = min(CG, C - c0);
     __syncthreads();
     for (int i = threadIdx.x; i < cg * n3; i += blockDim.x)
-      cp_async8(&sin_[i], &S_l[((int64_t)cell * C + c0) * n3 + i]);
-    cp_async_commit();
-    cp_async_wait_all();
+      sin_[i] = S_l[((int64_t)cell * C + c0) * n3 + i];
     __syncthreads();
     // z: Z[c][l1][l2][k3] = sum_l3 S[c][l1][l2][l3] w^(k3 l3),  w = e^{-2 pi i / m}
     for (int i = threadIdx.x; i < cg * n3; i += blockDim.x) {
       const int cc = i / n3, r = i % n3, l12 = r / n, k3 = r % n;
-      const double* s = sin_ + cc * n3 + l12 * n;
-      double re = 0, im = 0;
+      const T* s = sin_ + cc * n3 + l12 * n;
+      T re = 0, im = 0;
       int e = 0;
 #pragma unroll
       for (int l3 = 0; l3 < n; ++l3) {
@@ -64,62 +64,64 @@ __global__ void k_fft_fwd(const int* __restrict__ cells, const double* __restric
         e += k3;
         if (e >= m) e -= m;
       }
-      Z[i] = make_double2(re, im);
+      Z[i] = make_cplx<T>(re, im);
     }
     __syncthreads();
     // y: Y[c][l1][k2][k3] = sum_l2 Z[c][l1][l2][k3] w^(k2 l2)
     constexpr int ny = n * m * n;
     for (int i = threadIdx.x; i < cg * ny; i += blockDim.x) {
       const int cc = i / ny, r = i % ny, l1 = r / (m * n), k2 = (r / n) % m, k3 = r % n;
-      const double2* z = Z + cc * n3 + l1 * n2 + k3;
-      double re = 0, im = 0;
+      const C2* z = Z + cc * n3 + l1 * n2 + k3;
+      T re = 0, im = 0;
       int e = 0;
 #pragma unroll
       for (int l2 = 0; l2 < n; ++l2) {
-        const double2 v = z[l2 * n];
-        const double c = sc[e], s = ss[e];
+        const C2 v = z[l2 * n];
+        const T c = sc[e], s = ss[e];
         re += v.x * c + v.y * s;
         im += v.y * c - v.x * s;
         e += k2;
         if (e >= m) e -= m;
       }
-      Y[i] = make_double2(re, im);
+      Y[i] = make_cplx<T>(re, im);
     }
     __syncthreads();
     // x: X[k1][k2][k3][c] = sum_l1 Y[c][l1][k2][k3] w^(k1 l1)
     for (int i = threadIdx.x; i < cg * nk; i += blockDim.x) {
       const int k = i / cg, cc = i % cg;
       const int k1 = k / (m * n), k23 = k % (m * n);
-      const double2* y = Y + cc * ny + k23;
-      double re = 0, im = 0;
+      const C2* y = Y + cc * ny + k23;
+      T re = 0, im = 0;
       int e = 0;
 #pragma unroll
       for (int l1 = 0; l1 < n; ++l1) {
-        const double2 v = y[l1 * m * n];
-        const double c = sc[e], s = ss[e];
+        const C2 v = y[l1 * m * n];
+        const T c = sc[e], s = ss[e];
         re += v.x * c + v.y * s;
         im += v.y * c - v.x * s;
         e += k1;
         if (e >= m) e -= m;
       }
-      X_l[((int64_t)k * ncells + cell) * C + c0 + cc] = make_double2(re, im);
+      X_l[((int64_t)k * ncells + cell) * C + c0 + cc] = make_cplx<T>(re, im);
     }
   }
 }
 
 // Inverse: one CTA per nonempty target cell.  F = scale * IDFT(Y)/P at
 // grid positions (a + n) mod m.
-template <int n>
-__global__ void k_fft_inv(const int* __restrict__ cells, const double2* __restrict__ Y_l,
-                          double* __restrict__ F_l, int64_t ncells, int C, int CG,
-                          const double* __restrict__ twid, double invP, double scale) {
-  extern __shared__ double sm[];
+template <int n, typename T>
+__global__ void k_fft_inv(const int* __restrict__ cells, const cplx_t<T>* __restrict__ Y_l,
+                          T* __restrict__ F_l, int64_t ncells, int C, int CG,
+                          const T* __restrict__ twid, T invP, T scale) {
+  using C2 = cplx_t<T>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* sm = reinterpret_cast<T*>(smraw);
   constexpr int m = 2 * n - 1, n2 = n * n, n3 = n2 * n, nk = m * m * n;
-  double* sc = sm;
-  double* ss = sc + m;
-  double2* Yh = (double2*)(sm + 2 * m);                     // CG * nk   (k1, k2, k3)
-  double2* G = Yh + CG * nk;                                // CG * n*m*n (a1, k2, k3)
-  double2* H = G + CG * n * m * n;                          // CG * n3    (a1, a2, k3)
+  T* sc = sm;
+  T* ss = sc + m;
+  C2* Yh = (C2*)(sm + ((2 * m + 3) & ~3));  // CG * nk   (k1, k2, k3)
+  C2* G = Yh + CG * nk;                     // CG * n*m*n (a1, k2, k3)
+  C2* H = G + CG * n * m * n;               // CG * n3    (a1, a2, k3)
   for (int i = threadIdx.x; i < m; i += blockDim.x) {
     sc[i] = twid[i];
     ss[i] = twid[m + i];
@@ -130,7 +132,7 @@ __global__ void k_fft_inv(const int* __restrict__ cells, const double2* __restri
     __syncthreads();
     for (int i = threadIdx.x; i < cg * nk; i += blockDim.x) {
       const int k = i / cg, cc = i % cg;
-      cp_async16(&Yh[cc * nk + k], &Y_l[((int64_t)k * ncells + cell) * C + c0 + cc], 16);
+      cp_async_cplx(&Yh[cc * nk + k], &Y_l[((int64_t)k * ncells + cell) * C + c0 + cc], true);
     }
     cp_async_commit();
     cp_async_wait_all();
@@ -140,38 +142,38 @@ __global__ void k_fft_inv(const int* __restrict__ cells, const double2* __restri
     for (int i = threadIdx.x; i < cg * ng; i += blockDim.x) {
       const int cc = i / ng, r = i % ng, a1 = r / (m * n), k23 = r % (m * n);
       const int t1 = (a1 + n) % m;
-      const double2* y = Yh + cc * nk + k23;
-      double re = 0, im = 0;
+      const C2* y = Yh + cc * nk + k23;
+      T re = 0, im = 0;
       int e = 0;
 #pragma unroll
       for (int k1 = 0; k1 < m; ++k1) {
-        const double2 v = y[k1 * m * n];
-        const double c = sc[e], s = ss[e];
+        const C2 v = y[k1 * m * n];
+        const T c = sc[e], s = ss[e];
         re += v.x * c - v.y * s;
         im += v.y * c + v.x * s;
         e += t1;
         if (e >= m) e -= m;
       }
-      G[i] = make_double2(re, im);
+      G[i] = make_cplx<T>(re, im);
     }
     __syncthreads();
     // y: H[c][a1][a2][k3] = sum_k2 G[c][a1][k2][k3] e^{+2 pi i k2 t2 / m}
     for (int i = threadIdx.x; i < cg * n3; i += blockDim.x) {
       const int cc = i / n3, r = i % n3, a1 = r / n2, a2 = (r / n) % n, k3 = r % n;
       const int t2 = (a2 + n) % m;
-      const double2* g = G + cc * ng + a1 * m * n + k3;
-      double re = 0, im = 0;
+      const C2* g = G + cc * ng + a1 * m * n + k3;
+      T re = 0, im = 0;
       int e = 0;
 #pragma unroll
       for (int k2 = 0; k2 < m; ++k2) {
-        const double2 v = g[k2 * n];
-        const double c = sc[e], s = ss[e];
+        const C2 v = g[k2 * n];
+        const T c = sc[e], s = ss[e];
         re += v.x * c - v.y * s;
         im += v.y * c + v.x * s;
         e += t2;
         if (e >= m) e -= m;
       }
-      H[i] = make_double2(re, im);
+      H[i] = make_cplx<T>(re, im);
     }
     __syncthreads();
     // z (complex to real over the Hermitian half):
@@ -179,13 +181,13 @@ __global__ void k_fft_inv(const int* __restrict__ cells, const double2* __restri
     for (int i = threadIdx.x; i < cg * n3; i += blockDim.x) {
       const int cc = i / n3, r = i % n3, a12 = r / n, a3 = r % n;
       const int t3 = (a3 + n) % m;
-      const double2* h = H + cc * n3 + a12 * n;
-      double acc = h[0].x;
+      const C2* h = H + cc * n3 + a12 * n;
+      T acc = h[0].x;
       int e = t3;
 #pragma unroll
       for (int k3 = 1; k3 < n; ++k3) {
-        const double2 v = h[k3];
-        acc += 2.0 * (v.x * sc[e] - v.y * ss[e]);
+        const C2 v = h[k3];
+        acc += T(2) * (v.x * sc[e] - v.y * ss[e]);
         e += t3;
         if (e >= m) e -= m;
       }
@@ -247,17 +249,18 @@ __global__ void k_halo_tables(const int* __restrict__ sstart, const int* __restr
   (void)nbx;
 }
 
-template <int PBX, int KC, int CG>
+template <int PBX, int KC, int CG, typename T>
 __global__ void __launch_bounds__(4 * PBX * KC * CG)
-    k_m2l_unif_mac(const double2* __restrict__ X_l, double2* __restrict__ Y_l,
-                   const double2* __restrict__ op,  // nk x 343 for this level
+    k_m2l_unif_mac(const cplx_t<T>* __restrict__ X_l, cplx_t<T>* __restrict__ Y_l,
+                   const cplx_t<T>* __restrict__ op,  // nk x 343 for this level
                    const int* __restrict__ halo, int64_t ncells, int C, int nk) {
   using G = MacGeom<PBX>;
+  using C2 = cplx_t<T>;
   constexpr int NT = G::NPAR * KC * CG;
   constexpr int RC = G::RC;
-  extern __shared__ double2 smc[];
-  double2* reg = smc;                   // RC x KC x CG
-  double2* sop = reg + RC * KC * CG;    // KC x 343
+  extern __shared__ __align__(16) unsigned char smraw[];
+  C2* reg = reinterpret_cast<C2*>(smraw);  // RC x KC x CG
+  C2* sop = reg + RC * KC * CG;            // KC x 343
   int* s_src = (int*)(sop + KC * 343);  // RC source cells, then TC target cells
   int* s_tgt = s_src + RC;
   const int tid = threadIdx.x;
@@ -280,34 +283,34 @@ __global__ void __launch_bounds__(4 * PBX * KC * CG)
     const int r = i / (KC * CG), q = i % (KC * CG), kk = q / CG, c = q % CG;
     const int src = s_src[r];
     const bool ok = src >= 0 && k0 + kk < nk && c0 + c < C;
-    const double2* g = ok ? &X_l[((int64_t)(k0 + kk) * ncells + src) * C + c0 + c] : X_l;
-    cp_async16(&reg[i], g, ok ? 16 : 0);
+    const C2* g = ok ? &X_l[((int64_t)(k0 + kk) * ncells + src) * C + c0 + c] : X_l;
+    cp_async_cplx(&reg[i], g, ok);
   }
   for (int i = tid; i < KC * 343; i += NT) {
     const int kk = i / 343, e = i % 343;
     const bool ok = k0 + kk < nk;
-    cp_async16(&sop[i], ok ? &op[(int64_t)(k0 + kk) * 343 + e] : op, ok ? 16 : 0);
+    cp_async_cplx(&sop[i], ok ? &op[(int64_t)(k0 + kk) * 343 + e] : op, ok);
   }
   cp_async_commit();
   cp_async_wait_all();
   __syncthreads();
-  double ar[8], br[8], ai[8], bi[8];  // re = ar + br, im = ai + bi
+  T ar[8], br[8], ai[8], bi[8];  // re = ar + br, im = ai + bi
 #pragma unroll
-  for (int t = 0; t < 8; ++t) ar[t] = br[t] = ai[t] = bi[t] = 0.0;
-  const double2* myop = sop + kc * 343;
+  for (int t = 0; t < 8; ++t) ar[t] = br[t] = ai[t] = bi[t] = T(0);
+  const C2* myop = sop + kc * 343;
   // sx runs as a loop (keeps the unrolled body and its registers small);
   // for each (sy, sz, t) the y/z offsets are compile-time constants, so the
   // interaction test reduces to |ox| > 1 unless |oy| or |oz| already is > 1.
 #pragma unroll 1
   for (int sx = 0; sx < 6; ++sx) {
-    const double2* rrow = reg + (((2 * px + sx) << 6) * KC + kc) * CG + cc;
-    const double2* orow = myop + 49 * (sx + 1);  // lex of ox + 3 = sx + 1 - tx
+    const C2* rrow = reg + (((2 * px + sx) << 6) * KC + kc) * CG + cc;
+    const C2* orow = myop + 49 * (sx + 1);  // lex of ox + 3 = sx + 1 - tx
 #pragma unroll
     for (int sy = 0; sy < 6; ++sy)
 #pragma unroll
       for (int sz = 0; sz < 6; ++sz) {
         const int r = ((2 * py + sy) << 3) | (2 * pz + sz);
-        const double2 xv = rrow[r * KC * CG];
+        const C2 xv = rrow[r * KC * CG];
 #pragma unroll
         for (int t = 0; t < 8; ++t) {
           const int tx = (t >> 2) & 1;
@@ -316,7 +319,7 @@ __global__ void __launch_bounds__(4 * PBX * KC * CG)
           const int ox = sx - 2 - tx;
           const bool far_yz = oy > 1 || oy < -1 || oz > 1 || oz < -1;
           if (far_yz || ox > 1 || ox < -1) {
-            const double2 a = orow[-49 * tx + 7 * (oy + 3) + (oz + 3)];
+            const C2 a = orow[-49 * tx + 7 * (oy + 3) + (oz + 3)];
             ar[t] = fma(a.x, xv.x, ar[t]);
             br[t] = fma(-a.y, xv.y, br[t]);
             ai[t] = fma(a.x, xv.y, ai[t]);
@@ -333,13 +336,13 @@ __global__ void __launch_bounds__(4 * PBX * KC * CG)
       const int cm = s_tgt[q];
       if (cm >= 0)
         Y_l[((int64_t)(k0 + kc) * ncells + cm) * C + c0 + cc] =
-            make_double2(ar[t] + br[t], ai[t] + bi[t]);
+            make_cplx<T>(ar[t] + br[t], ai[t] + bi[t]);
     }
   }
 }
 
-template <int PBX, int KC, int CG>
-static int launch_mac(const double2* X, double2* Y, const double2* op, int* halo,
+template <int PBX, int KC, int CG, typename T>
+static int launch_mac(const cplx_t<T>* X, cplx_t<T>* Y, const cplx_t<T>* op, int* halo,
                       const int* sstart, const int* tstart, int span, int lev, int C, int nk,
                       cudaStream_t st) {
   using G = MacGeom<PBX>;
@@ -348,25 +351,30 @@ static int launch_mac(const double2* X, double2* Y, const double2* op, int* halo
   k_halo_tables<PBX><<<nblk, 256, 0, st>>>(sstart, tstart, span, lev, halo);
   PB_LAUNCH("halo_tables");
   dim3 g((unsigned)nblk, (unsigned)((nk + KC - 1) / KC), (unsigned)((C + CG - 1) / CG));
-  const size_t smem = sizeof(double2) * (G::RC * KC * CG + KC * 343) + sizeof(int) * G::STRIDE;
-  PB_CUDA(cudaFuncSetAttribute(k_m2l_unif_mac<PBX, KC, CG>,
+  const size_t smem =
+      sizeof(cplx_t<T>) * (G::RC * KC * CG + KC * 343) + sizeof(int) * G::STRIDE;
+  PB_CUDA(cudaFuncSetAttribute(k_m2l_unif_mac<PBX, KC, CG, T>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_m2l_unif_mac<PBX, KC, CG><<<g, G::NPAR * KC * CG, smem, st>>>(X, Y, op, halo, cells_at(lev),
-                                                                  C, nk);
+  k_m2l_unif_mac<PBX, KC, CG, T><<<g, G::NPAR * KC * CG, smem, st>>>(X, Y, op, halo,
+                                                                     cells_at(lev), C, nk);
   PB_LAUNCH("m2l_unif_mac");
   return PBBFMM_OK;
 }
 
-template <int PBX>
-static int launch_mac_cols(const double2* X, double2* Y, const double2* op, int* halo,
+template <int PBX, typename T>
+static int launch_mac_cols(const cplx_t<T>* X, cplx_t<T>* Y, const cplx_t<T>* op, int* halo,
                            const int* sstart, const int* tstart, int span, int lev, int C, int nk,
                            cudaStream_t st) {
-  if (C >= 8) return launch_mac<PBX, 1, 8>(X, Y, op, halo, sstart, tstart, span, lev, C, nk, st);
-  if (C >= 4) return launch_mac<PBX, 2, 4>(X, Y, op, halo, sstart, tstart, span, lev, C, nk, st);
-  if (C >= 2) return launch_mac<PBX, 4, 2>(X, Y, op, halo, sstart, tstart, span, lev, C, nk, st);
-  return launch_mac<PBX, 8, 1>(X, Y, op, halo, sstart, tstart, span, lev, C, nk, st);
+  if (C >= 8)
+    return launch_mac<PBX, 1, 8, T>(X, Y, op, halo, sstart, tstart, span, lev, C, nk, st);
+  if (C >= 4)
+    return launch_mac<PBX, 2, 4, T>(X, Y, op, halo, sstart, tstart, span, lev, C, nk, st);
+  if (C >= 2)
+    return launch_mac<PBX, 4, 2, T>(X, Y, op, halo, sstart, tstart, span, lev, C, nk, st);
+  return launch_mac<PBX, 8, 1, T>(X, Y, op, halo, sstart, tstart, span, lev, C, nk, st);
 }
 
+template <typename T>
 struct FftLaunch {
   pbbfmm_tree* t;
   int C, CGf, CGi;
@@ -378,53 +386,53 @@ struct FftLaunch {
   double scale = 1.0;
   template <int N>
   int run() {
-    const int L = t->p.tree_level, n3 = N * N * N, nk = (2 * N - 1) * (2 * N - 1) * N;
+    const int n3 = N * N * N, nk = (2 * N - 1) * (2 * N - 1) * N;
     Workspace& ws = t->ws;
     const int* lists = ws.lists.as<int>();
     const int64_t perS = (int64_t)C * n3, perX = (int64_t)nk * C;
     const int l = level;
+    const T* twid = sizeof(T) == 8 ? (const T*)t->d_twid : (const T*)t->f_twid;
     if (!inverse) {
-      PB_CUDA(cudaFuncSetAttribute(k_fft_fwd<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      PB_CUDA(cudaFuncSetAttribute(k_fft_fwd<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)smem_f));
-      k_fft_fwd<N><<<t->lists.nsrc[l], 128, smem_f, st>>>(
-          lists + t->lists.src_off[l], ws.S.as<double>() + level_offset(l, perS),
-          ws.proxy.as<double2>() + level_offset(l, perX), cells_at(l), C, CGf, t->d_twid);
+      k_fft_fwd<N, T><<<t->lists.nsrc[l], 128, smem_f, st>>>(
+          lists + t->lists.src_off[l], ws.S.as<T>() + level_offset(l, perS),
+          ws.proxy.as<cplx_t<T>>() + level_offset(l, perX), cells_at(l), C, CGf, twid);
       PB_LAUNCH("fft_fwd");
     } else {
-      PB_CUDA(cudaFuncSetAttribute(k_fft_inv<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      PB_CUDA(cudaFuncSetAttribute(k_fft_inv<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)smem_i));
-      k_fft_inv<N><<<t->lists.ntgt[l], 128, smem_i, st>>>(
-          lists + t->lists.tgt_off[l], ws.pf.as<double2>() + level_offset(l, perX),
-          ws.F.as<double>() + level_offset(l, perS), cells_at(l), C, CGi, t->d_twid, invP,
-          scale);
+      k_fft_inv<N, T><<<t->lists.ntgt[l], 128, smem_i, st>>>(
+          lists + t->lists.tgt_off[l], ws.pf.as<cplx_t<T>>() + level_offset(l, perX),
+          ws.F.as<T>() + level_offset(l, perS), cells_at(l), C, CGi, twid, (T)invP, (T)scale);
       PB_LAUNCH("fft_inv");
     }
     return PBBFMM_OK;
   }
 };
 
-int run_m2l_unif(pbbfmm_tree* t, int C, cudaStream_t st) {
+template <typename T>
+static int run_m2l_unif_t(pbbfmm_tree* t, int C, cudaStream_t st) {
+  using C2 = cplx_t<T>;
   const int L = t->p.tree_level, n = t->n, m = t->m, n3 = t->n3, nk = t->nk;
   Workspace& ws = t->ws;
-  const int* lists = ws.lists.as<int>();
-  const double* S = ws.S.as<double>();
-  double* F = ws.F.as<double>();
-  double2* X = ws.proxy.as<double2>();
-  double2* Y = ws.pf.as<double2>();
+  C2* X = ws.proxy.as<C2>();
+  C2* Y = ws.pf.as<C2>();
   const int* sstart = ws.sstart.as<int>();
   const int* tstart = ws.tstart.as<int>();
-  const int64_t perS = (int64_t)C * n3, perX = (int64_t)nk * C;
+  const int64_t perX = (int64_t)nk * C;
   const double invP = 1.0 / (double)(m * m * m);
+  const int ts = (int)sizeof(T);
   // forward transforms of all nonempty source cells, levels 2..L
-  const int fwd_col = n3 * 8 + n3 * 16 + n * m * n * 16;
+  const int fwd_col = n3 * ts + n3 * 2 * ts + n * m * n * 2 * ts;
   const int CGf = max(1, min(C, 60000 / fwd_col));
-  const size_t smem_f = sizeof(double) * (2 * m + ((CGf * n3 + 1) & ~1)) +
-                        sizeof(double2) * (CGf * n3 + CGf * n * m * n);
-  const int inv_col = nk * 16 + n * m * n * 16 + n3 * 16;
+  const size_t smem_f = (size_t)ts * (2 * m + ((CGf * n3 + 3) & ~3)) +
+                        (size_t)2 * ts * (CGf * n3 + CGf * n * m * n);
+  const int inv_col = (nk + n * m * n + n3) * 2 * ts;
   const int CGi = max(1, min(C, 60000 / inv_col));
-  const size_t smem_i =
-      sizeof(double) * (2 * m) + sizeof(double2) * (CGi * nk + CGi * n * m * n + CGi * n3);
-  FftLaunch fl{t, C, CGf, CGi, smem_f, smem_i, invP, st};
+  const size_t smem_i = (size_t)ts * ((2 * m + 3) & ~3) +
+                        (size_t)2 * ts * (CGi * nk + CGi * n * m * n + CGi * n3);
+  FftLaunch<T> fl{t, C, CGf, CGi, smem_f, smem_i, invP, st};
   for (int l = 2; l <= L; ++l) {
     if (t->lists.nsrc[l] == 0) continue;
     if (int rc_ = kt_begin(t, KS_FFT_FWD, st)) return rc_;
@@ -434,20 +442,21 @@ int run_m2l_unif(pbbfmm_tree* t, int C, cudaStream_t st) {
     if (int rc_ = kt_end(t, st)) return rc_;
   }
   int* halo = ws.halo.as<int>();
+  const OpsView<T> ov = ops_view<T>(t);
   for (int l = 2; l <= L; ++l) {
     if (t->lists.ntgt[l] == 0) continue;
     const int lvl = t->homog ? 0 : l - 2;
-    const double2* op = (const double2*)t->d_op + (int64_t)lvl * nk * 343;
+    const C2* op = ov.op + (int64_t)lvl * nk * 343;
     const int span = (int)cells_at(L - l);
     int rc;
     if ((rc = kt_begin(t, KS_MAC, st))) return rc;
-    const double2* Xl = X + level_offset(l, perX);
-    double2* Yl = Y + level_offset(l, perX);
+    const C2* Xl = X + level_offset(l, perX);
+    C2* Yl = Y + level_offset(l, perX);
     // 4x2x2 parent blocks from level 3 up (level 2 has 2 parents per side)
     if (l >= 3)
-      rc = launch_mac_cols<4>(Xl, Yl, op, halo, sstart, tstart, span, l, C, nk, st);
+      rc = launch_mac_cols<4, T>(Xl, Yl, op, halo, sstart, tstart, span, l, C, nk, st);
     else
-      rc = launch_mac_cols<2>(Xl, Yl, op, halo, sstart, tstart, span, l, C, nk, st);
+      rc = launch_mac_cols<2, T>(Xl, Yl, op, halo, sstart, tstart, span, l, C, nk, st);
     if (rc) return rc;
     if ((rc = kt_end(t, st))) return rc;
     double len = t->p.L;
@@ -461,6 +470,11 @@ int run_m2l_unif(pbbfmm_tree* t, int C, cudaStream_t st) {
     if (int rc_ = kt_end(t, st)) return rc_;
   }
   return PBBFMM_OK;
+}
+
+int run_m2l_unif(pbbfmm_tree* t, int C, cudaStream_t st) {
+  return t->cur_prec == PBBFMM_PREC_FP64 ? run_m2l_unif_t<double>(t, C, st)
+                                         : run_m2l_unif_t<float>(t, C, st);
 }
 
 }  // namespace pbbfmm

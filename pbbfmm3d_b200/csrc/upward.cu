@@ -33,9 +33,9 @@ __device__ __forceinline__ void cell_center(uint32_t m, int l, double box, doubl
 constexpr int kP2MChunk = 32;  // points per pass (one per lane)
 constexpr int kP2MCols = 8;    // columns per pass
 // warps per CTA: static shared memory (basis + weights) stays under 48 KB
-template <int N>
+template <int N, typename T>
 constexpr int p2m_warps() {
-  return (3 * N * kP2MChunk + kP2MChunk * kP2MCols) * 8 * 8 <= 40 * 1024 ? 8 : 4;
+  return (3 * N * kP2MChunk + kP2MChunk * kP2MCols) * (int)sizeof(T) * 8 <= 40 * 1024 ? 8 : 4;
 }
 
 // One warp per nonempty source leaf.  Lanes first evaluate the basis of up to
@@ -43,16 +43,18 @@ constexpr int p2m_warps() {
 // outputs o = lane + 32 r of the (column, l1, l2, l3) block and sums over the
 // staged points in point order.  Leaves with more than 32 points accumulate
 // chunk by chunk in the output array (each output has a single owner lane).
-template <int N, int kP2MWarps = p2m_warps<N>()>
+// T = float (mixed path): the basis is evaluated from float64 leaf-relative
+// coordinates and each chunk's sum is compensated (Kahan).
+template <int N, typename T, int kP2MWarps = p2m_warps<N, T>()>
 __global__ void __launch_bounds__(32 * kP2MWarps)
     k_p2m(const int* __restrict__ leaves, int nleaves, const int* __restrict__ sstart,
           const double* __restrict__ spos, int Ns, const double* __restrict__ wsorted, int C,
-          int cheb, const double* __restrict__ Tkz_g, double box, int L,
-          double* __restrict__ S_L) {
+          int cheb, const T* __restrict__ Tkz_g, double box, int L, T* __restrict__ S_L) {
   constexpr int n3 = N * N * N;
-  __shared__ double sTkz[N * N];
-  __shared__ double sB[kP2MWarps][3][N][kP2MChunk];
-  __shared__ double sW[kP2MWarps][kP2MChunk][kP2MCols];
+  constexpr bool kKahan = sizeof(T) == 4;
+  __shared__ T sTkz[N * N];
+  __shared__ T sB[kP2MWarps][3][N][kP2MChunk];
+  __shared__ T sW[kP2MWarps][kP2MChunk][kP2MCols];
   for (int i = threadIdx.x; i < N * N; i += blockDim.x) sTkz[i] = Tkz_g[i];
   __syncthreads();
   const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
@@ -67,32 +69,41 @@ __global__ void __launch_bounds__(32 * kP2MWarps)
   const double ihalfL = 2. / len;
   for (int c0 = 0; c0 < C; c0 += kP2MCols) {
     const int cg = min(kP2MCols, C - c0);
-    double* Sout = S_L + ((int64_t)leaf * C + c0) * n3;
+    T* Sout = S_L + ((int64_t)leaf * C + c0) * n3;
     for (int p0 = a; p0 < e; p0 += kP2MChunk) {
       const int cnt = min(kP2MChunk, e - p0);
       __syncwarp();
       if (lane < cnt) {
 #pragma unroll
         for (int d = 0; d < 3; ++d) {
-          const double q = ihalfL * (spos[(int64_t)d * Ns + p0 + lane] - c[d]);
+          const T q = (T)(ihalfL * (spos[(int64_t)d * Ns + p0 + lane] - c[d]));
 #pragma unroll
-          for (int m = 0; m < N; ++m) sB[wl][d][m][lane] = basis_one<double>(N, cheb, q, sTkz, m);
+          for (int m = 0; m < N; ++m) sB[wl][d][m][lane] = basis_one<T>(N, cheb, q, sTkz, m);
         }
-        for (int cc = 0; cc < cg; ++cc) sW[wl][lane][cc] = wsorted[(int64_t)(p0 + lane) * C + c0 + cc];
+        for (int cc = 0; cc < cg; ++cc)
+          sW[wl][lane][cc] = (T)wsorted[(int64_t)(p0 + lane) * C + c0 + cc];
       }
       __syncwarp();
       for (int o = lane; o < cg * n3; o += 32) {
         const int cc = o / n3, l = o % n3;
         const int l1 = l / (N * N), l2 = (l / N) % N, l3 = l % N;
-        double sum = p0 == a ? 0.0 : Sout[o];
-        for (int j = 0; j < cnt; ++j)
-          sum += sW[wl][j][cc] * sB[wl][0][l1][j] * sB[wl][1][l2][j] * sB[wl][2][l3][j];
-        Sout[o] = sum;
+        if (kKahan) {
+          Kahan<T> acc;
+          for (int j = 0; j < cnt; ++j)
+            acc.add(sW[wl][j][cc] * sB[wl][0][l1][j] * sB[wl][1][l2][j] * sB[wl][2][l3][j]);
+          Sout[o] = (T)(p0 == a ? acc.value() : (double)Sout[o] + acc.value());
+        } else {
+          T sum = p0 == a ? T(0) : Sout[o];
+          for (int j = 0; j < cnt; ++j)
+            sum += sW[wl][j][cc] * sB[wl][0][l1][j] * sB[wl][1][l2][j] * sB[wl][2][l3][j];
+          Sout[o] = sum;
+        }
       }
     }
   }
 }
 
+template <typename T>
 struct P2MLaunch {
   pbbfmm_tree* t;
   int C;
@@ -102,11 +113,12 @@ struct P2MLaunch {
     const int L = t->p.tree_level;
     Workspace& ws = t->ws;
     const int nl = t->lists.nsrc[L];
-    constexpr int W = p2m_warps<N>();
-    k_p2m<N><<<(nl + W - 1) / W, 32 * W, 0, st>>>(
+    constexpr int W = p2m_warps<N, T>();
+    const OpsView<T> ov = ops_view<T>(t);
+    k_p2m<N, T><<<(nl + W - 1) / W, 32 * W, 0, st>>>(
         ws.lists.as<int>() + t->lists.src_off[L], nl, ws.sstart.as<int>(), ws.spos.as<double>(),
-        (int)t->last_Ns, ws.wsorted.as<double>(), C, t->p.use_chebyshev, t->d_Tkz, t->p.L, L,
-        ws.S.as<double>() + level_offset(L, (int64_t)C * N * N * N));
+        (int)t->last_Ns, ws.wsorted.as<double>(), C, t->p.use_chebyshev, ov.Tkz, t->p.L, L,
+        ws.S.as<T>() + level_offset(L, (int64_t)C * N * N * N));
     PB_LAUNCH("p2m");
     return PBBFMM_OK;
   }
@@ -116,57 +128,56 @@ struct P2MLaunch {
 // nonempty children are staged in the warp's shared slice (cp.async), then
 // each child goes through the z, y and x passes and is added to the parent
 // (children in order 0..7, as the reference accumulates them).
-template <int N>
+template <int N, typename T>
 struct M2MCfg {
   static constexpr int n3 = N * N * N;
-  static constexpr int per_warp = 8 * n3 + 2 * n3;  // children + two pass buffers (doubles)
-  static constexpr int warps = (per_warp * 8 * 4 <= 96 * 1024) ? 4 : 1;
+  static constexpr int per_warp = 8 * n3 + 2 * n3;  // children + two pass buffers (elements)
+  static constexpr int warps = (per_warp * (int)sizeof(T) * 4 <= 96 * 1024) ? 4 : 1;
 };
 
-template <int N>
-__global__ void __launch_bounds__(32 * M2MCfg<N>::warps)
+template <int N, typename T>
+__global__ void __launch_bounds__(32 * M2MCfg<N, T>::warps)
     k_m2m(const int* __restrict__ parents, int npar, const int* __restrict__ sstart,
-          int span_child, const double* __restrict__ Schild, double* __restrict__ Spar, int C,
-          const double* __restrict__ Cw_g) {
-  using G = M2MCfg<N>;
+          int span_child, const T* __restrict__ Schild, T* __restrict__ Spar, int C,
+          const T* __restrict__ Cw_g) {
+  using G = M2MCfg<N, T>;
   constexpr int n2 = N * N, n3 = G::n3;
-  extern __shared__ double smd[];
-  __shared__ double sCw[2 * N * N];
+  extern __shared__ __align__(16) unsigned char smraw[];
+  T* smd = reinterpret_cast<T*>(smraw);
+  __shared__ T sCw[2 * N * N];
   for (int i = threadIdx.x; i < 2 * n2; i += blockDim.x) sCw[i] = Cw_g[i];
   __syncthreads();
   const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
   const int task = blockIdx.x * G::warps + wl;  // (parent, column)
   if (task >= npar * C) return;
   const int par = parents[task / C], col = task % C;
-  double* sch = smd + wl * G::per_warp;  // 8 x n3
-  double* b0 = sch + 8 * n3;
-  double* b1 = b0 + n3;
+  T* sch = smd + wl * G::per_warp;  // 8 x n3
+  T* b0 = sch + 8 * n3;
+  T* b1 = b0 + n3;
   unsigned present = 0;
   for (int ch = 0; ch < 8; ++ch) {
     const int cell = par * 8 + ch;
     const int64_t a = (int64_t)cell * span_child, b = (int64_t)(cell + 1) * span_child;
     if (sstart[b] == sstart[a]) continue;  // empty child: no moments
     present |= 1u << ch;
-    const double* src = Schild + ((int64_t)cell * C + col) * n3;
-    for (int i = lane; i < n3; i += 32) cp_async8(&sch[ch * n3 + i], &src[i]);
+    const T* src = Schild + ((int64_t)cell * C + col) * n3;
+    for (int i = lane; i < n3; i += 32) sch[ch * n3 + i] = src[i];
   }
-  cp_async_commit();
-  cp_async_wait_all();
   __syncwarp();
   constexpr int PER = (n3 + 31) / 32;
-  double acc[PER];
+  T acc[PER];
 #pragma unroll
   for (int r = 0; r < PER; ++r) acc[r] = 0;
   for (int ch = 0; ch < 8; ++ch) {
     if (!((present >> ch) & 1)) continue;
-    const double* wx = sCw + (((ch >> 2) & 1) ? n2 : 0);
-    const double* wy = sCw + (((ch >> 1) & 1) ? n2 : 0);
-    const double* wz = sCw + ((ch & 1) ? n2 : 0);
-    const double* sc = sch + ch * n3;
+    const T* wx = sCw + (((ch >> 2) & 1) ? n2 : 0);
+    const T* wy = sCw + (((ch >> 1) & 1) ? n2 : 0);
+    const T* wz = sCw + ((ch & 1) ? n2 : 0);
+    const T* sc = sch + ch * n3;
     // z: Sz[l1*n + l3] = sum_k S[l1*n + k] wz[l3*n + k]   (l1 over n^2)
     for (int i = lane; i < n3; i += 32) {
       const int l1 = i / N, l3 = i % N;
-      double v = 0;
+      T v = 0;
 #pragma unroll
       for (int k = 0; k < N; ++k) v += sc[l1 * N + k] * wz[l3 * N + k];
       b0[i] = v;
@@ -175,7 +186,7 @@ __global__ void __launch_bounds__(32 * M2MCfg<N>::warps)
     // y: Sy[l1 n2 + l2 n + l3] = sum_k Sz[l1 n2 + k n + l3] wy[l2 n + k]
     for (int i = lane; i < n3; i += 32) {
       const int l1 = i / n2, l2 = (i / N) % N, l3 = i % N;
-      double v = 0;
+      T v = 0;
 #pragma unroll
       for (int k = 0; k < N; ++k) v += b0[l1 * n2 + k * N + l3] * wy[l2 * N + k];
       b1[i] = v;
@@ -187,7 +198,7 @@ __global__ void __launch_bounds__(32 * M2MCfg<N>::warps)
       const int i = lane + 32 * r;
       if (i < n3) {
         const int l1 = i / n2, rem = i % n2;
-        double v = 0;
+        T v = 0;
 #pragma unroll
         for (int k = 0; k < N; ++k) v += b1[k * n2 + rem] * wx[l1 * N + k];
         acc[r] += v;
@@ -195,7 +206,7 @@ __global__ void __launch_bounds__(32 * M2MCfg<N>::warps)
     }
     __syncwarp();
   }
-  double* dst = Spar + ((int64_t)par * C + col) * n3;
+  T* dst = Spar + ((int64_t)par * C + col) * n3;
 #pragma unroll
   for (int r = 0; r < PER; ++r) {
     const int i = lane + 32 * r;
@@ -203,45 +214,52 @@ __global__ void __launch_bounds__(32 * M2MCfg<N>::warps)
   }
 }
 
+template <typename T>
 struct M2MLaunch {
   pbbfmm_tree* t;
   int C, l;
   cudaStream_t st;
   template <int N>
   int run() {
-    using G = M2MCfg<N>;
+    using G = M2MCfg<N, T>;
     const int L = t->p.tree_level;
     Workspace& ws = t->ws;
     const int64_t per = (int64_t)C * G::n3;
     const int np = t->lists.nsrc[l];
     const int64_t tasks = (int64_t)np * C;
-    const size_t smem = sizeof(double) * G::per_warp * G::warps;
-    PB_CUDA(cudaFuncSetAttribute(k_m2m<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k_m2m<N><<<(unsigned)((tasks + G::warps - 1) / G::warps), 32 * G::warps, smem, st>>>(
+    const size_t smem = sizeof(T) * G::per_warp * G::warps;
+    PB_CUDA(cudaFuncSetAttribute(k_m2m<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_m2m<N, T><<<(unsigned)((tasks + G::warps - 1) / G::warps), 32 * G::warps, smem, st>>>(
         ws.lists.as<int>() + t->lists.src_off[l], np, ws.sstart.as<int>(), (int)cells_at(L - l - 1),
-        ws.S.as<double>() + level_offset(l + 1, per), ws.S.as<double>() + level_offset(l, per), C,
-        t->d_Cw);
+        ws.S.as<T>() + level_offset(l + 1, per), ws.S.as<T>() + level_offset(l, per), C,
+        ops_view<T>(t).Cw);
     PB_LAUNCH("m2m");
     return PBBFMM_OK;
   }
 };
 
-int run_upward(pbbfmm_tree* t, int C, cudaStream_t st) {
+template <typename T>
+static int run_upward_t(pbbfmm_tree* t, int C, cudaStream_t st) {
   const int L = t->p.tree_level, n = t->n;
   if (t->lists.nsrc[L] > 0) {
     if (int rc_ = kt_begin(t, KS_P2M, st)) return rc_;
-    P2MLaunch pl{t, C, st};
+    P2MLaunch<T> pl{t, C, st};
     if (int rc_ = dispatch_order(n, pl)) return rc_;
     if (int rc_ = kt_end(t, st)) return rc_;
   }
   for (int l = L - 1; l >= 2; --l) {
     if (t->lists.nsrc[l] == 0) continue;
     if (int rc_ = kt_begin(t, KS_M2M, st)) return rc_;
-    M2MLaunch ml{t, C, l, st};
+    M2MLaunch<T> ml{t, C, l, st};
     if (int rc_ = dispatch_order(n, ml)) return rc_;
     if (int rc_ = kt_end(t, st)) return rc_;
   }
   return PBBFMM_OK;
+}
+
+int run_upward(pbbfmm_tree* t, int C, cudaStream_t st) {
+  return t->cur_prec == PBBFMM_PREC_FP64 ? run_upward_t<double>(t, C, st)
+                                         : run_upward_t<float>(t, C, st);
 }
 
 }  // namespace pbbfmm

@@ -204,3 +204,34 @@ def test_config1_accuracy_against_direct_sum():
         out = run_gpu(t, p, p, w, 1)
         d = oracle.direct("Laplacian", [0.0], p, p, w, 1, rows=rows)
         assert rel(out[rows], d) < bound, lo
+
+
+MIXED_CONFIGS = [
+    _meta("ExpCov", 0.3, 1.0, 5, 5, 1e-5, 0, 8),
+    _meta("Laplacian", 0.0, 1.0, 4, 5, 1e-7, 1, 1),
+    _meta("GaussSigma", 0.1, 1.0, 4, 4, 1e-6, 1, 2),
+    _meta("OneOverR2", 0.0, 1.0, 4, 4, 1e-5, 0, 3),
+]
+
+
+@pytest.mark.parametrize("meta", MIXED_CONFIGS,
+                         ids=[c["kernel"] + ("C" if c["cheb"] else "U") for c in MIXED_CONFIGS])
+def test_mixed_precision_close_to_fp64(meta):
+    """The mixed path (float32 far field and interpolation, compensated sums,
+    float64 positions) stays within 2e-6 relative L2 of the float64 path,
+    far below the FMM's own approximation error."""
+    rng = np.random.default_rng(21)
+    N = 30000
+    p = _points(rng, N, meta["box"])
+    w = rng.standard_normal(N * meta["ncols"])
+    t = gpu_tree(meta)
+    o64 = run_gpu(t, p, p, w, meta["ncols"])
+    t.set_precision(fmm.PREC_MIXED)
+    o32 = run_gpu(t, p, p, w, meta["ncols"])
+    assert rel(o32, o64) < 2e-6
+    rows = rng.choice(N, 512, replace=False)
+    d = oracle.direct(meta["kernel"], [meta["param"]], p, p, w, meta["ncols"], rows=rows)
+    C = meta["ncols"]
+    sel = (np.arange(C)[:, None] * N + rows[None, :]).ravel()
+    e64, e32 = rel(o64[sel], d), rel(o32[sel], d)
+    assert e32 < 1.05 * e64 + 2e-6, (e32, e64)
