@@ -40,6 +40,7 @@ extern "C" {
 #define PBBFMM_ERR_IO 5          /* operator cache file unreadable / malformed */
 #define PBBFMM_ERR_UNSUPPORTED 6 /* combination not implemented                */
 #define PBBFMM_ERR_NUMERIC 7     /* non-finite input detected                  */
+#define PBBFMM_ERR_TIMEOUT 8     /* a bounded device wait ran out (output invalid) */
 
 /* ---- built-in kernels (src/kernel_Types.cpp; the last three are the user
  * kernels of the reference's examples and python binding) ---- */
@@ -118,6 +119,16 @@ int pbbfmm_compute_device(pbbfmm_tree *tree, const double *d_target, int64_t Nf,
 /* Precision used by pbbfmm_compute (default PBBFMM_PREC_FP64). */
 int pbbfmm_set_precision(pbbfmm_tree *tree, int precision);
 
+/* Chebyshev M2L of the mixed path on the tensor cores (tcgen05, 3xTF32 with
+ * float32 accumulation; default on).  enable = 0 selects the CUDA-core float32
+ * kernel instead.  No reference counterpart: the reference has one CPU path.
+ * pbbfmm_tensor_core_m2l returns 1 when a mixed Chebyshev compute of this tree
+ * runs on the tensor cores (enabled, operators loaded, r_f <= 256).
+ * If a tensor-core wait ever times out (about 1 s), that compute's output is
+ * invalid and the next compute entry returns PBBFMM_ERR_TIMEOUT once. */
+int pbbfmm_set_tensor_cores(pbbfmm_tree *tree, int enable);
+int pbbfmm_tensor_core_m2l(const pbbfmm_tree *tree);
+
 /* Per-phase device times (ms) of the last compute, when timing is enabled
  * with pbbfmm_set_timing(tree, 1).  names: comma-separated phase names. */
 int pbbfmm_set_timing(pbbfmm_tree *tree, int enable);
@@ -127,7 +138,7 @@ int pbbfmm_get_phase_times(const pbbfmm_tree *tree, float *ms, int max_phases, i
 /* Per-kernel device times: with timing enabled, every launch of a compute
  * is bracketed by CUDA events on its stream.  Slots (names, comma-separated):
  * binning, p2m, m2m, m2l_pre, m2l, m2l_post, fft_fwd, m2l_mac, fft_inv,
- * l2l, leaf.  ms / launches are summed since the last reset. */
+ * l2l, leaf, m2l_split.  ms / launches are summed since the last reset. */
 int pbbfmm_reset_kernel_times(pbbfmm_tree *tree);
 int pbbfmm_get_kernel_times(pbbfmm_tree *tree, float *ms, int *launches, int max_slots,
                             int *nslots, const char **names);

@@ -132,6 +132,15 @@ class H2_3D_Tree:
         _lib.check(_lib.lib().pbbfmm_set_precision(self._h, int(precision)))
         self.precision = int(precision)
 
+    def set_tensor_cores(self, enable: bool = True) -> None:
+        """Chebyshev M2L of the mixed path on tcgen05 (3xTF32) or, with
+        enable=False, on the CUDA cores in float32."""
+        _lib.check(_lib.lib().pbbfmm_set_tensor_cores(self._h, int(bool(enable))))
+
+    def tensor_core_m2l(self) -> bool:
+        """True when a mixed Chebyshev compute of this tree runs its M2L on tcgen05."""
+        return bool(_lib.lib().pbbfmm_tensor_core_m2l(self._h))
+
     def set_timing(self, enable: bool = True) -> None:
         _lib.check(_lib.lib().pbbfmm_set_timing(self._h, 1 if enable else 0))
 

@@ -13,7 +13,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libpbbfmm3d_b200.so")
 
 # status codes
-OK, ERR_ARG, ERR_CUDA, ERR_ALLOC, ERR_STATE, ERR_IO, ERR_UNSUPPORTED, ERR_NUMERIC = range(8)
+OK, ERR_ARG, ERR_CUDA, ERR_ALLOC, ERR_STATE, ERR_IO, ERR_UNSUPPORTED, ERR_NUMERIC, ERR_TIMEOUT = range(9)
 PREC_FP64, PREC_MIXED = 0, 1
 
 
@@ -52,6 +52,8 @@ EXPORTS = {
     "pbbfmm_compute": ([_vp, _dp, _i64, _dp, _i64, _dp, ctypes.c_int, _dp], ctypes.c_int),
     "pbbfmm_compute_device": ([_vp, _vp, _i64, _vp, _i64, _vp, ctypes.c_int, _vp, ctypes.c_int, _vp], ctypes.c_int),
     "pbbfmm_set_precision": ([_vp, ctypes.c_int], ctypes.c_int),
+    "pbbfmm_set_tensor_cores": ([_vp, ctypes.c_int], ctypes.c_int),
+    "pbbfmm_tensor_core_m2l": ([_vp], ctypes.c_int),
     "pbbfmm_set_timing": ([_vp, ctypes.c_int], ctypes.c_int),
     "pbbfmm_get_phase_times": ([_vp, ctypes.POINTER(ctypes.c_float), ctypes.c_int, _ip,
                                 ctypes.POINTER(ctypes.c_char_p)], ctypes.c_int),

@@ -20,7 +20,7 @@ static std::atomic<long long> g_launches{0};
 void count_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 const char* const kSlotNames =
-    "binning,p2m,m2m,m2l_pre,m2l,m2l_post,fft_fwd,m2l_mac,fft_inv,l2l,leaf";
+    "binning,p2m,m2m,m2l_pre,m2l,m2l_post,fft_fwd,m2l_mac,fft_inv,l2l,leaf,m2l_split";
 
 int kt_begin(pbbfmm_tree* t, int slot, cudaStream_t st) {
   if (!t->timing) return PBBFMM_OK;
@@ -94,6 +94,59 @@ static int upload_f32(float** dst, const double* src, size_t count) {
   std::vector<float> h(src, src + count);
   PB_CUDA(cudaMalloc(dst, count * sizeof(float)));
   PB_CUDA(cudaMemcpy(*dst, h.data(), count * sizeof(float), cudaMemcpyHostToDevice));
+  return PBBFMM_OK;
+}
+
+// float32 value rounded to TF32 (10 explicit mantissa bits), to nearest with
+// ties away from zero -- the rounding of cvt.rna.tf32.f32.
+static float tf32_round(float x) {
+  uint32_t u;
+  memcpy(&u, &x, 4);
+  if ((u & 0x7f800000u) == 0x7f800000u) return x;
+  u = (u + 0x1000u) & 0xffffe000u;
+  float r;
+  memcpy(&r, &u, 4);
+  return r;
+}
+
+// Operands of the tensor-core Chebyshev M2L: for each level and operator o,
+// E_o^T as NP rows of KP floats (row f holds E_o[f][s], s < rs), split into
+// TF32 hi = tf32(x) and lo = tf32(x - hi), zero padded.
+static int upload_tc_operators(pbbfmm_tree* t) {
+  const int rf = t->ops.rf, rs = t->ops.rs, nlev = t->ops.nlev;
+  const int NP = (rf + 15) / 16 * 16, KP = (rs + 31) / 32 * 32;
+  if (t->f_Eth) cudaFree(t->f_Eth);
+  if (t->f_Etl) cudaFree(t->f_Etl);
+  t->f_Eth = t->f_Etl = nullptr;
+  t->tc_np = NP;
+  t->tc_kp = KP;
+  if (NP > kTcMaxN) return PBBFMM_OK;  // the float path uses the CUDA-core kernel
+  const size_t per = (size_t)316 * NP * KP, total = per * nlev;
+  std::vector<float> hi(total, 0.f), lo(total, 0.f);
+  const double* K = t->ops.K.data();
+  parallel_for((int64_t)nlev * 316, [&](int64_t b0, int64_t b1) {
+    for (int64_t b = b0; b < b1; ++b) {
+      const double* E = K + (size_t)b * rf * rs;  // column-major rf x rs
+      float* h = hi.data() + (size_t)b * NP * KP;
+      float* l = lo.data() + (size_t)b * NP * KP;
+      for (int f = 0; f < rf; ++f)
+        for (int s = 0; s < rs; ++s) {
+          const float x = (float)E[f + (size_t)rf * s];
+          const float xh = tf32_round(x);
+          h[(size_t)f * KP + s] = xh;
+          l[(size_t)f * KP + s] = tf32_round(x - xh);
+        }
+    }
+  });
+  PB_CUDA(cudaMalloc(&t->f_Eth, total * sizeof(float)));
+  PB_CUDA(cudaMalloc(&t->f_Etl, total * sizeof(float)));
+  PB_CUDA(cudaMemcpy(t->f_Eth, hi.data(), total * sizeof(float), cudaMemcpyHostToDevice));
+  PB_CUDA(cudaMemcpy(t->f_Etl, lo.data(), total * sizeof(float), cudaMemcpyHostToDevice));
+  if (!t->h_tc_err) {
+    PB_CUDA(cudaHostAlloc(&t->h_tc_err, sizeof(int), cudaHostAllocMapped));
+    *t->h_tc_err = 0;
+    PB_CUDA(cudaHostGetDevicePointer(&t->d_tc_err, t->h_tc_err, 0));
+  }
   return PBBFMM_OK;
 }
 
@@ -206,6 +259,7 @@ static int upload_operators(pbbfmm_tree* t) {
     if ((rc = upload_f32(&t->f_E, t->ops.K.data(), t->ops.K.size()))) return rc;
     if ((rc = upload_f32(&t->f_U, t->ops.U.data(), t->ops.U.size()))) return rc;
     if ((rc = upload_f32(&t->f_VT, t->ops.VT.data(), t->ops.VT.size()))) return rc;
+    if ((rc = upload_tc_operators(t))) return rc;
   } else {
     std::vector<double> op;
     unif_spectra(t->n, t->ops.stencil, t->ops.nlev, &op);
@@ -230,12 +284,17 @@ static void free_tree_device(pbbfmm_tree* t) {
   }
   if (t->d_offs) cudaFree(t->d_offs);
   t->d_offs = nullptr;
+  if (t->f_Eth) cudaFree(t->f_Eth);
+  if (t->f_Etl) cudaFree(t->f_Etl);
+  t->f_Eth = t->f_Etl = nullptr;
+  if (t->h_tc_err) cudaFreeHost(t->h_tc_err);
+  t->h_tc_err = t->d_tc_err = nullptr;
   Workspace& ws = t->ws;
   DevBuf* all[] = {&ws.bbox_part, &ws.ctr,   &ws.key,     &ws.key_sorted, &ws.idx,
                    &ws.tperm,     &ws.sperm, &ws.tstart,  &ws.sstart,     &ws.tpos,
                    &ws.spos,      &ws.wsorted, &ws.cub_temp, &ws.lists,    &ws.dcounts,
                    &ws.S,         &ws.F,     &ws.proxy,   &ws.pf,         &ws.io_tgt,
-                   &ws.io_src,    &ws.io_w,  &ws.io_out, &ws.halo};
+                   &ws.io_src,    &ws.io_w,  &ws.io_out, &ws.halo, &ws.tc_proxy};
   for (DevBuf* b : all) release(*b);
   for (int i = 0; i < 16; ++i)
     if (t->ev[i]) {
@@ -245,6 +304,19 @@ static void free_tree_device(pbbfmm_tree* t) {
   for (cudaEvent_t e : t->kev) cudaEventDestroy(e);
   t->kev.clear();
   t->kused = 0;
+}
+
+// A tensor-core M2L whose mbarrier wait timed out sets the mapped flag and
+// leaves that compute's output invalid; the next entry on the host reports
+// it (once).  Visible here after any synchronisation with the compute.
+static int take_tc_timeout(pbbfmm_tree* t) {
+  if (t->h_tc_err && *(volatile int*)t->h_tc_err) {
+    *(volatile int*)t->h_tc_err = 0;
+    set_error("tensor-core M2L: a wait for the tensor pipe timed out; that compute's output is "
+              "invalid");
+    return PBBFMM_ERR_TIMEOUT;
+  }
+  return PBBFMM_OK;
 }
 
 static const char* kPhaseNames = "binning,upward,far_field,downward,near_field";
@@ -604,6 +676,7 @@ int pbbfmm_compute_device(pbbfmm_tree* t, const double* d_target, int64_t Nf,
     set_error("bad precision mode");
     return PBBFMM_ERR_ARG;
   }
+  if (int rc = take_tc_timeout(t)) return rc;
   if (Nf == 0) return PBBFMM_OK;
   PB_CUDA(cudaSetDevice(t->device));
   cudaStream_t st = (cudaStream_t)stream;
@@ -658,8 +731,19 @@ int pbbfmm_compute(pbbfmm_tree* t, const double* target, int64_t Nf, const doubl
                              ws.io_out.as<double>(), t->precision, nullptr);
   if (rc) return rc;
   PB_CUDA(cudaMemcpy(output, ws.io_out.p, sizeof(double) * Nf * nCols, cudaMemcpyDeviceToHost));
+  return take_tc_timeout(t);
+}
+
+int pbbfmm_set_tensor_cores(pbbfmm_tree* t, int enable) {
+  if (!t) {
+    set_error("null tree");
+    return PBBFMM_ERR_ARG;
+  }
+  t->use_tc = enable != 0;
   return PBBFMM_OK;
 }
+
+int pbbfmm_tensor_core_m2l(const pbbfmm_tree* t) { return t && tc_eligible(t) ? 1 : 0; }
 
 int pbbfmm_debug_copy(pbbfmm_tree* t, int what, int level, double* host, int64_t count,
                       int64_t* written) {

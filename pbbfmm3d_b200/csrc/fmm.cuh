@@ -44,6 +44,7 @@ struct Workspace {
   DevBuf proxy;  // Cheb: sum_l 8^l * C * rs ;  Unif: spectra sum_l 8^l * nk * C (complex)
   DevBuf pf;     // Cheb: sum_l 8^l * C * rf ;  Unif: accumulated spectra
   DevBuf halo;   // Unif M2L: per parent block 512 halo + 64 target cells
+  DevBuf tc_proxy;  // tensor-core Cheb M2L: TF32 hi then lo proxies of one level
   // staging for the host-pointer entry point
   DevBuf io_tgt, io_src, io_w, io_out;
 };
@@ -92,6 +93,14 @@ struct pbbfmm_tree {
   float* f_VT = nullptr;
   float* f_op = nullptr;  // nlev x nk x 343 complex (float2)
   float* f_twid = nullptr;
+  // tensor-core Chebyshev M2L (mixed path): hi / lo TF32 parts of E_o^T,
+  // nlev x 316 x tc_np x tc_kp (rf padded to 16, rs padded to 32)
+  bool use_tc = true;
+  int tc_np = 0, tc_kp = 0;
+  float* f_Eth = nullptr;
+  float* f_Etl = nullptr;
+  int* h_tc_err = nullptr;  // mapped pinned flag: a tensor-core wait timed out
+  int* d_tc_err = nullptr;  // its device address
   int cur_prec = PBBFMM_PREC_FP64;  // precision of the compute in flight
   pbbfmm::Workspace ws;
   pbbfmm::LevelLists lists;
@@ -150,6 +159,11 @@ int run_binning(pbbfmm_tree* t, const double* d_tgt, int64_t Nf, const double* d
                 const double* d_w, int C, cudaStream_t st);
 int run_upward(pbbfmm_tree* t, int C, cudaStream_t st);
 int run_m2l_cheb(pbbfmm_tree* t, int C, cudaStream_t st);
+// tensor-core Chebyshev M2L (float path): N = rf padded to 16 must fit TMEM
+constexpr int kTcMaxN = 256;
+bool tc_eligible(const pbbfmm_tree* t);
+int run_m2l_cheb_tc_level(pbbfmm_tree* t, int C, int l, int lvl, const float* proxy, float* pf,
+                          cudaStream_t st);
 int run_m2l_unif(pbbfmm_tree* t, int C, cudaStream_t st);
 int run_downward(pbbfmm_tree* t, int C, cudaStream_t st);
 int run_leaves(pbbfmm_tree* t, int64_t Nf, int64_t Ns, int C, double* d_out, cudaStream_t st);
@@ -159,7 +173,7 @@ void unif_spectra(int n, const std::vector<double>& stencil, int nlev, std::vect
 // Kernel timer slots (pbbfmm_get_kernel_times).
 enum KSlot {
   KS_BINNING = 0, KS_P2M, KS_M2M, KS_M2L_PRE, KS_M2L, KS_M2L_POST, KS_FFT_FWD, KS_MAC, KS_FFT_INV,
-  KS_L2L, KS_LEAF, KS_COUNT
+  KS_L2L, KS_LEAF, KS_M2L_SPLIT, KS_COUNT
 };
 extern const char* const kSlotNames;
 // Record an event before / after a launch when timing is enabled.

@@ -9,6 +9,8 @@
 // (child type) share the same 189 offsets, so a tile of such targets walks
 // the 189 operators E_i once and multiplies each by the gathered proxies of
 // the tile -- one accumulated GEMM with K = 189 * r_s per tile.
+#include <type_traits>
+
 #include "fmm.cuh"
 
 namespace pbbfmm {
@@ -235,6 +237,15 @@ static int run_m2l_cheb_t(pbbfmm_tree* t, int C, cudaStream_t st) {
     const int lvl = t->homog ? 0 : l - 2;
     const int nt = t->lists.ntgt[l];
     if (nt == 0) continue;
+    bool on_tc = false;  // float path: tcgen05 3xTF32 kernel when rf fits TMEM
+    if constexpr (std::is_same<T, float>::value) {
+      if (tc_eligible(t)) {
+        if (int rc_ = run_m2l_cheb_tc_level(t, C, l, lvl, proxy + level_offset(l, (int64_t)C * rs),
+                                            pf + level_offset(l, (int64_t)C * rf), st))
+          return rc_;
+        on_tc = true;
+      }
+    }
     TypeTiles tt;
     const int per_tile = GBN / C;
     int tiles = 0;
@@ -245,7 +256,7 @@ static int run_m2l_cheb_t(pbbfmm_tree* t, int C, cudaStream_t st) {
       tiles += (tt.count[ty] + per_tile - 1) / per_tile;
     }
     tt.start[8] = tiles;
-    if (tiles > 0) {
+    if (tiles > 0 && !on_tc) {
       dim3 g((unsigned)tiles, (unsigned)((rf + GBM - 1) / GBM));
       if (int rc_ = kt_begin(t, KS_M2L, st)) return rc_;
       k_m2l_cheb<T><<<g, kGemmThreads, 0, st>>>(

@@ -1,0 +1,513 @@
+// Chebyshev M2L of the mixed-precision path on the 5th-generation tensor
+// cores (tcgen05 with TMEM accumulators), split precision 3xTF32:
+//     D += A_lo B_hi + A_hi B_lo + A_hi B_hi,
+// with x = hi + lo, hi = tf32(x), lo = tf32(x - hi), accumulated in float32.
+// The dropped A_lo B_lo term and the splitting leave a relative error near
+// 2^-21 per product, against 2^-11 for a single TF32 product.  The float32
+// accumulation inside the tensor pipe loses about one unit in the last place
+// per accumulation step, so accumulators are drained into pf every few
+// offsets (see `group`), which keeps the result within ~1e-6 of float64.
+//
+// Same product as k_m2l_cheb (reference: FarFieldInteractions / Moment2Local,
+// include/compute.hpp:402-508 and 881-914): for a tile of targets of one
+// level that share their child type, D[(target, col)][f] = sum over the 189
+// offsets o of sum_s proxy_{target+o}[col][s] E_o[f][s].
+//
+//   M = 128 rows (target, col) of one child type,  N = rf padded to 16,
+//   K = (offsets with a source in the tile) x (rs padded to 32).
+//
+// Operands are K-major, 128-byte-swizzled tiles (rows of 32 floats, groups of
+// 8 rows 1024 bytes apart), filled with cp.async (zero-fill for absent
+// sources) in NST stages.  Every wait is bounded: on timeout the kernel sets
+// *err, waits (bounded) for its last MMAs, frees its TMEM and returns.
+#include <cstdlib>
+
+#include "fmm.cuh"
+
+namespace pbbfmm {
+
+constexpr int TC_M = 128;
+constexpr int TC_KC = 32;          // K per stage: one 128-byte swizzle row of float32
+constexpr int TC_THREADS = 256;    // warps 0-3 producers, warps 4-7 drainers
+constexpr int TC_TMEM_COLS = 256;  // columns of one accumulator
+constexpr unsigned long long kWaitNs = 1000000000ull;  // 1 s
+constexpr long long kWaitIters = 1ll << 26;
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// K-major SWIZZLE_128B shared-memory matrix descriptor (sm100 format:
+// start>>4 in [0,14), LBO>>4 in [16,30) (unused for this layout, 1), SBO>>4 in
+// [32,46) = 1024 bytes between 8-row groups, version 1 in [46,48), layout
+// type 2 = SWIZZLE_128B in [61,64)).  Tile bases are 1024-byte aligned; a K
+// step of 8 float32 inside the 128-byte row advances the start by 32 bytes.
+__device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
+  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
+         ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+// Instruction descriptor for kind::tf32: D float32 (bits 4-5 = 1), A and B
+// TF32 (bits 7-9, 10-12 = 2), both K-major, N>>3 in bits 17-22, M>>4 in 24-28.
+__host__ __device__ constexpr uint32_t tf32_idesc(int M, int N) {
+  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) |
+         ((uint32_t)(M >> 4) << 24);
+}
+
+// Byte offset of (row r, 16-byte chunk j) in a K-major SWIZZLE_128B tile.
+__device__ __forceinline__ uint32_t sw128_off(int r, int j) {
+  return (uint32_t)((r >> 3) * 1024 + (r & 7) * 128 + ((j ^ (r & 7)) << 4));
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t* bar, int count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count)
+               : "memory");
+}
+
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
+  return t;
+}
+
+// Wait for the completion of the phase with parity `parity`; false after
+// about a second (or kWaitIters polls) without it, or once *abort is set
+// (abort may be null).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, int parity, const volatile int* abort) {
+  const uint32_t a = smem_u32(bar);
+  const unsigned long long t0 = global_ns();
+  for (long long it = 0; it < kWaitIters; ++it) {
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+        " selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(done)
+        : "r"(a), "r"(parity)
+        : "memory");
+    if (done) return true;
+    if ((it & 255) == 255 && ((abort && *abort) || global_ns() - t0 > kWaitNs)) return false;
+  }
+  return false;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Barrier 1 over the 128 producer threads, OR-reducing `pred`.
+__device__ __forceinline__ bool producers_sync_or(bool pred) {
+  int r;
+  asm volatile(
+      "{\n .reg .pred p, q;\n setp.ne.b32 p, %1, 0;\n"
+      " bar.red.or.pred q, 1, 128, p;\n selp.s32 %0, 1, 0, q;\n}\n"
+      : "=r"(r)
+      : "r"((int)pred)
+      : "memory");
+  return r != 0;
+}
+
+__device__ __forceinline__ void fence_async_smem() {
+  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_before() {
+  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
+}
+__device__ __forceinline__ void tc_fence_after() {
+  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
+}
+
+__device__ __forceinline__ void tc_mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                            uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+
+// Arrive on `bar` once every tcgen05.mma issued so far by this thread is done.
+__device__ __forceinline__ void tc_commit(uint64_t* bar) {
+  asm volatile(
+      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
+          smem_u32(bar))
+      : "memory");
+}
+
+// 16 consecutive float32 columns of this thread's TMEM lane.
+__device__ __forceinline__ void tc_ld16(uint32_t taddr, float* v) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
+      "%12, %13, %14, %15}, [%16];\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+        "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ float to_tf32(float x) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
+  return __uint_as_float(r);
+}
+
+struct TcTiles {
+  int start[9];  // first tile of each child type; start[8] = total tiles
+  int first[8];  // first list position of each type
+  int count[8];  // targets of each type
+};
+
+// Stage layout: A_hi 16 KB | A_lo 16 KB | B_hi NP*128 | B_lo NP*128, each
+// part 1024-byte aligned (NP is a multiple of 16).
+__host__ __device__ constexpr int tc_stage_bytes(int NP) { return 2 * 16384 + 2 * NP * 128; }
+__host__ __device__ constexpr int tc_smem_bytes(int NP, int nst) {
+  return nst * tc_stage_bytes(NP) + 1024;
+}
+
+// One CTA per tile of 128 (target, col) rows of one child type; NST stages.
+//   Eh, El : [316][NP][KP] hi / lo of E_o^T (row f holds E_o[f][s] over s), zero padded
+//   Ph, Pl : proxy hi / lo, row (cell * C + col) of KP floats, zero padded
+//   pf     : output rows (cell * C + col) of rf floats
+// Warps 0-3 (producers) look up source rows, fill the stages with cp.async
+// and thread 0 issues the MMAs.  Two TMEM accumulators of 256 columns take
+// turns, one per group of `group` consecutive offsets, so that every float32
+// accumulation chain inside the tensor pipe spans at most `group` offsets;
+// warps 4-7 (drainers) add each finished accumulator into pf while the MMAs
+// of the next group run.
+//   s_bar[s]  : MMAs of the stage's last fill done (tcgen05.commit)
+//   s_accf[b] : MMAs of accumulator b's group done (tcgen05.commit)
+//   s_acce[b] : accumulator b drained (128 drainer arrivals)
+template <int NST>
+__global__ void __launch_bounds__(TC_THREADS, 1)
+    k_m2l_cheb_tc(int rf, int NP, int KP, const float* __restrict__ Eh,
+                  const float* __restrict__ El, const int* __restrict__ typed, TcTiles tt, int C,
+                  int lev, const int* __restrict__ sstart, int span, const int* __restrict__ offs,
+                  const float* __restrict__ Ph, const float* __restrict__ Pl,
+                  float* __restrict__ pf, int group, int* __restrict__ err) {
+  extern __shared__ unsigned char smraw[];
+  const int bbytes = NP * 128;
+  const int stage_bytes = tc_stage_bytes(NP);
+  unsigned char* base = smraw + ((1024 - (smem_u32(smraw) & 1023)) & 1023);
+  __shared__ uint64_t s_bar[NST], s_accf[2], s_acce[2];
+  __shared__ uint32_t s_tmem;
+  __shared__ int s_cell[TC_M];     // target cell of each row, or -1
+  __shared__ int s_xyz[TC_M];      // target coordinates, x << 20 | y << 10 | z
+  __shared__ uint32_t s_valid[6];  // bit o: some target of the tile has a source at offset o
+  __shared__ int4 s_off[189];      // valid offsets: (ox, oy, oz, operator index)
+  __shared__ int s_nvalid;
+  __shared__ int s_abort_flag;
+  volatile int* s_abort = &s_abort_flag;
+  const int tid = threadIdx.x, warp = tid >> 5;
+
+  // child type of this tile (unrolled so the parameter arrays stay in registers)
+  int type = 0, tstart = 0, tlist = 0, tcount = 0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+    if ((int)blockIdx.x >= tt.start[i]) {
+      type = i;
+      tstart = tt.start[i];
+      tlist = tt.first[i];
+      tcount = tt.count[i];
+    }
+  const int per_tile = TC_M / C;
+  const int tfirst = (blockIdx.x - tstart) * per_tile;
+  const int ntile = min(per_tile, tcount - tfirst);
+  const int nside = 1 << lev;
+  const int* my_offs = offs + type * 189 * 4;
+
+  // producer thread tid owns A row tid; drainer thread owns TMEM lane (and row) 32 (warp % 4) + lane
+  const int row = tid < TC_M ? tid : 32 * (warp & 3) + (tid & 31);
+  int tx = 0, ty = 0, tz = 0;
+  const int cell = (row < per_tile * C && row / C < ntile) ? typed[tlist + tfirst + row / C] : -1;
+  if (cell >= 0) morton_decode((uint32_t)cell, &tx, &ty, &tz);
+  const int col = row % C;
+  if (tid < TC_M) {
+    s_cell[tid] = cell;
+    s_xyz[tid] = (tx << 20) | (ty << 10) | tz;
+  }
+  if (tid < 6) s_valid[tid] = 0;
+  if (warp == 0) {  // two accumulators: 128 lanes x 2 x 256 float32 columns
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                     smem_u32(&s_tmem)),
+                 "r"(2 * TC_TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  if (tid == 0) {
+    for (int i = 0; i < NST; ++i) mbar_init(&s_bar[i], 1);
+    for (int b = 0; b < 2; ++b) {
+      mbar_init(&s_accf[b], 1);
+      mbar_init(&s_acce[b], TC_THREADS - TC_M);
+    }
+    s_abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  // offsets with at least one source cell for some target of the tile
+  if (tid < TC_M && cell >= 0 && col == 0) {
+    for (int o = 0; o < 189; ++o) {
+      const int bx = tx + my_offs[4 * o], by = ty + my_offs[4 * o + 1], bz = tz + my_offs[4 * o + 2];
+      if (bx < 0 || by < 0 || bz < 0 || bx >= nside || by >= nside || bz >= nside) continue;
+      const uint32_t bm = morton_encode(bx, by, bz);
+      if (sstart[(int64_t)(bm + 1) * span] > sstart[(int64_t)bm * span])
+        atomicOr(&s_valid[o >> 5], 1u << (o & 31));
+    }
+  }
+  __syncthreads();
+  if (tid == 0) {
+    int nv = 0;
+    for (int o = 0; o < 189; ++o)
+      if ((s_valid[o >> 5] >> (o & 31)) & 1)
+        s_off[nv++] = make_int4(my_offs[4 * o], my_offs[4 * o + 1], my_offs[4 * o + 2],
+                                my_offs[4 * o + 3]);
+    s_nvalid = nv;
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s_tmem;
+  const int nvalid = s_nvalid;
+  const int kchunks = KP / TC_KC;
+  const int niter = nvalid * kchunks;
+  const int group_iters = max(group, 1) * kchunks;
+  const int ngroups = (niter + group_iters - 1) / group_iters;
+
+  if (tid < TC_M) {
+    // ---------------------------------------------------------------- producers
+    const uint32_t idesc = tf32_idesc(TC_M, NP);
+    // Source row of this thread for valid offset q: the lookup for q + 1 is
+    // started (two independent loads) when q is resolved and finished when
+    // q + 1 is needed, a whole offset (kchunks stages) later.
+    int cur_q = -1, pre_q = -1;
+    int64_t cur_row = -1;
+    int pre_a = 0, pre_b = 0;
+    uint32_t pre_bm = 0;
+    bool pre_in = false;
+    auto start_lookup = [&](int q) {
+      pre_q = q;
+      pre_in = false;
+      if (q >= nvalid || cell < 0) return;
+      const int4 o = s_off[q];
+      const int x = tx + o.x, y = ty + o.y, z = tz + o.z;
+      if (x < 0 || y < 0 || z < 0 || x >= nside || y >= nside || z >= nside) return;
+      pre_bm = morton_encode(x, y, z);
+      pre_a = sstart[(int64_t)pre_bm * span];
+      pre_b = sstart[(int64_t)(pre_bm + 1) * span];
+      pre_in = true;
+    };
+    auto row_for = [&](int q) -> int64_t {
+      if (q != cur_q) {
+        if (pre_q != q) start_lookup(q);
+        cur_row = (pre_in && pre_b > pre_a) ? ((int64_t)pre_bm * C + col) * KP : -1;
+        cur_q = q;
+        start_lookup(q + 1);
+      }
+      return cur_row;
+    };
+    // Fill stage s with K chunk `it`: row tid of A (hi, lo); rows tid, tid + 128 of B.
+    auto issue_loads = [&](int it, int s) {
+      unsigned char* st = base + s * stage_bytes;
+      const int q = it / kchunks, kc = it - q * kchunks;
+      const int64_t r = row_for(q);
+      const bool ok = r >= 0;
+      const float* gh = Ph + (ok ? r + kc * TC_KC : 0);
+      const float* gl = Pl + (ok ? r + kc * TC_KC : 0);
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        cp_async16(st + sw128_off(tid, j), gh + 4 * j, ok ? 16 : 0);
+        cp_async16(st + 16384 + sw128_off(tid, j), gl + 4 * j, ok ? 16 : 0);
+      }
+      const int opi = s_off[q].w;
+      const float* eh = Eh + (int64_t)opi * NP * KP + kc * TC_KC;
+      const float* el = El + (int64_t)opi * NP * KP + kc * TC_KC;
+      for (int n = tid; n < NP; n += TC_M) {
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          cp_async16(st + 32768 + sw128_off(n, j), eh + (int64_t)n * KP + 4 * j, 16);
+          cp_async16(st + 32768 + bbytes + sw128_off(n, j), el + (int64_t)n * KP + 4 * j, 16);
+        }
+      }
+    };
+
+    bool aborted = false;
+    int last = -1;  // thread 0: last iteration whose MMAs were committed
+#pragma unroll
+    for (int j = 0; j < NST - 1; ++j) {
+      if (j < niter) issue_loads(j, j);
+      cp_async_commit();
+    }
+    for (int it = 0; it < niter; ++it) {
+      const int s = it % NST;
+      asm volatile("cp.async.wait_group %0;\n" ::"n"(NST - 2) : "memory");  // loads of `it`
+      fence_async_smem();
+      asm volatile("bar.sync 1, 128;\n" ::: "memory");
+      const int g = it / group_iters;
+      const bool fresh = it == g * group_iters;
+      if (tid == 0) {
+        // accumulator g & 1 is free once the drain of group g - 2 is done
+        if (fresh && g >= 2 && !mbar_wait(&s_acce[g & 1], ((g - 2) >> 1) & 1, s_abort))
+          aborted = true;
+        if (!aborted) {
+          tc_fence_after();
+          const uint32_t a_hi = smem_u32(base + s * stage_bytes), a_lo = a_hi + 16384;
+          const uint32_t b_hi = a_hi + 32768, b_lo = b_hi + bbytes;
+          const uint32_t d = tmem + (uint32_t)((g & 1) * TC_TMEM_COLS);
+#pragma unroll
+          for (int k = 0; k < TC_KC / 8; ++k) {
+            const uint32_t off = k * 32;
+            tc_mma_tf32(d, sw128_desc(a_lo + off), sw128_desc(b_hi + off), idesc,
+                        (fresh && k == 0) ? 0u : 1u);
+            tc_mma_tf32(d, sw128_desc(a_hi + off), sw128_desc(b_lo + off), idesc, 1u);
+            tc_mma_tf32(d, sw128_desc(a_hi + off), sw128_desc(b_hi + off), idesc, 1u);
+          }
+          tc_commit(&s_bar[s]);
+          if (it + 1 == niter || it + 1 == (g + 1) * group_iters) tc_commit(&s_accf[g & 1]);
+          last = it;
+        }
+      }
+      // the stage of it - 1 can be refilled once its MMAs are done
+      if (!aborted && it >= 1 &&
+          !mbar_wait(&s_bar[(it - 1) % NST], ((it - 1) / NST) & 1, s_abort))
+        aborted = true;
+      if (producers_sync_or(aborted)) {
+        aborted = true;
+        break;
+      }
+      const int j = it + NST - 1;
+      if (j < niter) issue_loads(j, j % NST);
+      cp_async_commit();
+    }
+    if (aborted) *s_abort = 1;
+    // Before the TMEM is freed: MMAs complete in order, so the last commit
+    // covers all of them (waited for even after an abort, still bounded).
+    if (tid == 0 && last >= 0 && !mbar_wait(&s_bar[last % NST], (last / NST) & 1, nullptr))
+      *s_abort = 1;
+    cp_async_wait_all();
+  } else {
+    // ---------------------------------------------------------------- drainers
+    float* dst = cell >= 0 ? pf + ((int64_t)cell * C + col) * rf : nullptr;
+    const uint32_t lane_base = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
+    for (int g = 0; g < ngroups; ++g) {
+      const int b = g & 1;
+      if (!mbar_wait(&s_accf[b], (g >> 1) & 1, s_abort)) {
+        *s_abort = 1;
+        break;
+      }
+      tc_fence_after();
+      float v[16];
+      for (int n0 = 0; n0 < NP; n0 += 16) {
+        tc_ld16(lane_base + (uint32_t)(b * TC_TMEM_COLS + n0), v);
+        if (dst) {
+#pragma unroll
+          for (int i = 0; i < 16; ++i)
+            if (n0 + i < rf) dst[n0 + i] = g == 0 ? v[i] : dst[n0 + i] + v[i];
+        }
+      }
+      tc_fence_before();
+      mbar_arrive(&s_acce[b]);
+    }
+    if (ngroups == 0 && dst)  // no source in any interaction list of the tile
+      for (int n = 0; n < rf; ++n) dst[n] = 0.f;
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (tid == 0 && *s_abort) atomicExch(err, 1);
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem),
+                 "r"(2 * TC_TMEM_COLS)
+                 : "memory");
+  }
+}
+
+// Split the proxies of the listed source cells into TF32 hi / lo rows of KP
+// floats (zero padded from rs): thread per (row, k).
+__global__ void k_split_proxy(const int* __restrict__ cells, int64_t nrows, int C, int rs, int KP,
+                              const float* __restrict__ proxy, float* __restrict__ ph,
+                              float* __restrict__ pl) {
+  const int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+  if (e >= nrows * KP) return;
+  const int64_t r = e / KP;
+  const int k = (int)(e - r * KP);
+  const int64_t row = (int64_t)cells[r / C] * C + r % C;
+  const float v = k < rs ? proxy[row * rs + k] : 0.f;
+  const float h = to_tf32(v);
+  ph[row * KP + k] = h;
+  pl[row * KP + k] = to_tf32(v - h);
+}
+
+// Offsets per TMEM accumulation chain (PBBFMM_TC_GROUP overrides the default).
+static int tc_group() {
+  const char* e = getenv("PBBFMM_TC_GROUP");
+  const int g = e ? atoi(e) : 4;
+  return g < 1 ? 1 : (g > 189 ? 189 : g);
+}
+
+bool tc_eligible(const pbbfmm_tree* t) {
+  return t->p.use_chebyshev && t->use_tc && t->f_Eth && t->tc_np > 0 && t->tc_np <= kTcMaxN;
+}
+
+// Level l of the tensor-core M2L: split the proxies, then the MMA kernel.
+// proxy / pf are the level's float arrays (rows cell * C + col).
+int run_m2l_cheb_tc_level(pbbfmm_tree* t, int C, int l, int lvl, const float* proxy, float* pf,
+                          cudaStream_t st) {
+  const int L = t->p.tree_level, rf = t->ops.rf, rs = t->ops.rs;
+  const int NP = t->tc_np, KP = t->tc_kp;
+  Workspace& ws = t->ws;
+  const int* lists = ws.lists.as<int>();
+  if (C > TC_M) {
+    set_error("tensor-core M2L takes at most 128 columns per block");
+    return PBBFMM_ERR_UNSUPPORTED;
+  }
+  const int64_t per = cells_at(l) * C * KP;
+  if (int rc = grow(ws.tc_proxy, 2 * sizeof(float) * per)) return rc;
+  float* ph = ws.tc_proxy.as<float>();
+  float* pl = ph + per;
+  const int ns = t->lists.nsrc[l];
+  if (ns > 0) {
+    const int64_t nrows = (int64_t)ns * C;
+    if (int rc = kt_begin(t, KS_M2L_SPLIT, st)) return rc;
+    k_split_proxy<<<(unsigned)((nrows * KP + 255) / 256), 256, 0, st>>>(
+        lists + t->lists.src_off[l], nrows, C, rs, KP, proxy, ph, pl);
+    PB_LAUNCH("m2l_split");
+    if (int rc = kt_end(t, st)) return rc;
+  }
+  TcTiles tt;
+  const int per_tile = TC_M / C;
+  int tiles = 0;
+  for (int ty = 0; ty < 8; ++ty) {
+    tt.start[ty] = tiles;
+    tt.first[ty] = t->lists.ntyp[l][ty];
+    tt.count[ty] = t->lists.ntyp[l][ty + 1] - t->lists.ntyp[l][ty];
+    tiles += (tt.count[ty] + per_tile - 1) / per_tile;
+  }
+  tt.start[8] = tiles;
+  if (tiles == 0) return PBBFMM_OK;
+  // three stages when they fit in shared memory next to the static arrays
+  const int nst = tc_smem_bytes(NP, 3) + 8192 <= 232448 ? 3 : 2;
+  const int smem = tc_smem_bytes(NP, nst);
+  const int64_t eop = (int64_t)316 * NP * KP;
+  if (int rc = kt_begin(t, KS_M2L, st)) return rc;
+  if (nst == 3) {
+    PB_CUDA(cudaFuncSetAttribute(k_m2l_cheb_tc<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 smem));
+    k_m2l_cheb_tc<3><<<(unsigned)tiles, TC_THREADS, smem, st>>>(
+        rf, NP, KP, t->f_Eth + lvl * eop, t->f_Etl + lvl * eop, lists + t->lists.typ_off[l], tt,
+        C, l, ws.sstart.as<int>(), (int)cells_at(L - l), t->d_offs, ph, pl, pf, tc_group(),
+        t->d_tc_err);
+  } else {
+    PB_CUDA(cudaFuncSetAttribute(k_m2l_cheb_tc<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 smem));
+    k_m2l_cheb_tc<2><<<(unsigned)tiles, TC_THREADS, smem, st>>>(
+        rf, NP, KP, t->f_Eth + lvl * eop, t->f_Etl + lvl * eop, lists + t->lists.typ_off[l], tt,
+        C, l, ws.sstart.as<int>(), (int)cells_at(L - l), t->d_offs, ph, pl, pf, tc_group(),
+        t->d_tc_err);
+  }
+  PB_LAUNCH("m2l_cheb_tc");
+  return kt_end(t, st);
+}
+
+}  // namespace pbbfmm

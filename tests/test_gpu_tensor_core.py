@@ -1,0 +1,118 @@
+"""The Chebyshev M2L of the mixed path on the tensor cores (tcgen05, 3xTF32,
+float32 accumulation) against the float64 path and against the CUDA-core
+float32 kernel, through the C-ABI.
+
+Tolerance: 2e-6 relative L2 against float64 -- the bound the mixed path
+keeps everywhere (test_gpu_parity); 3xTF32 products carry ~2^-21 relative
+error each, and the TMEM accumulators are drained every few offsets."""
+import numpy as np
+import pytest
+
+import oracle
+import pbbfmm3d_b200 as fmm
+from helpers import make_tree, rel
+
+pytestmark = pytest.mark.gpu
+
+
+def _tree(kernel, param, level, order, eps):
+    t = make_tree(kernel, param, 1.0, level, order, eps, 1)
+    t.buildFMMTree()
+    return t
+
+
+def _run(t, p, w, ncols, precision, tc=True):
+    t.set_precision(precision)
+    t.set_tensor_cores(tc)
+    out = np.zeros(p.shape[0] * ncols)
+    fmm.H2_3D_Compute(t, p, p, w, ncols, out)
+    return out
+
+
+def _clustered(rng, n, blobs=16, sigma=0.03):
+    """90% of the points in Gaussian blobs, 10% uniform, clipped to the cube."""
+    nb = int(0.9 * n)
+    ctr = rng.uniform(-0.4, 0.4, (blobs, 3))
+    p = ctr[rng.integers(0, blobs, nb)] + sigma * rng.standard_normal((nb, 3))
+    p = np.clip(p, -0.5, 0.5)
+    return np.vstack([p, rng.uniform(-0.5, 0.5, (n - nb, 3))])
+
+
+CASES = [
+    # kernel, param, level, order, eps, ncols, clustered
+    ("Laplacian", 0.0, 4, 5, 1e-7, 1, False),
+    ("Laplacian", 0.0, 5, 6, 1e-7, 1, True),     # config-3 shape at 1/40 the size
+    ("GaussSigma", 0.1, 4, 4, 1e-6, 2, False),   # one operator set per level
+    ("OneOverR2", 0.0, 4, 4, 1e-5, 3, True),     # 42 targets x 3 columns per tile
+    ("Laplacian", 0.0, 3, 4, 1e-5, 64, False),   # two targets per tile
+    ("Laplacian", 0.0, 3, 7, 1e-9, 1, False),    # r_f near 256: two stages, N up to 256
+]
+
+
+@pytest.mark.parametrize("case", CASES, ids=[f"{c[0]}n{c[3]}C{c[5]}" for c in CASES])
+def test_tensor_core_m2l_matches_fp64(case):
+    kernel, param, level, order, eps, C, clustered = case
+    rng = np.random.default_rng(31)
+    N = 40000 if C < 8 else 3000
+    p = _clustered(rng, N) if clustered else rng.uniform(-0.5, 0.5, (N, 3))
+    w = rng.uniform(-1, 1, N * C)
+    t = _tree(kernel, param, level, order, eps)
+    o64 = _run(t, p, w, C, fmm.PREC_FP64)
+    o_tc = _run(t, p, w, C, fmm.PREC_MIXED, tc=True)
+    assert t.tensor_core_m2l() == (t.get_operators()["rf"] <= 256)
+    o_cc = _run(t, p, w, C, fmm.PREC_MIXED, tc=False)
+    assert rel(o_tc, o64) < 2e-6, rel(o_tc, o64)
+    assert rel(o_cc, o64) < 2e-6
+    assert rel(o_tc, o_cc) < 2e-6
+
+
+def test_tensor_core_locals_every_level():
+    """Locals F after the far field and L2L, level by level, mixed (tensor
+    cores) against float64."""
+    rng = np.random.default_rng(8)
+    N, C, level, n = 30000, 2, 4, 5
+    p = rng.uniform(-0.5, 0.5, (N, 3))
+    w = rng.standard_normal(N * C)
+    t = _tree("Laplacian", 0.0, level, n, 1e-7)
+    _run(t, p, w, C, fmm.PREC_FP64)
+    F64 = {l: t.debug_copy(1, l) for l in range(2, level + 1)}
+    _run(t, p, w, C, fmm.PREC_MIXED, tc=True)
+    for l in range(2, level + 1):
+        F = t.debug_copy(1, l)
+        assert rel(F, F64[l]) < 2e-6, (l, rel(F, F64[l]))
+
+
+def test_tensor_core_accuracy_against_direct_sum():
+    """Clustered Laplacian, Chebyshev n=6, eps 1e-7: the mixed result is as
+    close to the float64 direct sum as the float64 FMM is."""
+    rng = np.random.default_rng(77)
+    N = 100000
+    p = _clustered(rng, N, blobs=64, sigma=0.02)
+    w = rng.uniform(-1, 1, N)
+    t = _tree("Laplacian", 0.0, 5, 6, 1e-7)
+    o64 = _run(t, p, w, 1, fmm.PREC_FP64)
+    o_tc = _run(t, p, w, 1, fmm.PREC_MIXED)
+    rows = rng.choice(N, 1024, replace=False)
+    d = oracle.direct("Laplacian", [0.0], p, p, w, 1, rows=rows)
+    e64, etc = rel(o64[rows], d), rel(o_tc[rows], d)
+    assert etc < 1.05 * e64 + 1e-6, (etc, e64)
+
+
+def test_tensor_core_kernel_times_and_switch():
+    rng = np.random.default_rng(3)
+    p = rng.uniform(-0.5, 0.5, (5000, 3))
+    w = rng.standard_normal(5000)
+    t = _tree("Laplacian", 0.0, 3, 4, 1e-5)
+    t.set_timing(True)
+    t.reset_kernel_times()
+    _run(t, p, w, 1, fmm.PREC_MIXED, tc=True)
+    kt = t.kernel_times()
+    assert kt["m2l_split"][1] > 0 and kt["m2l"][1] > 0
+    t.reset_kernel_times()
+    _run(t, p, w, 1, fmm.PREC_MIXED, tc=False)
+    kt = t.kernel_times()
+    assert kt["m2l_split"][1] == 0 and kt["m2l"][1] > 0
+    t.set_tensor_cores(True)
+    assert t.tensor_core_m2l()
+    t.set_tensor_cores(False)
+    assert not t.tensor_core_m2l()
