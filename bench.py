@@ -10,6 +10,11 @@ K = exp(-r/0.3), N = 1,000,000 points uniform in the unit cube (sources =
 targets), nCols = 8 weights N(0,1), tree_level 6, uniform interpolation order
 5 with FFT M2L (use_chebyshev = 0).  Synthetic seeded data.
 
+The same line carries a "target_config" block for the clustered Laplacian
+workload (N = 4,000,000, 90% in 64 Gaussian blobs, Chebyshev order 6,
+eps 1e-7, tree_level 7, nCols 1) whose mixed path runs the M2L on the tensor
+cores; --no-target skips it, --workload clustered makes it the headline.
+
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
 One JSON line on rank 0.  Multi-GPU (torchrun): every rank runs its own
@@ -37,13 +42,22 @@ sys.path.insert(0, ROOT)
 
 WORKLOADS = {
     # the configuration the metric is quoted on
-    "bench": dict(name="expcov0.3_unif5_N1e6_C8_L6", kernel="ExpCov", ell=0.3, N=1_000_000, C=8,
-                  L=6, n=5, cheb=0, eps=1e-5, box=1.0, seed=1234),
-    # small case of the same kernels for ncu captures (~4.5 GB on the device)
-    "profile": dict(name="expcov0.3_unif5_N262144_C8_L5", kernel="ExpCov", ell=0.3, N=262_144,
-                    C=8, L=5, n=5, cheb=0, eps=1e-5, box=1.0, seed=1234),
+    "bench": dict(name="expcov0.3_unif5_N1e6_C8_L6", kernel="ExpCov", param=0.3, N=1_000_000,
+                  C=8, L=6, n=5, cheb=0, eps=1e-5, box=1.0, seed=1234, dist="uniform",
+                  weights="normal"),
+    # the mixed-precision target: clustered Laplacian, Chebyshev order 6 (tensor-core M2L)
+    "clustered": dict(name="laplace_cheb6_clustered_N4e6_C1_L7", kernel="Laplacian", param=0.0,
+                      N=4_000_000, C=1, L=7, n=6, cheb=1, eps=1e-7, box=1.0, seed=4321,
+                      dist="clustered", weights="uniform"),
+    # small cases of the same kernels for ncu captures (a few GB on the device)
+    "profile": dict(name="expcov0.3_unif5_N262144_C8_L5", kernel="ExpCov", param=0.3, N=262_144,
+                    C=8, L=5, n=5, cheb=0, eps=1e-5, box=1.0, seed=1234, dist="uniform",
+                    weights="normal"),
+    "profile_cheb": dict(name="laplace_cheb6_clustered_N5e5_C1_L6", kernel="Laplacian", param=0.0,
+                         N=500_000, C=1, L=6, n=6, cheb=1, eps=1e-7, box=1.0, seed=4321,
+                         dist="clustered", weights="uniform"),
 }
-WORKLOAD = WORKLOADS["bench"]
+KERNEL_TEXT = {"ExpCov": "exp(-r/%g)", "Laplacian": "1/r (0 at r=0)"}
 # bounded CPU sample: same kernel, order, columns and points per leaf (N / 8^L)
 CPU_SAMPLE = dict(N=15_625, L=4)
 N_SAMPLED_TARGETS = 4096
@@ -54,11 +68,36 @@ def log(*a):
 
 
 def gen_inputs(wl, rank=0):
+    """Seeded points in the unit cube -- uniform, or 90% from 64 isotropic
+    Gaussian blobs (centres uniform in [0.1, 0.9]^3, sigma 0.02, clipped to
+    the cube) plus 10% uniform background -- and column-major weights."""
     rng = np.random.default_rng(wl["seed"])
-    pts = rng.uniform(0.0, 1.0, (wl["N"], 3))
+    N = wl["N"]
+    if wl["dist"] == "uniform":
+        pts = rng.uniform(0.0, 1.0, (N, 3))
+    else:
+        nb = int(0.9 * N)
+        ctr = rng.uniform(0.1, 0.9, (64, 3))
+        blob = ctr[rng.integers(0, 64, nb)] + 0.02 * rng.standard_normal((nb, 3))
+        pts = np.vstack([np.clip(blob, 0.0, 1.0), rng.uniform(0.0, 1.0, (N - nb, 3))])
     wr = np.random.default_rng(wl["seed"] + 1000 + rank)
-    w = wr.standard_normal(wl["N"] * wl["C"])  # column-major N x C
+    if wl["weights"] == "normal":
+        w = wr.standard_normal(N * wl["C"])
+    else:
+        w = wr.uniform(-1.0, 1.0, N * wl["C"])
     return pts, w
+
+
+def make_tree(fmm, wl, device):
+    if wl["kernel"] == "ExpCov":
+        return fmm.kernel_ExpCov(wl["box"], wl["L"], wl["n"], wl["eps"], wl["cheb"],
+                                 ell=wl["param"], device=device)
+    return fmm.kernel_Laplacian(wl["box"], wl["L"], wl["n"], wl["eps"], wl["cheb"], device=device)
+
+
+def kernel_text(wl):
+    t = KERNEL_TEXT[wl["kernel"]]
+    return t % wl["param"] if "%" in t else t
 
 
 # ---------------------------------------------------------------- clocks
@@ -114,8 +153,9 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------ helpers
-def direct_sum_sampled(pts, w, C, rows, ell, device):
-    """float64 direct sum exp(-r/ell) at the sampled target rows (torch, GPU)."""
+def direct_sum_sampled(pts, w, C, rows, wl, device):
+    """float64 direct sum of the workload's kernel at the sampled target rows
+    (torch on the GPU; a coincident point contributes 0, as in the FMM)."""
     import torch
 
     P = torch.tensor(pts, device=device)
@@ -124,7 +164,11 @@ def direct_sum_sampled(pts, w, C, rows, ell, device):
     out = torch.zeros(C, len(rows), dtype=torch.float64, device=device)
     for a in range(0, P.shape[0], 1 << 16):
         d = torch.cdist(T, P[a:a + (1 << 16)])
-        out += W[:, a:a + (1 << 16)] @ torch.exp(-d / ell).T
+        if wl["kernel"] == "ExpCov":
+            k = torch.exp(-d / wl["param"])
+        else:
+            k = torch.where(d > 0, 1.0 / d, torch.zeros_like(d))
+        out += W[:, a:a + (1 << 16)] @ k.T
     return out.cpu().numpy()
 
 
@@ -181,7 +225,7 @@ def cpu_sample_run(wl, steps, warmup, threads):
     Ns = CPU_SAMPLE["N"]
     pts = rng.uniform(0.0, 1.0, (Ns, 3))
     w = rng.standard_normal(Ns * wl["C"])
-    out, timing, wd = oracle.run_reference(wl["kernel"], wl["ell"], wl["box"], CPU_SAMPLE["L"],
+    out, timing, wd = oracle.run_reference(wl["kernel"], wl["param"], wl["box"], CPU_SAMPLE["L"],
                                            wl["n"], wl["eps"], wl["cheb"], pts, w, wl["C"],
                                            repeat=warmup + steps, threads=threads)
     times = timing["matvec_s"][warmup:]
@@ -209,8 +253,8 @@ def reference_arm(args, rank):
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded uniform points, N(0,1) weights)",
         "config": {"workload": wl["name"], "sample_N": CPU_SAMPLE["N"],
-                   "sample_tree_level": CPU_SAMPLE["L"], "kernel": "exp(-r/0.3)",
-                   "interpolation": "uniform n=5, FFT M2L", "nCols": wl["C"]},
+                   "sample_tree_level": CPU_SAMPLE["L"], "kernel": kernel_text(wl),
+                   "interpolation_order": wl["n"], "use_chebyshev": wl["cheb"], "nCols": wl["C"]},
         "cpu_baseline": {"value": value, "unit": "N*nCols/s", "cores": th, "kind": "reference",
                          "sample": sample},
         "e2e": {"value": value, "unit": "N*nCols/s", "h2d_bytes_per_step": 0,
@@ -221,41 +265,13 @@ def reference_arm(args, rank):
 
 
 # ------------------------------------------------------------ our arm
-def our_arm(args, rank, world, local_rank):
-    import torch
-
-    import pbbfmm3d_b200 as fmm
-
-    wl = WORKLOADS[args.workload]
-    dev = torch.device("cuda", local_rank)
-    torch.cuda.set_device(dev)
-    dist = None
-    if world > 1:
-        import torch.distributed as dist  # noqa: F811
-
-    pts, w = gen_inputs(wl, rank)
-    N, C = wl["N"], wl["C"]
-    t0 = time.time()
-    tree = fmm.kernel_ExpCov(wl["box"], wl["L"], wl["n"], wl["eps"], wl["cheb"], ell=wl["ell"],
-                             device=local_rank)
-    tree.buildFMMTree()
-    log("precompute %.2fs" % (time.time() - t0))
-
-    d_pts = torch.tensor(pts, device=dev)
-    d_w = torch.tensor(w, device=dev)
-    d_out = torch.zeros(N * C, dtype=torch.float64, device=dev)
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > L2 (126 MB)
-    stream = torch.cuda.current_stream(dev)
-
-    def step(prec):
-        fmm.compute_device(tree, d_pts, d_pts, d_w, C, d_out, precision=prec,
-                           stream=stream.cuda_stream)
-
-    precisions = [("fp64", fmm.PREC_FP64), ("mixed", fmm.PREC_MIXED)]
+def time_precisions(fmm, torch, dist, tree, step, flush, args, world, local_rank):
+    """Warm-up, then exactly args.steps timed steps per precision (CUDA events
+    on the launching stream, L2 flushed between steps outside the events,
+    kernel timer and clocks sampled during the timed region)."""
     results = {}
-    for pname, prec in precisions:
+    for pname, prec in (("fp64", fmm.PREC_FP64), ("mixed", fmm.PREC_MIXED)):
         for _ in range(args.warmup):
-            d_out.zero_()
             step(prec)
         torch.cuda.synchronize()
         tree.set_timing(True)
@@ -266,6 +282,7 @@ def our_arm(args, rank, world, local_rank):
             dist.barrier()
         torch.cuda.synchronize()
         sampler.start()
+        stream = torch.cuda.current_stream()
         evs = []
         for _ in range(args.steps):
             flush.fill_(1.0)  # evict L2 between timed steps (outside the step events)
@@ -285,26 +302,136 @@ def our_arm(args, rank, world, local_rank):
         tree.set_timing(False)
         total_ms = sum(step_ms)
         if world > 1:
-            tt = torch.tensor([total_ms], device=dev)
+            tt = torch.tensor([total_ms], device="cuda")
             dist.all_reduce(tt, op=dist.ReduceOp.MAX)
             total_ms = float(tt.item())
         results[pname] = dict(total_ms=total_ms, step_ms=step_ms, ktimes=ktimes, clocks=clocks,
                               launches=launches)
-    # accuracy vs FP64 direct sum on sampled targets (outside the timed region)
+    return results
+
+
+def sampled_errors(fmm, torch, step, d_out, pts, w, wl, dev):
+    """rel-L2 error of each precision against the float64 direct sum on
+    N_SAMPLED_TARGETS seeded targets (outside the timed region)."""
+    N, C = wl["N"], wl["C"]
     rng = np.random.default_rng(7)
     rows = np.sort(rng.choice(N, N_SAMPLED_TARGETS, replace=False))
-    ref = direct_sum_sampled(pts, w, C, rows, wl["ell"], dev)
+    ref = direct_sum_sampled(pts, w, C, rows, wl, dev)
     errs = {}
-    for pname, prec in precisions:
-        d_out.zero_()
+    for pname, prec in (("fp64", fmm.PREC_FP64), ("mixed", fmm.PREC_MIXED)):
         step(prec)
         out = d_out.view(C, N)[:, torch.tensor(rows, device=dev)].cpu().numpy()
         errs[pname] = float(np.linalg.norm(out - ref) / np.linalg.norm(ref))
+    return errs
 
-    # end to end through the host-buffer public API (H2_3D_Compute)
+
+def per_step(kt, steps):
+    return {k: v[0] / steps for k, v in kt.items() if v[1]}
+
+
+def unif_roofline(fmm, tree, wl, results, steps, local_rank):
+    """Frequency-domain M2L (k_m2l_unif_mac): one complex MAC (8 flops) per
+    (M2L pair, frequency, column); float32 FMA throughput bounds it."""
+    kt = results["mixed"]["ktimes"]
+    tstart = tree.debug_copy(2).astype(np.int64)
+    pairs = interaction_pairs(tstart, wl["L"])
+    n, C = wl["n"], wl["C"]
+    m = 2 * n - 1
+    nk = m * m * n
+    flops = sum(pairs.values()) * nk * C * 8.0
+    nonempty = {l: int((np.diff(tstart).reshape(-1, 8 ** (wl["L"] - l)).sum(1) > 0).sum())
+                for l in range(2, wl["L"] + 1)}
+    nbytes = sum(2 * nonempty[l] * nk * C * 8 for l in nonempty)  # float2: read X^, write Y^
+    peaks, peak_kind = load_peaks()
+    fp64_peak = fmm.measure_fma_peak(local_rank, fmm.PREC_FP64)
+    fp32_peak = fmm.measure_fma_peak(local_rank, fmm.PREC_MIXED)
+    mac_ms = kt["m2l_mac"][0] / steps
+    mac64_ms = results["fp64"]["ktimes"]["m2l_mac"][0] / steps
+    achieved = flops / (mac_ms * 1e-3) / 1e12
+    return {
+        "kernel": "k_m2l_unif_mac<float> (frequency-domain M2L, mixed path)",
+        "bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+        "frac": achieved / fp32_peak, "traffic": None,
+        "peak_source": "measured in this run: float32 FMA loop on every SM "
+                       "(pbbfmm_measure_fma_peak); the kernel runs on the CUDA cores, so neither "
+                       "the HBM copy nor the bf16 tensor figure of MEASURED_PEAKS.json bounds it",
+        "fp64_path": {"achieved": flops / (mac64_ms * 1e-3) / 1e12, "peak": fp64_peak,
+                      "frac": flops / (mac64_ms * 1e-3) / 1e12 / fp64_peak, "unit": "TFLOP/s"},
+        "algorithmic": "%.4g flops per step = %d M2L pairs x %d freqs x %d cols x 8" % (
+            flops, sum(pairs.values()), nk, C),
+        "launches_per_step": kt["m2l_mac"][1] / steps,
+        "hbm": {"achieved": nbytes / (mac_ms * 1e-3) / 1e9, "peak": peaks["hbm_gbs"],
+                "unit": "GB/s", "frac": nbytes / (mac_ms * 1e-3) / 1e9 / peaks["hbm_gbs"],
+                "algorithmic_bytes": nbytes, "peak_kind": peak_kind},
+    }
+
+
+def cheb_roofline(fmm, tree, wl, results, steps, local_rank):
+    """Chebyshev M2L on the tensor cores (k_m2l_cheb_tc, 3xTF32): useful work
+    2 rf rs flops per (M2L pair, column); the tensor pipe issues three TF32
+    products per useful one, over padded tiles."""
+    kt = results["mixed"]["ktimes"]
+    tstart = tree.debug_copy(2).astype(np.int64)
+    pairs = interaction_pairs(tstart, wl["L"])
+    ops = tree.get_operators()
+    rf, rs, C = ops["rf"], ops["rs"], wl["C"]
+    flops = sum(pairs.values()) * rf * rs * C * 2.0
+    peaks, peak_kind = load_peaks()
+    tf32_peak = peaks["bf16_tflops"] / 2.0
+    ms = kt["m2l"][0] / steps
+    ms64 = results["fp64"]["ktimes"]["m2l"][0] / steps
+    achieved = flops / (ms * 1e-3) / 1e12
+    fp64_peak = fmm.measure_fma_peak(local_rank, fmm.PREC_FP64)
+    on_tc = tree.tensor_core_m2l()
+    return {
+        "kernel": "k_m2l_cheb_tc (tcgen05 kind::tf32, 3xTF32 split, TMEM accumulators)"
+                  if on_tc else "k_m2l_cheb<float> (CUDA cores)",
+        "bound": "tensor" if on_tc else "fp32", "achieved": achieved, "peak": tf32_peak,
+        "unit": "TFLOP/s", "frac": achieved / tf32_peak, "traffic": None,
+        "peak_source": "dense TF32 = half the %s bf16 tensor figure of MEASURED_PEAKS.json "
+                       "(%.0f TFLOP/s)" % (peak_kind, peaks["bf16_tflops"]),
+        "tensor_pipe_issued_frac": 3.0 * achieved / tf32_peak,
+        "algorithmic": "%.4g useful flops per step = %d M2L pairs x rf %d x rs %d x %d cols x 2"
+                       % (flops, sum(pairs.values()), rf, rs, C),
+        "launches_per_step": kt["m2l"][1] / steps,
+        "fp64_path": {"kernel": "k_m2l_cheb<double> (CUDA cores)",
+                      "achieved": flops / (ms64 * 1e-3) / 1e12, "peak": fp64_peak,
+                      "frac": flops / (ms64 * 1e-3) / 1e12 / fp64_peak, "unit": "TFLOP/s"},
+    }
+
+
+def run_workload(wl, args, rank, world, local_rank, e2e_wanted):
+    import torch
+
+    import pbbfmm3d_b200 as fmm
+
+    dev = torch.device("cuda", local_rank)
+    dist = None
+    if world > 1:
+        import torch.distributed as dist  # noqa: F811
+    pts, w = gen_inputs(wl, rank)
+    N, C = wl["N"], wl["C"]
+    t0 = time.time()
+    tree = make_tree(fmm, wl, local_rank)
+    tree.buildFMMTree()
+    log("%s: precompute %.2fs" % (wl["name"], time.time() - t0))
+    d_pts = torch.tensor(pts, device=dev)
+    d_w = torch.tensor(w, device=dev)
+    d_out = torch.zeros(N * C, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)  # > L2 (126 MB)
+    stream = torch.cuda.current_stream(dev)
+
+    def step(prec):
+        d_out.zero_()
+        fmm.compute_device(tree, d_pts, d_pts, d_w, C, d_out, precision=prec,
+                           stream=stream.cuda_stream)
+
+    results = time_precisions(fmm, torch, dist, tree, step, flush, args, world, local_rank)
+    errs = sampled_errors(fmm, torch, step, d_out, pts, w, wl, dev)
+
     e2e = None
     tree.set_precision(fmm.PREC_MIXED)
-    if not args.no_e2e:
+    if e2e_wanted:
         host_out = np.zeros(N * C)
         fmm.H2_3D_Compute(tree, pts, pts, w, C, host_out)  # warm-up
         if world > 1:
@@ -323,44 +450,49 @@ def our_arm(args, rank, world, local_rank):
         e2e = {"value": world * N * C / e2e_s, "unit": "N*nCols/s",
                "h2d_bytes_per_step": int(8 * (3 * N + N * C + N * C)),
                "d2h_bytes_per_step": int(8 * N * C), "ms_per_step": 1e3 * e2e_s,
-               "api": "pbbfmm_compute (host buffers, pageable)"}
-
-    # roofline of the dominant kernel (headline = mixed path)
-    r = results["mixed"]
+               "api": "H2_3D_Compute -> pbbfmm_compute (host buffers, pageable)"}
+    roof = (cheb_roofline if wl["cheb"] else unif_roofline)(fmm, tree, wl, results, args.steps,
+                                                             local_rank)
+    r, r64 = results["mixed"], results["fp64"]
+    value = world * N * C * args.steps / (r["total_ms"] * 1e-3)
+    value64 = world * N * C * args.steps / (r64["total_ms"] * 1e-3)
     kt = r["ktimes"]
-    dom = max(kt, key=lambda k: kt[k][0])
-    tstart = tree.debug_copy(2).astype(np.int64)
-    pairs = interaction_pairs(tstart, wl["L"])
-    n, m = wl["n"], 2 * wl["n"] - 1
-    nk = m * m * n
-    mac_flops = sum(pairs.values()) * nk * C * 8.0  # one complex MAC = 8 flops
-    nonempty = {l: int((np.diff(tstart).reshape(-1, 8 ** (wl["L"] - l)).sum(1) > 0).sum())
-                for l in range(2, wl["L"] + 1)}
-    mac_bytes = sum(2 * nonempty[l] * nk * C * 16 for l in nonempty)  # read X^, write Y^
-    peaks, peak_kind = load_peaks()
-    fp64_peak = fmm.measure_fma_peak(local_rank, fmm.PREC_FP64)
-    fp32_peak = fmm.measure_fma_peak(local_rank, fmm.PREC_MIXED)
-    mac_ms = kt["m2l_mac"][0] / args.steps
-    mac_launches = kt["m2l_mac"][1] / args.steps
-    achieved_tf = mac_flops / (mac_ms * 1e-3) / 1e12
-    mac64_ms = results["fp64"]["ktimes"]["m2l_mac"][0] / args.steps
-    roofline = {
-        "kernel": "k_m2l_unif_mac<float> (frequency-domain M2L, mixed path)",
-        "bound": "fp32", "achieved": achieved_tf, "peak": fp32_peak, "unit": "TFLOP/s",
-        "frac": achieved_tf / fp32_peak, "traffic": None,
-        "peak_source": "measured in this run: float32 FMA loop on every SM (pbbfmm_measure_fma_peak); "
-                       "MEASURED_PEAKS.json has only HBM copy and bf16 tensor figures",
-        "fp64_path": {"achieved": mac_flops / (mac64_ms * 1e-3) / 1e12, "peak": fp64_peak,
-                      "frac": mac_flops / (mac64_ms * 1e-3) / 1e12 / fp64_peak,
-                      "unit": "TFLOP/s"},
-        "algorithmic": "%.4g flops per step = %d M2L pairs x %d freqs x %d cols x 8" % (
-            mac_flops, sum(pairs.values()), nk, C),
-        "launches_per_step": mac_launches,
-        "hbm": {"achieved": mac_bytes / (mac_ms * 1e-3) / 1e9, "peak": peaks["hbm_gbs"],
-                "unit": "GB/s", "frac": mac_bytes / (mac_ms * 1e-3) / 1e9 / peaks["hbm_gbs"],
-                "algorithmic_bytes": mac_bytes, "peak_kind": peak_kind},
+    out = {
+        "value": value, "ms_per_step": r["total_ms"] / args.steps, "rel_l2_err": errs["mixed"],
+        "fp64": {"value": value64, "unit": "N*nCols/s", "ms_per_step": r64["total_ms"] / args.steps,
+                 "rel_l2_err": errs["fp64"], "phase_ms_per_step": per_step(r64["ktimes"], args.steps)},
+        "mixed_over_fp64": value / value64,
+        "phase_ms_per_step": per_step(kt, args.steps),
+        "dominant_kernel": max(kt, key=lambda k: kt[k][0]),
+        "roofline": roof, "e2e": e2e,
+        "gpu_launches": int(r["launches"]), "gpu_launches_per_step": r["launches"] / args.steps,
+        "clocks": r["clocks"],
+        "config": {"workload": wl["name"], "N": N, "nCols": C, "tree_level": wl["L"],
+                   "interpolation_order": wl["n"], "use_chebyshev": wl["cheb"],
+                   "epsilon": wl["eps"], "kernel": kernel_text(wl), "points": wl["dist"],
+                   "precision": "mixed: float32 interpolation and near field with compensated "
+                                "sums, %s, float64 positions, operators and output" % (
+                                    "3xTF32 tensor-core M2L" if wl["cheb"] else "float32 FFT M2L"),
+                   "l2": "256 MB buffer written between timed steps",
+                   "parallelism": "independent column blocks per rank" if world > 1 else "1 GPU"},
     }
+    tree.close()
+    return out
 
+
+def our_arm(args, rank, world, local_rank):
+    import torch
+
+    torch.cuda.set_device(local_rank)
+    wl = WORKLOADS[args.workload]
+    head = run_workload(wl, args, rank, world, local_rank, not args.no_e2e)
+    target = None
+    if args.workload == "bench" and not args.no_target:
+        t = run_workload(WORKLOADS["clustered"], args, rank, world, local_rank, False)
+        target = {k: t[k] for k in ("config", "value", "ms_per_step", "rel_l2_err", "fp64",
+                                    "mixed_over_fp64", "phase_ms_per_step", "dominant_kernel",
+                                    "roofline", "gpu_launches_per_step", "clocks")}
+        target["unit"] = "N*nCols/s"
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -372,39 +504,29 @@ def our_arm(args, rank, world, local_rank):
         except Exception as e:  # noqa: BLE001
             cpu = {"value": None, "unit": "N*nCols/s", "cores": 0, "kind": "reference",
                    "sample": "failed: %s" % e}
-
     if rank != 0:
         return 0
-    value = world * N * C * args.steps / (r["total_ms"] * 1e-3)
-    r64 = results["fp64"]
-    value64 = world * N * C * args.steps / (r64["total_ms"] * 1e-3)
     line = {
         "metric": "FMM matvec N*nCols/s (rel-L2 vs FP64 direct sum on 4096 sampled targets)",
-        "value": value, "unit": "N*nCols/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": r["total_ms"] / args.steps, "higher_is_better": True,
+        "value": head["value"], "unit": "N*nCols/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic: seeded uniform points in the unit cube, N(0,1) weights",
-        "config": {"workload": wl["name"], "N": N, "nCols": C, "tree_level": wl["L"],
-                   "interpolation_order": wl["n"], "use_chebyshev": 0, "kernel": "exp(-r/0.3)",
-                   "precision": "mixed: float32 far field and interpolation with compensated "
-                                "sums, float64 positions, operators and output",
-                   "l2": "256 MB buffer written between timed steps",
-                   "parallelism": "independent 8-column blocks per rank" if world > 1 else "1 GPU"},
-        "rel_l2_err": errs["mixed"],
-        "fp64": {"value": value64, "unit": "N*nCols/s", "ms_per_step": r64["total_ms"] / args.steps,
-                 "rel_l2_err": errs["fp64"],
-                 "phase_ms_per_step": {k: v[0] / args.steps for k, v in r64["ktimes"].items()
-                                       if v[1]}},
-        "mixed_over_fp64": value / value64,
-        "phase_ms_per_step": {k: v[0] / args.steps for k, v in kt.items() if v[1]},
-        "dominant_kernel": dom,
-        "roofline": roofline,
+        "data": "synthetic: seeded %s points in the unit cube, %s weights" % (
+            wl["dist"], "N(0,1)" if wl["weights"] == "normal" else "U[-1,1]"),
+        "config": head["config"],
+        "rel_l2_err": head["rel_l2_err"], "fp64": head["fp64"],
+        "mixed_over_fp64": head["mixed_over_fp64"],
+        "phase_ms_per_step": head["phase_ms_per_step"],
+        "dominant_kernel": head["dominant_kernel"],
+        "roofline": head["roofline"],
         "cpu_baseline": cpu,
-        "e2e": e2e,
-        "gpu_launches": int(r["launches"] / args.steps) * args.steps,
-        "gpu_launches_per_step": r["launches"] / args.steps,
-        "clocks": r["clocks"],
+        "e2e": head["e2e"],
+        "gpu_launches": head["gpu_launches"],
+        "gpu_launches_per_step": head["gpu_launches_per_step"],
+        "clocks": head["clocks"],
     }
+    if target is not None:
+        line["target_config"] = target
     print(json.dumps(line))
     return 0
 
@@ -417,6 +539,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-target", action="store_true",
+                    help="skip the clustered Chebyshev (tensor-core) workload block")
     ap.add_argument("--workload", default="bench", choices=sorted(WORKLOADS))
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))

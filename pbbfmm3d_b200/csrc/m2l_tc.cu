@@ -29,7 +29,7 @@ namespace pbbfmm {
 constexpr int TC_M = 128;
 constexpr int TC_KC = 32;          // K per stage: one 128-byte swizzle row of float32
 constexpr int TC_THREADS = 256;    // warps 0-3 producers, warps 4-7 drainers
-constexpr int TC_TMEM_COLS = 256;  // columns of one accumulator
+constexpr int TC_TMEM_COLS = 512;  // columns allocated (accumulators and running sum)
 constexpr unsigned long long kWaitNs = 1000000000ull;  // 1 s
 constexpr long long kWaitIters = 1ll << 26;
 
@@ -148,6 +148,23 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, float* v) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// Store 16 consecutive float32 columns of this thread's TMEM lane.
+__device__ __forceinline__ void tc_st16(uint32_t taddr, const float* v) {
+  asm volatile(
+      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
+      "%11, %12, %13, %14, %15, %16};\n" ::"r"(taddr),
+      "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
+      "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
+      "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])), "r"(__float_as_uint(v[8])),
+      "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
+      "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])),
+      "r"(__float_as_uint(v[15]))
+      : "memory");
+}
+__device__ __forceinline__ void tc_wait_st() {
+  asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory");
+}
+
 __device__ __forceinline__ float to_tf32(float x) {
   uint32_t r;
   asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
@@ -167,16 +184,22 @@ __host__ __device__ constexpr int tc_smem_bytes(int NP, int nst) {
   return nst * tc_stage_bytes(NP) + 1024;
 }
 
+// TMEM columns (512 allocated): accumulator b at b * stride; when three
+// regions fit (N <= 160), a running sum at 2 * stride that the drains update
+// inside TMEM, so that pf is written once; otherwise drains add into pf.
+__host__ __device__ constexpr int tc_acc_stride(int NP) { return NP <= 160 ? (NP + 31) / 32 * 32 : 256; }
+__host__ __device__ constexpr bool tc_sum_in_tmem(int NP) { return NP <= 160; }
+
 // One CTA per tile of 128 (target, col) rows of one child type; NST stages.
 //   Eh, El : [316][NP][KP] hi / lo of E_o^T (row f holds E_o[f][s] over s), zero padded
 //   Ph, Pl : proxy hi / lo, row (cell * C + col) of KP floats, zero padded
 //   pf     : output rows (cell * C + col) of rf floats
 // Warps 0-3 (producers) look up source rows, fill the stages with cp.async
-// and thread 0 issues the MMAs.  Two TMEM accumulators of 256 columns take
-// turns, one per group of `group` consecutive offsets, so that every float32
-// accumulation chain inside the tensor pipe spans at most `group` offsets;
-// warps 4-7 (drainers) add each finished accumulator into pf while the MMAs
-// of the next group run.
+// and thread 0 issues the MMAs.  Two TMEM accumulators take turns, one per
+// group of `group` consecutive offsets, so that every float32 accumulation
+// chain inside the tensor pipe spans at most `group` offsets; warps 4-7
+// (drainers) add each finished accumulator into the running sum while the
+// MMAs of the next group run.
 //   s_bar[s]  : MMAs of the stage's last fill done (tcgen05.commit)
 //   s_accf[b] : MMAs of accumulator b's group done (tcgen05.commit)
 //   s_acce[b] : accumulator b drained (128 drainer arrivals)
@@ -229,10 +252,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     s_xyz[tid] = (tx << 20) | (ty << 10) | tz;
   }
   if (tid < 6) s_valid[tid] = 0;
-  if (warp == 0) {  // two accumulators: 128 lanes x 2 x 256 float32 columns
+  if (warp == 0) {  // 128 lanes x 512 float32 columns
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
                      smem_u32(&s_tmem)),
-                 "r"(2 * TC_TMEM_COLS)
+                 "r"(TC_TMEM_COLS)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
   }
@@ -354,7 +377,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
           tc_fence_after();
           const uint32_t a_hi = smem_u32(base + s * stage_bytes), a_lo = a_hi + 16384;
           const uint32_t b_hi = a_hi + 32768, b_lo = b_hi + bbytes;
-          const uint32_t d = tmem + (uint32_t)((g & 1) * TC_TMEM_COLS);
+          const uint32_t d = tmem + (uint32_t)((g & 1) * tc_acc_stride(NP));
 #pragma unroll
           for (int k = 0; k < TC_KC / 8; ++k) {
             const uint32_t off = k * 32;
@@ -390,6 +413,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     // ---------------------------------------------------------------- drainers
     float* dst = cell >= 0 ? pf + ((int64_t)cell * C + col) * rf : nullptr;
     const uint32_t lane_base = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
+    const int astride = tc_acc_stride(NP);
+    const bool tsum = tc_sum_in_tmem(NP);
+    const uint32_t sum_base = lane_base + (uint32_t)(2 * astride);
     for (int g = 0; g < ngroups; ++g) {
       const int b = g & 1;
       if (!mbar_wait(&s_accf[b], (g >> 1) & 1, s_abort)) {
@@ -397,15 +423,30 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         break;
       }
       tc_fence_after();
-      float v[16];
+      const bool final_group = g + 1 == ngroups;
+      float v[16], u[16];
       for (int n0 = 0; n0 < NP; n0 += 16) {
-        tc_ld16(lane_base + (uint32_t)(b * TC_TMEM_COLS + n0), v);
-        if (dst) {
+        tc_ld16(lane_base + (uint32_t)(b * astride + n0), v);
+        if (tsum) {
+          if (g > 0) {
+            tc_ld16(sum_base + (uint32_t)n0, u);
+#pragma unroll
+            for (int i = 0; i < 16; ++i) v[i] += u[i];
+          }
+          if (!final_group) {
+            tc_st16(sum_base + (uint32_t)n0, v);
+          } else if (dst) {
+#pragma unroll
+            for (int i = 0; i < 16; ++i)
+              if (n0 + i < rf) dst[n0 + i] = v[i];
+          }
+        } else if (dst) {
 #pragma unroll
           for (int i = 0; i < 16; ++i)
             if (n0 + i < rf) dst[n0 + i] = g == 0 ? v[i] : dst[n0 + i] + v[i];
         }
       }
+      if (tsum && !final_group) tc_wait_st();
       tc_fence_before();
       mbar_arrive(&s_acce[b]);
     }
@@ -418,7 +459,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   if (warp == 0) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem),
-                 "r"(2 * TC_TMEM_COLS)
+                 "r"(TC_TMEM_COLS)
                  : "memory");
   }
 }
