@@ -163,7 +163,9 @@ def direct_sum_sampled(pts, w, C, rows, wl, device):
     T = P[torch.tensor(rows, device=device)]
     out = torch.zeros(C, len(rows), dtype=torch.float64, device=device)
     for a in range(0, P.shape[0], 1 << 16):
-        d = torch.cdist(T, P[a:a + (1 << 16)])
+        # exact per-pair distances: the matrix-product form of cdist turns a
+        # coincident pair into ~1e-9, which 1/r would blow up
+        d = torch.cdist(T, P[a:a + (1 << 16)], compute_mode="donot_use_mm_for_euclid_dist")
         if wl["kernel"] == "ExpCov":
             k = torch.exp(-d / wl["param"])
         else:

@@ -39,7 +39,12 @@ __host__ __device__ inline void morton_decode(uint32_t m, int* x, int* y, int* z
 }
 
 // ------------------------------------------------------------ kernels
-// K(t, s) with d = s - t, exactly the arithmetic of src/kernel_Types.cpp.
+// K(t, s) with d = s - t, the arithmetic of src/kernel_Types.cpp (float64;
+// the float32 instantiations of the 1/r^k kernels use rsqrtf).
+// 1/sqrt(r2), +inf at 0: rsqrtf in float32 (a few ulp), division in float64.
+__device__ __forceinline__ float inv_sqrt(float r2) { return rsqrtf(r2); }
+__device__ __forceinline__ double inv_sqrt(double r2) { return 1.0 / sqrt(r2); }
+
 template <int KID>
 struct Kern;
 
@@ -47,14 +52,14 @@ template <>
 struct Kern<PBBFMM_KERNEL_LAPLACIAN> {
   template <typename T>
   __device__ static T eval(T dx, T dy, T dz, const double*) {
-    return T(1) / sqrt(dx * dx + dy * dy + dz * dz);
+    return inv_sqrt(dx * dx + dy * dy + dz * dz);
   }
 };
 template <>
 struct Kern<PBBFMM_KERNEL_ONEOVERR2> {
   template <typename T>
   __device__ static T eval(T dx, T dy, T dz, const double*) {
-    T ri = T(1) / sqrt(dx * dx + dy * dy + dz * dz);
+    T ri = inv_sqrt(dx * dx + dy * dy + dz * dz);
     return ri * ri;
   }
 };
@@ -62,7 +67,7 @@ template <>
 struct Kern<PBBFMM_KERNEL_ONEOVERR4> {
   template <typename T>
   __device__ static T eval(T dx, T dy, T dz, const double*) {
-    T ri = T(1) / sqrt(dx * dx + dy * dy + dz * dz);
+    T ri = inv_sqrt(dx * dx + dy * dy + dz * dz);
     return ri * ri * ri * ri;
   }
 };

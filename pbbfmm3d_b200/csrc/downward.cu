@@ -8,6 +8,8 @@
 // leaves (no atomics, no symmetry assumption, sources may differ from
 // targets), and the far-field interpolation, the near-field sum and the
 // scatter to the caller's output are one kernel.
+#include <type_traits>
+
 #include "fmm.cuh"
 
 namespace pbbfmm {
@@ -122,16 +124,50 @@ struct L2LLaunch {
   }
 };
 
-// Leaf phase: one warp per nonempty target leaf, lanes over the sources of
-// the 27 neighbour leaves (and over the n^3 local coefficients for L2P);
-// warp-reduced per target point, then scattered to out[col*Nf + index].
+// Leaf phase (L2P + P2P): one warp per nonempty target leaf, one lane per
+// target (32 targets per pass).  The sources of the 27 neighbour leaves are
+// staged through a per-warp shared-memory tile of 32 (coalesced loads), and
+// every lane sweeps the tile by broadcast reads; the far field evaluates the
+// n^3 local coefficients (broadcast loads) against the lane's own basis.
+// Reference: Local2Particle / DirectInteractions, include/compute.hpp:692-778.
 constexpr int kLeafWarps = 4;
 constexpr int kLeafCols = 8;  // columns per pass (registers)
 
-// T = float (mixed path): the kernel is evaluated in float32 on differences
-// formed in float64, the far-field interpolation runs in float32, and every
-// lane's partial sums are compensated (Kahan); the warp reduction and the
-// output update are float64.
+// Source coordinates relative to the target leaf's centre.  float (mixed
+// path): hi = float(d), lo = float(d - hi), so that differences of nearby
+// points keep ~48 bits; double: the offsets themselves.
+template <typename T>
+struct RelPos;
+template <>
+struct RelPos<float> {
+  float h[3], l[3];
+  __device__ void set(double dx, double dy, double dz) {
+    h[0] = (float)dx, h[1] = (float)dy, h[2] = (float)dz;
+    l[0] = (float)(dx - h[0]), l[1] = (float)(dy - h[1]), l[2] = (float)(dz - h[2]);
+  }
+  // source minus target
+  __device__ void diff(const float4& sh, const float4& sl, float* d) const {
+    d[0] = (sh.x - h[0]) + (sl.x - l[0]);
+    d[1] = (sh.y - h[1]) + (sl.y - l[1]);
+    d[2] = (sh.z - h[2]) + (sl.z - l[2]);
+  }
+};
+template <>
+struct RelPos<double> {
+  double h[3];
+  __device__ void set(double dx, double dy, double dz) { h[0] = dx, h[1] = dy, h[2] = dz; }
+  __device__ void diff(const double4& sh, const double4&, double* d) const {
+    d[0] = sh.x - h[0];
+    d[1] = sh.y - h[1];
+    d[2] = sh.z - h[2];
+  }
+};
+template <typename T>
+using vec4_t = typename std::conditional<sizeof(T) == 4, float4, double4>::type;
+
+// T = float (mixed path): kernel values, interpolation and per-tile partial
+// sums in float32, each lane's running sums compensated (Kahan), the output
+// update in float64.  T = double: everything in float64.
 template <class KF, typename T>
 __global__ void __launch_bounds__(32 * kLeafWarps)
     k_leaf(const int* __restrict__ leaves, int nleaves, const int* __restrict__ tstart,
@@ -140,12 +176,16 @@ __global__ void __launch_bounds__(32 * kLeafWarps)
            const double* __restrict__ wsorted, int Nf, int Ns, int C,
            const T* __restrict__ F_L, int n, int cheb, const T* __restrict__ Tkz_g,
            double box, int L, const double* __restrict__ kparam_g, double* __restrict__ out) {
-  constexpr bool kKahan = sizeof(T) == 4;
+  constexpr bool kMixed = sizeof(T) == 4;
+  using V4 = vec4_t<T>;
   __shared__ T sTkz[kMaxOrder * kMaxOrder];
   __shared__ double kp[4];
-  __shared__ int s_nb[kLeafWarps][27][2];      // neighbour source ranges
-  __shared__ int s_pre[kLeafWarps][28];        // exclusive prefix of their lengths
-  __shared__ T s_b[kLeafWarps][3][kMaxOrder];  // basis values of the current target
+  __shared__ int s_nb[kLeafWarps][27][2];  // neighbour source ranges
+  __shared__ int s_pre[kLeafWarps][28];    // exclusive prefix of their lengths
+  __shared__ V4 s_sh[kLeafWarps][32];      // staged sources: position (hi)
+  __shared__ V4 s_sl[kLeafWarps][kMixed ? 32 : 1];  // position (lo), mixed path
+  __shared__ T s_w[kLeafWarps][32][kLeafCols];      // staged weights
+  __shared__ T s_b[kLeafWarps][3][kMaxOrder][32];   // basis values of each lane's target
   for (int i = threadIdx.x; i < n * n; i += blockDim.x) sTkz[i] = Tkz_g[i];
   if (threadIdx.x < 4) kp[threadIdx.x] = kparam_g[threadIdx.x];
   __syncthreads();
@@ -189,68 +229,83 @@ __global__ void __launch_bounds__(32 * kLeafWarps)
   const int nsrc_total = s_pre[wl][27];
   for (int c0 = 0; c0 < C; c0 += kLeafCols) {
     const int cg = min(kLeafCols, C - c0);
-    for (int i = ta; i < te; ++i) {
-      const double x = tpos[i], y = tpos[(int64_t)Nf + i], z = tpos[2 * (int64_t)Nf + i];
+    for (int t0 = ta; t0 < te; t0 += 32) {
+      const int i = t0 + lane;
+      const bool active = i < te;
+      double x = c[0], y = c[1], z = c[2];
+      if (active) x = tpos[i], y = tpos[(int64_t)Nf + i], z = tpos[2 * (int64_t)Nf + i];
+      RelPos<T> tp;
+      tp.set(x - c[0], y - c[1], z - c[2]);
       Kahan<T> acc[kLeafCols];
       // far field: phi += sum_l F[l] Sx[l1] Sy[l2] Sz[l3]
-      {
-        __syncwarp();
-        if (lane < 3 * n) {
-          const int d = lane / n, mm = lane % n;
-          const T q = (T)(ihalfL * ((d == 0 ? x : d == 1 ? y : z) - c[d]));
-          s_b[wl][d][mm] = basis_one<T>(n, cheb, q, sTkz, mm);
+      if (active) {
+        T(*b)[kMaxOrder][32] = s_b[wl];  // b[d][m][lane]: conflict-free, no local memory
+        for (int m = 0; m < n; ++m) {
+          b[0][m][lane] = basis_one<T>(n, cheb, (T)(ihalfL * (x - c[0])), sTkz, m);
+          b[1][m][lane] = basis_one<T>(n, cheb, (T)(ihalfL * (y - c[1])), sTkz, m);
+          b[2][m][lane] = basis_one<T>(n, cheb, (T)(ihalfL * (z - c[2])), sTkz, m);
         }
-        __syncwarp();
         const T* Fl = F_L + ((int64_t)leaf * C + c0) * n3;
-        for (int l = lane; l < n3; l += 32) {
-          const int l1 = l / (n * n), l2 = (l / n) % n, l3 = l % n;
-          const T tmp2 = s_b[wl][0][l1] * s_b[wl][1][l2];
-          const T bz3 = s_b[wl][2][l3];
+        int l = 0;
+        for (int l1 = 0; l1 < n; ++l1)
+          for (int l2 = 0; l2 < n; ++l2) {
+            const T b12 = b[0][l1][lane] * b[1][l2][lane];
+            for (int l3 = 0; l3 < n; ++l3, ++l) {
+              const T v = b12 * b[2][l3][lane];
 #pragma unroll
-          for (int cc = 0; cc < kLeafCols; ++cc)
-            if (cc < cg) {
-              if (kKahan)
-                acc[cc].add(Fl[cc * n3 + l] * tmp2 * bz3);
-              else
-                acc[cc].s += Fl[cc * n3 + l] * tmp2 * bz3;
+              for (int cc = 0; cc < kLeafCols; ++cc)
+                if (cc < cg) acc[cc].add(Fl[cc * n3 + l] * v);
             }
-        }
+          }
       }
-      // near field over the 27 neighbour leaves, their source ranges
-      // concatenated so that the lanes stay busy when leaves are small
-      {
-        int q = 0;
-        for (int v = lane; v < nsrc_total; v += 32) {
+      // near field: the 27 neighbours' source ranges, concatenated, in tiles of 32
+      int q = 0;
+      for (int v0 = 0; v0 < nsrc_total; v0 += 32) {
+        const int v = v0 + lane;
+        if (v < nsrc_total) {
           while (v >= s_pre[wl][q + 1]) ++q;
           const int j = s_nb[wl][q][0] + (v - s_pre[wl][q]);
-          const T dx = (T)(spos[j] - x), dy = (T)(spos[(int64_t)Ns + j] - y),
-                  dz = (T)(spos[2 * (int64_t)Ns + j] - z);
-          T kv = KF::template eval<T>(dx, dy, dz, kp);
-          if (isinf(kv)) kv = 0;
+          RelPos<T> sp;
+          sp.set(spos[j] - c[0], spos[(int64_t)Ns + j] - c[1], spos[2 * (int64_t)Ns + j] - c[2]);
+          V4 h;
+          h.x = sp.h[0], h.y = sp.h[1], h.z = sp.h[2], h.w = 0;
+          s_sh[wl][lane] = h;
+          if constexpr (kMixed) {
+            V4 lo;
+            lo.x = sp.l[0], lo.y = sp.l[1], lo.z = sp.l[2], lo.w = 0;
+            s_sl[wl][lane] = lo;
+          }
           const double* wj = wsorted + (int64_t)j * C + c0;
 #pragma unroll
-          for (int cc = 0; cc < kLeafCols; ++cc)
-            if (cc < cg) {
-              if (kKahan)
-                acc[cc].add(kv * (T)wj[cc]);
-              else
-                acc[cc].s += kv * wj[cc];
-            }
+          for (int cc = 0; cc < kLeafCols; ++cc) s_w[wl][lane][cc] = cc < cg ? (T)wj[cc] : T(0);
         }
-      }
-      double tot[kLeafCols];
+        __syncwarp();
+        if (active) {
+          const int m = min(32, nsrc_total - v0);
+          T part[kLeafCols];
 #pragma unroll
-      for (int cc = 0; cc < kLeafCols; ++cc) {
-        double v = kKahan ? acc[cc].value() : (double)acc[cc].s;
+          for (int cc = 0; cc < kLeafCols; ++cc) part[cc] = 0;
+#pragma unroll 4
+          for (int jj = 0; jj < m; ++jj) {
+            T d[3];
+            tp.diff(s_sh[wl][jj], s_sl[wl][kMixed ? jj : 0], d);
+            T kv = KF::template eval<T>(d[0], d[1], d[2], kp);
+            if (isinf(kv)) kv = 0;  // coincident points (include/compute.hpp:767)
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        tot[cc] = v;
+            for (int cc = 0; cc < kLeafCols; ++cc)
+              if (cc < cg) part[cc] = fma(kv, s_w[wl][jj][cc], part[cc]);
+          }
+#pragma unroll
+          for (int cc = 0; cc < kLeafCols; ++cc)
+            if (cc < cg) acc[cc].add(part[cc]);
+        }
+        __syncwarp();
       }
-      if (lane == 0) {
+      if (active) {
         const int64_t oi = tperm[i];
 #pragma unroll
         for (int cc = 0; cc < kLeafCols; ++cc)
-          if (cc < cg) out[(int64_t)(c0 + cc) * Nf + oi] += tot[cc];
+          if (cc < cg) out[(int64_t)(c0 + cc) * Nf + oi] += (double)acc[cc].value();
       }
     }
   }

@@ -220,6 +220,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   __shared__ int s_xyz[TC_M];      // target coordinates, x << 20 | y << 10 | z
   __shared__ uint32_t s_valid[6];  // bit o: some target of the tile has a source at offset o
   __shared__ int4 s_off[189];      // valid offsets: (ox, oy, oz, operator index)
+  __shared__ long long s_src[2][TC_M];  // A source row offsets (or -1) of two offsets
   __shared__ int s_nvalid;
   __shared__ int s_abort_flag;
   volatile int* s_abort = &s_abort_flag;
@@ -330,33 +331,41 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       }
       return cur_row;
     };
-    // Fill stage s with K chunk `it`: row tid of A (hi, lo); rows tid, tid + 128 of B.
-    auto issue_loads = [&](int it, int s) {
+    // Source row offsets of valid offset q for all 128 rows, double buffered
+    // by the parity of q: thread tid publishes its own row before a producer
+    // barrier, and every producer reads them after it.
+    auto publish = [&](int j) {
+      const int q = j / kchunks;
+      s_src[q & 1][tid] = row_for(q);
+    };
+    // Fill stage s with K chunk j.  Eight consecutive lanes copy the eight
+    // 16-byte chunks of one 128-byte row, so a warp instruction touches four
+    // rows (four cache lines) of A or B.
+    auto issue_loads = [&](int j, int s) {
       unsigned char* st = base + s * stage_bytes;
-      const int q = it / kchunks, kc = it - q * kchunks;
-      const int64_t r = row_for(q);
-      const bool ok = r >= 0;
-      const float* gh = Ph + (ok ? r + kc * TC_KC : 0);
-      const float* gl = Pl + (ok ? r + kc * TC_KC : 0);
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        cp_async16(st + sw128_off(tid, j), gh + 4 * j, ok ? 16 : 0);
-        cp_async16(st + 16384 + sw128_off(tid, j), gl + 4 * j, ok ? 16 : 0);
+      const int q = j / kchunks, kc = j - q * kchunks;
+      const long long* src = s_src[q & 1];
+      const int ch = tid & 7;
+      for (int r = tid >> 3; r < TC_M; r += TC_M / 8) {
+        const long long rr = src[r];
+        const bool ok = rr >= 0;
+        const int64_t off = ok ? rr + kc * TC_KC + 4 * ch : 0;
+        cp_async16(st + sw128_off(r, ch), Ph + off, ok ? 16 : 0);
+        cp_async16(st + 16384 + sw128_off(r, ch), Pl + off, ok ? 16 : 0);
       }
-      const int opi = s_off[q].w;
-      const float* eh = Eh + (int64_t)opi * NP * KP + kc * TC_KC;
-      const float* el = El + (int64_t)opi * NP * KP + kc * TC_KC;
-      for (int n = tid; n < NP; n += TC_M) {
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          cp_async16(st + 32768 + sw128_off(n, j), eh + (int64_t)n * KP + 4 * j, 16);
-          cp_async16(st + 32768 + bbytes + sw128_off(n, j), el + (int64_t)n * KP + 4 * j, 16);
-        }
+      const int64_t eoff = (int64_t)s_off[q].w * NP * KP + kc * TC_KC + 4 * ch;
+      for (int n = tid >> 3; n < NP; n += TC_M / 8) {
+        cp_async16(st + 32768 + sw128_off(n, ch), Eh + eoff + (int64_t)n * KP, 16);
+        cp_async16(st + 32768 + bbytes + sw128_off(n, ch), El + eoff + (int64_t)n * KP, 16);
       }
     };
 
     bool aborted = false;
     int last = -1;  // thread 0: last iteration whose MMAs were committed
+#pragma unroll
+    for (int j = 0; j < NST - 1; ++j)
+      if (j < niter) publish(j);
+    asm volatile("bar.sync 1, 128;\n" ::: "memory");
 #pragma unroll
     for (int j = 0; j < NST - 1; ++j) {
       if (j < niter) issue_loads(j, j);
@@ -395,11 +404,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       if (!aborted && it >= 1 &&
           !mbar_wait(&s_bar[(it - 1) % NST], ((it - 1) / NST) & 1, s_abort))
         aborted = true;
+      const int j = it + NST - 1;
+      if (j < niter) publish(j);
       if (producers_sync_or(aborted)) {
         aborted = true;
         break;
       }
-      const int j = it + NST - 1;
       if (j < niter) issue_loads(j, j % NST);
       cp_async_commit();
     }
@@ -480,10 +490,12 @@ __global__ void k_split_proxy(const int* __restrict__ cells, int64_t nrows, int 
   pl[row * KP + k] = to_tf32(v - h);
 }
 
-// Offsets per TMEM accumulation chain (PBBFMM_TC_GROUP overrides the default).
-static int tc_group() {
+// Offsets per TMEM accumulation chain (PBBFMM_TC_GROUP overrides the
+// default): one offset when the running sum stays in TMEM (drains then cost
+// nothing measurable), four when drains add into pf in global memory.
+static int tc_group(int NP) {
   const char* e = getenv("PBBFMM_TC_GROUP");
-  const int g = e ? atoi(e) : 4;
+  const int g = e ? atoi(e) : (tc_sum_in_tmem(NP) ? 1 : 4);
   return g < 1 ? 1 : (g > 189 ? 189 : g);
 }
 
@@ -537,14 +549,14 @@ int run_m2l_cheb_tc_level(pbbfmm_tree* t, int C, int l, int lvl, const float* pr
                                  smem));
     k_m2l_cheb_tc<3><<<(unsigned)tiles, TC_THREADS, smem, st>>>(
         rf, NP, KP, t->f_Eth + lvl * eop, t->f_Etl + lvl * eop, lists + t->lists.typ_off[l], tt,
-        C, l, ws.sstart.as<int>(), (int)cells_at(L - l), t->d_offs, ph, pl, pf, tc_group(),
+        C, l, ws.sstart.as<int>(), (int)cells_at(L - l), t->d_offs, ph, pl, pf, tc_group(NP),
         t->d_tc_err);
   } else {
     PB_CUDA(cudaFuncSetAttribute(k_m2l_cheb_tc<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  smem));
     k_m2l_cheb_tc<2><<<(unsigned)tiles, TC_THREADS, smem, st>>>(
         rf, NP, KP, t->f_Eth + lvl * eop, t->f_Etl + lvl * eop, lists + t->lists.typ_off[l], tt,
-        C, l, ws.sstart.as<int>(), (int)cells_at(L - l), t->d_offs, ph, pl, pf, tc_group(),
+        C, l, ws.sstart.as<int>(), (int)cells_at(L - l), t->d_offs, ph, pl, pf, tc_group(NP),
         t->d_tc_err);
   }
   PB_LAUNCH("m2l_cheb_tc");
