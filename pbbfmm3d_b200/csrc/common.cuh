@@ -40,10 +40,10 @@ __host__ __device__ inline void morton_decode(uint32_t m, int* x, int* y, int* z
 
 // ------------------------------------------------------------ kernels
 // K(t, s) with d = s - t, the arithmetic of src/kernel_Types.cpp (float64;
-// the float32 instantiations of the 1/r^k kernels use rsqrtf).
-// 1/sqrt(r2), +inf at 0: rsqrtf in float32 (a few ulp), division in float64.
+// the 1/r^k kernels use the reciprocal square root functions).
+// 1/sqrt(r2), +inf at 0: rsqrtf in float32 (a few ulp), rsqrt in float64.
 __device__ __forceinline__ float inv_sqrt(float r2) { return rsqrtf(r2); }
-__device__ __forceinline__ double inv_sqrt(double r2) { return 1.0 / sqrt(r2); }
+__device__ __forceinline__ double inv_sqrt(double r2) { return rsqrt(r2); }
 
 template <int KID>
 struct Kern;

@@ -124,14 +124,17 @@ struct L2LLaunch {
   }
 };
 
-// Leaf phase (L2P + P2P): one warp per nonempty target leaf, one lane per
-// target (32 targets per pass).  The sources of the 27 neighbour leaves are
-// staged through a per-warp shared-memory tile of 32 (coalesced loads), and
-// every lane sweeps the tile by broadcast reads; the far field evaluates the
-// n^3 local coefficients (broadcast loads) against the lane's own basis.
+// Leaf phase (L2P + P2P): one warp per nonempty target leaf.  Dense leaves
+// (kLaneLeafMin targets or more): one lane per target, 32 targets per pass;
+// the sources of the 27 neighbour leaves are staged through a per-warp
+// shared-memory tile of 32 (coalesced loads) that every lane sweeps by
+// broadcast reads, and the far field evaluates the n^3 local coefficients
+// (broadcast loads) against the lane's own basis.  Sparse leaves: one target
+// at a time, lanes over its sources and coefficients, warp shuffle reduction.
 // Reference: Local2Particle / DirectInteractions, include/compute.hpp:692-778.
 constexpr int kLeafWarps = 4;
 constexpr int kLeafCols = 8;  // columns per pass (registers)
+constexpr int kLaneLeafMin = 12;  // leaves with fewer targets take the warp-per-target path
 
 // Source coordinates relative to the target leaf's centre.  float (mixed
 // path): hi = float(d), lo = float(d - hi), so that differences of nearby
@@ -227,6 +230,61 @@ __global__ void __launch_bounds__(32 * kLeafWarps)
   }
   __syncwarp();
   const int nsrc_total = s_pre[wl][27];
+  if (te - ta < kLaneLeafMin) {
+    // Sparse leaf: one target at a time, lanes over its sources and over the
+    // n^3 local coefficients, warp-reduced in float64.
+    for (int c0 = 0; c0 < C; c0 += kLeafCols) {
+      const int cg = min(kLeafCols, C - c0);
+      for (int i = ta; i < te; ++i) {
+        const double x = tpos[i], y = tpos[(int64_t)Nf + i], z = tpos[2 * (int64_t)Nf + i];
+        Kahan<T> acc[kLeafCols];
+        __syncwarp();
+        if (lane < 3 * n) {
+          const int d = lane / n, mm = lane % n;
+          const T u = (T)(ihalfL * ((d == 0 ? x : d == 1 ? y : z) - c[d]));
+          s_b[wl][d][mm][0] = basis_one<T>(n, cheb, u, sTkz, mm);
+        }
+        __syncwarp();
+        const T* Fl = F_L + ((int64_t)leaf * C + c0) * n3;
+        for (int l = lane; l < n3; l += 32) {
+          const int l1 = l / (n * n), l2 = (l / n) % n, l3 = l % n;
+          const T v = s_b[wl][0][l1][0] * s_b[wl][1][l2][0] * s_b[wl][2][l3][0];
+#pragma unroll
+          for (int cc = 0; cc < kLeafCols; ++cc)
+            if (cc < cg) acc[cc].add(Fl[cc * n3 + l] * v);
+        }
+        int q = 0;
+        for (int v = lane; v < nsrc_total; v += 32) {
+          while (v >= s_pre[wl][q + 1]) ++q;
+          const int j = s_nb[wl][q][0] + (v - s_pre[wl][q]);
+          const T dx = (T)(spos[j] - x), dy = (T)(spos[(int64_t)Ns + j] - y),
+                  dz = (T)(spos[2 * (int64_t)Ns + j] - z);
+          T kv = KF::template eval<T>(dx, dy, dz, kp);
+          if (isinf(kv)) kv = 0;  // coincident points (include/compute.hpp:767)
+          const double* wj = wsorted + (int64_t)j * C + c0;
+#pragma unroll
+          for (int cc = 0; cc < kLeafCols; ++cc)
+            if (cc < cg) acc[cc].add(kv * (T)wj[cc]);
+        }
+        double tot[kLeafCols];
+#pragma unroll
+        for (int cc = 0; cc < kLeafCols; ++cc) {
+          double v = acc[cc].value();
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+          tot[cc] = v;
+        }
+        if (lane == 0) {
+          const int64_t oi = tperm[i];
+#pragma unroll
+          for (int cc = 0; cc < kLeafCols; ++cc)
+            if (cc < cg) out[(int64_t)(c0 + cc) * Nf + oi] += tot[cc];
+        }
+      }
+    }
+    return;
+  }
+  // Dense leaf: one target per lane, sources through shared-memory tiles.
   for (int c0 = 0; c0 < C; c0 += kLeafCols) {
     const int cg = min(kLeafCols, C - c0);
     for (int t0 = ta; t0 < te; t0 += 32) {
