@@ -28,7 +28,9 @@ namespace pbbfmm {
 
 constexpr int TC_M = 128;
 constexpr int TC_KC = 32;          // K per stage: one 128-byte swizzle row of float32
-constexpr int TC_THREADS = 256;    // warps 0-3 producers, warps 4-7 drainers
+constexpr int TC_PRODUCERS = 128;  // warps 0-3: operand loads
+constexpr int TC_MMA_WARP = 4;     // warp 4: TMEM allocation, MMA issue (one thread)
+constexpr int TC_THREADS = 288;    // + warps 5-8: accumulator drains
 constexpr int TC_TMEM_COLS = 512;  // columns allocated (accumulators and running sum)
 constexpr unsigned long long kWaitNs = 1000000000ull;  // 1 s
 constexpr long long kWaitIters = 1ll << 26;
@@ -94,16 +96,11 @@ __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
 }
 
-// Barrier 1 over the 128 producer threads, OR-reducing `pred`.
-__device__ __forceinline__ bool producers_sync_or(bool pred) {
-  int r;
-  asm volatile(
-      "{\n .reg .pred p, q;\n setp.ne.b32 p, %1, 0;\n"
-      " bar.red.or.pred q, 1, 128, p;\n selp.s32 %0, 1, 0, q;\n}\n"
-      : "=r"(r)
-      : "r"((int)pred)
-      : "memory");
-  return r != 0;
+// Arrive on `bar` once every cp.async issued so far by this thread has
+// landed (the barrier's expected count includes this arrival).
+__device__ __forceinline__ void cp_async_arrive(uint64_t* bar) {
+  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(smem_u32(bar))
+               : "memory");
 }
 
 __device__ __forceinline__ void fence_async_smem() {
@@ -194,15 +191,21 @@ __host__ __device__ constexpr bool tc_sum_in_tmem(int NP) { return NP <= 160; }
 //   Eh, El : [316][NP][KP] hi / lo of E_o^T (row f holds E_o[f][s] over s), zero padded
 //   Ph, Pl : proxy hi / lo, row (cell * C + col) of KP floats, zero padded
 //   pf     : output rows (cell * C + col) of rf floats
-// Warps 0-3 (producers) look up source rows, fill the stages with cp.async
-// and thread 0 issues the MMAs.  Two TMEM accumulators take turns, one per
-// group of `group` consecutive offsets, so that every float32 accumulation
-// chain inside the tensor pipe spans at most `group` offsets; warps 4-7
-// (drainers) add each finished accumulator into the running sum while the
-// MMAs of the next group run.
-//   s_bar[s]  : MMAs of the stage's last fill done (tcgen05.commit)
-//   s_accf[b] : MMAs of accumulator b's group done (tcgen05.commit)
-//   s_acce[b] : accumulator b drained (128 drainer arrivals)
+// Warp roles:
+//   warps 0-3  producers: each warp fills its 32 rows of A and its share of
+//              B for every stage with cp.async and signals the stage's full
+//              barrier when its copies land (cp.async.mbarrier.arrive);
+//   warp 4     allocates TMEM; one thread waits for full stages, issues the
+//              MMAs and commits them to the stage's empty barrier;
+//   warps 5-8  drain accumulators into the running sum (TMEM lane quadrant
+//              warp % 4).
+// Two TMEM accumulators take turns, one per group of `group` consecutive
+// offsets, so every float32 accumulation chain inside the tensor pipe spans
+// at most `group` offsets.
+//   s_full[s]  : 128 producer arrivals, one per thread, when its copies land
+//   s_empty[s] : MMAs reading stage s done (tcgen05.commit)
+//   s_accf[b]  : MMAs of accumulator b's group done (tcgen05.commit)
+//   s_acce[b]  : accumulator b drained (128 drainer arrivals)
 template <int NST>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     k_m2l_cheb_tc(int rf, int NP, int KP, const float* __restrict__ Eh,
@@ -214,17 +217,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   const int bbytes = NP * 128;
   const int stage_bytes = tc_stage_bytes(NP);
   unsigned char* base = smraw + ((1024 - (smem_u32(smraw) & 1023)) & 1023);
-  __shared__ uint64_t s_bar[NST], s_accf[2], s_acce[2];
+  __shared__ uint64_t s_full[NST], s_empty[NST], s_accf[2], s_acce[2];
   __shared__ uint32_t s_tmem;
   __shared__ int s_cell[TC_M];     // target cell of each row, or -1
   __shared__ int s_xyz[TC_M];      // target coordinates, x << 20 | y << 10 | z
   __shared__ uint32_t s_valid[6];  // bit o: some target of the tile has a source at offset o
   __shared__ int4 s_off[189];      // valid offsets: (ox, oy, oz, operator index)
-  __shared__ long long s_src[2][TC_M];  // A source row offsets (or -1) of two offsets
   __shared__ int s_nvalid;
   __shared__ int s_abort_flag;
   volatile int* s_abort = &s_abort_flag;
-  const int tid = threadIdx.x, warp = tid >> 5;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
 
   // child type of this tile (unrolled so the parameter arrays stay in registers)
   int type = 0, tstart = 0, tlist = 0, tcount = 0;
@@ -242,18 +244,15 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   const int nside = 1 << lev;
   const int* my_offs = offs + type * 189 * 4;
 
-  // producer thread tid owns A row tid; drainer thread owns TMEM lane (and row) 32 (warp % 4) + lane
-  const int row = tid < TC_M ? tid : 32 * (warp & 3) + (tid & 31);
-  int tx = 0, ty = 0, tz = 0;
-  const int cell = (row < per_tile * C && row / C < ntile) ? typed[tlist + tfirst + row / C] : -1;
-  if (cell >= 0) morton_decode((uint32_t)cell, &tx, &ty, &tz);
-  const int col = row % C;
   if (tid < TC_M) {
+    const int cell = (tid < per_tile * C && tid / C < ntile) ? typed[tlist + tfirst + tid / C] : -1;
+    int x = 0, y = 0, z = 0;
+    if (cell >= 0) morton_decode((uint32_t)cell, &x, &y, &z);
     s_cell[tid] = cell;
-    s_xyz[tid] = (tx << 20) | (ty << 10) | tz;
+    s_xyz[tid] = (x << 20) | (y << 10) | z;
   }
   if (tid < 6) s_valid[tid] = 0;
-  if (warp == 0) {  // 128 lanes x 512 float32 columns
+  if (warp == TC_MMA_WARP) {  // 128 lanes x 512 float32 columns
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
                      smem_u32(&s_tmem)),
                  "r"(TC_TMEM_COLS)
@@ -261,19 +260,23 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
   }
   if (tid == 0) {
-    for (int i = 0; i < NST; ++i) mbar_init(&s_bar[i], 1);
+    for (int i = 0; i < NST; ++i) {
+      mbar_init(&s_full[i], TC_PRODUCERS);
+      mbar_init(&s_empty[i], 1);
+    }
     for (int b = 0; b < 2; ++b) {
       mbar_init(&s_accf[b], 1);
-      mbar_init(&s_acce[b], TC_THREADS - TC_M);
+      mbar_init(&s_acce[b], TC_M);
     }
     s_abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   __syncthreads();
   // offsets with at least one source cell for some target of the tile
-  if (tid < TC_M && cell >= 0 && col == 0) {
+  if (tid < TC_M && s_cell[tid] >= 0 && tid % C == 0) {
+    const int x = s_xyz[tid] >> 20, y = (s_xyz[tid] >> 10) & 1023, z = s_xyz[tid] & 1023;
     for (int o = 0; o < 189; ++o) {
-      const int bx = tx + my_offs[4 * o], by = ty + my_offs[4 * o + 1], bz = tz + my_offs[4 * o + 2];
+      const int bx = x + my_offs[4 * o], by = y + my_offs[4 * o + 1], bz = z + my_offs[4 * o + 2];
       if (bx < 0 || by < 0 || bz < 0 || bx >= nside || by >= nside || bz >= nside) continue;
       const uint32_t bm = morton_encode(bx, by, bz);
       if (sstart[(int64_t)(bm + 1) * span] > sstart[(int64_t)bm * span])
@@ -299,129 +302,112 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   const int group_iters = max(group, 1) * kchunks;
   const int ngroups = (niter + group_iters - 1) / group_iters;
 
-  if (tid < TC_M) {
+  if (warp < TC_PRODUCERS / 32) {
     // ---------------------------------------------------------------- producers
-    const uint32_t idesc = tf32_idesc(TC_M, NP);
-    // Source row of this thread for valid offset q: the lookup for q + 1 is
-    // started (two independent loads) when q is resolved and finished when
-    // q + 1 is needed, a whole offset (kchunks stages) later.
-    int cur_q = -1, pre_q = -1;
-    int64_t cur_row = -1;
-    int pre_a = 0, pre_b = 0;
+    // Lane l copies 16-byte chunk (l & 7) of rows 4 warp + (l >> 3) + 16 i of
+    // A (i < 8) and B (i < NP / 16): four 128-byte rows per warp instruction.
+    // Lane l also owns A row 4 warp + (l & 3) + 16 (l >> 2): it looks up that
+    // row's source once per offset (one offset ahead) and the lanes copying
+    // the row fetch the result by shuffle.
+    const int own = 4 * warp + (lane & 3) + 16 * (lane >> 2);
+    const int ocell = s_cell[own], ocol = own % C;
+    const int ox = s_xyz[own] >> 20, oy = (s_xyz[own] >> 10) & 1023, oz = s_xyz[own] & 1023;
+    const int ch = lane & 7, r0 = 4 * warp + (lane >> 3);
+    const uint32_t soff0 = sw128_off(r0, ch);  // row r0 + 16 i lies 2048 i bytes further
+    int pre_q = -1, pre_a = 0, pre_b = 0;
     uint32_t pre_bm = 0;
     bool pre_in = false;
     auto start_lookup = [&](int q) {
       pre_q = q;
       pre_in = false;
-      if (q >= nvalid || cell < 0) return;
+      if (q >= nvalid || ocell < 0) return;
       const int4 o = s_off[q];
-      const int x = tx + o.x, y = ty + o.y, z = tz + o.z;
+      const int x = ox + o.x, y = oy + o.y, z = oz + o.z;
       if (x < 0 || y < 0 || z < 0 || x >= nside || y >= nside || z >= nside) return;
       pre_bm = morton_encode(x, y, z);
       pre_a = sstart[(int64_t)pre_bm * span];
       pre_b = sstart[(int64_t)(pre_bm + 1) * span];
       pre_in = true;
     };
-    auto row_for = [&](int q) -> int64_t {
+    int cur_q = -1;
+    long long cur_row = -1;  // this lane's own row: source row offset or -1
+    start_lookup(0);
+    for (int j = 0; j < niter; ++j) {
+      const int s = j % NST;
+      if (j >= NST && !mbar_wait(&s_empty[s], (j / NST - 1) & 1, s_abort)) {
+        *s_abort = 1;
+        break;
+      }
+      const int q = j / kchunks, kc = j - q * kchunks;
       if (q != cur_q) {
         if (pre_q != q) start_lookup(q);
-        cur_row = (pre_in && pre_b > pre_a) ? ((int64_t)pre_bm * C + col) * KP : -1;
+        cur_row = (pre_in && pre_b > pre_a) ? ((long long)pre_bm * C + ocol) * KP : -1;
         cur_q = q;
         start_lookup(q + 1);
       }
-      return cur_row;
-    };
-    // Source row offsets of valid offset q for all 128 rows, double buffered
-    // by the parity of q: thread tid publishes its own row before a producer
-    // barrier, and every producer reads them after it.
-    auto publish = [&](int j) {
-      const int q = j / kchunks;
-      s_src[q & 1][tid] = row_for(q);
-    };
-    // Fill stage s with K chunk j.  Eight consecutive lanes copy the eight
-    // 16-byte chunks of one 128-byte row, so a warp instruction touches four
-    // rows (four cache lines) of A or B.
-    auto issue_loads = [&](int j, int s) {
       unsigned char* st = base + s * stage_bytes;
-      const int q = j / kchunks, kc = j - q * kchunks;
-      const long long* src = s_src[q & 1];
-      const int ch = tid & 7;
-      for (int r = tid >> 3; r < TC_M; r += TC_M / 8) {
-        const long long rr = src[r];
+#pragma unroll
+      for (int i = 0; i < 8; ++i) {
+        const long long rr = __shfl_sync(0xffffffffu, cur_row, (lane >> 3) | (i << 2));
         const bool ok = rr >= 0;
         const int64_t off = ok ? rr + kc * TC_KC + 4 * ch : 0;
-        cp_async16(st + sw128_off(r, ch), Ph + off, ok ? 16 : 0);
-        cp_async16(st + 16384 + sw128_off(r, ch), Pl + off, ok ? 16 : 0);
+        cp_async16(st + soff0 + 2048 * i, Ph + off, ok ? 16 : 0);
+        cp_async16(st + 16384 + soff0 + 2048 * i, Pl + off, ok ? 16 : 0);
       }
       const int64_t eoff = (int64_t)s_off[q].w * NP * KP + kc * TC_KC + 4 * ch;
-      for (int n = tid >> 3; n < NP; n += TC_M / 8) {
-        cp_async16(st + 32768 + sw128_off(n, ch), Eh + eoff + (int64_t)n * KP, 16);
-        cp_async16(st + 32768 + bbytes + sw128_off(n, ch), El + eoff + (int64_t)n * KP, 16);
+      for (int i = 0, n = r0; n < NP; ++i, n += 16) {
+        cp_async16(st + 32768 + soff0 + 2048 * i, Eh + eoff + (int64_t)n * KP, 16);
+        cp_async16(st + 32768 + bbytes + soff0 + 2048 * i, El + eoff + (int64_t)n * KP, 16);
       }
-    };
-
-    bool aborted = false;
-    int last = -1;  // thread 0: last iteration whose MMAs were committed
-#pragma unroll
-    for (int j = 0; j < NST - 1; ++j)
-      if (j < niter) publish(j);
-    asm volatile("bar.sync 1, 128;\n" ::: "memory");
-#pragma unroll
-    for (int j = 0; j < NST - 1; ++j) {
-      if (j < niter) issue_loads(j, j);
-      cp_async_commit();
+      cp_async_arrive(&s_full[s]);
     }
-    for (int it = 0; it < niter; ++it) {
-      const int s = it % NST;
-      asm volatile("cp.async.wait_group %0;\n" ::"n"(NST - 2) : "memory");  // loads of `it`
-      fence_async_smem();
-      asm volatile("bar.sync 1, 128;\n" ::: "memory");
-      const int g = it / group_iters;
-      const bool fresh = it == g * group_iters;
-      if (tid == 0) {
-        // accumulator g & 1 is free once the drain of group g - 2 is done
-        if (fresh && g >= 2 && !mbar_wait(&s_acce[g & 1], ((g - 2) >> 1) & 1, s_abort))
-          aborted = true;
-        if (!aborted) {
-          tc_fence_after();
-          const uint32_t a_hi = smem_u32(base + s * stage_bytes), a_lo = a_hi + 16384;
-          const uint32_t b_hi = a_hi + 32768, b_lo = b_hi + bbytes;
-          const uint32_t d = tmem + (uint32_t)((g & 1) * tc_acc_stride(NP));
-#pragma unroll
-          for (int k = 0; k < TC_KC / 8; ++k) {
-            const uint32_t off = k * 32;
-            tc_mma_tf32(d, sw128_desc(a_lo + off), sw128_desc(b_hi + off), idesc,
-                        (fresh && k == 0) ? 0u : 1u);
-            tc_mma_tf32(d, sw128_desc(a_hi + off), sw128_desc(b_lo + off), idesc, 1u);
-            tc_mma_tf32(d, sw128_desc(a_hi + off), sw128_desc(b_hi + off), idesc, 1u);
-          }
-          tc_commit(&s_bar[s]);
-          if (it + 1 == niter || it + 1 == (g + 1) * group_iters) tc_commit(&s_accf[g & 1]);
-          last = it;
-        }
-      }
-      // the stage of it - 1 can be refilled once its MMAs are done
-      if (!aborted && it >= 1 &&
-          !mbar_wait(&s_bar[(it - 1) % NST], ((it - 1) / NST) & 1, s_abort))
-        aborted = true;
-      const int j = it + NST - 1;
-      if (j < niter) publish(j);
-      if (producers_sync_or(aborted)) {
-        aborted = true;
-        break;
-      }
-      if (j < niter) issue_loads(j, j % NST);
-      cp_async_commit();
-    }
-    if (aborted) *s_abort = 1;
-    // Before the TMEM is freed: MMAs complete in order, so the last commit
-    // covers all of them (waited for even after an abort, still bounded).
-    if (tid == 0 && last >= 0 && !mbar_wait(&s_bar[last % NST], (last / NST) & 1, nullptr))
-      *s_abort = 1;
     cp_async_wait_all();
+  } else if (warp == TC_MMA_WARP) {
+    // ---------------------------------------------------------------- MMA issue
+    if (lane == 0) {
+      const uint32_t idesc = tf32_idesc(TC_M, NP);
+      const int astride = tc_acc_stride(NP);
+      int last = -1;  // last iteration whose MMAs were committed
+      for (int it = 0; it < niter; ++it) {
+        const int s = it % NST;
+        const int g = it / group_iters;
+        const bool fresh = it == g * group_iters;
+        // accumulator g & 1 is free once the drain of group g - 2 is done
+        if (fresh && g >= 2 && !mbar_wait(&s_acce[g & 1], ((g - 2) >> 1) & 1, s_abort)) {
+          *s_abort = 1;
+          break;
+        }
+        if (!mbar_wait(&s_full[s], (it / NST) & 1, s_abort)) {
+          *s_abort = 1;
+          break;
+        }
+        fence_async_smem();  // the producers' copies, seen through the barrier, to the async proxy
+        tc_fence_after();
+        const uint32_t a_hi = smem_u32(base + s * stage_bytes), a_lo = a_hi + 16384;
+        const uint32_t b_hi = a_hi + 32768, b_lo = b_hi + bbytes;
+        const uint32_t d = tmem + (uint32_t)((g & 1) * astride);
+#pragma unroll
+        for (int k = 0; k < TC_KC / 8; ++k) {
+          const uint32_t off = k * 32;
+          tc_mma_tf32(d, sw128_desc(a_lo + off), sw128_desc(b_hi + off), idesc,
+                      (fresh && k == 0) ? 0u : 1u);
+          tc_mma_tf32(d, sw128_desc(a_hi + off), sw128_desc(b_lo + off), idesc, 1u);
+          tc_mma_tf32(d, sw128_desc(a_hi + off), sw128_desc(b_hi + off), idesc, 1u);
+        }
+        tc_commit(&s_empty[s]);
+        if (it + 1 == niter || it + 1 == (g + 1) * group_iters) tc_commit(&s_accf[g & 1]);
+        last = it;
+      }
+      // Before the TMEM is freed: MMAs complete in order, so the last commit
+      // covers all of them (waited for even after an abort, still bounded).
+      if (last >= 0 && !mbar_wait(&s_empty[last % NST], (last / NST) & 1, nullptr)) *s_abort = 1;
+    }
+    __syncwarp();
   } else {
     // ---------------------------------------------------------------- drainers
-    float* dst = cell >= 0 ? pf + ((int64_t)cell * C + col) * rf : nullptr;
+    const int row = 32 * (warp & 3) + lane;  // TMEM lane quadrant of this warp
+    const int cell = s_cell[row];
+    float* dst = cell >= 0 ? pf + ((int64_t)cell * C + row % C) * rf : nullptr;
     const uint32_t lane_base = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
     const int astride = tc_acc_stride(NP);
     const bool tsum = tc_sum_in_tmem(NP);
@@ -466,7 +452,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   tc_fence_before();
   __syncthreads();
   if (tid == 0 && *s_abort) atomicExch(err, 1);
-  if (warp == 0) {
+  if (warp == TC_MMA_WARP) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem),
                  "r"(TC_TMEM_COLS)
