@@ -168,11 +168,21 @@ struct RelPos<double> {
 template <typename T>
 using vec4_t = typename std::conditional<sizeof(T) == 4, float4, double4>::type;
 
+// Running sum of the float64 path (plain; the mixed path uses Kahan<float>).
+template <typename T>
+struct PlainSum {
+  T s = 0;
+  __device__ __forceinline__ void add(T x) { s += x; }
+  __device__ __forceinline__ double value() const { return (double)s; }
+};
+template <typename T>
+using LeafAcc = typename std::conditional<sizeof(T) == 4, Kahan<T>, PlainSum<T>>::type;
+
 // T = float (mixed path): kernel values, interpolation and per-tile partial
 // sums in float32, each lane's running sums compensated (Kahan), the output
 // update in float64.  T = double: everything in float64.
-template <class KF, typename T>
-__global__ void __launch_bounds__(32 * kLeafWarps)
+template <class KF, typename T, int KC>
+__global__ void __launch_bounds__(32 * kLeafWarps, 4)
     k_leaf(const int* __restrict__ leaves, int nleaves, const int* __restrict__ tstart,
            const int* __restrict__ sstart, const int* __restrict__ tperm,
            const double* __restrict__ tpos, const double* __restrict__ spos,
@@ -187,8 +197,10 @@ __global__ void __launch_bounds__(32 * kLeafWarps)
   __shared__ int s_pre[kLeafWarps][28];    // exclusive prefix of their lengths
   __shared__ V4 s_sh[kLeafWarps][32];      // staged sources: position (hi)
   __shared__ V4 s_sl[kLeafWarps][kMixed ? 32 : 1];  // position (lo), mixed path
-  __shared__ T s_w[kLeafWarps][32][kLeafCols];      // staged weights
-  __shared__ T s_b[kLeafWarps][3][kMaxOrder][32];   // basis values of each lane's target
+  __shared__ T s_w[kLeafWarps][32][KC];             // staged weights
+  // basis values of each lane's target, [warp][dim][m < n][lane] (dynamic, sized by n)
+  extern __shared__ __align__(16) unsigned char leaf_dyn[];
+  T* s_bw = reinterpret_cast<T*>(leaf_dyn) + (threadIdx.x >> 5) * 3 * n * 32;
   for (int i = threadIdx.x; i < n * n; i += blockDim.x) sTkz[i] = Tkz_g[i];
   if (threadIdx.x < 4) kp[threadIdx.x] = kparam_g[threadIdx.x];
   __syncthreads();
@@ -233,24 +245,24 @@ __global__ void __launch_bounds__(32 * kLeafWarps)
   if (te - ta < kLaneLeafMin) {
     // Sparse leaf: one target at a time, lanes over its sources and over the
     // n^3 local coefficients, warp-reduced in float64.
-    for (int c0 = 0; c0 < C; c0 += kLeafCols) {
-      const int cg = min(kLeafCols, C - c0);
+    for (int c0 = 0; c0 < C; c0 += KC) {
+      const int cg = min(KC, C - c0);
       for (int i = ta; i < te; ++i) {
         const double x = tpos[i], y = tpos[(int64_t)Nf + i], z = tpos[2 * (int64_t)Nf + i];
-        Kahan<T> acc[kLeafCols];
+        LeafAcc<T> acc[KC];
         __syncwarp();
         if (lane < 3 * n) {
           const int d = lane / n, mm = lane % n;
           const T u = (T)(ihalfL * ((d == 0 ? x : d == 1 ? y : z) - c[d]));
-          s_b[wl][d][mm][0] = basis_one<T>(n, cheb, u, sTkz, mm);
+          s_bw[(d * n + mm) * 32] = basis_one<T>(n, cheb, u, sTkz, mm);
         }
         __syncwarp();
         const T* Fl = F_L + ((int64_t)leaf * C + c0) * n3;
         for (int l = lane; l < n3; l += 32) {
           const int l1 = l / (n * n), l2 = (l / n) % n, l3 = l % n;
-          const T v = s_b[wl][0][l1][0] * s_b[wl][1][l2][0] * s_b[wl][2][l3][0];
+          const T v = s_bw[l1 * 32] * s_bw[(n + l2) * 32] * s_bw[(2 * n + l3) * 32];
 #pragma unroll
-          for (int cc = 0; cc < kLeafCols; ++cc)
+          for (int cc = 0; cc < KC; ++cc)
             if (cc < cg) acc[cc].add(Fl[cc * n3 + l] * v);
         }
         int q = 0;
@@ -263,12 +275,12 @@ __global__ void __launch_bounds__(32 * kLeafWarps)
           if (isinf(kv)) kv = 0;  // coincident points (include/compute.hpp:767)
           const double* wj = wsorted + (int64_t)j * C + c0;
 #pragma unroll
-          for (int cc = 0; cc < kLeafCols; ++cc)
+          for (int cc = 0; cc < KC; ++cc)
             if (cc < cg) acc[cc].add(kv * (T)wj[cc]);
         }
-        double tot[kLeafCols];
+        double tot[KC];
 #pragma unroll
-        for (int cc = 0; cc < kLeafCols; ++cc) {
+        for (int cc = 0; cc < KC; ++cc) {
           double v = acc[cc].value();
 #pragma unroll
           for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
@@ -277,7 +289,7 @@ __global__ void __launch_bounds__(32 * kLeafWarps)
         if (lane == 0) {
           const int64_t oi = tperm[i];
 #pragma unroll
-          for (int cc = 0; cc < kLeafCols; ++cc)
+          for (int cc = 0; cc < KC; ++cc)
             if (cc < cg) out[(int64_t)(c0 + cc) * Nf + oi] += tot[cc];
         }
       }
@@ -285,8 +297,8 @@ __global__ void __launch_bounds__(32 * kLeafWarps)
     return;
   }
   // Dense leaf: one target per lane, sources through shared-memory tiles.
-  for (int c0 = 0; c0 < C; c0 += kLeafCols) {
-    const int cg = min(kLeafCols, C - c0);
+  for (int c0 = 0; c0 < C; c0 += KC) {
+    const int cg = min(KC, C - c0);
     for (int t0 = ta; t0 < te; t0 += 32) {
       const int i = t0 + lane;
       const bool active = i < te;
@@ -294,24 +306,24 @@ __global__ void __launch_bounds__(32 * kLeafWarps)
       if (active) x = tpos[i], y = tpos[(int64_t)Nf + i], z = tpos[2 * (int64_t)Nf + i];
       RelPos<T> tp;
       tp.set(x - c[0], y - c[1], z - c[2]);
-      Kahan<T> acc[kLeafCols];
+      LeafAcc<T> acc[KC];
       // far field: phi += sum_l F[l] Sx[l1] Sy[l2] Sz[l3]
       if (active) {
-        T(*b)[kMaxOrder][32] = s_b[wl];  // b[d][m][lane]: conflict-free, no local memory
+        T* b = s_bw + lane;  // b[(d n + m) 32]: conflict-free, no local memory
         for (int m = 0; m < n; ++m) {
-          b[0][m][lane] = basis_one<T>(n, cheb, (T)(ihalfL * (x - c[0])), sTkz, m);
-          b[1][m][lane] = basis_one<T>(n, cheb, (T)(ihalfL * (y - c[1])), sTkz, m);
-          b[2][m][lane] = basis_one<T>(n, cheb, (T)(ihalfL * (z - c[2])), sTkz, m);
+          b[m * 32] = basis_one<T>(n, cheb, (T)(ihalfL * (x - c[0])), sTkz, m);
+          b[(n + m) * 32] = basis_one<T>(n, cheb, (T)(ihalfL * (y - c[1])), sTkz, m);
+          b[(2 * n + m) * 32] = basis_one<T>(n, cheb, (T)(ihalfL * (z - c[2])), sTkz, m);
         }
         const T* Fl = F_L + ((int64_t)leaf * C + c0) * n3;
         int l = 0;
         for (int l1 = 0; l1 < n; ++l1)
           for (int l2 = 0; l2 < n; ++l2) {
-            const T b12 = b[0][l1][lane] * b[1][l2][lane];
+            const T b12 = b[l1 * 32] * b[(n + l2) * 32];
             for (int l3 = 0; l3 < n; ++l3, ++l) {
-              const T v = b12 * b[2][l3][lane];
+              const T v = b12 * b[(2 * n + l3) * 32];
 #pragma unroll
-              for (int cc = 0; cc < kLeafCols; ++cc)
+              for (int cc = 0; cc < KC; ++cc)
                 if (cc < cg) acc[cc].add(Fl[cc * n3 + l] * v);
             }
           }
@@ -335,14 +347,14 @@ __global__ void __launch_bounds__(32 * kLeafWarps)
           }
           const double* wj = wsorted + (int64_t)j * C + c0;
 #pragma unroll
-          for (int cc = 0; cc < kLeafCols; ++cc) s_w[wl][lane][cc] = cc < cg ? (T)wj[cc] : T(0);
+          for (int cc = 0; cc < KC; ++cc) s_w[wl][lane][cc] = cc < cg ? (T)wj[cc] : T(0);
         }
         __syncwarp();
         if (active) {
           const int m = min(32, nsrc_total - v0);
-          T part[kLeafCols];
+          T part[KC];
 #pragma unroll
-          for (int cc = 0; cc < kLeafCols; ++cc) part[cc] = 0;
+          for (int cc = 0; cc < KC; ++cc) part[cc] = 0;
 #pragma unroll 4
           for (int jj = 0; jj < m; ++jj) {
             T d[3];
@@ -350,11 +362,11 @@ __global__ void __launch_bounds__(32 * kLeafWarps)
             T kv = KF::template eval<T>(d[0], d[1], d[2], kp);
             if (isinf(kv)) kv = 0;  // coincident points (include/compute.hpp:767)
 #pragma unroll
-            for (int cc = 0; cc < kLeafCols; ++cc)
+            for (int cc = 0; cc < KC; ++cc)
               if (cc < cg) part[cc] = fma(kv, s_w[wl][jj][cc], part[cc]);
           }
 #pragma unroll
-          for (int cc = 0; cc < kLeafCols; ++cc)
+          for (int cc = 0; cc < KC; ++cc)
             if (cc < cg) acc[cc].add(part[cc]);
         }
         __syncwarp();
@@ -362,7 +374,7 @@ __global__ void __launch_bounds__(32 * kLeafWarps)
       if (active) {
         const int64_t oi = tperm[i];
 #pragma unroll
-        for (int cc = 0; cc < kLeafCols; ++cc)
+        for (int cc = 0; cc < KC; ++cc)
           if (cc < cg) out[(int64_t)(c0 + cc) * Nf + oi] += (double)acc[cc].value();
       }
     }
@@ -385,7 +397,10 @@ struct LeafLaunch {
     Workspace& ws = t->ws;
     const int64_t perS = (int64_t)C * t->n3;
     if (int rc_ = kt_begin(t, KS_LEAF, st)) return rc_;
-    k_leaf<KF, T><<<(nl + kLeafWarps - 1) / kLeafWarps, 32 * kLeafWarps, 0, st>>>(
+    const size_t dyn = sizeof(T) * kLeafWarps * 3 * t->n * 32;
+    // one column: registers for one; otherwise columns in passes of kLeafCols
+    auto kern = C == 1 ? k_leaf<KF, T, 1> : k_leaf<KF, T, kLeafCols>;
+    kern<<<(nl + kLeafWarps - 1) / kLeafWarps, 32 * kLeafWarps, dyn, st>>>(
         ws.lists.as<int>() + t->lists.tgt_off[L], nl, ws.tstart.as<int>(), ws.sstart.as<int>(),
         ws.tperm.as<int>(), ws.tpos.as<double>(), ws.spos.as<double>(), ws.wsorted.as<double>(),
         (int)Nf, (int)Ns, C, ws.F.as<T>() + level_offset(L, perS), t->n, t->p.use_chebyshev,
