@@ -181,8 +181,8 @@ using LeafAcc = typename std::conditional<sizeof(T) == 4, Kahan<T>, PlainSum<T>>
 // T = float (mixed path): kernel values, interpolation and per-tile partial
 // sums in float32, each lane's running sums compensated (Kahan), the output
 // update in float64.  T = double: everything in float64.
-template <class KF, typename T, int KC>
-__global__ void __launch_bounds__(32 * kLeafWarps, 4)
+template <class KF, typename T, int KC, bool DENSE>
+__global__ void __launch_bounds__(32 * kLeafWarps, DENSE ? 4 : 6)
     k_leaf(const int* __restrict__ leaves, int nleaves, const int* __restrict__ tstart,
            const int* __restrict__ sstart, const int* __restrict__ tperm,
            const double* __restrict__ tpos, const double* __restrict__ spos,
@@ -195,12 +195,13 @@ __global__ void __launch_bounds__(32 * kLeafWarps, 4)
   __shared__ double kp[4];
   __shared__ int s_nb[kLeafWarps][27][2];  // neighbour source ranges
   __shared__ int s_pre[kLeafWarps][28];    // exclusive prefix of their lengths
-  __shared__ V4 s_sh[kLeafWarps][32];      // staged sources: position (hi)
-  __shared__ V4 s_sl[kLeafWarps][kMixed ? 32 : 1];  // position (lo), mixed path
-  __shared__ T s_w[kLeafWarps][32][KC];             // staged weights
+  __shared__ V4 s_sh[kLeafWarps][DENSE ? 32 : 1];              // staged sources: position (hi)
+  __shared__ V4 s_sl[kLeafWarps][DENSE && kMixed ? 32 : 1];    // position (lo), mixed path
+  __shared__ T s_w[kLeafWarps][DENSE ? 32 : 1][KC];            // staged weights
   // basis values of each lane's target, [warp][dim][m < n][lane] (dynamic, sized by n)
   extern __shared__ __align__(16) unsigned char leaf_dyn[];
   T* s_bw = reinterpret_cast<T*>(leaf_dyn) + (threadIdx.x >> 5) * 3 * n * 32;
+  __shared__ T s_bs[kLeafWarps][DENSE ? 1 : 3 * kMaxOrder];  // sparse path: the warp's target
   for (int i = threadIdx.x; i < n * n; i += blockDim.x) sTkz[i] = Tkz_g[i];
   if (threadIdx.x < 4) kp[threadIdx.x] = kparam_g[threadIdx.x];
   __syncthreads();
@@ -209,6 +210,7 @@ __global__ void __launch_bounds__(32 * kLeafWarps, 4)
   if (wid >= nleaves) return;
   const int leaf = leaves[wid];
   const int ta = tstart[leaf], te = tstart[leaf + 1];
+  if ((te - ta >= kLaneLeafMin) != DENSE) return;  // the other instantiation's leaf
   const int n3 = n * n * n;
   double c[3];
   cell_center_d((uint32_t)leaf, L, box, c);
@@ -242,7 +244,7 @@ __global__ void __launch_bounds__(32 * kLeafWarps, 4)
   }
   __syncwarp();
   const int nsrc_total = s_pre[wl][27];
-  if (te - ta < kLaneLeafMin) {
+  if constexpr (!DENSE) {
     // Sparse leaf: one target at a time, lanes over its sources and over the
     // n^3 local coefficients, warp-reduced in float64.
     for (int c0 = 0; c0 < C; c0 += KC) {
@@ -254,13 +256,13 @@ __global__ void __launch_bounds__(32 * kLeafWarps, 4)
         if (lane < 3 * n) {
           const int d = lane / n, mm = lane % n;
           const T u = (T)(ihalfL * ((d == 0 ? x : d == 1 ? y : z) - c[d]));
-          s_bw[(d * n + mm) * 32] = basis_one<T>(n, cheb, u, sTkz, mm);
+          s_bs[wl][d * n + mm] = basis_one<T>(n, cheb, u, sTkz, mm);
         }
         __syncwarp();
         const T* Fl = F_L + ((int64_t)leaf * C + c0) * n3;
         for (int l = lane; l < n3; l += 32) {
           const int l1 = l / (n * n), l2 = (l / n) % n, l3 = l % n;
-          const T v = s_bw[l1 * 32] * s_bw[(n + l2) * 32] * s_bw[(2 * n + l3) * 32];
+          const T v = s_bs[wl][l1] * s_bs[wl][n + l2] * s_bs[wl][2 * n + l3];
 #pragma unroll
           for (int cc = 0; cc < KC; ++cc)
             if (cc < cg) acc[cc].add(Fl[cc * n3 + l] * v);
@@ -294,8 +296,7 @@ __global__ void __launch_bounds__(32 * kLeafWarps, 4)
         }
       }
     }
-    return;
-  }
+  } else {
   // Dense leaf: one target per lane, sources through shared-memory tiles.
   for (int c0 = 0; c0 < C; c0 += KC) {
     const int cg = min(KC, C - c0);
@@ -379,6 +380,7 @@ __global__ void __launch_bounds__(32 * kLeafWarps, 4)
       }
     }
   }
+  }
 }
 
 template <typename T>
@@ -398,14 +400,18 @@ struct LeafLaunch {
     const int64_t perS = (int64_t)C * t->n3;
     if (int rc_ = kt_begin(t, KS_LEAF, st)) return rc_;
     const size_t dyn = sizeof(T) * kLeafWarps * 3 * t->n * 32;
-    // one column: registers for one; otherwise columns in passes of kLeafCols
-    auto kern = C == 1 ? k_leaf<KF, T, 1> : k_leaf<KF, T, kLeafCols>;
-    kern<<<(nl + kLeafWarps - 1) / kLeafWarps, 32 * kLeafWarps, dyn, st>>>(
-        ws.lists.as<int>() + t->lists.tgt_off[L], nl, ws.tstart.as<int>(), ws.sstart.as<int>(),
-        ws.tperm.as<int>(), ws.tpos.as<double>(), ws.spos.as<double>(), ws.wsorted.as<double>(),
-        (int)Nf, (int)Ns, C, ws.F.as<T>() + level_offset(L, perS), t->n, t->p.use_chebyshev,
-        ops_view<T>(t).Tkz, t->p.L, L, kparam, out);
-    PB_LAUNCH("leaf");
+    // one column: registers for one; otherwise columns in passes of kLeafCols.
+    // Dense and sparse leaves run as two launches over the same leaf list.
+    for (int dense = 1; dense >= 0; --dense) {
+      auto kern = C == 1 ? (dense ? k_leaf<KF, T, 1, true> : k_leaf<KF, T, 1, false>)
+                         : (dense ? k_leaf<KF, T, kLeafCols, true> : k_leaf<KF, T, kLeafCols, false>);
+      kern<<<(nl + kLeafWarps - 1) / kLeafWarps, 32 * kLeafWarps, dense ? dyn : 0, st>>>(
+          ws.lists.as<int>() + t->lists.tgt_off[L], nl, ws.tstart.as<int>(), ws.sstart.as<int>(),
+          ws.tperm.as<int>(), ws.tpos.as<double>(), ws.spos.as<double>(), ws.wsorted.as<double>(),
+          (int)Nf, (int)Ns, C, ws.F.as<T>() + level_offset(L, perS), t->n, t->p.use_chebyshev,
+          ops_view<T>(t).Tkz, t->p.L, L, kparam, out);
+      PB_LAUNCH("leaf");
+    }
     if (int rc_ = kt_end(t, st)) return rc_;
     return PBBFMM_OK;
   }
