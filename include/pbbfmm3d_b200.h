@@ -116,6 +116,25 @@ int pbbfmm_compute_device(pbbfmm_tree *tree, const double *d_target, int64_t Nf,
                           const double *d_source, int64_t Ns, const double *d_weight, int nCols,
                           double *d_output, int precision, void *stream);
 
+/* Adjoint of the matvec f = K(target, source) w, for a loss L with upstream
+ * gradient g = dL/df (Nf x nCols, column-major, device).  No counterpart in
+ * the reference, which has no derivatives; its transposed product is the
+ * reference's H2_3D_Compute with sources and targets swapped.  Each output is
+ * accumulated into when non-NULL:
+ *   d_grad_weight (Ns x nCols) += K^T g, the exact transpose of this tree's
+ *       FMM (same box, same interaction lists, transposed operators);
+ *   d_grad_source (Ns x 3, xyz AoS) += dL/dy_j = sum_c w_jc grad_y phi_c(y_j),
+ *       phi = K^T g, through the differentiated interpolation basis and the
+ *       kernel gradient (needs d_weight);
+ *   d_grad_target (Nf x 3, xyz AoS) += dL/dx_i = sum_c g_ic grad_x f_c(x_i)
+ *       (needs d_weight).
+ * Asynchronous on `stream`; precision: PBBFMM_PREC_*. */
+int pbbfmm_compute_adjoint_device(pbbfmm_tree *tree, const double *d_target, int64_t Nf,
+                                  const double *d_source, int64_t Ns, const double *d_weight,
+                                  const double *d_g, int nCols, double *d_grad_weight,
+                                  double *d_grad_source, double *d_grad_target, int precision,
+                                  void *stream);
+
 /* Precision used by pbbfmm_compute (default PBBFMM_PREC_FP64). */
 int pbbfmm_set_precision(pbbfmm_tree *tree, int precision);
 

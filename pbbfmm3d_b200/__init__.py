@@ -278,3 +278,46 @@ def compute_device(tree: H2_3D_Tree, target, source, weight, nCols: int, output,
         tree._h, target.data_ptr(), Nf, source.data_ptr(), Ns, weight.data_ptr(), int(nCols),
         output.data_ptr(), prec, ctypes.c_void_p(stream)))
     return output
+
+
+def compute_adjoint_device(tree: H2_3D_Tree, target, source, weight, g, nCols: int,
+                           grad_weight=None, grad_source=None, grad_target=None,
+                           precision: Optional[int] = None, stream=None):
+    """Adjoint of ``compute_device`` on torch CUDA tensors (float64,
+    contiguous): given g = dL/d(output) (nCols, Nf), accumulate
+    grad_weight (nCols, Ns) += K^T g, grad_source (Ns, 3) += dL/d(source) and
+    grad_target (Nf, 3) += dL/d(target), each when given.  ``weight`` is
+    needed for the position gradients.  No synchronisation."""
+    import torch
+
+    def ok(x):
+        return (isinstance(x, torch.Tensor) and x.is_cuda and x.dtype == torch.float64
+                and x.is_contiguous())
+
+    for name, x in (("target", target), ("source", source), ("g", g)):
+        if not ok(x):
+            raise TypeError(name + " must be a contiguous float64 CUDA tensor")
+    for name, x in (("weight", weight), ("grad_weight", grad_weight),
+                    ("grad_source", grad_source), ("grad_target", grad_target)):
+        if x is not None and not ok(x):
+            raise TypeError(name + " must be a contiguous float64 CUDA tensor")
+    Nf, Ns = target.numel() // 3, source.numel() // 3
+    if g.numel() != Nf * nCols:
+        raise ValueError("g must hold Nf*nCols values")
+    if grad_weight is not None and grad_weight.numel() != Ns * nCols:
+        raise ValueError("grad_weight must hold Ns*nCols values")
+    if grad_source is not None and grad_source.numel() != Ns * 3:
+        raise ValueError("grad_source must hold Ns*3 values")
+    if grad_target is not None and grad_target.numel() != Nf * 3:
+        raise ValueError("grad_target must hold Nf*3 values")
+    if stream is None:
+        stream = torch.cuda.current_stream(target.device).cuda_stream
+    prec = tree.precision if precision is None else int(precision)
+
+    def ptr(x):
+        return None if x is None else x.data_ptr()
+
+    _lib.check(_lib.lib().pbbfmm_compute_adjoint_device(
+        tree._h, target.data_ptr(), Nf, source.data_ptr(), Ns, ptr(weight), g.data_ptr(),
+        int(nCols), ptr(grad_weight), ptr(grad_source), ptr(grad_target), prec,
+        ctypes.c_void_p(stream)))

@@ -51,6 +51,8 @@ EXPORTS = {
     "pbbfmm_tree_destroy": ([_vp], ctypes.c_int),
     "pbbfmm_compute": ([_vp, _dp, _i64, _dp, _i64, _dp, ctypes.c_int, _dp], ctypes.c_int),
     "pbbfmm_compute_device": ([_vp, _vp, _i64, _vp, _i64, _vp, ctypes.c_int, _vp, ctypes.c_int, _vp], ctypes.c_int),
+    "pbbfmm_compute_adjoint_device": ([_vp, _vp, _i64, _vp, _i64, _vp, _vp, ctypes.c_int, _vp, _vp,
+                                       _vp, ctypes.c_int, _vp], ctypes.c_int),
     "pbbfmm_set_precision": ([_vp, ctypes.c_int], ctypes.c_int),
     "pbbfmm_set_tensor_cores": ([_vp, ctypes.c_int], ctypes.c_int),
     "pbbfmm_tensor_core_m2l": ([_vp], ctypes.c_int),

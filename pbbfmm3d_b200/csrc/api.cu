@@ -9,6 +9,7 @@
 #include <cstring>
 #include <atomic>
 #include <string>
+#include <utility>
 
 #include "fmm.cuh"
 
@@ -111,22 +112,23 @@ static float tf32_round(float x) {
 
 // Operands of the tensor-core Chebyshev M2L: for each level and operator o,
 // E_o^T as NP rows of KP floats (row f holds E_o[f][s], s < rs), split into
-// TF32 hi = tf32(x) and lo = tf32(x - hi), zero padded.
-static int upload_tc_operators(pbbfmm_tree* t) {
-  const int rf = t->ops.rf, rs = t->ops.rs, nlev = t->ops.nlev;
+// TF32 hi = tf32(x) and lo = tf32(x - hi), zero padded.  K: nlev x 316
+// column-major rf x rs blocks.  Leaves eth / etl null when NP exceeds the
+// tensor-core limit (the float path then uses the CUDA-core kernel).
+static int upload_tc_split(const double* K, int nlev, int rf, int rs, float** eth, float** etl,
+                           int* np, int* kp) {
   const int NP = (rf + 15) / 16 * 16, KP = (rs + 31) / 32 * 32;
-  if (t->f_Eth) cudaFree(t->f_Eth);
-  if (t->f_Etl) cudaFree(t->f_Etl);
-  t->f_Eth = t->f_Etl = nullptr;
-  t->tc_np = NP;
-  t->tc_kp = KP;
-  if (NP > kTcMaxN) return PBBFMM_OK;  // the float path uses the CUDA-core kernel
+  if (*eth) cudaFree(*eth);
+  if (*etl) cudaFree(*etl);
+  *eth = *etl = nullptr;
+  *np = NP;
+  *kp = KP;
+  if (NP > kTcMaxN) return PBBFMM_OK;
   const size_t per = (size_t)316 * NP * KP, total = per * nlev;
   std::vector<float> hi(total, 0.f), lo(total, 0.f);
-  const double* K = t->ops.K.data();
   parallel_for((int64_t)nlev * 316, [&](int64_t b0, int64_t b1) {
     for (int64_t b = b0; b < b1; ++b) {
-      const double* E = K + (size_t)b * rf * rs;  // column-major rf x rs
+      const double* E = K + (size_t)b * rf * rs;
       float* h = hi.data() + (size_t)b * NP * KP;
       float* l = lo.data() + (size_t)b * NP * KP;
       for (int f = 0; f < rf; ++f)
@@ -138,10 +140,17 @@ static int upload_tc_operators(pbbfmm_tree* t) {
         }
     }
   });
-  PB_CUDA(cudaMalloc(&t->f_Eth, total * sizeof(float)));
-  PB_CUDA(cudaMalloc(&t->f_Etl, total * sizeof(float)));
-  PB_CUDA(cudaMemcpy(t->f_Eth, hi.data(), total * sizeof(float), cudaMemcpyHostToDevice));
-  PB_CUDA(cudaMemcpy(t->f_Etl, lo.data(), total * sizeof(float), cudaMemcpyHostToDevice));
+  PB_CUDA(cudaMalloc(eth, total * sizeof(float)));
+  PB_CUDA(cudaMalloc(etl, total * sizeof(float)));
+  PB_CUDA(cudaMemcpy(*eth, hi.data(), total * sizeof(float), cudaMemcpyHostToDevice));
+  PB_CUDA(cudaMemcpy(*etl, lo.data(), total * sizeof(float), cudaMemcpyHostToDevice));
+  return PBBFMM_OK;
+}
+
+static int upload_tc_operators(pbbfmm_tree* t) {
+  if (int rc = upload_tc_split(t->ops.K.data(), t->ops.nlev, t->ops.rf, t->ops.rs, &t->f_Eth,
+                               &t->f_Etl, &t->tc_np, &t->tc_kp))
+    return rc;
   if (!t->h_tc_err) {
     PB_CUDA(cudaHostAlloc(&t->h_tc_err, sizeof(int), cudaHostAllocMapped));
     *t->h_tc_err = 0;
@@ -245,12 +254,95 @@ static std::vector<int> m2l_offsets(const int* Ktable) {
   return offs;
 }
 
+static void free_adjoint_ops(pbbfmm_tree* t) {
+  double** d[] = {&t->adj.E, &t->adj.U, &t->adj.VT};
+  for (double** b : d) {
+    if (*b) cudaFree(*b);
+    *b = nullptr;
+  }
+  float** f[] = {&t->adj.fE, &t->adj.fU, &t->adj.fVT, &t->adj.fEth, &t->adj.fEtl};
+  for (float** b : f) {
+    if (*b) cudaFree(*b);
+    *b = nullptr;
+  }
+  t->adj_ready = false;
+}
+
+// Transposed Chebyshev operators for the adjoint pass (reference operator
+// layout: E_p column-major rf x rs, U column-major n^3 x rf, VT column-major
+// rs x n^3): U' = VT^T, VT' = U^T and E'_p = E_q^T where q is the operator of
+// the opposite offset, since the pair (s <- t) has offset -(t <- s).
+static int build_adjoint_ops(pbbfmm_tree* t) {
+  free_adjoint_ops(t);
+  const int rf = t->ops.rf, rs = t->ops.rs, nlev = t->ops.nlev, n3 = t->n3;
+  std::vector<double> E((size_t)nlev * 316 * rf * rs), U((size_t)nlev * n3 * rs),
+      VT((size_t)nlev * rf * n3);
+  std::vector<int> neg(316, -1);
+  for (int a = -3; a <= 3; ++a)
+    for (int b = -3; b <= 3; ++b)
+      for (int c = -3; c <= 3; ++c) {
+        const int p = t->w.Ktable[49 * (a + 3) + 7 * (b + 3) + (c + 3)];
+        const int q = t->w.Ktable[49 * (3 - a) + 7 * (3 - b) + (3 - c)];
+        if (p >= 0) neg[p] = q;
+      }
+  for (int p = 0; p < 316; ++p)
+    if (neg[p] < 0) {
+      set_error("operator table has no opposite offset");
+      return PBBFMM_ERR_STATE;
+    }
+  for (int lv = 0; lv < nlev; ++lv) {
+    for (int p = 0; p < 316; ++p) {
+      const double* Eq = t->ops.K.data() + ((size_t)lv * 316 + neg[p]) * rf * rs;
+      double* Ep = E.data() + ((size_t)lv * 316 + p) * rf * rs;  // rs x rf column-major
+      for (int i = 0; i < rs; ++i)
+        for (int j = 0; j < rf; ++j) Ep[i + (size_t)rs * j] = Eq[j + (size_t)rf * i];
+    }
+    const double* Ul = t->ops.U.data() + (size_t)lv * n3 * rf;
+    const double* Vl = t->ops.VT.data() + (size_t)lv * rs * n3;
+    for (int l = 0; l < n3; ++l) {
+      for (int s2 = 0; s2 < rs; ++s2) U[(size_t)lv * n3 * rs + l + (size_t)n3 * s2] = Vl[s2 + (size_t)rs * l];
+      for (int f = 0; f < rf; ++f) VT[(size_t)lv * rf * n3 + f + (size_t)rf * l] = Ul[l + (size_t)n3 * f];
+    }
+  }
+  int rc;
+  if ((rc = upload(&t->adj.E, E.data(), E.size()))) return rc;
+  if ((rc = upload(&t->adj.U, U.data(), U.size()))) return rc;
+  if ((rc = upload(&t->adj.VT, VT.data(), VT.size()))) return rc;
+  if ((rc = upload_f32(&t->adj.fE, E.data(), E.size()))) return rc;
+  if ((rc = upload_f32(&t->adj.fU, U.data(), U.size()))) return rc;
+  if ((rc = upload_f32(&t->adj.fVT, VT.data(), VT.size()))) return rc;
+  if ((rc = upload_tc_split(E.data(), nlev, rs, rf, &t->adj.fEth, &t->adj.fEtl, &t->adj.np,
+                            &t->adj.kp)))
+    return rc;
+  t->adj.rf = rs;
+  t->adj.rs = rf;
+  t->adj_ready = true;
+  return PBBFMM_OK;
+}
+
+// Exchange the forward and adjoint Chebyshev operator sets (an involution).
+static void swap_adjoint_ops(pbbfmm_tree* t) {
+  std::swap(t->d_E, t->adj.E);
+  std::swap(t->d_U, t->adj.U);
+  std::swap(t->d_VT, t->adj.VT);
+  std::swap(t->f_E, t->adj.fE);
+  std::swap(t->f_U, t->adj.fU);
+  std::swap(t->f_VT, t->adj.fVT);
+  std::swap(t->f_Eth, t->adj.fEth);
+  std::swap(t->f_Etl, t->adj.fEtl);
+  std::swap(t->ops.rf, t->adj.rf);
+  std::swap(t->ops.rs, t->adj.rs);
+  std::swap(t->tc_np, t->adj.np);
+  std::swap(t->tc_kp, t->adj.kp);
+}
+
 static int upload_operators(pbbfmm_tree* t) {
   if (t->device < 0) {
     t->ops_ready = true;
     return PBBFMM_OK;
   }
   PB_CUDA(cudaSetDevice(t->device));
+  free_adjoint_ops(t);  // rebuilt from the new operators on the next adjoint
   int rc;
   if (t->p.use_chebyshev) {
     if ((rc = upload(&t->d_E, t->ops.K.data(), t->ops.K.size()))) return rc;
@@ -289,6 +381,7 @@ static void free_tree_device(pbbfmm_tree* t) {
   t->f_Eth = t->f_Etl = nullptr;
   if (t->h_tc_err) cudaFreeHost(t->h_tc_err);
   t->h_tc_err = t->d_tc_err = nullptr;
+  free_adjoint_ops(t);
   Workspace& ws = t->ws;
   DevBuf* all[] = {&ws.bbox_part, &ws.ctr,   &ws.key,     &ws.key_sorted, &ws.idx,
                    &ws.tperm,     &ws.sperm, &ws.tstart,  &ws.sstart,     &ws.tpos,
@@ -689,6 +782,96 @@ int pbbfmm_compute_device(pbbfmm_tree* t, const double* d_target, int64_t Nf,
     int rc = compute_chunk(t, d_target, Nf, d_source, Ns, d_weight + (int64_t)c0 * Ns, cc,
                            d_output + (int64_t)c0 * Nf, precision, st);
     if (rc) return rc;
+  }
+  return PBBFMM_OK;
+}
+
+// Restores the forward configuration of a tree after an adjoint or gradient
+// pass, on every exit path.
+struct PassGuard {
+  pbbfmm_tree* t;
+  bool swapped = false;
+  ~PassGuard() {
+    if (swapped) swap_adjoint_ops(t);
+    t->bbox_pts = nullptr;
+    t->bbox_n = 0;
+    t->gl = pbbfmm_tree::GradLeaf{};
+  }
+};
+
+int pbbfmm_compute_adjoint_device(pbbfmm_tree* t, const double* d_target, int64_t Nf,
+                                  const double* d_source, int64_t Ns, const double* d_weight,
+                                  const double* d_g, int nCols, double* d_grad_weight,
+                                  double* d_grad_source, double* d_grad_target, int precision,
+                                  void* stream) {
+  if (!t) {
+    set_error("null tree");
+    return PBBFMM_ERR_ARG;
+  }
+  if (!t->ops_ready || t->device < 0) {
+    set_error("tree cannot compute: host-only or operators missing");
+    return PBBFMM_ERR_STATE;
+  }
+  if (Nf < 0 || Ns < 0 || nCols < 1 || Nf > INT32_MAX || Ns > INT32_MAX) {
+    set_error("bad sizes (0 <= Nf, Ns < 2^31, nCols >= 1)");
+    return PBBFMM_ERR_ARG;
+  }
+  if (precision != PBBFMM_PREC_FP64 && precision != PBBFMM_PREC_MIXED) {
+    set_error("bad precision mode");
+    return PBBFMM_ERR_ARG;
+  }
+  if (Nf > 0 && Ns > 0 &&
+      (!d_target || !d_source || !d_g || ((d_grad_source || d_grad_target) && !d_weight))) {
+    set_error("null data pointer (gradients with respect to positions need the weights)");
+    return PBBFMM_ERR_ARG;
+  }
+  if (int rc = take_tc_timeout(t)) return rc;
+  if (Nf == 0 || Ns == 0) return PBBFMM_OK;
+  PB_CUDA(cudaSetDevice(t->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  const int cmax = 64;
+  if (d_grad_weight || d_grad_source) {
+    // Transposed pass on the forward tree: the sources become targets, the
+    // targets sources carrying g, the box stays the forward targets' one.
+    PassGuard guard{t};
+    if (t->p.use_chebyshev) {
+      if (!t->adj_ready)
+        if (int rc = build_adjoint_ops(t)) return rc;
+      swap_adjoint_ops(t);
+      guard.swapped = true;
+    }
+    t->bbox_pts = d_target;
+    t->bbox_n = Nf;
+    for (int c0 = 0; c0 < nCols; c0 += cmax) {
+      const int cc = nCols - c0 < cmax ? nCols - c0 : cmax;
+      t->gl = pbbfmm_tree::GradLeaf{};
+      if (d_grad_source) {
+        t->gl.on = true;
+        t->gl.contract = d_weight + (int64_t)c0 * Ns;
+        t->gl.grad_out = d_grad_source;
+        t->gl.values = d_grad_weight != nullptr;
+      }
+      int rc = compute_chunk(t, d_source, Ns, d_target, Nf, d_g + (int64_t)c0 * Nf, cc,
+                             d_grad_weight ? d_grad_weight + (int64_t)c0 * Ns : nullptr,
+                             precision, st);
+      if (rc) return rc;
+    }
+  }
+  if (d_grad_target) {
+    // forward pass whose leaf phase evaluates the potentials' gradients at the
+    // targets, contracted with g
+    PassGuard guard{t};
+    for (int c0 = 0; c0 < nCols; c0 += cmax) {
+      const int cc = nCols - c0 < cmax ? nCols - c0 : cmax;
+      t->gl = pbbfmm_tree::GradLeaf{};
+      t->gl.on = true;
+      t->gl.contract = d_g + (int64_t)c0 * Nf;
+      t->gl.grad_out = d_grad_target;
+      t->gl.values = false;
+      int rc = compute_chunk(t, d_target, Nf, d_source, Ns, d_weight + (int64_t)c0 * Ns, cc,
+                             nullptr, precision, st);
+      if (rc) return rc;
+    }
   }
   return PBBFMM_OK;
 }

@@ -54,6 +54,14 @@ struct Kern<PBBFMM_KERNEL_LAPLACIAN> {
   __device__ static T eval(T dx, T dy, T dz, const double*) {
     return inv_sqrt(dx * dx + dy * dy + dz * dz);
   }
+  // value, and g = dK/dd (the gradient with respect to the target is -g); g = 0 at d = 0
+  template <typename T>
+  __device__ static T grad(T dx, T dy, T dz, const double* p, T* g) {
+    const T r2 = dx * dx + dy * dy + dz * dz, ri = inv_sqrt(r2);
+    const T f = r2 > T(0) ? -ri * ri * ri : T(0);
+    g[0] = f * dx, g[1] = f * dy, g[2] = f * dz;
+    return ri;
+  }
 };
 template <>
 struct Kern<PBBFMM_KERNEL_ONEOVERR2> {
@@ -61,6 +69,14 @@ struct Kern<PBBFMM_KERNEL_ONEOVERR2> {
   __device__ static T eval(T dx, T dy, T dz, const double*) {
     T ri = inv_sqrt(dx * dx + dy * dy + dz * dz);
     return ri * ri;
+  }
+  // value, and g = dK/dd (the gradient with respect to the target is -g); g = 0 at d = 0
+  template <typename T>
+  __device__ static T grad(T dx, T dy, T dz, const double* p, T* g) {
+    const T r2 = dx * dx + dy * dy + dz * dz, ri2 = T(1) / r2;
+    const T f = r2 > T(0) ? T(-2) * ri2 * ri2 : T(0);
+    g[0] = f * dx, g[1] = f * dy, g[2] = f * dz;
+    return ri2;
   }
 };
 template <>
@@ -70,6 +86,14 @@ struct Kern<PBBFMM_KERNEL_ONEOVERR4> {
     T ri = inv_sqrt(dx * dx + dy * dy + dz * dz);
     return ri * ri * ri * ri;
   }
+  // value, and g = dK/dd (the gradient with respect to the target is -g); g = 0 at d = 0
+  template <typename T>
+  __device__ static T grad(T dx, T dy, T dz, const double* p, T* g) {
+    const T r2 = dx * dx + dy * dy + dz * dz, ri2 = T(1) / r2;
+    const T f = r2 > T(0) ? T(-4) * ri2 * ri2 * ri2 : T(0);
+    g[0] = f * dx, g[1] = f * dy, g[2] = f * dz;
+    return ri2 * ri2;
+  }
 };
 template <>
 struct Kern<PBBFMM_KERNEL_GAUSSIAN> {
@@ -77,6 +101,13 @@ struct Kern<PBBFMM_KERNEL_GAUSSIAN> {
   __device__ static T eval(T dx, T dy, T dz, const double*) {
     T r = sqrt(dx * dx + dy * dy + dz * dz);
     return exp(-r * r);
+  }
+  // value, and g = dK/dd (the gradient with respect to the target is -g); g = 0 at d = 0
+  template <typename T>
+  __device__ static T grad(T dx, T dy, T dz, const double* p, T* g) {
+    const T k = eval(dx, dy, dz, p), f = T(-2) * k;
+    g[0] = f * dx, g[1] = f * dy, g[2] = f * dz;
+    return k;
   }
 };
 template <>
@@ -86,6 +117,14 @@ struct Kern<PBBFMM_KERNEL_LOGARITHM> {
     T r2 = dx * dx + dy * dy + dz * dz;
     return r2 == T(0) ? T(0) : T(0.5) * log(r2);
   }
+  // value, and g = dK/dd (the gradient with respect to the target is -g); g = 0 at d = 0
+  template <typename T>
+  __device__ static T grad(T dx, T dy, T dz, const double* p, T* g) {
+    const T r2 = dx * dx + dy * dy + dz * dz;
+    const T f = r2 > T(0) ? T(1) / r2 : T(0);
+    g[0] = f * dx, g[1] = f * dy, g[2] = f * dz;
+    return eval(dx, dy, dz, p);
+  }
 };
 template <>
 struct Kern<PBBFMM_KERNEL_QUADRIC> {
@@ -93,12 +132,25 @@ struct Kern<PBBFMM_KERNEL_QUADRIC> {
   __device__ static T eval(T dx, T dy, T dz, const double*) {
     return T(1) + (dx * dx + dy * dy + dz * dz);
   }
+  // value, and g = dK/dd (the gradient with respect to the target is -g); g = 0 at d = 0
+  template <typename T>
+  __device__ static T grad(T dx, T dy, T dz, const double* p, T* g) {
+    g[0] = T(2) * dx, g[1] = T(2) * dy, g[2] = T(2) * dz;
+    return eval(dx, dy, dz, p);
+  }
 };
 template <>
 struct Kern<PBBFMM_KERNEL_INVQUADRIC> {
   template <typename T>
   __device__ static T eval(T dx, T dy, T dz, const double*) {
     return T(1) / (T(1) + (dx * dx + dy * dy + dz * dz));
+  }
+  // value, and g = dK/dd (the gradient with respect to the target is -g); g = 0 at d = 0
+  template <typename T>
+  __device__ static T grad(T dx, T dy, T dz, const double* p, T* g) {
+    const T q = eval(dx, dy, dz, p), f = T(-2) * q * q;
+    g[0] = f * dx, g[1] = f * dy, g[2] = f * dz;
+    return q;
   }
 };
 template <>
@@ -108,12 +160,28 @@ struct Kern<PBBFMM_KERNEL_THINPLATESPLINE> {
     T r2 = dx * dx + dy * dy + dz * dz;
     return r2 == T(0) ? T(0) : T(0.5) * r2 * log(r2);
   }
+  // value, and g = dK/dd (the gradient with respect to the target is -g); g = 0 at d = 0
+  template <typename T>
+  __device__ static T grad(T dx, T dy, T dz, const double* p, T* g) {
+    const T r2 = dx * dx + dy * dy + dz * dz;
+    const T f = r2 > T(0) ? log(r2) + T(1) : T(0);
+    g[0] = f * dx, g[1] = f * dy, g[2] = f * dz;
+    return eval(dx, dy, dz, p);
+  }
 };
 template <>
 struct Kern<PBBFMM_KERNEL_EXPCOV> {
   template <typename T>
   __device__ static T eval(T dx, T dy, T dz, const double* p) {
     return exp(-sqrt(dx * dx + dy * dy + dz * dz) / T(p[0]));
+  }
+  // value, and g = dK/dd (the gradient with respect to the target is -g); g = 0 at d = 0
+  template <typename T>
+  __device__ static T grad(T dx, T dy, T dz, const double* p, T* g) {
+    const T r = sqrt(dx * dx + dy * dy + dz * dz), k = exp(-r / T(p[0]));
+    const T f = r > T(0) ? -k / (T(p[0]) * r) : T(0);
+    g[0] = f * dx, g[1] = f * dy, g[2] = f * dz;
+    return k;
   }
 };
 template <>
@@ -122,12 +190,28 @@ struct Kern<PBBFMM_KERNEL_GAUSSSIGMA> {
   __device__ static T eval(T dx, T dy, T dz, const double* p) {
     return exp(-(dx * dx + dy * dy + dz * dz) / (T(2) * T(p[0]) * T(p[0])));
   }
+  // value, and g = dK/dd (the gradient with respect to the target is -g); g = 0 at d = 0
+  template <typename T>
+  __device__ static T grad(T dx, T dy, T dz, const double* p, T* g) {
+    const T s2 = T(2) * T(p[0]) * T(p[0]);
+    const T k = exp(-(dx * dx + dy * dy + dz * dz) / s2), f = T(-2) * k / s2;
+    g[0] = f * dx, g[1] = f * dy, g[2] = f * dz;
+    return k;
+  }
 };
 template <>
 struct Kern<PBBFMM_KERNEL_ANISOEXP> {
   template <typename T>
   __device__ static T eval(T dx, T dy, T dz, const double*) {
     return T(0.75) * exp(-sqrt(dx * dx / T(100) + dy * dy / T(100) + dz * dz / T(2.25)));
+  }
+  // value, and g = dK/dd (the gradient with respect to the target is -g); g = 0 at d = 0
+  template <typename T>
+  __device__ static T grad(T dx, T dy, T dz, const double* p, T* g) {
+    const T q = sqrt(dx * dx / T(100) + dy * dy / T(100) + dz * dz / T(2.25));
+    const T k = T(0.75) * exp(-q), f = q > T(0) ? -k / q : T(0);
+    g[0] = f * dx / T(100), g[1] = f * dy / T(100), g[2] = f * dz / T(2.25);
+    return k;
   }
 };
 
@@ -264,6 +348,37 @@ __device__ __forceinline__ T basis_one(int n, int cheb, T x, const T* Tkz, int m
       den *= T(-2) * (T(m) - T(j)) / T(n - 1);
     }
   return num / den;
+}
+
+// dS_m/dx on [-1, 1].  Chebyshev: S_m(x) = (2/n) (1/2 + sum_{k>=1} T_k(x_m)
+// T_k(x)), so S_m'(x) = (2/n) sum_{k>=1} T_k(x_m) k U_{k-1}(x) with U the
+// Chebyshev polynomials of the second kind.  Uniform: the derivative of the
+// Lagrange polynomial, sum over i != m of prod_{j != m, i} (x - x_j) / den.
+template <typename T>
+__device__ __forceinline__ T basis_deriv(int n, int cheb, T x, const T* Tkz, int m) {
+  if (cheb) {
+    const T* Tk = Tkz + m * n;
+    T u0 = 1, u1 = T(2) * x, s = 0;  // U_{k-1}, U_k
+    for (int k = 1; k < n; ++k) {
+      s += Tk[k] * T(k) * u0;
+      const T u2 = T(2) * x * u1 - u0;
+      u0 = u1;
+      u1 = u2;
+    }
+    return (T(2) / T(n)) * s;
+  }
+  T den = 1;
+  for (int j = 0; j < n; j++)
+    if (m != j) den *= T(-2) * (T(m) - T(j)) / T(n - 1);
+  T sum = 0;
+  for (int i = 0; i < n; ++i) {
+    if (i == m) continue;
+    T prod = 1;
+    for (int j = 0; j < n; ++j)
+      if (j != m && j != i) prod *= x - (T(1) - T(2) * T(j) / T(n - 1));
+    sum += prod;
+  }
+  return sum / den;
 }
 
 // out[m * stride] = S_m(x), m < n

@@ -383,6 +383,181 @@ __global__ void __launch_bounds__(32 * kLeafWarps, DENSE ? 4 : 6)
   }
 }
 
+// Gradient leaf phase (adjoint and position gradients): for each target x
+// and column c, phi_c(x) = sum_l F_lc S_l(x) + sum_j w_jc K(x, y_j) and its
+// gradient, from the differentiated interpolation basis (chain factor
+// 2 / cell length) and the kernel gradient.  grad_out[i*3 + d] gets
+// sum_c contract[c*Nf + i] d phi_c / d x_d; out[c*Nf + i] gets phi_c when
+// non-null.  One warp per target leaf, one target at a time, lanes over its
+// sources and coefficients.
+constexpr int kGradCols = 4;  // columns per pass (4 accumulators each)
+
+template <class KF, typename T>
+__global__ void __launch_bounds__(32 * kLeafWarps)
+    k_leaf_grad(const int* __restrict__ leaves, int nleaves, const int* __restrict__ tstart,
+                const int* __restrict__ sstart, const int* __restrict__ tperm,
+                const double* __restrict__ tpos, const double* __restrict__ spos,
+                const double* __restrict__ wsorted, int Nf, int Ns, int C,
+                const T* __restrict__ F_L, int n, int cheb, const T* __restrict__ Tkz_g,
+                double box, int L, const double* __restrict__ kparam_g, double* __restrict__ out,
+                const double* __restrict__ contract, double* __restrict__ grad_out) {
+  __shared__ T sTkz[kMaxOrder * kMaxOrder];
+  __shared__ double kp[4];
+  __shared__ int s_nb[kLeafWarps][27][2];
+  __shared__ int s_pre[kLeafWarps][28];
+  __shared__ T s_b[kLeafWarps][6 * kMaxOrder];  // S_m per dimension, then dS_m/dx
+  for (int i = threadIdx.x; i < n * n; i += blockDim.x) sTkz[i] = Tkz_g[i];
+  if (threadIdx.x < 4) kp[threadIdx.x] = kparam_g[threadIdx.x];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+  const int wid = blockIdx.x * kLeafWarps + wl;
+  if (wid >= nleaves) return;
+  const int leaf = leaves[wid];
+  const int ta = tstart[leaf], te = tstart[leaf + 1];
+  const int n3 = n * n * n;
+  double c[3];
+  cell_center_d((uint32_t)leaf, L, box, c);
+  double len = box;
+  for (int i = 0; i < L; ++i) len = 0.5 * len;
+  const double ihalfL = 2. / len;
+  int ax, ay, az;
+  morton_decode((uint32_t)leaf, &ax, &ay, &az);
+  const int nside = 1 << L;
+  if (lane < 27) {
+    const int q = lane;
+    const int bx = ax + q / 9 - 1, by = ay + (q / 3) % 3 - 1, bz = az + q % 3 - 1;
+    int a = 0, e = 0;
+    if (bx >= 0 && by >= 0 && bz >= 0 && bx < nside && by < nside && bz < nside) {
+      const uint32_t bm = morton_encode(bx, by, bz);
+      a = sstart[bm];
+      e = sstart[bm + 1];
+    }
+    s_nb[wl][q][0] = a;
+    s_nb[wl][q][1] = e;
+  }
+  __syncwarp();
+  if (lane == 0) {
+    int acc = 0;
+    for (int q = 0; q < 27; ++q) {
+      s_pre[wl][q] = acc;
+      acc += s_nb[wl][q][1] - s_nb[wl][q][0];
+    }
+    s_pre[wl][27] = acc;
+  }
+  __syncwarp();
+  const int nsrc_total = s_pre[wl][27];
+  const T* Sb = s_b[wl];
+  const T* Db = s_b[wl] + 3 * n;
+  for (int c0 = 0; c0 < C; c0 += kGradCols) {
+    const int cg = min(kGradCols, C - c0);
+    for (int i = ta; i < te; ++i) {
+      const double x = tpos[i], y = tpos[(int64_t)Nf + i], z = tpos[2 * (int64_t)Nf + i];
+      __syncwarp();
+      if (lane < 3 * n) {
+        const int d = lane / n, mm = lane % n;
+        const T u = (T)(ihalfL * ((d == 0 ? x : d == 1 ? y : z) - c[d]));
+        s_b[wl][d * n + mm] = basis_one<T>(n, cheb, u, sTkz, mm);
+        s_b[wl][3 * n + d * n + mm] = basis_deriv<T>(n, cheb, u, sTkz, mm) * (T)ihalfL;
+      }
+      __syncwarp();
+      LeafAcc<T> v[kGradCols], g[kGradCols][3];
+      const T* Fl = F_L + ((int64_t)leaf * C + c0) * n3;
+      for (int l = lane; l < n3; l += 32) {
+        const int l1 = l / (n * n), l2 = (l / n) % n, l3 = l % n;
+        const T b1 = Sb[l1], b2 = Sb[n + l2], b3 = Sb[2 * n + l3];
+        const T e0 = Db[l1] * b2 * b3, e1 = b1 * Db[n + l2] * b3, e2 = b1 * b2 * Db[2 * n + l3];
+        const T val = b1 * b2 * b3;
+#pragma unroll
+        for (int cc = 0; cc < kGradCols; ++cc)
+          if (cc < cg) {
+            const T f = Fl[cc * n3 + l];
+            v[cc].add(f * val);
+            g[cc][0].add(f * e0);
+            g[cc][1].add(f * e1);
+            g[cc][2].add(f * e2);
+          }
+      }
+      int q = 0;
+      for (int vv = lane; vv < nsrc_total; vv += 32) {
+        while (vv >= s_pre[wl][q + 1]) ++q;
+        const int j = s_nb[wl][q][0] + (vv - s_pre[wl][q]);
+        const T dx = (T)(spos[j] - x), dy = (T)(spos[(int64_t)Ns + j] - y),
+                dz = (T)(spos[2 * (int64_t)Ns + j] - z);
+        T gk[3];
+        T kv = KF::template grad<T>(dx, dy, dz, kp, gk);
+        if (isinf(kv)) kv = 0;  // coincident points (include/compute.hpp:767)
+        const double* wj = wsorted + (int64_t)j * C + c0;
+#pragma unroll
+        for (int cc = 0; cc < kGradCols; ++cc)
+          if (cc < cg) {
+            const T w = (T)wj[cc];
+            v[cc].add(kv * w);
+            // d K(x, y_j) / d x = -dK/dd with d = y_j - x
+            g[cc][0].add(-gk[0] * w);
+            g[cc][1].add(-gk[1] * w);
+            g[cc][2].add(-gk[2] * w);
+          }
+      }
+      double tv[kGradCols], tg[kGradCols][3];
+#pragma unroll
+      for (int cc = 0; cc < kGradCols; ++cc) {
+        double a = v[cc].value(), b0 = g[cc][0].value(), b1 = g[cc][1].value(),
+               b2 = g[cc][2].value();
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          a += __shfl_xor_sync(0xffffffffu, a, o);
+          b0 += __shfl_xor_sync(0xffffffffu, b0, o);
+          b1 += __shfl_xor_sync(0xffffffffu, b1, o);
+          b2 += __shfl_xor_sync(0xffffffffu, b2, o);
+        }
+        tv[cc] = a, tg[cc][0] = b0, tg[cc][1] = b1, tg[cc][2] = b2;
+      }
+      if (lane == 0) {
+        const int64_t oi = tperm[i];
+        double gs[3] = {0, 0, 0};
+#pragma unroll
+        for (int cc = 0; cc < kGradCols; ++cc)
+          if (cc < cg) {
+            if (out) out[(int64_t)(c0 + cc) * Nf + oi] += tv[cc];
+            if (grad_out) {
+              const double wc = contract[(int64_t)(c0 + cc) * Nf + oi];
+              gs[0] += wc * tg[cc][0], gs[1] += wc * tg[cc][1], gs[2] += wc * tg[cc][2];
+            }
+          }
+        if (grad_out)
+          for (int d = 0; d < 3; ++d) grad_out[oi * 3 + d] += gs[d];
+      }
+    }
+  }
+}
+
+template <typename T>
+struct LeafGradLaunch {
+  pbbfmm_tree* t;
+  int64_t Nf, Ns;
+  int C;
+  double* out;
+  cudaStream_t st;
+  const double* kparam;
+  template <class KF>
+  int run() {
+    const int L = t->p.tree_level;
+    const int nl = t->lists.ntgt[L];
+    if (nl == 0) return PBBFMM_OK;
+    Workspace& ws = t->ws;
+    const int64_t perS = (int64_t)C * t->n3;
+    if (int rc_ = kt_begin(t, KS_LEAF, st)) return rc_;
+    k_leaf_grad<KF, T><<<(nl + kLeafWarps - 1) / kLeafWarps, 32 * kLeafWarps, 0, st>>>(
+        ws.lists.as<int>() + t->lists.tgt_off[L], nl, ws.tstart.as<int>(), ws.sstart.as<int>(),
+        ws.tperm.as<int>(), ws.tpos.as<double>(), ws.spos.as<double>(), ws.wsorted.as<double>(),
+        (int)Nf, (int)Ns, C, ws.F.as<T>() + level_offset(L, perS), t->n, t->p.use_chebyshev,
+        ops_view<T>(t).Tkz, t->p.L, L, kparam, t->gl.values ? out : nullptr, t->gl.contract,
+        t->gl.grad_out);
+    PB_LAUNCH("leaf_grad");
+    return kt_end(t, st);
+  }
+};
+
 template <typename T>
 struct LeafLaunch {
   pbbfmm_tree* t;
@@ -437,6 +612,14 @@ int run_downward(pbbfmm_tree* t, int C, cudaStream_t st) {
 }
 
 int run_leaves(pbbfmm_tree* t, int64_t Nf, int64_t Ns, int C, double* d_out, cudaStream_t st) {
+  if (t->gl.on) {
+    if (t->cur_prec == PBBFMM_PREC_FP64) {
+      LeafGradLaunch<double> ll{t, Nf, Ns, C, d_out, st, t->d_kparam};
+      return dispatch_kernel(t->p.kernel, ll);
+    }
+    LeafGradLaunch<float> ll{t, Nf, Ns, C, d_out, st, t->d_kparam};
+    return dispatch_kernel(t->p.kernel, ll);
+  }
   if (t->cur_prec == PBBFMM_PREC_FP64) {
     LeafLaunch<double> ll{t, Nf, Ns, C, d_out, st, t->d_kparam};
     return dispatch_kernel(t->p.kernel, ll);

@@ -101,6 +101,24 @@ struct pbbfmm_tree {
   float* f_Etl = nullptr;
   int* h_tc_err = nullptr;  // mapped pinned flag: a tensor-core wait timed out
   int* d_tc_err = nullptr;  // its device address
+  // Adjoint (transposed) Chebyshev operators: U' = VT^T, E'_p = E_{-p}^T,
+  // VT' = U^T, so r_f' = r_s and r_s' = r_f.  Swapped with the forward set
+  // (swap_adjoint_ops) for the duration of an adjoint pass.
+  struct OpSet {
+    double *E = nullptr, *U = nullptr, *VT = nullptr;
+    float *fE = nullptr, *fU = nullptr, *fVT = nullptr, *fEth = nullptr, *fEtl = nullptr;
+    int rf = 0, rs = 0, np = 0, kp = 0;
+  } adj;
+  bool adj_ready = false;
+  // pass settings (set by the adjoint / gradient entry points, cleared after)
+  const double* bbox_pts = nullptr;  // recentre on these points instead of the targets
+  int64_t bbox_n = 0;
+  struct GradLeaf {
+    bool on = false;
+    const double* contract = nullptr;  // [col * Nf + i]: weights of each target's gradient
+    double* grad_out = nullptr;        // [i * 3 + d] += sum_col contract * d phi_col / d x_d
+    bool values = true;                // also add the potentials to the compute's output
+  } gl;
   int cur_prec = PBBFMM_PREC_FP64;  // precision of the compute in flight
   pbbfmm::Workspace ws;
   pbbfmm::LevelLists lists;

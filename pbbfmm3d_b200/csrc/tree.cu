@@ -211,8 +211,11 @@ int run_binning(pbbfmm_tree* t, const double* d_tgt, int64_t Nf, const double* d
   int* idx = ws.idx.as<int>();
   int* lists = ws.lists.as<int>();
 
-  // recentre on the target bounding box
-  k_bbox_partial<<<kBBoxBlocks, kBBoxThreads, 0, st>>>(d_tgt, Nf, ws.bbox_part.as<double>());
+  // recentre on the target bounding box (an adjoint pass keeps the forward
+  // targets' box, given by bbox_pts)
+  const double* bpts = t->bbox_pts ? t->bbox_pts : d_tgt;
+  const int64_t bn = t->bbox_pts ? t->bbox_n : Nf;
+  k_bbox_partial<<<kBBoxBlocks, kBBoxThreads, 0, st>>>(bpts, bn, ws.bbox_part.as<double>());
   k_bbox_final<<<1, 32, 0, st>>>(ws.bbox_part.as<double>(), kBBoxBlocks, ctr);
   PB_LAUNCH_N("bbox", 2);
 
