@@ -50,6 +50,10 @@ WORKLOADS = {
                       N=4_000_000, C=1, L=7, n=6, cheb=1, eps=1e-7, box=1.0, seed=4321,
                       dist="clustered", weights="uniform"),
     # small cases of the same kernels for ncu captures (a few GB on the device)
+    # differentiation: separate sources and targets, loss = sum(f * g)
+    "grad": dict(name="gauss0.1_cheb5_S1e6_T1e6_C4_L6", kernel="GaussSigma", param=0.1,
+                 N=1_000_000, C=4, L=6, n=5, cheb=1, eps=1e-6, box=1.0, seed=777,
+                 dist="uniform", weights="normal"),
     "profile": dict(name="expcov0.3_unif5_N262144_C8_L5", kernel="ExpCov", param=0.3, N=262_144,
                     C=8, L=5, n=5, cheb=0, eps=1e-5, box=1.0, seed=1234, dist="uniform",
                     weights="normal"),
@@ -57,7 +61,8 @@ WORKLOADS = {
                          N=500_000, C=1, L=6, n=6, cheb=1, eps=1e-7, box=1.0, seed=4321,
                          dist="clustered", weights="uniform"),
 }
-KERNEL_TEXT = {"ExpCov": "exp(-r/%g)", "Laplacian": "1/r (0 at r=0)"}
+KERNEL_TEXT = {"ExpCov": "exp(-r/%g)", "Laplacian": "1/r (0 at r=0)",
+               "GaussSigma": "exp(-r^2/(2*%g^2))"}
 # bounded CPU sample: same kernel, order, columns and points per leaf (N / 8^L)
 CPU_SAMPLE = dict(N=15_625, L=4)
 N_SAMPLED_TARGETS = 4096
@@ -92,6 +97,9 @@ def make_tree(fmm, wl, device):
     if wl["kernel"] == "ExpCov":
         return fmm.kernel_ExpCov(wl["box"], wl["L"], wl["n"], wl["eps"], wl["cheb"],
                                  ell=wl["param"], device=device)
+    if wl["kernel"] == "GaussSigma":
+        return fmm.kernel_GaussSigma(wl["box"], wl["L"], wl["n"], wl["eps"], wl["cheb"],
+                                     sigma=wl["param"], device=device)
     return fmm.kernel_Laplacian(wl["box"], wl["L"], wl["n"], wl["eps"], wl["cheb"], device=device)
 
 
@@ -482,6 +490,108 @@ def run_workload(wl, args, rank, world, local_rank, e2e_wanted):
     return out
 
 
+def run_grad_workload(wl, args, local_rank):
+    """Forward and forward+backward of L = sum(f * g) with f = K(T, S) w:
+    the backward is the adjoint FMM (dL/dw = K^T g and dL/dS).  Also checks
+    dL/dS against float64 central differences of the forward FMM (h = 1e-6)
+    on 64 seeded source coordinates whose move crosses no leaf boundary."""
+    import torch
+
+    import pbbfmm3d_b200 as fmm
+
+    dev = torch.device("cuda", local_rank)
+    rng = np.random.default_rng(wl["seed"])
+    N, C = wl["N"], wl["C"]
+    S = rng.uniform(0.0, 1.0, (N, 3))
+    T = rng.uniform(0.0, 1.0, (N, 3))
+    W = rng.standard_normal((C, N))
+    G = rng.standard_normal((C, N))
+    tree = make_tree(fmm, wl, local_rank)
+    tree.buildFMMTree()
+    dT, dS, dW, dG = (torch.tensor(x, device=dev) for x in (T, S, W, G))
+    out = torch.zeros(C, N, dtype=torch.float64, device=dev)
+    gw = torch.zeros(C, N, dtype=torch.float64, device=dev)
+    gs = torch.zeros(N, 3, dtype=torch.float64, device=dev)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+
+    def fwd(prec):
+        out.zero_()
+        fmm.compute_device(tree, dT, dS, dW, C, out, precision=prec, stream=stream.cuda_stream)
+
+    def bwd(prec):
+        gw.zero_()
+        gs.zero_()
+        fmm.compute_adjoint_device(tree, dT, dS, dW, dG, C, grad_weight=gw, grad_source=gs,
+                                   precision=prec, stream=stream.cuda_stream)
+
+    def timed(fn):
+        evs = []
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            fn()
+            e1.record(stream)
+            evs.append((e0, e1))
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(b) for a, b in evs) / args.steps
+
+    res = {}
+    grads = {}
+    for pname, prec in (("fp64", fmm.PREC_FP64), ("mixed", fmm.PREC_MIXED)):
+        for _ in range(args.warmup):
+            fwd(prec)
+            bwd(prec)
+        torch.cuda.synchronize()
+        f_ms = timed(lambda: fwd(prec))
+        fb_ms = timed(lambda: (fwd(prec), bwd(prec)))
+        res[pname] = {"fwd_ms": f_ms, "fwd_bwd_ms": fb_ms, "fwd_bwd_over_fwd": fb_ms / f_ms}
+        grads[pname] = (gw.cpu().numpy(), gs.cpu().numpy())
+    # float64 central differences on 64 source coordinates
+    fwd(fmm.PREC_FP64)
+    bwd(fmm.PREC_FP64)
+    an_all = gs.cpu().numpy()
+    ctr = 0.5 * (T.min(0) + T.max(0))
+    u = (S - (ctr - 0.5 * wl["box"])) / (wl["box"] / (1 << wl["L"]))
+    frac = u - np.floor(u)
+    cand = np.argwhere(np.minimum(frac, 1 - frac) > 1e-3)
+    pick = cand[np.random.default_rng(99).choice(len(cand), 64, replace=False)]
+    h = 1e-6
+
+    def loss():
+        fwd(fmm.PREC_FP64)
+        return float((out * dG).sum().item())
+
+    fd, an = [], []
+    for j, d in pick:
+        v0 = float(dS[j, d].item())
+        dS[j, d] = v0 + h
+        lp = loss()
+        dS[j, d] = v0 - h
+        lm = loss()
+        dS[j, d] = v0
+        fd.append((lp - lm) / (2 * h))
+        an.append(an_all[j, d])
+    fd, an = np.array(fd), np.array(an)
+    g64w, g64s = grads["fp64"]
+    g32w, g32s = grads["mixed"]
+    tree.close()
+    return {
+        "config": {"workload": wl["name"], "N_sources": N, "N_targets": N, "nCols": C,
+                   "tree_level": wl["L"], "interpolation_order": wl["n"], "use_chebyshev": 1,
+                   "epsilon": wl["eps"], "kernel": kernel_text(wl),
+                   "loss": "sum(f * g), g ~ N(0,1)", "backward": "dL/dw and dL/d(source xyz)"},
+        "fp64": res["fp64"], "mixed": res["mixed"],
+        "fd_check": {"coordinates": int(len(fd)), "h": h,
+                     "rel_l2": float(np.linalg.norm(an - fd) / np.linalg.norm(fd)),
+                     "max_abs_rel": float(np.max(np.abs(an - fd)) / np.max(np.abs(fd)))},
+        "mixed_vs_fp64": {"grad_weight_rel_l2": float(np.linalg.norm(g32w - g64w) / np.linalg.norm(g64w)),
+                          "grad_source_rel_l2": float(np.linalg.norm(g32s - g64s) / np.linalg.norm(g64s))},
+    }
+
+
 def our_arm(args, rank, world, local_rank):
     import torch
 
@@ -495,6 +605,9 @@ def our_arm(args, rank, world, local_rank):
                                     "mixed_over_fp64", "phase_ms_per_step", "dominant_kernel",
                                     "roofline", "gpu_launches_per_step", "clocks")}
         target["unit"] = "N*nCols/s"
+    diff = None
+    if args.workload == "bench" and not args.no_grad:
+        diff = run_grad_workload(WORKLOADS["grad"], args, local_rank)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -529,6 +642,8 @@ def our_arm(args, rank, world, local_rank):
     }
     if target is not None:
         line["target_config"] = target
+    if diff is not None:
+        line["differentiation"] = diff
     print(json.dumps(line))
     return 0
 
@@ -541,6 +656,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-grad", action="store_true",
+                    help="skip the forward+backward (adjoint) workload block")
     ap.add_argument("--no-target", action="store_true",
                     help="skip the clustered Chebyshev (tensor-core) workload block")
     ap.add_argument("--workload", default="bench", choices=sorted(WORKLOADS))
