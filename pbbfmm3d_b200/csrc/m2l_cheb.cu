@@ -97,106 +97,160 @@ struct TypeTiles {
   int count[8];  // targets of each type
 };
 
-// M2L for one level.  Grid: (tiles over all types, M-tiles).  A tile holds
-// up to GBN / C targets of one child type; columns are (target, col).
+// M2L for one level on the CUDA cores (float64 path; also the float32 path
+// when r_f exceeds the tensor-core tile).  A CTA owns 128 (target, column)
+// rows of one child type and 128 rows of r_f; it walks the offsets that have
+// a source in the tile and, for each, r_s in chunks of 16, with the gathered
+// proxies (A, 128 x 16) and the operator (B, 128 x 16) in double-buffered
+// shared memory (cp.async, element-wise so the A tile is stored transposed).
+// Each thread accumulates an 8 x 8 block (rows ty + 16 i, columns tx + 16 j).
+constexpr int CG_M = 128, CG_N = 128, CG_K = 16, CG_THREADS = 256;
+constexpr int CG_APAD = CG_M + 1;  // A rows padded: conflict-free transposed stores
+
 template <typename T>
-__global__ void __launch_bounds__(kGemmThreads)
+__host__ __device__ constexpr size_t cg_smem_bytes() {
+  return sizeof(T) * 2 * CG_K * (CG_APAD + CG_N);
+}
+
+template <typename T>
+__global__ void __launch_bounds__(CG_THREADS, 1)
     k_m2l_cheb(int rf, int rs, const T* __restrict__ E, const int* __restrict__ typed,
                TypeTiles tt, int C, int lev, const int* __restrict__ sstart, int span,
                const int* __restrict__ offs, const T* __restrict__ proxy, T* __restrict__ pf) {
-  __shared__ T As[GBK][GBM];
-  __shared__ T Bs[GBK][GBN];
-  __shared__ int s_tx[GBN], s_ty[GBN], s_tz[GBN];
-  __shared__ int64_t s_src[GBN];  // proxy column base of the source, or -1
-  __shared__ int s_tcell[GBN];
-  const int tid = threadIdx.x;
-  const int tx = tid % (GBN / GTN), ty = tid / (GBN / GTN);
-  const int m0 = blockIdx.y * GBM;
-  int type = 0;
-  while (type < 7 && (int)blockIdx.x >= tt.start[type + 1]) ++type;
-  const int per_tile = GBN / C;
-  const int tfirst = (blockIdx.x - tt.start[type]) * per_tile;
-  const int ntile = min(per_tile, tt.count[type] - tfirst);
-  if (tid < GBN) {
-    const int tt_i = tid / C;
-    if (tid < per_tile * C && tt_i < ntile) {
-      const int cell = typed[tt.first[type] + tfirst + tt_i];
-      int x, y, z;
-      morton_decode((uint32_t)cell, &x, &y, &z);
-      s_tx[tid] = x;
-      s_ty[tid] = y;
-      s_tz[tid] = z;
-      s_tcell[tid] = cell;
-    } else {
-      s_tcell[tid] = -1;
+  extern __shared__ __align__(16) unsigned char cg_raw[];
+  T* As = reinterpret_cast<T*>(cg_raw);         // [2][CG_K][CG_APAD]
+  T* Bs = As + 2 * CG_K * CG_APAD;              // [2][CG_K][CG_N]
+  __shared__ long long s_src[2][CG_M];          // proxy row offset of each row's source, or -1
+  __shared__ int s_cell[CG_M], s_xyz[CG_M];
+  __shared__ uint32_t s_valid[6];
+  __shared__ int4 s_off[189];
+  __shared__ int s_nvalid;
+  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int n0 = blockIdx.y * CG_N;
+  int type = 0, tstart = 0, tlist = 0, tcount = 0;
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+    if ((int)blockIdx.x >= tt.start[i]) {
+      type = i;
+      tstart = tt.start[i];
+      tlist = tt.first[i];
+      tcount = tt.count[i];
     }
-  }
+  const int per_tile = CG_M / C;
+  const int tfirst = (blockIdx.x - tstart) * per_tile;
+  const int ntile = min(per_tile, tcount - tfirst);
   const int nside = 1 << lev;
-  T acc[GTM][GTN];
-#pragma unroll
-  for (int i = 0; i < GTM; ++i)
-#pragma unroll
-    for (int j = 0; j < GTN; ++j) acc[i][j] = 0;
   const int* my_offs = offs + type * 189 * 4;
-  for (int o = 0; o < 189; ++o) {
-    const int ox = my_offs[4 * o + 0], oy = my_offs[4 * o + 1], oz = my_offs[4 * o + 2];
-    const int opi = my_offs[4 * o + 3];
-    __syncthreads();
-    int any = 0;
-    if (tid < GBN) {
-      int64_t src = -1;
-      if (s_tcell[tid] >= 0) {
-        const int bx = s_tx[tid] + ox, by = s_ty[tid] + oy, bz = s_tz[tid] + oz;
-        if (bx >= 0 && by >= 0 && bz >= 0 && bx < nside && by < nside && bz < nside) {
-          const uint32_t bm = morton_encode(bx, by, bz);
-          if (sstart[(int64_t)(bm + 1) * span] > sstart[(int64_t)bm * span])
-            src = ((int64_t)bm * C + tid % C) * rs;
-        }
-      }
-      s_src[tid] = src;
-      any = src >= 0;
+  if (tid < CG_M) {
+    const int cell = (tid < per_tile * C && tid / C < ntile) ? typed[tlist + tfirst + tid / C] : -1;
+    int x = 0, y = 0, z = 0;
+    if (cell >= 0) morton_decode((uint32_t)cell, &x, &y, &z);
+    s_cell[tid] = cell;
+    s_xyz[tid] = (x << 20) | (y << 10) | z;
+  }
+  if (tid < 6) s_valid[tid] = 0;
+  __syncthreads();
+  if (tid < CG_M && s_cell[tid] >= 0 && tid % C == 0) {
+    const int x = s_xyz[tid] >> 20, y = (s_xyz[tid] >> 10) & 1023, z = s_xyz[tid] & 1023;
+    for (int o = 0; o < 189; ++o) {
+      const int bx = x + my_offs[4 * o], by = y + my_offs[4 * o + 1], bz = z + my_offs[4 * o + 2];
+      if (bx < 0 || by < 0 || bz < 0 || bx >= nside || by >= nside || bz >= nside) continue;
+      const uint32_t bm = morton_encode(bx, by, bz);
+      if (sstart[(int64_t)(bm + 1) * span] > sstart[(int64_t)bm * span])
+        atomicOr(&s_valid[o >> 5], 1u << (o & 31));
     }
-    if (!__syncthreads_or(any)) continue;
-    const T* Eo = E + (int64_t)opi * rf * rs;
-    for (int k0 = 0; k0 < rs; k0 += GBK) {
-#pragma unroll
-      for (int r = 0; r < (GBM * GBK) / kGemmThreads; ++r) {
-        const int e = tid + r * kGemmThreads, mm = e % GBM, kk = e / GBM;
-        const int gm = m0 + mm, gk = k0 + kk;
-        As[kk][mm] = (gm < rf && gk < rs) ? Eo[gm + (int64_t)rf * gk] : T(0);
+  }
+  __syncthreads();
+  if (tid == 0) {
+    int nv = 0;
+    for (int o = 0; o < 189; ++o)
+      if ((s_valid[o >> 5] >> (o & 31)) & 1)
+        s_off[nv++] = make_int4(my_offs[4 * o], my_offs[4 * o + 1], my_offs[4 * o + 2],
+                                my_offs[4 * o + 3]);
+    s_nvalid = nv;
+  }
+  __syncthreads();
+  const int nvalid = s_nvalid;
+  const int kchunks = (rs + CG_K - 1) / CG_K;
+  const int niter = nvalid * kchunks;
+  // row tid's source for valid offset q, into s_src[q & 1]
+  auto lookup = [&](int q) {
+    if (tid >= CG_M) return;
+    long long r = -1;
+    const int cell = s_cell[tid];
+    if (cell >= 0) {
+      const int4 o = s_off[q];
+      const int x = (s_xyz[tid] >> 20) + o.x, y = ((s_xyz[tid] >> 10) & 1023) + o.y,
+                z = (s_xyz[tid] & 1023) + o.z;
+      if (x >= 0 && y >= 0 && z >= 0 && x < nside && y < nside && z < nside) {
+        const uint32_t bm = morton_encode(x, y, z);
+        if (sstart[(int64_t)(bm + 1) * span] > sstart[(int64_t)bm * span])
+          r = ((long long)bm * C + tid % C) * rs;
       }
+    }
+    s_src[q & 1][tid] = r;
+  };
+  auto load = [&](int j) {
+    const int q = j / kchunks, k0 = (j - q * kchunks) * CG_K, st = j & 1;
+    T* as = As + st * CG_K * CG_APAD;
+    T* bs = Bs + st * CG_K * CG_N;
+    for (int e = tid; e < CG_M * CG_K; e += CG_THREADS) {
+      const int m = e / CG_K, kk = e - m * CG_K;
+      const long long r = s_src[q & 1][m];
+      const bool ok = r >= 0 && k0 + kk < rs;
+      cp_async_elem(as + kk * CG_APAD + m, proxy + (ok ? r + k0 + kk : 0), ok);
+    }
+    const T* Eo = E + (int64_t)s_off[q].w * rf * rs;
+    for (int e = tid; e < CG_N * CG_K; e += CG_THREADS) {
+      const int kk = e / CG_N, nn = e - kk * CG_N;
+      const bool ok = n0 + nn < rf && k0 + kk < rs;
+      cp_async_elem(bs + kk * CG_N + nn, Eo + (ok ? (int64_t)(n0 + nn) + (int64_t)rf * (k0 + kk) : 0),
+                    ok);
+    }
+    cp_async_commit();
+  };
+  T acc[8][8];
 #pragma unroll
-      for (int r = 0; r < (GBN * GBK) / kGemmThreads; ++r) {
-        const int e = tid + r * kGemmThreads, kk = e % GBK, jj = e / GBK;
-        const int gk = k0 + kk;
-        const int64_t sb = s_src[jj];
-        Bs[kk][jj] = (sb >= 0 && gk < rs) ? proxy[sb + gk] : T(0);
-      }
-      __syncthreads();
+  for (int i = 0; i < 8; ++i)
 #pragma unroll
-      for (int kk = 0; kk < GBK; ++kk) {
-        T a[GTM], b[GTN];
+    for (int j = 0; j < 8; ++j) acc[i][j] = 0;
+  if (niter > 0) {
+    lookup(0);
+    __syncthreads();
+    load(0);
+  }
+  for (int it = 0; it < niter; ++it) {
+    // the next offset's sources, one iteration ahead (other parity buffer)
+    const int qn = (it + 1) / kchunks;
+    if (it + 1 < niter && qn != it / kchunks) lookup(qn);
+    cp_async_wait_all();
+    __syncthreads();
+    if (it + 1 < niter) load(it + 1);
+    const T* as = As + (it & 1) * CG_K * CG_APAD;
+    const T* bs = Bs + (it & 1) * CG_K * CG_N;
 #pragma unroll
-        for (int i = 0; i < GTM; ++i) a[i] = As[kk][ty * GTM + i];
+    for (int kk = 0; kk < CG_K; ++kk) {
+      T a[8], b[8];
 #pragma unroll
-        for (int j = 0; j < GTN; ++j) b[j] = Bs[kk][tx * GTN + j];
+      for (int i = 0; i < 8; ++i) a[i] = as[kk * CG_APAD + ty + 16 * i];
 #pragma unroll
-        for (int i = 0; i < GTM; ++i)
+      for (int j = 0; j < 8; ++j) b[j] = bs[kk * CG_N + tx + 16 * j];
 #pragma unroll
-          for (int j = 0; j < GTN; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
-      }
-      __syncthreads();
+      for (int i = 0; i < 8; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
     }
   }
 #pragma unroll
-  for (int j = 0; j < GTN; ++j) {
-    const int jj = tx * GTN + j;
-    const int cell = s_tcell[jj];
+  for (int i = 0; i < 8; ++i) {
+    const int m = ty + 16 * i;
+    const int cell = s_cell[m];
     if (cell < 0) continue;
+    T* dst = pf + ((int64_t)cell * C + m % C) * rf;
 #pragma unroll
-    for (int i = 0; i < GTM; ++i) {
-      const int gm = m0 + ty * GTM + i;
-      if (gm < rf) pf[((int64_t)cell * C + jj % C) * rf + gm] = acc[i][j];
+    for (int j = 0; j < 8; ++j) {
+      const int n = n0 + tx + 16 * j;
+      if (n < rf) dst[n] = acc[i][j];
     }
   }
 }
@@ -247,7 +301,7 @@ static int run_m2l_cheb_t(pbbfmm_tree* t, int C, cudaStream_t st) {
       }
     }
     TypeTiles tt;
-    const int per_tile = GBN / C;
+    const int per_tile = CG_M / C;
     int tiles = 0;
     for (int ty = 0; ty < 8; ++ty) {
       tt.start[ty] = tiles;
@@ -257,9 +311,11 @@ static int run_m2l_cheb_t(pbbfmm_tree* t, int C, cudaStream_t st) {
     }
     tt.start[8] = tiles;
     if (tiles > 0 && !on_tc) {
-      dim3 g((unsigned)tiles, (unsigned)((rf + GBM - 1) / GBM));
+      dim3 g((unsigned)tiles, (unsigned)((rf + CG_N - 1) / CG_N));
+      PB_CUDA(cudaFuncSetAttribute(k_m2l_cheb<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)cg_smem_bytes<T>()));
       if (int rc_ = kt_begin(t, KS_M2L, st)) return rc_;
-      k_m2l_cheb<T><<<g, kGemmThreads, 0, st>>>(
+      k_m2l_cheb<T><<<g, CG_THREADS, cg_smem_bytes<T>(), st>>>(
           rf, rs, ov.E + (int64_t)lvl * 316 * rf * rs, lists + t->lists.typ_off[l], tt, C, l,
           sstart, (int)cells_at(L - l), t->d_offs, proxy + level_offset(l, (int64_t)C * rs),
           pf + level_offset(l, (int64_t)C * rf));
