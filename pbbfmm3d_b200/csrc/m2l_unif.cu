@@ -249,15 +249,14 @@ __global__ void k_halo_tables(const int* __restrict__ sstart, const int* __restr
   (void)nbx;
 }
 
-template <int PBX, int KC, int CG, int CPT, typename T>
-__global__ void __launch_bounds__(4 * PBX * KC * (CG / CPT))
+template <int PBX, int KC, int CG, typename T>
+__global__ void __launch_bounds__(4 * PBX * KC * CG)
     k_m2l_unif_mac(const cplx_t<T>* __restrict__ X_l, cplx_t<T>* __restrict__ Y_l,
                    const cplx_t<T>* __restrict__ op,  // nk x 343 for this level
                    const int* __restrict__ halo, int64_t ncells, int C, int nk) {
   using G = MacGeom<PBX>;
   using C2 = cplx_t<T>;
-  constexpr int NG = CG / CPT;  // column groups
-  constexpr int NT = G::NPAR * KC * NG;
+  constexpr int NT = G::NPAR * KC * CG;
   constexpr int RC = G::RC;
   extern __shared__ __align__(16) unsigned char smraw[];
   C2* reg = reinterpret_cast<C2*>(smraw);  // RC x KC x CG
@@ -265,7 +264,7 @@ __global__ void __launch_bounds__(4 * PBX * KC * (CG / CPT))
   int* s_src = (int*)(sop + KC * 343);  // RC source cells, then TC target cells
   int* s_tgt = s_src + RC;
   const int tid = threadIdx.x;
-  const int g = tid % NG, kc = (tid / NG) % KC, p = tid / (NG * KC);
+  const int cc = tid % CG, kc = (tid / CG) % KC, p = tid / (CG * KC);
   const int px = p >> 2, py = (p >> 1) & 1, pz = p & 1;
   const int* hb = halo + (int64_t)blockIdx.x * G::STRIDE;
   int mine = 0;
@@ -284,8 +283,8 @@ __global__ void __launch_bounds__(4 * PBX * KC * (CG / CPT))
     const int r = i / (KC * CG), q = i % (KC * CG), kk = q / CG, c = q % CG;
     const int src = s_src[r];
     const bool ok = src >= 0 && k0 + kk < nk && c0 + c < C;
-    const C2* gp = ok ? &X_l[((int64_t)(k0 + kk) * ncells + src) * C + c0 + c] : X_l;
-    cp_async_cplx(&reg[i], gp, ok);
+    const C2* g = ok ? &X_l[((int64_t)(k0 + kk) * ncells + src) * C + c0 + c] : X_l;
+    cp_async_cplx(&reg[i], g, ok);
   }
   for (int i = tid; i < KC * 343; i += NT) {
     const int kk = i / 343, e = i % 343;
@@ -295,68 +294,54 @@ __global__ void __launch_bounds__(4 * PBX * KC * (CG / CPT))
   cp_async_commit();
   cp_async_wait_all();
   __syncthreads();
-  // 8 children x CPT columns per thread: each staged source value serves the
-  // 8 children, each operator value the CPT columns
-  T re[8][CPT], im[8][CPT];
+  T ar[8], br[8], ai[8], bi[8];  // re = ar + br, im = ai + bi
 #pragma unroll
-  for (int t = 0; t < 8; ++t)
-#pragma unroll
-    for (int c = 0; c < CPT; ++c) re[t][c] = im[t][c] = T(0);
+  for (int t = 0; t < 8; ++t) ar[t] = br[t] = ai[t] = bi[t] = T(0);
   const C2* myop = sop + kc * 343;
-  // sx runs as a loop (keeps the unrolled body small); for each (sy, sz, t)
-  // the y/z offsets are compile-time constants, so the interaction test
-  // reduces to |ox| > 1 unless |oy| or |oz| already is > 1.
+  // sx runs as a loop (keeps the unrolled body and its registers small);
+  // for each (sy, sz, t) the y/z offsets are compile-time constants, so the
+  // interaction test reduces to |ox| > 1 unless |oy| or |oz| already is > 1.
 #pragma unroll 1
   for (int sx = 0; sx < 6; ++sx) {
-    const C2* rrow = reg + (((2 * px + sx) << 6) * KC + kc) * CG + g * CPT;
+    const C2* rrow = reg + (((2 * px + sx) << 6) * KC + kc) * CG + cc;
     const C2* orow = myop + 49 * (sx + 1);  // lex of ox + 3 = sx + 1 - tx
-    const bool xfar0 = sx > 3 || sx < 1;    // |sx - 2| > 1
-    const bool xfar1 = sx > 4 || sx < 2;    // |sx - 3| > 1
 #pragma unroll
     for (int sy = 0; sy < 6; ++sy)
 #pragma unroll
       for (int sz = 0; sz < 6; ++sz) {
         const int r = ((2 * py + sy) << 3) | (2 * pz + sz);
-        C2 xv[CPT];
-#pragma unroll
-        for (int c = 0; c < CPT; ++c) xv[c] = rrow[r * KC * CG + c];
+        const C2 xv = rrow[r * KC * CG];
 #pragma unroll
         for (int t = 0; t < 8; ++t) {
           const int tx = (t >> 2) & 1;
           const int oy = sy - 2 - ((t >> 1) & 1);
           const int oz = sz - 2 - (t & 1);
+          const int ox = sx - 2 - tx;
           const bool far_yz = oy > 1 || oy < -1 || oz > 1 || oz < -1;
-          if (far_yz || (tx ? xfar1 : xfar0)) {
+          if (far_yz || ox > 1 || ox < -1) {
             const C2 a = orow[-49 * tx + 7 * (oy + 3) + (oz + 3)];
-#pragma unroll
-            for (int c = 0; c < CPT; ++c) {
-              re[t][c] = fma(a.x, xv[c].x, re[t][c]);
-              re[t][c] = fma(-a.y, xv[c].y, re[t][c]);
-              im[t][c] = fma(a.x, xv[c].y, im[t][c]);
-              im[t][c] = fma(a.y, xv[c].x, im[t][c]);
-            }
+            ar[t] = fma(a.x, xv.x, ar[t]);
+            br[t] = fma(-a.y, xv.y, br[t]);
+            ai[t] = fma(a.x, xv.y, ai[t]);
+            bi[t] = fma(a.y, xv.x, bi[t]);
           }
         }
       }
   }
-  if (k0 + kc < nk) {
+  if (k0 + kc < nk && c0 + cc < C) {
 #pragma unroll
     for (int t = 0; t < 8; ++t) {
       const int q = ((2 * px + ((t >> 2) & 1)) << 4) | ((2 * py + ((t >> 1) & 1)) << 2) |
                     (2 * pz + (t & 1));
       const int cm = s_tgt[q];
-      if (cm < 0) continue;
-#pragma unroll
-      for (int c = 0; c < CPT; ++c) {
-        const int col = c0 + g * CPT + c;
-        if (col < C)
-          Y_l[((int64_t)(k0 + kc) * ncells + cm) * C + col] = make_cplx<T>(re[t][c], im[t][c]);
-      }
+      if (cm >= 0)
+        Y_l[((int64_t)(k0 + kc) * ncells + cm) * C + c0 + cc] =
+            make_cplx<T>(ar[t] + br[t], ai[t] + bi[t]);
     }
   }
 }
 
-template <int PBX, int KC, int CG, int CPT, typename T>
+template <int PBX, int KC, int CG, typename T>
 static int launch_mac(const cplx_t<T>* X, cplx_t<T>* Y, const cplx_t<T>* op, int* halo,
                       const int* sstart, const int* tstart, int span, int lev, int C, int nk,
                       cudaStream_t st) {
@@ -368,10 +353,10 @@ static int launch_mac(const cplx_t<T>* X, cplx_t<T>* Y, const cplx_t<T>* op, int
   dim3 g((unsigned)nblk, (unsigned)((nk + KC - 1) / KC), (unsigned)((C + CG - 1) / CG));
   const size_t smem =
       sizeof(cplx_t<T>) * (G::RC * KC * CG + KC * 343) + sizeof(int) * G::STRIDE;
-  PB_CUDA(cudaFuncSetAttribute(k_m2l_unif_mac<PBX, KC, CG, CPT, T>,
+  PB_CUDA(cudaFuncSetAttribute(k_m2l_unif_mac<PBX, KC, CG, T>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_m2l_unif_mac<PBX, KC, CG, CPT, T><<<g, G::NPAR * KC * (CG / CPT), smem, st>>>(
-      X, Y, op, halo, cells_at(lev), C, nk);
+  k_m2l_unif_mac<PBX, KC, CG, T><<<g, G::NPAR * KC * CG, smem, st>>>(X, Y, op, halo,
+                                                                     cells_at(lev), C, nk);
   PB_LAUNCH("m2l_unif_mac");
   return PBBFMM_OK;
 }
@@ -380,16 +365,13 @@ template <int PBX, typename T>
 static int launch_mac_cols(const cplx_t<T>* X, cplx_t<T>* Y, const cplx_t<T>* op, int* halo,
                            const int* sstart, const int* tstart, int span, int lev, int C, int nk,
                            cudaStream_t st) {
-  // columns per thread: 4 in float32 (the operator value is reused 4 times),
-  // 2 in float64 (register and shared-memory budget)
-  constexpr int CPT = sizeof(T) == 4 ? 4 : 2;
   if (C >= 8)
-    return launch_mac<PBX, 1, 8, CPT, T>(X, Y, op, halo, sstart, tstart, span, lev, C, nk, st);
+    return launch_mac<PBX, 1, 8, T>(X, Y, op, halo, sstart, tstart, span, lev, C, nk, st);
   if (C >= 4)
-    return launch_mac<PBX, 2, 4, CPT, T>(X, Y, op, halo, sstart, tstart, span, lev, C, nk, st);
+    return launch_mac<PBX, 2, 4, T>(X, Y, op, halo, sstart, tstart, span, lev, C, nk, st);
   if (C >= 2)
-    return launch_mac<PBX, 4, 2, 2, T>(X, Y, op, halo, sstart, tstart, span, lev, C, nk, st);
-  return launch_mac<PBX, 8, 1, 1, T>(X, Y, op, halo, sstart, tstart, span, lev, C, nk, st);
+    return launch_mac<PBX, 4, 2, T>(X, Y, op, halo, sstart, tstart, span, lev, C, nk, st);
+  return launch_mac<PBX, 8, 1, T>(X, Y, op, halo, sstart, tstart, span, lev, C, nk, st);
 }
 
 template <typename T>
