@@ -258,15 +258,10 @@ __global__ void __launch_bounds__(4 * PBX * KC * CG)
   using C2 = cplx_t<T>;
   constexpr int NT = G::NPAR * KC * CG;
   constexpr int RC = G::RC;
-  // float32: the operator is staged as pairs P[i] = (op[i-1], op[i]) so that
-  // the two children of a (tx, ty) column -- operator indices i-1 and i --
-  // take one 16-byte load
-  constexpr bool kPairs = sizeof(T) == 4;
-  constexpr int OPW = kPairs ? 2 : 1;  // complex values per operator slot
   extern __shared__ __align__(16) unsigned char smraw[];
   C2* reg = reinterpret_cast<C2*>(smraw);  // RC x KC x CG
-  C2* sop = reg + RC * KC * CG;            // KC x 343 (x 2 with pairs)
-  int* s_src = (int*)(sop + KC * 343 * OPW);  // RC source cells, then TC target cells
+  C2* sop = reg + RC * KC * CG;            // KC x 343
+  int* s_src = (int*)(sop + KC * 343);  // RC source cells, then TC target cells
   int* s_tgt = s_src + RC;
   const int tid = threadIdx.x;
   const int cc = tid % CG, kc = (tid / CG) % KC, p = tid / (CG * KC);
@@ -294,13 +289,7 @@ __global__ void __launch_bounds__(4 * PBX * KC * CG)
   for (int i = tid; i < KC * 343; i += NT) {
     const int kk = i / 343, e = i % 343;
     const bool ok = k0 + kk < nk;
-    if constexpr (kPairs) {
-      const bool okp = ok && e > 0;
-      cp_async_cplx(&sop[2 * i], okp ? &op[(int64_t)(k0 + kk) * 343 + e - 1] : op, okp);
-      cp_async_cplx(&sop[2 * i + 1], ok ? &op[(int64_t)(k0 + kk) * 343 + e] : op, ok);
-    } else {
-      cp_async_cplx(&sop[i], ok ? &op[(int64_t)(k0 + kk) * 343 + e] : op, ok);
-    }
+    cp_async_cplx(&sop[i], ok ? &op[(int64_t)(k0 + kk) * 343 + e] : op, ok);
   }
   cp_async_commit();
   cp_async_wait_all();
@@ -308,14 +297,14 @@ __global__ void __launch_bounds__(4 * PBX * KC * CG)
   T ar[8], br[8], ai[8], bi[8];  // re = ar + br, im = ai + bi
 #pragma unroll
   for (int t = 0; t < 8; ++t) ar[t] = br[t] = ai[t] = bi[t] = T(0);
-  const C2* myop = sop + kc * 343 * OPW;
+  const C2* myop = sop + kc * 343;
   // sx runs as a loop (keeps the unrolled body and its registers small);
   // for each (sy, sz, t) the y/z offsets are compile-time constants, so the
   // interaction test reduces to |ox| > 1 unless |oy| or |oz| already is > 1.
 #pragma unroll 1
   for (int sx = 0; sx < 6; ++sx) {
     const C2* rrow = reg + (((2 * px + sx) << 6) * KC + kc) * CG + cc;
-    const C2* orow = myop + 49 * (sx + 1) * OPW;  // lex of ox + 3 = sx + 1 - tx
+    const C2* orow = myop + 49 * (sx + 1);  // lex of ox + 3 = sx + 1 - tx
 #pragma unroll
     for (int sy = 0; sy < 6; ++sy)
 #pragma unroll
@@ -323,39 +312,18 @@ __global__ void __launch_bounds__(4 * PBX * KC * CG)
         const int r = ((2 * py + sy) << 3) | (2 * pz + sz);
         const C2 xv = rrow[r * KC * CG];
 #pragma unroll
-        for (int tp = 0; tp < 4; ++tp) {  // (tx, ty); tz = 0, 1 below
-          const int tx = (tp >> 1) & 1;
-          const int oy = sy - 2 - (tp & 1);
+        for (int t = 0; t < 8; ++t) {
+          const int tx = (t >> 2) & 1;
+          const int oy = sy - 2 - ((t >> 1) & 1);
+          const int oz = sz - 2 - (t & 1);
           const int ox = sx - 2 - tx;
-          const bool xfar = ox > 1 || ox < -1;
-          // tz = 0: oz = sz - 2 (index i); tz = 1: oz = sz - 3 (index i - 1)
-          const int i0 = -49 * tx + 7 * (oy + 3) + (sz + 1);
-          const bool yfar = oy > 1 || oy < -1;
-          const bool use0 = yfar || sz - 2 > 1 || sz - 2 < -1 || xfar;
-          const bool use1 = yfar || sz - 3 > 1 || sz - 3 < -1 || xfar;
-          if (use0 || use1) {
-            C2 a0, a1;
-            if constexpr (kPairs) {
-              const float4 pr = *reinterpret_cast<const float4*>(orow + 2 * i0);
-              a1 = make_cplx<T>(pr.x, pr.y);  // op[i0 - 1]
-              a0 = make_cplx<T>(pr.z, pr.w);  // op[i0]
-            } else {
-              a0 = orow[i0];
-              a1 = orow[i0 - 1];
-            }
-            const int t0 = 2 * tp, t1 = 2 * tp + 1;
-            if (use0) {
-              ar[t0] = fma(a0.x, xv.x, ar[t0]);
-              br[t0] = fma(-a0.y, xv.y, br[t0]);
-              ai[t0] = fma(a0.x, xv.y, ai[t0]);
-              bi[t0] = fma(a0.y, xv.x, bi[t0]);
-            }
-            if (use1) {
-              ar[t1] = fma(a1.x, xv.x, ar[t1]);
-              br[t1] = fma(-a1.y, xv.y, br[t1]);
-              ai[t1] = fma(a1.x, xv.y, ai[t1]);
-              bi[t1] = fma(a1.y, xv.x, bi[t1]);
-            }
+          const bool far_yz = oy > 1 || oy < -1 || oz > 1 || oz < -1;
+          if (far_yz || ox > 1 || ox < -1) {
+            const C2 a = orow[-49 * tx + 7 * (oy + 3) + (oz + 3)];
+            ar[t] = fma(a.x, xv.x, ar[t]);
+            br[t] = fma(-a.y, xv.y, br[t]);
+            ai[t] = fma(a.x, xv.y, ai[t]);
+            bi[t] = fma(a.y, xv.x, bi[t]);
           }
         }
       }
@@ -383,8 +351,8 @@ static int launch_mac(const cplx_t<T>* X, cplx_t<T>* Y, const cplx_t<T>* op, int
   k_halo_tables<PBX><<<nblk, 256, 0, st>>>(sstart, tstart, span, lev, halo);
   PB_LAUNCH("halo_tables");
   dim3 g((unsigned)nblk, (unsigned)((nk + KC - 1) / KC), (unsigned)((C + CG - 1) / CG));
-  const size_t smem = sizeof(cplx_t<T>) * (G::RC * KC * CG + KC * 343 * (sizeof(T) == 4 ? 2 : 1)) +
-                      sizeof(int) * G::STRIDE;
+  const size_t smem =
+      sizeof(cplx_t<T>) * (G::RC * KC * CG + KC * 343) + sizeof(int) * G::STRIDE;
   PB_CUDA(cudaFuncSetAttribute(k_m2l_unif_mac<PBX, KC, CG, T>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_m2l_unif_mac<PBX, KC, CG, T><<<g, G::NPAR * KC * CG, smem, st>>>(X, Y, op, halo,
