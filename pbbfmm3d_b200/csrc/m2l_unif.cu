@@ -15,183 +15,244 @@
 // the operator spectra stored as conj(DFT3(A)).  Only the k3 < n half of each
 // spectrum is kept (Hermitian symmetry), nk = m*m*n complex values per cell
 // and column.  Same sums as the reference, different rounding.
+#include <cmath>
+#include <mutex>
+
 #include "fmm.cuh"
 
 namespace pbbfmm {
 
 // ----------------------------------------------------------------- FFT
-// twid[j] = cos(2 pi j / m), twid[m + j] = sin(2 pi j / m)
+// Each thread computes one whole 1-D transform of a stage: its n (or m)
+// inputs are read once from shared memory and every output is accumulated in
+// registers, with the loops fully unrolled so that every twiddle index
+// (k l mod m) is a compile-time constant into the __constant__ tables below
+// (constant-bank operands of the FMAs, no loads).
+
+// cos / sin of 2 pi j / m for m = 2n - 1, n = 2..kMaxOrder, back to back.
+constexpr int kTwTotal = kMaxOrder * kMaxOrder - 1;  // sum_{n=2}^{N} (2n - 1)
+__host__ __device__ constexpr int tw_off(int n) { return n <= 2 ? 0 : tw_off(n - 1) + 2 * n - 3; }
+__constant__ double c_tw_cos_d[kTwTotal];
+__constant__ double c_tw_sin_d[kTwTotal];
+__constant__ float c_tw_cos_f[kTwTotal];
+__constant__ float c_tw_sin_f[kTwTotal];
+
+template <int n, typename T>
+struct Tw {
+  static constexpr int m = 2 * n - 1, off = tw_off(n);
+  static __device__ __forceinline__ T c(int j) {
+    if constexpr (sizeof(T) == 8) return c_tw_cos_d[off + j];
+    else return c_tw_cos_f[off + j];
+  }
+  static __device__ __forceinline__ T s(int j) {
+    if constexpr (sizeof(T) == 8) return c_tw_sin_d[off + j];
+    else return c_tw_sin_f[off + j];
+  }
+};
+
+// Fill the tables on the current device (once per device).
+int init_fft_twiddles() {
+  static std::mutex mu;
+  static bool done[64] = {};
+  int dev = 0;
+  PB_CUDA(cudaGetDevice(&dev));
+  std::lock_guard<std::mutex> lk(mu);
+  if (dev < 64 && done[dev]) return PBBFMM_OK;
+  double cd[kTwTotal], sd[kTwTotal];
+  float cf[kTwTotal], sf[kTwTotal];
+  for (int n = 2; n <= kMaxOrder; ++n) {
+    const int m = 2 * n - 1;
+    for (int j = 0; j < m; ++j) {
+      cd[tw_off(n) + j] = cos(2.0 * M_PI * j / m);
+      sd[tw_off(n) + j] = sin(2.0 * M_PI * j / m);
+      cf[tw_off(n) + j] = (float)cd[tw_off(n) + j];
+      sf[tw_off(n) + j] = (float)sd[tw_off(n) + j];
+    }
+  }
+  PB_CUDA(cudaMemcpyToSymbol(c_tw_cos_d, cd, sizeof(cd)));
+  PB_CUDA(cudaMemcpyToSymbol(c_tw_sin_d, sd, sizeof(sd)));
+  PB_CUDA(cudaMemcpyToSymbol(c_tw_cos_f, cf, sizeof(cf)));
+  PB_CUDA(cudaMemcpyToSymbol(c_tw_sin_f, sf, sizeof(sf)));
+  if (dev < 64) done[dev] = true;
+  return PBBFMM_OK;
+}
 
 // Spectra of a level are stored frequency-major: X[(k * ncells + cell) * C + col]
 // (ncells = 8^level), so that one frequency plane of a level is contiguous.
 
 // Forward: one CTA per nonempty source cell; columns in groups of CG.
-// Templated on the order so that all index arithmetic is by constants.
+// w = e^{-2 pi i / m}; (a + ib) w^j = (a c + b s) + i (b c - a s).
 template <int n, typename T>
 __global__ void k_fft_fwd(const int* __restrict__ cells, const T* __restrict__ S_l,
                           cplx_t<T>* __restrict__ X_l, int64_t ncells, int C, int CG,
                           const T* __restrict__ twid) {
   using C2 = cplx_t<T>;
+  using W = Tw<n, T>;
   extern __shared__ __align__(16) unsigned char smraw[];
   T* sm = reinterpret_cast<T*>(smraw);
-  constexpr int m = 2 * n - 1, n2 = n * n, n3 = n2 * n, nk = m * m * n;
-  T* sc = sm;        // m
-  T* ss = sc + m;    // m
-  T* sin_ = ss + m;  // CG * n3 real moments
+  constexpr int m = 2 * n - 1, n2 = n * n, n3 = n2 * n, ny = n * m * n;
+  T* sin_ = sm + 2 * m;                         // CG * n3 real moments
   C2* Z = (C2*)(sin_ + ((CG * n3 + 3) & ~3));  // CG * n * n * n   (l1, l2, k3)
   C2* Y = Z + CG * n3;                         // CG * n * m * n   (l1, k2, k3)
-  for (int i = threadIdx.x; i < m; i += blockDim.x) {
-    sc[i] = twid[i];
-    ss[i] = twid[m + i];
-  }
+  (void)twid;
   const int cell = cells[blockIdx.x];
+  const int tid = threadIdx.x, bd = blockDim.x;
   for (int c0 = 0; c0 < C; c0 += CG) {
     const int cg = min(CG, C - c0);
     __syncthreads();
-    for (int i = threadIdx.x; i < cg * n3; i += blockDim.x)
-      sin_[i] = S_l[((int64_t)cell * C + c0) * n3 + i];
+    for (int i = tid; i < cg * n3; i += bd) sin_[i] = S_l[((int64_t)cell * C + c0) * n3 + i];
     __syncthreads();
-    // z: Z[c][l1][l2][k3] = sum_l3 S[c][l1][l2][l3] w^(k3 l3),  w = e^{-2 pi i / m}
-    for (int i = threadIdx.x; i < cg * n3; i += blockDim.x) {
-      const int cc = i / n3, r = i % n3, l12 = r / n, k3 = r % n;
-      const T* s = sin_ + cc * n3 + l12 * n;
-      T re = 0, im = 0;
-      int e = 0;
+    // z: Z[c][l1][l2][k3] = sum_l3 S[c][l1][l2][l3] w^(k3 l3), real input
+    for (int job = tid; job < cg * n2; job += bd) {
+      const T* s = sin_ + job * n;
+      T x[n];
 #pragma unroll
-      for (int l3 = 0; l3 < n; ++l3) {
-        re += s[l3] * sc[e];
-        im -= s[l3] * ss[e];
-        e += k3;
-        if (e >= m) e -= m;
+      for (int l = 0; l < n; ++l) x[l] = s[l];
+      C2* z = Z + job * n;
+#pragma unroll
+      for (int k = 0; k < n; ++k) {
+        T re = 0, im = 0;
+#pragma unroll
+        for (int l = 0; l < n; ++l) {
+          re = fma(x[l], W::c((k * l) % m), re);
+          im = fma(-x[l], W::s((k * l) % m), im);
+        }
+        z[k] = make_cplx<T>(re, im);
       }
-      Z[i] = make_cplx<T>(re, im);
     }
     __syncthreads();
-    // y: Y[c][l1][k2][k3] = sum_l2 Z[c][l1][l2][k3] w^(k2 l2)
-    constexpr int ny = n * m * n;
-    for (int i = threadIdx.x; i < cg * ny; i += blockDim.x) {
-      const int cc = i / ny, r = i % ny, l1 = r / (m * n), k2 = (r / n) % m, k3 = r % n;
+    // y: Y[c][l1][k2][k3] = sum_l2 Z[c][l1][l2][k3] w^(k2 l2); job (c, l1, k3)
+    for (int job = tid; job < cg * n2; job += bd) {
+      const int k3 = job % n, l1 = (job / n) % n, cc = job / n2;
       const C2* z = Z + cc * n3 + l1 * n2 + k3;
-      T re = 0, im = 0;
-      int e = 0;
+      C2 v[n];
 #pragma unroll
-      for (int l2 = 0; l2 < n; ++l2) {
-        const C2 v = z[l2 * n];
-        const T c = sc[e], s = ss[e];
-        re += v.x * c + v.y * s;
-        im += v.y * c - v.x * s;
-        e += k2;
-        if (e >= m) e -= m;
+      for (int l = 0; l < n; ++l) v[l] = z[l * n];
+      C2* y = Y + cc * ny + l1 * m * n + k3;
+#pragma unroll
+      for (int k = 0; k < m; ++k) {
+        T re = 0, im = 0;
+#pragma unroll
+        for (int l = 0; l < n; ++l) {
+          const T c = W::c((k * l) % m), s = W::s((k * l) % m);
+          re = fma(v[l].x, c, fma(v[l].y, s, re));
+          im = fma(v[l].y, c, fma(-v[l].x, s, im));
+        }
+        y[k * n] = make_cplx<T>(re, im);
       }
-      Y[i] = make_cplx<T>(re, im);
     }
     __syncthreads();
-    // x: X[k1][k2][k3][c] = sum_l1 Y[c][l1][k2][k3] w^(k1 l1)
-    for (int i = threadIdx.x; i < cg * nk; i += blockDim.x) {
-      const int k = i / cg, cc = i % cg;
-      const int k1 = k / (m * n), k23 = k % (m * n);
+    // x: X[k1][k2][k3][c] = sum_l1 Y[c][l1][k2][k3] w^(k1 l1); job (k23, c), c fastest
+    for (int job = tid; job < cg * m * n; job += bd) {
+      const int cc = job % cg, k23 = job / cg;
       const C2* y = Y + cc * ny + k23;
-      T re = 0, im = 0;
-      int e = 0;
+      C2 v[n];
 #pragma unroll
-      for (int l1 = 0; l1 < n; ++l1) {
-        const C2 v = y[l1 * m * n];
-        const T c = sc[e], s = ss[e];
-        re += v.x * c + v.y * s;
-        im += v.y * c - v.x * s;
-        e += k1;
-        if (e >= m) e -= m;
+      for (int l = 0; l < n; ++l) v[l] = y[l * m * n];
+      C2* out = X_l + ((int64_t)k23 * ncells + cell) * C + c0 + cc;
+#pragma unroll
+      for (int k = 0; k < m; ++k) {
+        T re = 0, im = 0;
+#pragma unroll
+        for (int l = 0; l < n; ++l) {
+          const T c = W::c((k * l) % m), s = W::s((k * l) % m);
+          re = fma(v[l].x, c, fma(v[l].y, s, re));
+          im = fma(v[l].y, c, fma(-v[l].x, s, im));
+        }
+        out[(int64_t)k * m * n * ncells * C] = make_cplx<T>(re, im);
       }
-      X_l[((int64_t)k * ncells + cell) * C + c0 + cc] = make_cplx<T>(re, im);
     }
   }
 }
 
-// Inverse: one CTA per nonempty target cell.  F = scale * IDFT(Y)/P at
-// grid positions (a + n) mod m.
+// Inverse: one CTA per nonempty target cell.  F = scale * IDFT(Y)/P at grid
+// positions (a + n) mod m; (a + ib) e^{+2 pi i j / m} = (a c - b s) + i (b c + a s).
 template <int n, typename T>
 __global__ void k_fft_inv(const int* __restrict__ cells, const cplx_t<T>* __restrict__ Y_l,
                           T* __restrict__ F_l, int64_t ncells, int C, int CG,
                           const T* __restrict__ twid, T invP, T scale) {
   using C2 = cplx_t<T>;
+  using W = Tw<n, T>;
   extern __shared__ __align__(16) unsigned char smraw[];
   T* sm = reinterpret_cast<T*>(smraw);
-  constexpr int m = 2 * n - 1, n2 = n * n, n3 = n2 * n, nk = m * m * n;
-  T* sc = sm;
-  T* ss = sc + m;
+  constexpr int m = 2 * n - 1, n2 = n * n, n3 = n2 * n, nk = m * m * n, ng = n * m * n;
   C2* Yh = (C2*)(sm + ((2 * m + 3) & ~3));  // CG * nk   (k1, k2, k3)
   C2* G = Yh + CG * nk;                     // CG * n*m*n (a1, k2, k3)
-  C2* H = G + CG * n * m * n;               // CG * n3    (a1, a2, k3)
-  for (int i = threadIdx.x; i < m; i += blockDim.x) {
-    sc[i] = twid[i];
-    ss[i] = twid[m + i];
-  }
+  C2* H = G + CG * ng;                      // CG * n3    (a1, a2, k3)
+  (void)twid;
   const int cell = cells[blockIdx.x];
+  const int tid = threadIdx.x, bd = blockDim.x;
   for (int c0 = 0; c0 < C; c0 += CG) {
     const int cg = min(CG, C - c0);
     __syncthreads();
-    for (int i = threadIdx.x; i < cg * nk; i += blockDim.x) {
+    for (int i = tid; i < cg * nk; i += bd) {
       const int k = i / cg, cc = i % cg;
       cp_async_cplx(&Yh[cc * nk + k], &Y_l[((int64_t)k * ncells + cell) * C + c0 + cc], true);
     }
     cp_async_commit();
     cp_async_wait_all();
     __syncthreads();
-    // x: G[c][a1][k2][k3] = sum_k1 Yh[c][k1][k2][k3] e^{+2 pi i k1 t1 / m}
-    constexpr int ng = n * m * n;
-    for (int i = threadIdx.x; i < cg * ng; i += blockDim.x) {
-      const int cc = i / ng, r = i % ng, a1 = r / (m * n), k23 = r % (m * n);
-      const int t1 = (a1 + n) % m;
+    // x: G[c][a1][k2][k3] = sum_k1 Yh[c][k1][k2][k3] e^{+2 pi i k1 t1 / m}; job (c, k23)
+    for (int job = tid; job < cg * m * n; job += bd) {
+      const int k23 = job % (m * n), cc = job / (m * n);
       const C2* y = Yh + cc * nk + k23;
-      T re = 0, im = 0;
-      int e = 0;
+      C2 v[m];
 #pragma unroll
-      for (int k1 = 0; k1 < m; ++k1) {
-        const C2 v = y[k1 * m * n];
-        const T c = sc[e], s = ss[e];
-        re += v.x * c - v.y * s;
-        im += v.y * c + v.x * s;
-        e += t1;
-        if (e >= m) e -= m;
+      for (int k = 0; k < m; ++k) v[k] = y[k * m * n];
+      C2* g = G + cc * ng + k23;
+#pragma unroll
+      for (int a = 0; a < n; ++a) {
+        const int t = (a + n) % m;
+        T re = 0, im = 0;
+#pragma unroll
+        for (int k = 0; k < m; ++k) {
+          const T c = W::c((k * t) % m), s = W::s((k * t) % m);
+          re = fma(v[k].x, c, fma(-v[k].y, s, re));
+          im = fma(v[k].y, c, fma(v[k].x, s, im));
+        }
+        g[a * m * n] = make_cplx<T>(re, im);
       }
-      G[i] = make_cplx<T>(re, im);
     }
     __syncthreads();
-    // y: H[c][a1][a2][k3] = sum_k2 G[c][a1][k2][k3] e^{+2 pi i k2 t2 / m}
-    for (int i = threadIdx.x; i < cg * n3; i += blockDim.x) {
-      const int cc = i / n3, r = i % n3, a1 = r / n2, a2 = (r / n) % n, k3 = r % n;
-      const int t2 = (a2 + n) % m;
+    // y: H[c][a1][a2][k3] = sum_k2 G[c][a1][k2][k3] e^{+2 pi i k2 t2 / m}; job (c, a1, k3)
+    for (int job = tid; job < cg * n2; job += bd) {
+      const int k3 = job % n, a1 = (job / n) % n, cc = job / n2;
       const C2* g = G + cc * ng + a1 * m * n + k3;
-      T re = 0, im = 0;
-      int e = 0;
+      C2 v[m];
 #pragma unroll
-      for (int k2 = 0; k2 < m; ++k2) {
-        const C2 v = g[k2 * n];
-        const T c = sc[e], s = ss[e];
-        re += v.x * c - v.y * s;
-        im += v.y * c + v.x * s;
-        e += t2;
-        if (e >= m) e -= m;
+      for (int k = 0; k < m; ++k) v[k] = g[k * n];
+      C2* h = H + cc * n3 + a1 * n2 + k3;
+#pragma unroll
+      for (int a = 0; a < n; ++a) {
+        const int t = (a + n) % m;
+        T re = 0, im = 0;
+#pragma unroll
+        for (int k = 0; k < m; ++k) {
+          const T c = W::c((k * t) % m), s = W::s((k * t) % m);
+          re = fma(v[k].x, c, fma(-v[k].y, s, re));
+          im = fma(v[k].y, c, fma(v[k].x, s, im));
+        }
+        h[a * n] = make_cplx<T>(re, im);
       }
-      H[i] = make_cplx<T>(re, im);
     }
     __syncthreads();
     // z (complex to real over the Hermitian half):
-    // out = Re H[..][0] + 2 sum_{k3>=1} Re(H[..][k3] e^{+2 pi i k3 t3 / m})
-    for (int i = threadIdx.x; i < cg * n3; i += blockDim.x) {
-      const int cc = i / n3, r = i % n3, a12 = r / n, a3 = r % n;
-      const int t3 = (a3 + n) % m;
-      const C2* h = H + cc * n3 + a12 * n;
-      T acc = h[0].x;
-      int e = t3;
+    // out = Re H[..][0] + 2 sum_{k3>=1} Re(H[..][k3] e^{+2 pi i k3 t3 / m}); job (c, a1, a2)
+    for (int job = tid; job < cg * n2; job += bd) {
+      const C2* h = H + job * n;
+      C2 v[n];
 #pragma unroll
-      for (int k3 = 1; k3 < n; ++k3) {
-        const C2 v = h[k3];
-        acc += T(2) * (v.x * sc[e] - v.y * ss[e]);
-        e += t3;
-        if (e >= m) e -= m;
+      for (int k = 0; k < n; ++k) v[k] = h[k];
+      T* out = F_l + ((int64_t)cell * C + c0) * n3 + job * n;
+#pragma unroll
+      for (int a = 0; a < n; ++a) {
+        const int t = (a + n) % m;
+        T acc = v[0].x;
+#pragma unroll
+        for (int k = 1; k < n; ++k)
+          acc = fma(T(2), fma(v[k].x, W::c((k * t) % m), -v[k].y * W::s((k * t) % m)), acc);
+        out[a] = scale * (acc * invP);
       }
-      F_l[((int64_t)cell * C + c0 + cc) * n3 + r] = scale * (acc * invP);
     }
   }
 }
@@ -413,6 +474,7 @@ struct FftLaunch {
 
 template <typename T>
 static int run_m2l_unif_t(pbbfmm_tree* t, int C, cudaStream_t st) {
+  if (int rc = init_fft_twiddles()) return rc;
   using C2 = cplx_t<T>;
   const int L = t->p.tree_level, n = t->n, m = t->m, n3 = t->n3, nk = t->nk;
   Workspace& ws = t->ws;
