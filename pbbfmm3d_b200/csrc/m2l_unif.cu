@@ -310,6 +310,35 @@ __global__ void k_halo_tables(const int* __restrict__ sstart, const int* __restr
   (void)nbx;
 }
 
+// One sx slab of the MAC: the 6 x 6 (sy, sz) sources of the slab against
+// the 8 children.  F0 / F1: children with tx = 0 / 1 are far in x at this sx
+// (|sx - 2 - tx| > 1), so every interaction test is a compile-time constant.
+template <bool F0, bool F1, int RS, typename C2, typename T>
+__device__ __forceinline__ void mac_slab(const C2* __restrict__ rrow, const C2* __restrict__ orow,
+                                         int py, int pz, T* ar, T* br, T* ai, T* bi) {
+#pragma unroll
+  for (int sy = 0; sy < 6; ++sy)
+#pragma unroll
+    for (int sz = 0; sz < 6; ++sz) {
+      const int r = ((2 * py + sy) << 3) | (2 * pz + sz);
+      const C2 xv = rrow[r * RS];
+#pragma unroll
+      for (int t = 0; t < 8; ++t) {
+        const int tx = (t >> 2) & 1;
+        const int oy = sy - 2 - ((t >> 1) & 1);
+        const int oz = sz - 2 - (t & 1);
+        const bool far_yz = oy > 1 || oy < -1 || oz > 1 || oz < -1;
+        if (far_yz || (tx ? F1 : F0)) {
+          const C2 a = orow[-49 * tx + 7 * (oy + 3) + (oz + 3)];
+          ar[t] = fma(a.x, xv.x, ar[t]);
+          br[t] = fma(-a.y, xv.y, br[t]);
+          ai[t] = fma(a.x, xv.y, ai[t]);
+          bi[t] = fma(a.y, xv.x, bi[t]);
+        }
+      }
+    }
+}
+
 template <int PBX, int KC, int CG, typename T>
 __global__ void __launch_bounds__(4 * PBX * KC * CG)
     k_m2l_unif_mac(const cplx_t<T>* __restrict__ X_l, cplx_t<T>* __restrict__ Y_l,
@@ -359,35 +388,21 @@ __global__ void __launch_bounds__(4 * PBX * KC * CG)
 #pragma unroll
   for (int t = 0; t < 8; ++t) ar[t] = br[t] = ai[t] = bi[t] = T(0);
   const C2* myop = sop + kc * 343;
-  // sx runs as a loop (keeps the unrolled body and its registers small);
-  // for each (sy, sz, t) the y/z offsets are compile-time constants, so the
-  // interaction test reduces to |ox| > 1 unless |oy| or |oz| already is > 1.
+  // sx runs as a loop; the body for each sx is one of four compile-time
+  // specialisations (whether the children with tx = 0 / 1 are far in x at
+  // this sx), so no interaction test is left to run time.
 #pragma unroll 1
   for (int sx = 0; sx < 6; ++sx) {
     const C2* rrow = reg + (((2 * px + sx) << 6) * KC + kc) * CG + cc;
     const C2* orow = myop + 49 * (sx + 1);  // lex of ox + 3 = sx + 1 - tx
-#pragma unroll
-    for (int sy = 0; sy < 6; ++sy)
-#pragma unroll
-      for (int sz = 0; sz < 6; ++sz) {
-        const int r = ((2 * py + sy) << 3) | (2 * pz + sz);
-        const C2 xv = rrow[r * KC * CG];
-#pragma unroll
-        for (int t = 0; t < 8; ++t) {
-          const int tx = (t >> 2) & 1;
-          const int oy = sy - 2 - ((t >> 1) & 1);
-          const int oz = sz - 2 - (t & 1);
-          const int ox = sx - 2 - tx;
-          const bool far_yz = oy > 1 || oy < -1 || oz > 1 || oz < -1;
-          if (far_yz || ox > 1 || ox < -1) {
-            const C2 a = orow[-49 * tx + 7 * (oy + 3) + (oz + 3)];
-            ar[t] = fma(a.x, xv.x, ar[t]);
-            br[t] = fma(-a.y, xv.y, br[t]);
-            ai[t] = fma(a.x, xv.y, ai[t]);
-            bi[t] = fma(a.y, xv.x, bi[t]);
-          }
-        }
-      }
+    if (sx == 0 || sx == 5)
+      mac_slab<true, true, KC * CG>(rrow, orow, py, pz, ar, br, ai, bi);
+    else if (sx == 1)
+      mac_slab<false, true, KC * CG>(rrow, orow, py, pz, ar, br, ai, bi);
+    else if (sx == 4)
+      mac_slab<true, false, KC * CG>(rrow, orow, py, pz, ar, br, ai, bi);
+    else
+      mac_slab<false, false, KC * CG>(rrow, orow, py, pz, ar, br, ai, bi);
   }
   if (k0 + kc < nk && c0 + cc < C) {
 #pragma unroll
