@@ -2,8 +2,8 @@
 backward (pbbfmm3d_b200.solve).
 
 - The GMRES residual, recomputed with the FMM operator, meets the tolerance.
-- Against the exact dense operator the residual is the FMM's approximation
-  level.
+- Against the exact dense operator the residual is explained by the FMM's
+  operator error on x (itself at the approximation level, 1e-4).
 - dL/db and dL/d(points) of L = sum(x * g0) match central finite differences
   of the solve (h = 1e-6, solves to 1e-12): agreement to 1e-4 relative, the
   limit set by solver tolerance / h."""
@@ -41,10 +41,16 @@ def test_gmres_converges():
     x, info = gmres(kernel_operator(t, Pt, LAM), bt, tol=1e-8, restart=60, maxiter=3000)
     assert info["converged"], info
     assert np.all(info["rel_residual"] < 1e-8)
+    # With the exact dense operator the residual is the FMM's operator error
+    # on x (amplified by the conditioning: lam = 1e-2 makes ||x|| >> ||b||):
+    # b - A x = (b - A_fmm x) + (K_fmm - K) x.
     K = _dense(P)
     xs = x.cpu().numpy()
-    r = b - (xs @ K.T + LAM * xs)
-    assert np.linalg.norm(r) / np.linalg.norm(b) < 1e-3
+    kx = xs @ K.T
+    kx_fmm = (kernel_operator(t, Pt, 0.0)(x)).cpu().numpy()
+    assert rel(kx_fmm, kx) < 1e-4  # the FMM's approximation level
+    r = b - (kx + LAM * xs)
+    assert np.linalg.norm(r) <= 1.01 * np.linalg.norm(kx_fmm - kx) + 1e-7 * np.linalg.norm(b)
 
 
 def test_mixed_precision_solve_converges():
