@@ -3,7 +3,7 @@ backward (pbbfmm3d_b200.solve).
 
 - The GMRES residual, recomputed with the FMM operator, meets the tolerance.
 - Against the exact dense operator the residual is explained by the FMM's
-  operator error on x (itself at the approximation level, 1e-4).
+  operator error on x (itself at the approximation level, 1e-4 of K|x|).
 - dL/db and dL/d(points) of L = sum(x * g0) match central finite differences
   of the solve (h = 1e-6, solves to 1e-12): agreement to 1e-4 relative, the
   limit set by solver tolerance / h."""
@@ -48,7 +48,9 @@ def test_gmres_converges():
     xs = x.cpu().numpy()
     kx = xs @ K.T
     kx_fmm = (kernel_operator(t, Pt, 0.0)(x)).cpu().numpy()
-    assert rel(kx_fmm, kx) < 1e-4  # the FMM's approximation level
+    # the FMM's approximation level, against the cancellation-free scale K|x|
+    # (x carries large components that cancel in K x: lam = 1e-2)
+    assert np.linalg.norm(kx_fmm - kx) < 1e-4 * np.linalg.norm(np.abs(xs) @ K.T)
     r = b - (kx + LAM * xs)
     assert np.linalg.norm(r) <= 1.01 * np.linalg.norm(kx_fmm - kx) + 1e-7 * np.linalg.norm(b)
 
