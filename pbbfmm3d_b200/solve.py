@@ -100,6 +100,36 @@ def gmres(apply: Callable[[torch.Tensor], torch.Tensor], b: torch.Tensor, tol: f
                "converged": bool(np.all(rel <= tol * 1.0000001))}
 
 
+def gmres_ir(apply_fast: Callable[[torch.Tensor], torch.Tensor],
+             apply_exact: Callable[[torch.Tensor], torch.Tensor], b: torch.Tensor,
+             tol: float = 1e-6, inner_tol: float = 1e-3, restart: int = 50,
+             maxiter: int = 2000, max_outer: int = 30):
+    """Mixed-precision iterative refinement: residuals r = b - A x with the
+    float64 operator, corrections from GMRES on the fast (mixed-precision)
+    operator to ``inner_tol``.  The fast operator's rounding sets a floor
+    near eps * ||K|x|||, which a plain mixed GMRES cannot go below when
+    ||x|| >> ||b||; refinement reaches the float64 residual ``tol``.
+    Returns (x, info) like ``gmres`` plus "outer" and "exact_matvecs"."""
+    bnorm = torch.linalg.norm(b, dim=1)
+    bnorm = torch.where(bnorm > 0, bnorm, torch.ones_like(bnorm))
+    x = torch.zeros_like(b)
+    r = b.clone()
+    fast = exact = outer = 0
+    while outer < max_outer and fast < maxiter:
+        rel = torch.linalg.norm(r, dim=1) / bnorm
+        if bool((rel <= tol).all()):
+            break
+        d, info = gmres(apply_fast, r, inner_tol, restart, maxiter - fast)
+        fast += info["matvecs"]
+        x += d
+        r = b - apply_exact(x)
+        exact += 1
+        outer += 1
+    rel = (torch.linalg.norm(r, dim=1) / bnorm).cpu().numpy()
+    return x, {"matvecs": fast, "exact_matvecs": exact, "outer": outer, "rel_residual": rel,
+               "converged": bool(np.all(rel <= tol * 1.0000001))}
+
+
 def kernel_operator(tree: H2_3D_Tree, points: torch.Tensor, lam: float,
                     precision: int = PREC_FP64, adjoint: bool = False):
     """v (C, N) -> (K + lam I) v, or its transpose (the adjoint FMM)."""
@@ -119,13 +149,24 @@ def kernel_operator(tree: H2_3D_Tree, points: torch.Tensor, lam: float,
     return apply
 
 
+def _solve(tree, points, b, lam, tol, precision, restart, maxiter, adjoint=False):
+    """float64: GMRES; mixed: GMRES on the mixed operator inside float64
+    iterative refinement."""
+    exact = kernel_operator(tree, points, lam, PREC_FP64, adjoint)
+    if precision == PREC_FP64:
+        return gmres(exact, b, tol, restart, maxiter)
+    fast = kernel_operator(tree, points, lam, precision, adjoint)
+    return gmres_ir(fast, exact, b, tol, 1e-3, restart, maxiter)
+
+
 class KernelSolve(torch.autograd.Function):
-    """x = (K(P, P) + lam I)^{-1} b, differentiable in b and in the points P."""
+    """x = (K(P, P) + lam I)^{-1} b, differentiable in b and in the points P.
+    Mixed precision: GMRES on the mixed-precision FMM inside float64 iterative
+    refinement, so the float64 residual meets ``tol``."""
 
     @staticmethod
     def forward(ctx, points, b, tree, lam, tol, precision, restart, maxiter):
-        x, info = gmres(kernel_operator(tree, points, lam, precision), b.contiguous(), tol,
-                        restart, maxiter)
+        x, info = _solve(tree, points, b.contiguous(), lam, tol, precision, restart, maxiter)
         ctx.save_for_backward(points, x)
         ctx.cfg = (tree, lam, tol, precision, restart, maxiter)
         ctx.info = info
@@ -135,8 +176,8 @@ class KernelSolve(torch.autograd.Function):
     def backward(ctx, gx):
         points, x = ctx.saved_tensors
         tree, lam, tol, precision, restart, maxiter = ctx.cfg
-        mu, _ = gmres(kernel_operator(tree, points, lam, precision, adjoint=True),
-                      gx.contiguous(), tol, restart, maxiter)
+        mu, _ = _solve(tree, points, gx.contiguous(), lam, tol, precision, restart, maxiter,
+                       adjoint=True)
         grad_points = None
         if ctx.needs_input_grad[0]:
             gt = torch.zeros_like(points)
