@@ -387,7 +387,7 @@ static void free_tree_device(pbbfmm_tree* t) {
                    &ws.tperm,     &ws.sperm, &ws.tstart,  &ws.sstart,     &ws.tpos,
                    &ws.spos,      &ws.wsorted, &ws.cub_temp, &ws.lists,    &ws.dcounts,
                    &ws.S,         &ws.F,     &ws.proxy,   &ws.pf,         &ws.io_tgt,
-                   &ws.io_src,    &ws.io_w,  &ws.io_out, &ws.halo, &ws.tc_proxy};
+                   &ws.io_src,    &ws.io_w,  &ws.io_out, &ws.halo, &ws.tc_proxy, &ws.leafpart};
   for (DevBuf* b : all) release(*b);
   for (int i = 0; i < 16; ++i)
     if (t->ev[i]) {

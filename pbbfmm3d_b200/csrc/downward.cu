@@ -8,6 +8,8 @@
 // leaves (no atomics, no symmetry assumption, sources may differ from
 // targets), and the far-field interpolation, the near-field sum and the
 // scatter to the caller's output are one kernel.
+#include <cub/cub.cuh>
+
 #include <type_traits>
 
 #include "fmm.cuh"
@@ -183,7 +185,8 @@ using LeafAcc = typename std::conditional<sizeof(T) == 4, Kahan<T>, PlainSum<T>>
 // update in float64.  T = double: everything in float64.
 template <class KF, typename T, int KC, bool DENSE>
 __global__ void __launch_bounds__(32 * kLeafWarps, DENSE ? 4 : 6)
-    k_leaf(const int* __restrict__ leaves, int nleaves, const int* __restrict__ tstart,
+    k_leaf(const int* __restrict__ leaves, int nleaves, const int* __restrict__ part_count,
+           const int* __restrict__ tstart,
            const int* __restrict__ sstart, const int* __restrict__ tperm,
            const double* __restrict__ tpos, const double* __restrict__ spos,
            const double* __restrict__ wsorted, int Nf, int Ns, int C,
@@ -207,8 +210,11 @@ __global__ void __launch_bounds__(32 * kLeafWarps, DENSE ? 4 : 6)
   __syncthreads();
   const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
   const int wid = blockIdx.x * kLeafWarps + wl;
-  if (wid >= nleaves) return;
-  const int leaf = leaves[wid];
+  // leaves are partitioned: the dense ones first, the sparse ones after
+  const int nd = *part_count;
+  const int count = DENSE ? nd : nleaves - nd;
+  if (wid >= count) return;
+  const int leaf = DENSE ? leaves[wid] : leaves[nd + wid];
   const int ta = tstart[leaf], te = tstart[leaf + 1];
   if ((te - ta >= kLaneLeafMin) != DENSE) return;  // the other instantiation's leaf
   const int n3 = n * n * n;
@@ -558,6 +564,13 @@ struct LeafGradLaunch {
   }
 };
 
+struct DenseLeaf {
+  const int* tstart;
+  __host__ __device__ bool operator()(int leaf) const {
+    return tstart[leaf + 1] - tstart[leaf] >= kLaneLeafMin;
+  }
+};
+
 template <typename T>
 struct LeafLaunch {
   pbbfmm_tree* t;
@@ -575,13 +588,25 @@ struct LeafLaunch {
     const int64_t perS = (int64_t)C * t->n3;
     if (int rc_ = kt_begin(t, KS_LEAF, st)) return rc_;
     const size_t dyn = sizeof(T) * kLeafWarps * 3 * t->n * 32;
+    // partition the leaves (dense first) so that each launch's active warps
+    // are packed into the first CTAs of its grid
+    const int* leaves = ws.lists.as<int>() + t->lists.tgt_off[L];
+    if (int rc_ = grow(ws.leafpart, sizeof(int) * ((size_t)nl + 1))) return rc_;
+    int* part = ws.leafpart.as<int>();
+    int* nsel = part + nl;
+    size_t tb = 0;
+    DenseLeaf pred{ws.tstart.as<int>()};
+    PB_CUDA(cub::DevicePartition::If(nullptr, tb, leaves, part, nsel, nl, pred, st));
+    if (int rc_ = grow(ws.cub_temp, tb)) return rc_;
+    tb = ws.cub_temp.cap;
+    PB_CUDA(cub::DevicePartition::If(ws.cub_temp.p, tb, leaves, part, nsel, nl, pred, st));
+    count_launches(2);
     // one column: registers for one; otherwise columns in passes of kLeafCols.
-    // Dense and sparse leaves run as two launches over the same leaf list.
     for (int dense = 1; dense >= 0; --dense) {
       auto kern = C == 1 ? (dense ? k_leaf<KF, T, 1, true> : k_leaf<KF, T, 1, false>)
                          : (dense ? k_leaf<KF, T, kLeafCols, true> : k_leaf<KF, T, kLeafCols, false>);
       kern<<<(nl + kLeafWarps - 1) / kLeafWarps, 32 * kLeafWarps, dense ? dyn : 0, st>>>(
-          ws.lists.as<int>() + t->lists.tgt_off[L], nl, ws.tstart.as<int>(), ws.sstart.as<int>(),
+          part, nl, nsel, ws.tstart.as<int>(), ws.sstart.as<int>(),
           ws.tperm.as<int>(), ws.tpos.as<double>(), ws.spos.as<double>(), ws.wsorted.as<double>(),
           (int)Nf, (int)Ns, C, ws.F.as<T>() + level_offset(L, perS), t->n, t->p.use_chebyshev,
           ops_view<T>(t).Tkz, t->p.L, L, kparam, out);
