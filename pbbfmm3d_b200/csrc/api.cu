@@ -9,6 +9,7 @@
 #include <cstring>
 #include <atomic>
 #include <string>
+#include <thread>
 #include <utility>
 
 #include "fmm.cuh"
@@ -389,6 +390,12 @@ static void free_tree_device(pbbfmm_tree* t) {
                    &ws.S,         &ws.F,     &ws.proxy,   &ws.pf,         &ws.io_tgt,
                    &ws.io_src,    &ws.io_w,  &ws.io_out, &ws.halo, &ws.tc_proxy, &ws.leafpart};
   for (DevBuf* b : all) release(*b);
+  if (ws.h_in) cudaFreeHost(ws.h_in);
+  if (ws.h_out) cudaFreeHost(ws.h_out);
+  ws.h_in = ws.h_out = nullptr;
+  ws.h_in_cap = ws.h_out_cap = 0;
+  if (ws.io_stream) cudaStreamDestroy(ws.io_stream);
+  ws.io_stream = nullptr;
   for (int i = 0; i < 16; ++i)
     if (t->ev[i]) {
       cudaEventDestroy(t->ev[i]);
@@ -410,6 +417,66 @@ static int take_tc_timeout(pbbfmm_tree* t) {
     return PBBFMM_ERR_TIMEOUT;
   }
   return PBBFMM_OK;
+}
+
+// ---- host staging of the host-buffer entry point
+constexpr size_t kStageChunk = 16u << 20;
+
+static int grow_pinned(void** p, size_t* cap, size_t bytes) {
+  if (bytes == 0) bytes = 16;
+  if (*p && *cap >= bytes) return PBBFMM_OK;
+  if (*p) cudaFreeHost(*p);
+  *p = nullptr;
+  *cap = 0;
+  PB_CUDA(cudaHostAlloc(p, bytes, cudaHostAllocDefault));
+  *cap = bytes;
+  return PBBFMM_OK;
+}
+
+static int host_threads(size_t bytes) {
+  const unsigned hw = std::thread::hardware_concurrency();
+  const size_t by_size = bytes / (1u << 20) + 1;  // about 1 MB per thread at least
+  size_t n = hw ? (hw < 16 ? hw : 16) : 4;
+  return (int)(n < by_size ? n : by_size);
+}
+
+// memcpy split over host threads (pageable source into pinned staging)
+static void host_copy_mt(void* dst, const void* src, size_t bytes) {
+  const int nt = host_threads(bytes);
+  if (nt <= 1) {
+    memcpy(dst, src, bytes);
+    return;
+  }
+  std::vector<std::thread> th;
+  const size_t per = (bytes + nt - 1) / nt;
+  for (int i = 0; i < nt; ++i) {
+    const size_t a = i * per, b = a + per < bytes ? a + per : bytes;
+    if (a >= b) break;
+    th.emplace_back([=] {
+      memcpy(static_cast<unsigned char*>(dst) + a, static_cast<const unsigned char*>(src) + a, b - a);
+    });
+  }
+  for (auto& x : th) x.join();
+}
+
+// dst[i] += src[i], split over host threads
+static void host_add_mt(double* dst, const double* src, size_t n) {
+  const int nt = host_threads(n * sizeof(double));
+  auto add = [](double* d, const double* s, size_t a, size_t b) {
+    for (size_t i = a; i < b; ++i) d[i] += s[i];
+  };
+  if (nt <= 1) {
+    add(dst, src, 0, n);
+    return;
+  }
+  std::vector<std::thread> th;
+  const size_t per = (n + nt - 1) / nt;
+  for (int i = 0; i < nt; ++i) {
+    const size_t a = i * per, b = a + per < n ? a + per : n;
+    if (a >= b) break;
+    th.emplace_back(add, dst, src, a, b);
+  }
+  for (auto& x : th) x.join();
 }
 
 static const char* kPhaseNames = "binning,upward,far_field,downward,near_field";
@@ -898,22 +965,65 @@ int pbbfmm_compute(pbbfmm_tree* t, const double* target, int64_t Nf, const doubl
   PB_CUDA(cudaSetDevice(t->device));
   Workspace& ws = t->ws;
   int rc;
+  if (!ws.io_stream) PB_CUDA(cudaStreamCreateWithFlags(&ws.io_stream, cudaStreamNonBlocking));
+  cudaStream_t st = ws.io_stream;
   const bool same = (source == target && Ns == Nf);
-  if ((rc = grow(ws.io_tgt, sizeof(double) * 3 * Nf))) return rc;
-  if (!same && (rc = grow(ws.io_src, sizeof(double) * 3 * (Ns ? Ns : 1)))) return rc;
-  if ((rc = grow(ws.io_w, sizeof(double) * (size_t)(Ns ? Ns : 1) * nCols))) return rc;
-  if ((rc = grow(ws.io_out, sizeof(double) * (size_t)Nf * nCols))) return rc;
+  const size_t bt = sizeof(double) * 3 * Nf, bs = same ? 0 : sizeof(double) * 3 * Ns;
+  const size_t bw = sizeof(double) * (size_t)Ns * nCols, bo = sizeof(double) * (size_t)Nf * nCols;
+  if ((rc = grow(ws.io_tgt, bt))) return rc;
+  if (!same && (rc = grow(ws.io_src, bs ? bs : 16))) return rc;
+  if ((rc = grow(ws.io_w, bw ? bw : 16))) return rc;
+  if ((rc = grow(ws.io_out, bo))) return rc;
+  if ((rc = grow_pinned(&ws.h_in, &ws.h_in_cap, bt + bs + bw))) return rc;
+  if ((rc = grow_pinned(&ws.h_out, &ws.h_out_cap, bo))) return rc;
   double* dt = ws.io_tgt.as<double>();
   double* ds = same ? dt : ws.io_src.as<double>();
-  PB_CUDA(cudaMemcpy(dt, target, sizeof(double) * 3 * Nf, cudaMemcpyHostToDevice));
-  if (!same && Ns > 0) PB_CUDA(cudaMemcpy(ds, source, sizeof(double) * 3 * Ns, cudaMemcpyHostToDevice));
-  if (Ns > 0)
-    PB_CUDA(cudaMemcpy(ws.io_w.p, weight, sizeof(double) * Ns * nCols, cudaMemcpyHostToDevice));
-  PB_CUDA(cudaMemcpy(ws.io_out.p, output, sizeof(double) * Nf * nCols, cudaMemcpyHostToDevice));
+  // inputs: multithreaded copy into pinned staging, chunk by chunk, each
+  // chunk's DMA overlapping the next chunk's host copy
+  unsigned char* hin = static_cast<unsigned char*>(ws.h_in);
+  struct Seg {
+    const void* src;
+    void* dev;
+    size_t bytes;
+  } segs[3] = {{target, dt, bt}, {source, ds, bs}, {weight, ws.io_w.p, bw}};
+  size_t off = 0;
+  for (const Seg& g : segs)
+    for (size_t c = 0; c < g.bytes; c += kStageChunk) {
+      const size_t n = g.bytes - c < kStageChunk ? g.bytes - c : kStageChunk;
+      host_copy_mt(hin + off, static_cast<const unsigned char*>(g.src) + c, n);
+      PB_CUDA(cudaMemcpyAsync(static_cast<unsigned char*>(g.dev) + c, hin + off, n,
+                              cudaMemcpyHostToDevice, st));
+      off += n;
+    }
+  // the result comes back into a zeroed buffer and is added to the caller's
+  // output on the host (accumulate semantics without uploading the output)
+  PB_CUDA(cudaMemsetAsync(ws.io_out.p, 0, bo, st));
   rc = pbbfmm_compute_device(t, dt, Nf, ds, Ns, ws.io_w.as<double>(), nCols,
-                             ws.io_out.as<double>(), t->precision, nullptr);
+                             ws.io_out.as<double>(), t->precision, st);
   if (rc) return rc;
-  PB_CUDA(cudaMemcpy(output, ws.io_out.p, sizeof(double) * Nf * nCols, cudaMemcpyDeviceToHost));
+  double* hout = static_cast<double*>(ws.h_out);
+  const size_t chunk_d = kStageChunk / sizeof(double);
+  const size_t total_d = (size_t)Nf * nCols;
+  std::vector<cudaEvent_t> evs;
+  for (size_t c = 0; c < total_d; c += chunk_d) {
+    const size_t n = total_d - c < chunk_d ? total_d - c : chunk_d;
+    PB_CUDA(cudaMemcpyAsync(hout + c, ws.io_out.as<double>() + c, n * sizeof(double),
+                            cudaMemcpyDeviceToHost, st));
+    cudaEvent_t e;
+    PB_CUDA(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    PB_CUDA(cudaEventRecord(e, st));
+    evs.push_back(e);
+  }
+  int status = PBBFMM_OK;
+  size_t k = 0;
+  for (size_t c = 0; c < total_d; c += chunk_d, ++k) {
+    const size_t n = total_d - c < chunk_d ? total_d - c : chunk_d;
+    cudaError_t e = cudaEventSynchronize(evs[k]);
+    if (e != cudaSuccess && status == PBBFMM_OK) status = cuda_status(e, "result copy");
+    if (status == PBBFMM_OK) host_add_mt(output + c, hout + c, n);
+  }
+  for (cudaEvent_t e : evs) cudaEventDestroy(e);
+  if (status) return status;
   return take_tc_timeout(t);
 }
 

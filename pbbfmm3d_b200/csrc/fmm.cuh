@@ -48,6 +48,12 @@ struct Workspace {
   DevBuf leafpart;  // leaf phase: target leaves partitioned dense-first, then their count
   // staging for the host-pointer entry point
   DevBuf io_tgt, io_src, io_w, io_out;
+  // pinned host staging of the host-buffer entry point (cudaHostAlloc)
+  void* h_in = nullptr;
+  size_t h_in_cap = 0;
+  void* h_out = nullptr;
+  size_t h_out_cap = 0;
+  cudaStream_t io_stream = nullptr;  // the host entry's stream (created on first use)
 };
 
 struct LevelLists {
