@@ -310,12 +310,6 @@ __global__ void k_halo_tables(const int* __restrict__ sstart, const int* __restr
   (void)nbx;
 }
 
-// d += a * b on two packed float32 lanes (Blackwell's paired FP32 FMA).
-__device__ __forceinline__ void ffma2(unsigned long long& d, unsigned long long a,
-                                      unsigned long long b) {
-  asm("fma.rn.f32x2 %0, %1, %2, %0;\n" : "+l"(d) : "l"(a), "l"(b));
-}
-
 // One sx slab of the MAC: the 6 x 6 (sy, sz) sources of the slab against
 // the 8 children.  F0 / F1: children with tx = 0 / 1 are far in x at this sx
 // (|sx - 2 - tx| > 1), so every interaction test is a compile-time constant.
@@ -354,13 +348,10 @@ __global__ void __launch_bounds__(4 * PBX * KC * CG)
   using C2 = cplx_t<T>;
   constexpr int NT = G::NPAR * KC * CG;
   constexpr int RC = G::RC;
-  // float32: the operator is staged as quads (a.x, a.x, -a.y, a.y) for the
-  // packed FP32 FMAs below (two complex slots per entry)
-  constexpr int OPW = sizeof(T) == 4 ? 2 : 1;
   extern __shared__ __align__(16) unsigned char smraw[];
   C2* reg = reinterpret_cast<C2*>(smraw);  // RC x KC x CG
-  C2* sop = reg + RC * KC * CG;            // KC x 343 (x OPW)
-  int* s_src = (int*)(sop + KC * 343 * OPW);  // RC source cells, then TC target cells
+  C2* sop = reg + RC * KC * CG;            // KC x 343
+  int* s_src = (int*)(sop + KC * 343);  // RC source cells, then TC target cells
   int* s_tgt = s_src + RC;
   const int tid = threadIdx.x;
   const int cc = tid % CG, kc = (tid / CG) % KC, p = tid / (CG * KC);
@@ -388,12 +379,7 @@ __global__ void __launch_bounds__(4 * PBX * KC * CG)
   for (int i = tid; i < KC * 343; i += NT) {
     const int kk = i / 343, e = i % 343;
     const bool ok = k0 + kk < nk;
-    if constexpr (sizeof(T) == 4) {
-      const C2 a = ok ? op[(int64_t)(k0 + kk) * 343 + e] : make_cplx<T>(0, 0);
-      reinterpret_cast<float4*>(sop)[i] = make_float4(a.x, a.x, -a.y, a.y);
-    } else {
-      cp_async_cplx(&sop[i], ok ? &op[(int64_t)(k0 + kk) * 343 + e] : op, ok);
-    }
+    cp_async_cplx(&sop[i], ok ? &op[(int64_t)(k0 + kk) * 343 + e] : op, ok);
   }
   cp_async_commit();
   cp_async_wait_all();
@@ -401,10 +387,7 @@ __global__ void __launch_bounds__(4 * PBX * KC * CG)
   T ar[8], br[8], ai[8], bi[8];  // re = ar + br, im = ai + bi
 #pragma unroll
   for (int t = 0; t < 8; ++t) ar[t] = br[t] = ai[t] = bi[t] = T(0);
-  unsigned long long pa[8], pb[8];  // float32: packed (ar, ai), (br, bi)
-#pragma unroll
-  for (int t = 0; t < 8; ++t) pa[t] = pb[t] = 0ull;
-  const C2* myop = sop + kc * 343 * OPW;
+  const C2* myop = sop + kc * 343;
   // sx runs as a loop.  float64: the body for each sx is one of four
   // compile-time specialisations (whether the children with tx = 0 / 1 are
   // far in x at this sx), so no interaction test is left to run time (9 %
@@ -425,17 +408,12 @@ __global__ void __launch_bounds__(4 * PBX * KC * CG)
       else
         mac_slab<false, false, KC * CG>(rrow, orow, py, pz, ar, br, ai, bi);
     } else {
-      // packed FP32: (ar, ai) += (a.x, a.x) * (x.x, x.y) and
-      // (br, bi) += (-a.y, a.y) * (x.y, x.x), two FMAs per instruction
-      const ulonglong2* oq = reinterpret_cast<const ulonglong2*>(myop) + 49 * (sx + 1);
 #pragma unroll
       for (int sy = 0; sy < 6; ++sy)
 #pragma unroll
         for (int sz = 0; sz < 6; ++sz) {
           const int r = ((2 * py + sy) << 3) | (2 * pz + sz);
-          const unsigned long long xv =
-              *reinterpret_cast<const unsigned long long*>(&rrow[r * KC * CG]);
-          const unsigned long long xs = (xv >> 32) | (xv << 32);
+          const C2 xv = rrow[r * KC * CG];
 #pragma unroll
           for (int t = 0; t < 8; ++t) {
             const int tx = (t >> 2) & 1;
@@ -444,21 +422,14 @@ __global__ void __launch_bounds__(4 * PBX * KC * CG)
             const int ox = sx - 2 - tx;
             const bool far_yz = oy > 1 || oy < -1 || oz > 1 || oz < -1;
             if (far_yz || ox > 1 || ox < -1) {
-              const ulonglong2 q = oq[-49 * tx + 7 * (oy + 3) + (oz + 3)];
-              ffma2(pa[t], q.x, xv);
-              ffma2(pb[t], q.y, xs);
+              const C2 a = orow[-49 * tx + 7 * (oy + 3) + (oz + 3)];
+              ar[t] = fma(a.x, xv.x, ar[t]);
+              br[t] = fma(-a.y, xv.y, br[t]);
+              ai[t] = fma(a.x, xv.y, ai[t]);
+              bi[t] = fma(a.y, xv.x, bi[t]);
             }
           }
         }
-    }
-  }
-  if constexpr (sizeof(T) == 4) {
-#pragma unroll
-    for (int t = 0; t < 8; ++t) {
-      ar[t] = __uint_as_float((unsigned)pa[t]);
-      ai[t] = __uint_as_float((unsigned)(pa[t] >> 32));
-      br[t] = __uint_as_float((unsigned)pb[t]);
-      bi[t] = __uint_as_float((unsigned)(pb[t] >> 32));
     }
   }
   if (k0 + kc < nk && c0 + cc < C) {
@@ -484,8 +455,8 @@ static int launch_mac(const cplx_t<T>* X, cplx_t<T>* Y, const cplx_t<T>* op, int
   k_halo_tables<PBX><<<nblk, 256, 0, st>>>(sstart, tstart, span, lev, halo);
   PB_LAUNCH("halo_tables");
   dim3 g((unsigned)nblk, (unsigned)((nk + KC - 1) / KC), (unsigned)((C + CG - 1) / CG));
-  const size_t smem = sizeof(cplx_t<T>) * (G::RC * KC * CG + KC * 343 * (sizeof(T) == 4 ? 2 : 1)) +
-                      sizeof(int) * G::STRIDE;
+  const size_t smem =
+      sizeof(cplx_t<T>) * (G::RC * KC * CG + KC * 343) + sizeof(int) * G::STRIDE;
   PB_CUDA(cudaFuncSetAttribute(k_m2l_unif_mac<PBX, KC, CG, T>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k_m2l_unif_mac<PBX, KC, CG, T><<<g, G::NPAR * KC * CG, smem, st>>>(X, Y, op, halo,
