@@ -93,6 +93,21 @@ def gen_inputs(wl, rank=0):
     return pts, w
 
 
+def max_over_ranks(x, dist, device):
+    """Largest x over all ranks (a float; every rank gets it)."""
+    import torch
+
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(world, N, C, steps, max_total_ms):
+    """Whole-job N*nCols/s: every rank runs its own nCols-column block on the
+    same points; time is the slowest rank's."""
+    return world * N * C * steps / (max_total_ms * 1e-3)
+
+
 def make_tree(fmm, wl, device):
     if wl["kernel"] == "ExpCov":
         return fmm.kernel_ExpCov(wl["box"], wl["L"], wl["n"], wl["eps"], wl["cheb"],
@@ -312,9 +327,7 @@ def time_precisions(fmm, torch, dist, tree, step, flush, args, world, local_rank
         tree.set_timing(False)
         total_ms = sum(step_ms)
         if world > 1:
-            tt = torch.tensor([total_ms], device="cuda")
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            total_ms = float(tt.item())
+            total_ms = max_over_ranks(total_ms, dist, "cuda")
         results[pname] = dict(total_ms=total_ms, step_ms=step_ms, ktimes=ktimes, clocks=clocks,
                               launches=launches)
     return results
@@ -454,9 +467,7 @@ def run_workload(wl, args, rank, world, local_rank, e2e_wanted):
             ts.append(time.perf_counter() - t1)
         e2e_s = sum(ts) / len(ts)
         if world > 1:
-            tt = torch.tensor([e2e_s], device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            e2e_s = float(tt.item())
+            e2e_s = max_over_ranks(e2e_s, dist, dev)
         e2e = {"value": world * N * C / e2e_s, "unit": "N*nCols/s",
                "h2d_bytes_per_step": int(8 * (3 * N + N * C)),
                "d2h_bytes_per_step": int(8 * N * C), "ms_per_step": 1e3 * e2e_s,
@@ -465,8 +476,8 @@ def run_workload(wl, args, rank, world, local_rank, e2e_wanted):
     roof = (cheb_roofline if wl["cheb"] else unif_roofline)(fmm, tree, wl, results, args.steps,
                                                              local_rank)
     r, r64 = results["mixed"], results["fp64"]
-    value = world * N * C * args.steps / (r["total_ms"] * 1e-3)
-    value64 = world * N * C * args.steps / (r64["total_ms"] * 1e-3)
+    value = job_throughput(world, N, C, args.steps, r["total_ms"])
+    value64 = job_throughput(world, N, C, args.steps, r64["total_ms"])
     kt = r["ktimes"]
     out = {
         "value": value, "ms_per_step": r["total_ms"] / args.steps, "rel_l2_err": errs["mixed"],
@@ -607,7 +618,7 @@ def our_arm(args, rank, world, local_rank):
                                     "roofline", "gpu_launches_per_step", "clocks")}
         target["unit"] = "N*nCols/s"
     diff = None
-    if args.workload == "bench" and not args.no_grad:
+    if args.workload == "bench" and not args.no_grad and world == 1:
         diff = run_grad_workload(WORKLOADS["grad"], args, local_rank)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
