@@ -66,6 +66,7 @@ KERNEL_TEXT = {"ExpCov": "exp(-r/%g)", "Laplacian": "1/r (0 at r=0)",
 # bounded CPU sample: same kernel, order, columns and points per leaf (N / 8^L)
 CPU_SAMPLE = dict(N=15_625, L=4)
 N_SAMPLED_TARGETS = 4096
+METRIC = "FMM matvec N*nCols/s (rel-L2 vs FP64 direct sum on 4096 sampled targets)"
 
 
 def log(*a):
@@ -273,7 +274,7 @@ def reference_arm(args, rank):
         return 0
     ms = 1e3 * sum(times) / len(times)
     line = {
-        "impl": "reference", "metric": "FMM matvec N*nCols/s", "value": value,
+        "impl": "reference", "metric": METRIC, "value": value,
         "unit": "N*nCols/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded uniform points, N(0,1) weights)",
@@ -634,7 +635,7 @@ def our_arm(args, rank, world, local_rank):
     if rank != 0:
         return 0
     line = {
-        "metric": "FMM matvec N*nCols/s (rel-L2 vs FP64 direct sum on 4096 sampled targets)",
+        "metric": METRIC,
         "value": head["value"], "unit": "N*nCols/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": head["ms_per_step"], "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
