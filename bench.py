@@ -49,6 +49,10 @@ WORKLOADS = {
     "clustered": dict(name="laplace_cheb6_clustered_N4e6_C1_L7", kernel="Laplacian", param=0.0,
                       N=4_000_000, C=1, L=7, n=6, cheb=1, eps=1e-7, box=1.0, seed=4321,
                       dist="clustered", weights="uniform"),
+    # the same, at Chebyshev order 7: the order at which the FMM itself meets 1e-6
+    "clustered7": dict(name="laplace_cheb7_clustered_N4e6_C1_L7", kernel="Laplacian", param=0.0,
+                       N=4_000_000, C=1, L=7, n=7, cheb=1, eps=1e-7, box=1.0, seed=4321,
+                       dist="clustered", weights="uniform"),
     # small cases of the same kernels for ncu captures (a few GB on the device)
     # differentiation: separate sources and targets, loss = sum(f * g)
     "grad": dict(name="gauss0.1_cheb5_S1e6_T1e6_C4_L6", kernel="GaussSigma", param=0.1,
