@@ -186,7 +186,7 @@ using LeafAcc = typename std::conditional<sizeof(T) == 4, Kahan<T>, PlainSum<T>>
 template <class KF, typename T, int KC, bool DENSE>
 __global__ void __launch_bounds__(32 * kLeafWarps, DENSE ? 4 : 6)
     k_leaf(const int* __restrict__ leaves, int nleaves, const int* __restrict__ part_count,
-           const int* __restrict__ tstart,
+           const int* __restrict__ chunk_prefix, const int* __restrict__ tstart,
            const int* __restrict__ sstart, const int* __restrict__ tperm,
            const double* __restrict__ tpos, const double* __restrict__ spos,
            const double* __restrict__ wsorted, int Nf, int Ns, int C,
@@ -212,10 +212,27 @@ __global__ void __launch_bounds__(32 * kLeafWarps, DENSE ? 4 : 6)
   const int wid = blockIdx.x * kLeafWarps + wl;
   // leaves are partitioned: the dense ones first, the sparse ones after
   const int nd = *part_count;
-  const int count = DENSE ? nd : nleaves - nd;
-  if (wid >= count) return;
-  const int leaf = DENSE ? leaves[wid] : leaves[nd + wid];
-  const int ta = tstart[leaf], te = tstart[leaf + 1];
+  int leaf, ta, te, tc0 = 0;
+  if constexpr (DENSE) {
+    // warp = one 32-target chunk of a dense leaf; chunk_prefix[i] is the first
+    // chunk of dense leaf i (exclusive scan), chunk_prefix[nd] the total
+    if (wid >= chunk_prefix[nd]) return;
+    int lo = 0, hi = nd - 1;
+    while (lo < hi) {  // last i with chunk_prefix[i] <= wid
+      const int mid = (lo + hi + 1) >> 1;
+      if (chunk_prefix[mid] <= wid) lo = mid;
+      else hi = mid - 1;
+    }
+    leaf = leaves[lo];
+    ta = tstart[leaf];
+    te = tstart[leaf + 1];
+    tc0 = ta + 32 * (wid - chunk_prefix[lo]);
+  } else {
+    if (wid >= nleaves - nd) return;
+    leaf = leaves[nd + wid];
+    ta = tstart[leaf];
+    te = tstart[leaf + 1];
+  }
   if ((te - ta >= kLaneLeafMin) != DENSE) return;  // the other instantiation's leaf
   const int n3 = n * n * n;
   double c[3];
@@ -306,7 +323,7 @@ __global__ void __launch_bounds__(32 * kLeafWarps, DENSE ? 4 : 6)
   // Dense leaf: one target per lane, sources through shared-memory tiles.
   for (int c0 = 0; c0 < C; c0 += KC) {
     const int cg = min(KC, C - c0);
-    for (int t0 = ta; t0 < te; t0 += 32) {
+    for (int t0 = tc0; t0 < te && t0 < tc0 + 32; t0 += 32) {  // this warp's chunk
       const int i = t0 + lane;
       const bool active = i < te;
       double x = c[0], y = c[1], z = c[2];
@@ -564,6 +581,19 @@ struct LeafGradLaunch {
   }
 };
 
+// counts[i] = 32-target chunks of dense leaf i (i < *nsel), 0 otherwise (i <= nl)
+__global__ void k_chunk_counts(const int* __restrict__ part, const int* __restrict__ nsel, int nl,
+                               const int* __restrict__ tstart, int* __restrict__ counts) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i > nl) return;
+  int c = 0;
+  if (i < *nsel) {
+    const int leaf = part[i];
+    c = (tstart[leaf + 1] - tstart[leaf] + 31) / 32;
+  }
+  counts[i] = c;
+}
+
 struct DenseLeaf {
   const int* tstart;
   __host__ __device__ bool operator()(int leaf) const {
@@ -591,7 +621,7 @@ struct LeafLaunch {
     // partition the leaves (dense first) so that each launch's active warps
     // are packed into the first CTAs of its grid
     const int* leaves = ws.lists.as<int>() + t->lists.tgt_off[L];
-    if (int rc_ = grow(ws.leafpart, sizeof(int) * ((size_t)nl + 1))) return rc_;
+    if (int rc_ = grow(ws.leafpart, sizeof(int) * 3 * ((size_t)nl + 1))) return rc_;
     int* part = ws.leafpart.as<int>();
     int* nsel = part + nl;
     size_t tb = 0;
@@ -601,12 +631,27 @@ struct LeafLaunch {
     tb = ws.cub_temp.cap;
     PB_CUDA(cub::DevicePartition::If(ws.cub_temp.p, tb, leaves, part, nsel, nl, pred, st));
     count_launches(2);
+    // 32-target chunks of the dense leaves, exclusive scan -> one warp each
+    int* chunks = part + nl + 1;  // nl + 1 counts, then nl + 1 prefixes
+    int* prefix = chunks + nl + 1;
+    k_chunk_counts<<<(unsigned)((nl + 1 + 255) / 256), 256, 0, st>>>(part, nsel, nl,
+                                                                   ws.tstart.as<int>(), chunks);
+    PB_LAUNCH("leaf_chunks");
+    size_t tb2 = 0;
+    PB_CUDA(cub::DeviceScan::ExclusiveSum(nullptr, tb2, chunks, prefix, nl + 1, st));
+    if (int rc_ = grow(ws.cub_temp, tb2)) return rc_;
+    tb2 = ws.cub_temp.cap;
+    PB_CUDA(cub::DeviceScan::ExclusiveSum(ws.cub_temp.p, tb2, chunks, prefix, nl + 1, st));
+    count_launches(2);
+    // upper bound of the chunk count: Nf / 32 + one partial chunk per leaf
+    const int64_t max_chunks = Nf / 32 + nl;
     // one column: registers for one; otherwise columns in passes of kLeafCols.
     for (int dense = 1; dense >= 0; --dense) {
       auto kern = C == 1 ? (dense ? k_leaf<KF, T, 1, true> : k_leaf<KF, T, 1, false>)
                          : (dense ? k_leaf<KF, T, kLeafCols, true> : k_leaf<KF, T, kLeafCols, false>);
-      kern<<<(nl + kLeafWarps - 1) / kLeafWarps, 32 * kLeafWarps, dense ? dyn : 0, st>>>(
-          part, nl, nsel, ws.tstart.as<int>(), ws.sstart.as<int>(),
+      const int64_t warps = dense ? max_chunks : nl;
+      kern<<<(unsigned)((warps + kLeafWarps - 1) / kLeafWarps), 32 * kLeafWarps, dense ? dyn : 0,
+             st>>>(part, nl, nsel, prefix, ws.tstart.as<int>(), ws.sstart.as<int>(),
           ws.tperm.as<int>(), ws.tpos.as<double>(), ws.spos.as<double>(), ws.wsorted.as<double>(),
           (int)Nf, (int)Ns, C, ws.F.as<T>() + level_offset(L, perS), t->n, t->p.use_chebyshev,
           ops_view<T>(t).Tkz, t->p.L, L, kparam, out);
