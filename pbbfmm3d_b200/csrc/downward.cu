@@ -643,8 +643,9 @@ struct LeafLaunch {
     tb2 = ws.cub_temp.cap;
     PB_CUDA(cub::DeviceScan::ExclusiveSum(ws.cub_temp.p, tb2, chunks, prefix, nl + 1, st));
     count_launches(2);
-    // upper bound of the chunk count: Nf / 32 + one partial chunk per leaf
-    const int64_t max_chunks = Nf / 32 + nl;
+    // upper bound of the chunk count: Nf / 32 + one partial chunk per dense
+    // leaf (at most Nf / kLaneLeafMin of them)
+    const int64_t max_chunks = Nf / 32 + (nl < Nf / kLaneLeafMin ? nl : Nf / kLaneLeafMin) + 1;
     // one column: registers for one; otherwise columns in passes of kLeafCols.
     for (int dense = 1; dense >= 0; --dense) {
       auto kern = C == 1 ? (dense ? k_leaf<KF, T, 1, true> : k_leaf<KF, T, 1, false>)
