@@ -20,7 +20,11 @@
 // 8 rows 1024 bytes apart), filled with cp.async (zero-fill for absent
 // sources) in NST stages.  Every wait is bounded: on timeout the kernel sets
 // *err, waits (bounded) for its last MMAs, frees its TMEM and returns.
+#include <cuda.h>
+#include <cudaTypedefs.h>
+
 #include <cstdlib>
+#include <mutex>
 
 #include "fmm.cuh"
 
@@ -94,6 +98,25 @@ __device__ __forceinline__ bool mbar_wait(uint64_t* bar, int parity, const volat
 
 __device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// Arrive on `bar` and add `bytes` to the transaction count it waits for.
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)),
+               "r"(bytes)
+               : "memory");
+}
+
+// 2-D tiled TMA load (no multicast) into this CTA's shared memory, completing
+// `bytes` of the transaction count of `bar`; x (the innermost coordinate)
+// is a multiple of 32 floats (128 bytes).
+__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y,
+                                            uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, "
+      "%4}], [%2];\n" ::"r"(smem_u32(dst)),
+      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
+      : "memory");
 }
 
 // Arrive on `bar` once every cp.async issued so far by this thread has
@@ -192,9 +215,10 @@ __host__ __device__ constexpr bool tc_sum_in_tmem(int NP) { return NP <= 160; }
 //   Ph, Pl : proxy hi / lo, row (cell * C + col) of KP floats, zero padded
 //   pf     : output rows (cell * C + col) of rf floats
 // Warp roles:
-//   warps 0-3  producers: each warp fills its 32 rows of A and its share of
-//              B for every stage with cp.async and signals the stage's full
-//              barrier when its copies land (cp.async.mbarrier.arrive);
+//   warps 0-3  producers: each warp gathers its 32 rows of A with cp.async and
+//              signals the stage's full barrier when its copies land
+//              (cp.async.mbarrier.arrive); thread 0 also loads B (the
+//              operator tile, hi and lo) with two TMA copies;
 //   warp 4     allocates TMEM; one thread waits for full stages, issues the
 //              MMAs and commits them to the stage's empty barrier;
 //   warps 5-8  drain accumulators into the running sum (TMEM lane quadrant
@@ -203,13 +227,15 @@ __host__ __device__ constexpr bool tc_sum_in_tmem(int NP) { return NP <= 160; }
 // offsets, so every float32 accumulation chain inside the tensor pipe spans
 // at most `group` offsets.
 //   s_full[s]  : 128 producer arrivals, one per thread, when its copies land
+//   s_tfull[s] : the operator tile's TMA bytes (thread 0's expect_tx)
 //   s_empty[s] : MMAs reading stage s done (tcgen05.commit)
 //   s_accf[b]  : MMAs of accumulator b's group done (tcgen05.commit)
 //   s_acce[b]  : accumulator b drained (128 drainer arrivals)
 template <int NST>
 __global__ void __launch_bounds__(TC_THREADS, 1)
-    k_m2l_cheb_tc(int rf, int NP, int KP, const float* __restrict__ Eh,
-                  const float* __restrict__ El, const int* __restrict__ typed, TcTiles tt, int C,
+    k_m2l_cheb_tc(int rf, int NP, int KP, const __grid_constant__ CUtensorMap tm_eh,
+                  const __grid_constant__ CUtensorMap tm_el, int lvl,
+                  const int* __restrict__ typed, TcTiles tt, int C,
                   int lev, const int* __restrict__ sstart, int span, const int* __restrict__ offs,
                   const float* __restrict__ Ph, const float* __restrict__ Pl,
                   float* __restrict__ pf, int group, int* __restrict__ err) {
@@ -217,7 +243,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   const int bbytes = NP * 128;
   const int stage_bytes = tc_stage_bytes(NP);
   unsigned char* base = smraw + ((1024 - (smem_u32(smraw) & 1023)) & 1023);
-  __shared__ uint64_t s_full[NST], s_empty[NST], s_accf[2], s_acce[2];
+  __shared__ uint64_t s_full[NST], s_tfull[NST], s_empty[NST], s_accf[2], s_acce[2];
   __shared__ uint32_t s_tmem;
   __shared__ int s_cell[TC_M];     // target cell of each row, or -1
   __shared__ int s_xyz[TC_M];      // target coordinates, x << 20 | y << 10 | z
@@ -262,6 +288,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   if (tid == 0) {
     for (int i = 0; i < NST; ++i) {
       mbar_init(&s_full[i], TC_PRODUCERS);
+      mbar_init(&s_tfull[i], 1);
       mbar_init(&s_empty[i], 1);
     }
     for (int b = 0; b < 2; ++b) {
@@ -331,6 +358,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     };
     int cur_q = -1;
     long long cur_row = -1;  // this lane's own row: source row offset or -1
+    int tma_last[NST];       // thread 0: last iteration whose TMA went into each stage
+#pragma unroll
+    for (int i = 0; i < NST; ++i) tma_last[i] = -1;
     start_lookup(0);
     for (int j = 0; j < niter; ++j) {
       const int s = j % NST;
@@ -354,14 +384,23 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         cp_async16(st + soff0 + 2048 * i, Ph + off, ok ? 16 : 0);
         cp_async16(st + 16384 + soff0 + 2048 * i, Pl + off, ok ? 16 : 0);
       }
-      const int64_t eoff = (int64_t)s_off[q].w * NP * KP + kc * TC_KC + 4 * ch;
-      for (int i = 0, n = r0; n < NP; ++i, n += 16) {
-        cp_async16(st + 32768 + soff0 + 2048 * i, Eh + eoff + (int64_t)n * KP, 16);
-        cp_async16(st + 32768 + bbytes + soff0 + 2048 * i, El + eoff + (int64_t)n * KP, 16);
+      if (tid == 0) {
+        // the operator tile (NP rows x 32 floats, hi and lo) by TMA
+        const int y = (lvl * 316 + s_off[q].w) * NP;
+        mbar_arrive_expect_tx(&s_tfull[s], 2u * NP * 128u);
+        tma_load_2d(st + 32768, &tm_eh, kc * TC_KC, y, &s_tfull[s]);
+        tma_load_2d(st + 32768 + bbytes, &tm_el, kc * TC_KC, y, &s_tfull[s]);
+        tma_last[s] = j;
       }
       cp_async_arrive(&s_full[s]);
     }
     cp_async_wait_all();
+    // no TMA may still be writing when the CTA ends: wait (bounded) for the
+    // last load issued into each stage
+    if (tid == 0)
+      for (int s2 = 0; s2 < NST; ++s2)
+        if (tma_last[s2] >= 0 && !mbar_wait(&s_tfull[s2], (tma_last[s2] / NST) & 1, nullptr))
+          *s_abort = 1;
   } else if (warp == TC_MMA_WARP) {
     // ---------------------------------------------------------------- MMA issue
     if (lane == 0) {
@@ -377,7 +416,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
           *s_abort = 1;
           break;
         }
-        if (!mbar_wait(&s_full[s], (it / NST) & 1, s_abort)) {
+        if (!mbar_wait(&s_full[s], (it / NST) & 1, s_abort) ||
+            !mbar_wait(&s_tfull[s], (it / NST) & 1, s_abort)) {
           *s_abort = 1;
           break;
         }
@@ -476,6 +516,45 @@ __global__ void k_split_proxy(const int* __restrict__ cells, int64_t nrows, int 
   pl[row * KP + k] = to_tf32(v - h);
 }
 
+// cuTensorMapEncodeTiled through the runtime's driver entry point (the
+// library links no driver library).
+static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
+  static std::once_flag once;
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  std::call_once(once, [] {
+    void* p = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(p);
+  });
+  return fn;
+}
+
+// Tensor map over an operator half (rows of KP floats, nrows rows): boxes of
+// 32 x NP floats, 128-byte swizzle (the layout the MMA descriptors read).
+static int operator_tensor_map(CUtensorMap* m, const float* base, int NP, int KP, int64_t nrows) {
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
+  if (!enc) {
+    set_error("cuTensorMapEncodeTiled is not available from the driver");
+    return PBBFMM_ERR_CUDA;
+  }
+  const cuuint64_t dims[2] = {(cuuint64_t)KP, (cuuint64_t)nrows};
+  const cuuint64_t strides[1] = {(cuuint64_t)KP * sizeof(float)};
+  const cuuint32_t box[2] = {(cuuint32_t)TC_KC, (cuuint32_t)NP};
+  const cuuint32_t estr[2] = {1, 1};
+  const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims,
+                         strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                         CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                         CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  if (r != CUDA_SUCCESS) {
+    set_error("cuTensorMapEncodeTiled failed for the tensor-core operator tiles");
+    return PBBFMM_ERR_CUDA;
+  }
+  return PBBFMM_OK;
+}
+
 // Offsets per TMEM accumulation chain (PBBFMM_TC_GROUP overrides the
 // default): one offset when the running sum stays in TMEM (drains then cost
 // nothing measurable), four when drains add into pf in global memory.
@@ -528,21 +607,22 @@ int run_m2l_cheb_tc_level(pbbfmm_tree* t, int C, int l, int lvl, const float* pr
   // three stages when they fit in shared memory next to the static arrays
   const int nst = tc_smem_bytes(NP, 3) + 8192 <= 232448 ? 3 : 2;
   const int smem = tc_smem_bytes(NP, nst);
-  const int64_t eop = (int64_t)316 * NP * KP;
+  CUtensorMap tm_h, tm_l;
+  const int64_t nrows = (int64_t)t->ops.nlev * 316 * NP;
+  if (int rc = operator_tensor_map(&tm_h, t->f_Eth, NP, KP, nrows)) return rc;
+  if (int rc = operator_tensor_map(&tm_l, t->f_Etl, NP, KP, nrows)) return rc;
   if (int rc = kt_begin(t, KS_M2L, st)) return rc;
   if (nst == 3) {
     PB_CUDA(cudaFuncSetAttribute(k_m2l_cheb_tc<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  smem));
     k_m2l_cheb_tc<3><<<(unsigned)tiles, TC_THREADS, smem, st>>>(
-        rf, NP, KP, t->f_Eth + lvl * eop, t->f_Etl + lvl * eop, lists + t->lists.typ_off[l], tt,
-        C, l, ws.sstart.as<int>(), (int)cells_at(L - l), t->d_offs, ph, pl, pf, tc_group(NP),
+        rf, NP, KP, tm_h, tm_l, lvl, lists + t->lists.typ_off[l], tt, C, l, ws.sstart.as<int>(), (int)cells_at(L - l), t->d_offs, ph, pl, pf, tc_group(NP),
         t->d_tc_err);
   } else {
     PB_CUDA(cudaFuncSetAttribute(k_m2l_cheb_tc<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  smem));
     k_m2l_cheb_tc<2><<<(unsigned)tiles, TC_THREADS, smem, st>>>(
-        rf, NP, KP, t->f_Eth + lvl * eop, t->f_Etl + lvl * eop, lists + t->lists.typ_off[l], tt,
-        C, l, ws.sstart.as<int>(), (int)cells_at(L - l), t->d_offs, ph, pl, pf, tc_group(NP),
+        rf, NP, KP, tm_h, tm_l, lvl, lists + t->lists.typ_off[l], tt, C, l, ws.sstart.as<int>(), (int)cells_at(L - l), t->d_offs, ph, pl, pf, tc_group(NP),
         t->d_tc_err);
   }
   PB_LAUNCH("m2l_cheb_tc");
