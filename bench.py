@@ -396,9 +396,10 @@ def unif_roofline(fmm, tree, wl, results, steps, local_rank):
 
 
 def cheb_roofline(fmm, tree, wl, results, steps, local_rank):
-    """Chebyshev M2L on the tensor cores (k_m2l_cheb_tc, 3xTF32): useful work
-    2 rf rs flops per (M2L pair, column); the tensor pipe issues three TF32
-    products per useful one, over padded tiles."""
+    """Chebyshev M2L on the tensor cores (k_m2l_cheb_tc): useful work 2 rf rs
+    flops per (M2L pair, column); the tensor pipe issues three products (hi /
+    lo splits) per useful one, over padded tiles.  Peak: the dense F16 rate
+    (= the bf16 figure) for F16 operands, half of it for TF32."""
     kt = results["mixed"]["ktimes"]
     tstart = tree.debug_copy(2).astype(np.int64)
     pairs = interaction_pairs(tstart, wl["L"])
@@ -406,20 +407,25 @@ def cheb_roofline(fmm, tree, wl, results, steps, local_rank):
     rf, rs, C = ops["rf"], ops["rs"], wl["C"]
     flops = sum(pairs.values()) * rf * rs * C * 2.0
     peaks, peak_kind = load_peaks()
-    tf32_peak = peaks["bf16_tflops"] / 2.0
+    fmt = tree.tensor_core_format()
+    tc_peak = peaks["bf16_tflops"] / (2.0 if fmt == "tf32" else 1.0)
     ms = kt["m2l"][0] / steps
     ms64 = results["fp64"]["ktimes"]["m2l"][0] / steps
     achieved = flops / (ms * 1e-3) / 1e12
     fp64_peak = fmm.measure_fma_peak(local_rank, fmm.PREC_FP64)
-    on_tc = tree.tensor_core_m2l()
+    on_tc = fmt is not None
+    kernels = {"f16": "k_m2l_cheb_tc (tcgen05 kind::f16, power-of-two scaled F16 hi/lo split, "
+                      "3 products, TMEM accumulators)",
+               "tf32": "k_m2l_cheb_tc (tcgen05 kind::tf32, 3xTF32 split, TMEM accumulators)"}
     return {
-        "kernel": "k_m2l_cheb_tc (tcgen05 kind::tf32, 3xTF32 split, TMEM accumulators)"
-                  if on_tc else "k_m2l_cheb<float> (CUDA cores)",
-        "bound": "tensor" if on_tc else "fp32", "achieved": achieved, "peak": tf32_peak,
-        "unit": "TFLOP/s", "frac": achieved / tf32_peak, "traffic": None,
-        "peak_source": "dense TF32 = half the %s bf16 tensor figure of MEASURED_PEAKS.json "
-                       "(%.0f TFLOP/s)" % (peak_kind, peaks["bf16_tflops"]),
-        "tensor_pipe_issued_frac": 3.0 * achieved / tf32_peak,
+        "kernel": kernels[fmt] if on_tc else "k_m2l_cheb<float> (CUDA cores)",
+        "bound": "tensor" if on_tc else "fp32", "achieved": achieved, "peak": tc_peak,
+        "unit": "TFLOP/s", "frac": achieved / tc_peak, "traffic": None,
+        "peak_source": ("dense F16 = the %s bf16 tensor figure of MEASURED_PEAKS.json (%.0f "
+                        "TFLOP/s)" if fmt != "tf32" else
+                        "dense TF32 = half the %s bf16 tensor figure of MEASURED_PEAKS.json "
+                        "(%.0f TFLOP/s)") % (peak_kind, peaks["bf16_tflops"]),
+        "tensor_pipe_issued_frac": 3.0 * achieved / tc_peak,
         "algorithmic": "%.4g useful flops per step = %d M2L pairs x rf %d x rs %d x %d cols x 2"
                        % (flops, sum(pairs.values()), rf, rs, C),
         "launches_per_step": kt["m2l"][1] / steps,
@@ -500,7 +506,11 @@ def run_workload(wl, args, rank, world, local_rank, e2e_wanted):
                    "epsilon": wl["eps"], "kernel": kernel_text(wl), "points": wl["dist"],
                    "precision": "mixed: float32 interpolation and near field with compensated "
                                 "sums, %s, float64 positions, operators and output" % (
-                                    "3xTF32 tensor-core M2L" if wl["cheb"] else "float32 FFT M2L"),
+                                    {"f16": "tensor-core M2L with scaled F16 hi/lo operands "
+                                             "(3 products, float32 accumulation)",
+                                     "tf32": "3xTF32 tensor-core M2L"}.get(
+                                        tree.tensor_core_format(), "float32 CUDA-core M2L")
+                                    if wl["cheb"] else "float32 FFT M2L"),
                    "l2": "256 MB buffer written between timed steps",
                    "parallelism": "independent column blocks per rank" if world > 1 else "1 GPU"},
     }

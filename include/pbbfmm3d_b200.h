@@ -138,14 +138,23 @@ int pbbfmm_compute_adjoint_device(pbbfmm_tree *tree, const double *d_target, int
 /* Precision used by pbbfmm_compute (default PBBFMM_PREC_FP64). */
 int pbbfmm_set_precision(pbbfmm_tree *tree, int precision);
 
-/* Chebyshev M2L of the mixed path on the tensor cores (tcgen05, 3xTF32 with
- * float32 accumulation; default on).  enable = 0 selects the CUDA-core float32
- * kernel instead.  No reference counterpart: the reference has one CPU path.
- * pbbfmm_tensor_core_m2l returns 1 when a mixed Chebyshev compute of this tree
- * runs on the tensor cores (enabled, operators loaded, r_f <= 256).
+/* Chebyshev M2L of the mixed path on the tensor cores (tcgen05, split
+ * precision hi + lo with three products and float32 accumulation; default on).
+ * mode: PBBFMM_TC_F16 (default): F16 hi / lo parts of power-of-two scaled
+ *       proxies and operators (kind::f16);
+ *       PBBFMM_TC_TF32: TF32 hi / lo parts (kind::tf32, "3xTF32");
+ *       PBBFMM_TC_OFF: the CUDA-core float32 kernel instead.
+ * (1 still means "on"; it is PBBFMM_TC_F16.)  No reference counterpart: the
+ * reference has one CPU path.  pbbfmm_tensor_core_m2l returns the format a
+ * mixed Chebyshev compute of this tree runs with (PBBFMM_TC_F16 or
+ * PBBFMM_TC_TF32), or PBBFMM_TC_OFF when it runs on the CUDA cores (disabled,
+ * operators not loaded, or r_f > 256).
  * If a tensor-core wait ever times out (about 1 s), that compute's output is
  * invalid and the next compute entry returns PBBFMM_ERR_TIMEOUT once. */
-int pbbfmm_set_tensor_cores(pbbfmm_tree *tree, int enable);
+#define PBBFMM_TC_OFF 0
+#define PBBFMM_TC_F16 1
+#define PBBFMM_TC_TF32 2
+int pbbfmm_set_tensor_cores(pbbfmm_tree *tree, int mode);
 int pbbfmm_tensor_core_m2l(const pbbfmm_tree *tree);
 
 /* Per-phase device times (ms) of the last compute, when timing is enabled

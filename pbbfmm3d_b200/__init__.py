@@ -45,6 +45,8 @@ def _dp(a: np.ndarray):
     return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
 
 
+_TC_FORMATS = {"f16": _lib.TC_F16, "tf32": _lib.TC_TF32}
+
 class H2_3D_Tree:
     """FMM tree: box, levels, interpolation order and kernel (H2_3D_Tree,
     include/H2_3D_Tree.hpp:16-116).  Subclasses fix the kernel like the
@@ -132,14 +134,24 @@ class H2_3D_Tree:
         _lib.check(_lib.lib().pbbfmm_set_precision(self._h, int(precision)))
         self.precision = int(precision)
 
-    def set_tensor_cores(self, enable: bool = True) -> None:
-        """Chebyshev M2L of the mixed path on tcgen05 (3xTF32) or, with
-        enable=False, on the CUDA cores in float32."""
-        _lib.check(_lib.lib().pbbfmm_set_tensor_cores(self._h, int(bool(enable))))
+    def set_tensor_cores(self, enable: bool = True, fmt: str = "f16") -> None:
+        """Chebyshev M2L of the mixed path on tcgen05 or, with enable=False,
+        on the CUDA cores in float32.  fmt: "f16" (power-of-two scaled F16
+        hi / lo operands, the default) or "tf32" (3xTF32)."""
+        if fmt not in _TC_FORMATS:
+            raise ValueError("fmt must be 'f16' or 'tf32'")
+        mode = _TC_FORMATS[fmt] if enable else _lib.TC_OFF
+        _lib.check(_lib.lib().pbbfmm_set_tensor_cores(self._h, mode))
 
     def tensor_core_m2l(self) -> bool:
         """True when a mixed Chebyshev compute of this tree runs its M2L on tcgen05."""
         return bool(_lib.lib().pbbfmm_tensor_core_m2l(self._h))
+
+    def tensor_core_format(self):
+        """"f16" or "tf32": the operand format of the tensor-core M2L a mixed
+        Chebyshev compute of this tree runs with; None on the CUDA cores."""
+        m = _lib.lib().pbbfmm_tensor_core_m2l(self._h)
+        return {v: k for k, v in _TC_FORMATS.items()}.get(m)
 
     def set_timing(self, enable: bool = True) -> None:
         _lib.check(_lib.lib().pbbfmm_set_timing(self._h, 1 if enable else 0))

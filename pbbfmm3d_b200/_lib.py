@@ -15,6 +15,7 @@ LIB_PATH = os.path.join(HERE, "libpbbfmm3d_b200.so")
 # status codes
 OK, ERR_ARG, ERR_CUDA, ERR_ALLOC, ERR_STATE, ERR_IO, ERR_UNSUPPORTED, ERR_NUMERIC, ERR_TIMEOUT = range(9)
 PREC_FP64, PREC_MIXED = 0, 1
+TC_OFF, TC_F16, TC_TF32 = 0, 1, 2
 
 
 class FMMError(RuntimeError):

@@ -4,6 +4,9 @@
 // Phase order follows H2_3D_Compute (include/compute.hpp:140-222):
 // distribute (binning) -> upward (P2M, M2M) -> far field (M2L with its pre-
 // and post-transforms) -> downward (L2L) -> near field (L2P, P2P, scatter).
+#include <cuda_fp16.h>
+
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -111,46 +114,83 @@ static float tf32_round(float x) {
   return r;
 }
 
-// Operands of the tensor-core Chebyshev M2L: for each level and operator o,
-// E_o^T as NP rows of KP floats (row f holds E_o[f][s], s < rs), split into
-// TF32 hi = tf32(x) and lo = tf32(x - hi), zero padded.  K: nlev x 316
-// column-major rf x rs blocks.  Leaves eth / etl null when NP exceeds the
-// tensor-core limit (the float path then uses the CUDA-core kernel).
-static int upload_tc_split(const double* K, int nlev, int rf, int rs, float** eth, float** etl,
-                           int* np, int* kp) {
-  const int NP = (rf + 15) / 16 * 16, KP = (rs + 31) / 32 * 32;
-  if (*eth) cudaFree(*eth);
-  if (*etl) cudaFree(*etl);
-  *eth = *etl = nullptr;
-  *np = NP;
-  *kp = KP;
+static void free_tc_ops(TcOps* o) {
+  void* b[] = {o->eth, o->etl, o->eh16, o->el16, o->eexp};
+  for (void* p : b)
+    if (p) cudaFree(p);
+  *o = TcOps{};
+}
+
+template <typename V>
+static int upload_vec(V** dst, const std::vector<V>& h) {
+  PB_CUDA(cudaMalloc(dst, h.size() * sizeof(V)));
+  PB_CUDA(cudaMemcpy(*dst, h.data(), h.size() * sizeof(V), cudaMemcpyHostToDevice));
+  return PBBFMM_OK;
+}
+
+// Operands of the tensor-core Chebyshev M2L (both formats, see TcOps): for
+// each level and operator o, E_o^T as NP rows (row f holds E_o[f][s], s < rs),
+// zero padded,
+//   TF32: hi = tf32(x), lo = tf32(x - hi) of x = float(E);
+//   F16 : x = float(E) 2^e with e such that max |x| lies in [2^14, 2^15)
+//         (e = 0 for a zero operator), hi = fp16(x), lo = fp16(x - hi).
+// K: nlev x 316 column-major rf x rs blocks.  Leaves everything null when NP
+// exceeds the tensor-core limit (the float path then uses the CUDA-core
+// kernel).
+static int upload_tc_split(const double* K, int nlev, int rf, int rs, TcOps* o) {
+  free_tc_ops(o);
+  const int NP = (rf + 15) / 16 * 16, KP = (rs + 31) / 32 * 32, KP16 = (rs + 63) / 64 * 64;
+  o->np = NP;
+  o->kp = KP;
+  o->kp16 = KP16;
   if (NP > kTcMaxN) return PBBFMM_OK;
-  const size_t per = (size_t)316 * NP * KP, total = per * nlev;
+  const size_t total = (size_t)nlev * 316 * NP * KP, total16 = (size_t)nlev * 316 * NP * KP16;
   std::vector<float> hi(total, 0.f), lo(total, 0.f);
+  std::vector<uint16_t> hi16(total16, 0), lo16(total16, 0);
+  std::vector<int> ex((size_t)nlev * 316, 0);
   parallel_for((int64_t)nlev * 316, [&](int64_t b0, int64_t b1) {
     for (int64_t b = b0; b < b1; ++b) {
       const double* E = K + (size_t)b * rf * rs;
       float* h = hi.data() + (size_t)b * NP * KP;
       float* l = lo.data() + (size_t)b * NP * KP;
+      float m = 0.f;
       for (int f = 0; f < rf; ++f)
         for (int s = 0; s < rs; ++s) {
           const float x = (float)E[f + (size_t)rf * s];
           const float xh = tf32_round(x);
           h[(size_t)f * KP + s] = xh;
           l[(size_t)f * KP + s] = tf32_round(x - xh);
+          m = std::max(m, std::fabs(x));
+        }
+      int e = 0;
+      if (m > 0.f) {
+        int k2;
+        std::frexp(m, &k2);
+        e = 15 - k2;
+      }
+      ex[b] = e;
+      uint16_t* h16 = hi16.data() + (size_t)b * NP * KP16;
+      uint16_t* l16 = lo16.data() + (size_t)b * NP * KP16;
+      for (int f = 0; f < rf; ++f)
+        for (int s = 0; s < rs; ++s) {
+          const float x = std::ldexp((float)E[f + (size_t)rf * s], e);
+          const __half xh = __float2half_rn(x);
+          const __half xl = __float2half_rn(x - __half2float(xh));
+          memcpy(&h16[(size_t)f * KP16 + s], &xh, 2);
+          memcpy(&l16[(size_t)f * KP16 + s], &xl, 2);
         }
     }
   });
-  PB_CUDA(cudaMalloc(eth, total * sizeof(float)));
-  PB_CUDA(cudaMalloc(etl, total * sizeof(float)));
-  PB_CUDA(cudaMemcpy(*eth, hi.data(), total * sizeof(float), cudaMemcpyHostToDevice));
-  PB_CUDA(cudaMemcpy(*etl, lo.data(), total * sizeof(float), cudaMemcpyHostToDevice));
+  int rc;
+  if ((rc = upload_vec(&o->eth, hi)) || (rc = upload_vec(&o->etl, lo)) ||
+      (rc = upload_vec(&o->eh16, hi16)) || (rc = upload_vec(&o->el16, lo16)) ||
+      (rc = upload_vec(&o->eexp, ex)))
+    return rc;
   return PBBFMM_OK;
 }
 
 static int upload_tc_operators(pbbfmm_tree* t) {
-  if (int rc = upload_tc_split(t->ops.K.data(), t->ops.nlev, t->ops.rf, t->ops.rs, &t->f_Eth,
-                               &t->f_Etl, &t->tc_np, &t->tc_kp))
+  if (int rc = upload_tc_split(t->ops.K.data(), t->ops.nlev, t->ops.rf, t->ops.rs, &t->tc))
     return rc;
   if (!t->h_tc_err) {
     PB_CUDA(cudaHostAlloc(&t->h_tc_err, sizeof(int), cudaHostAllocMapped));
@@ -261,11 +301,12 @@ static void free_adjoint_ops(pbbfmm_tree* t) {
     if (*b) cudaFree(*b);
     *b = nullptr;
   }
-  float** f[] = {&t->adj.fE, &t->adj.fU, &t->adj.fVT, &t->adj.fEth, &t->adj.fEtl};
+  float** f[] = {&t->adj.fE, &t->adj.fU, &t->adj.fVT};
   for (float** b : f) {
     if (*b) cudaFree(*b);
     *b = nullptr;
   }
+  free_tc_ops(&t->adj.tc);
   t->adj_ready = false;
 }
 
@@ -312,9 +353,7 @@ static int build_adjoint_ops(pbbfmm_tree* t) {
   if ((rc = upload_f32(&t->adj.fE, E.data(), E.size()))) return rc;
   if ((rc = upload_f32(&t->adj.fU, U.data(), U.size()))) return rc;
   if ((rc = upload_f32(&t->adj.fVT, VT.data(), VT.size()))) return rc;
-  if ((rc = upload_tc_split(E.data(), nlev, rs, rf, &t->adj.fEth, &t->adj.fEtl, &t->adj.np,
-                            &t->adj.kp)))
-    return rc;
+  if ((rc = upload_tc_split(E.data(), nlev, rs, rf, &t->adj.tc))) return rc;
   t->adj.rf = rs;
   t->adj.rs = rf;
   t->adj_ready = true;
@@ -329,12 +368,9 @@ static void swap_adjoint_ops(pbbfmm_tree* t) {
   std::swap(t->f_E, t->adj.fE);
   std::swap(t->f_U, t->adj.fU);
   std::swap(t->f_VT, t->adj.fVT);
-  std::swap(t->f_Eth, t->adj.fEth);
-  std::swap(t->f_Etl, t->adj.fEtl);
+  std::swap(t->tc, t->adj.tc);
   std::swap(t->ops.rf, t->adj.rf);
   std::swap(t->ops.rs, t->adj.rs);
-  std::swap(t->tc_np, t->adj.np);
-  std::swap(t->tc_kp, t->adj.kp);
 }
 
 static int upload_operators(pbbfmm_tree* t) {
@@ -377,9 +413,7 @@ static void free_tree_device(pbbfmm_tree* t) {
   }
   if (t->d_offs) cudaFree(t->d_offs);
   t->d_offs = nullptr;
-  if (t->f_Eth) cudaFree(t->f_Eth);
-  if (t->f_Etl) cudaFree(t->f_Etl);
-  t->f_Eth = t->f_Etl = nullptr;
+  free_tc_ops(&t->tc);
   if (t->h_tc_err) cudaFreeHost(t->h_tc_err);
   t->h_tc_err = t->d_tc_err = nullptr;
   free_adjoint_ops(t);
@@ -1027,16 +1061,23 @@ int pbbfmm_compute(pbbfmm_tree* t, const double* target, int64_t Nf, const doubl
   return take_tc_timeout(t);
 }
 
-int pbbfmm_set_tensor_cores(pbbfmm_tree* t, int enable) {
+int pbbfmm_set_tensor_cores(pbbfmm_tree* t, int mode) {
   if (!t) {
     set_error("null tree");
     return PBBFMM_ERR_ARG;
   }
-  t->use_tc = enable != 0;
+  if (mode != PBBFMM_TC_OFF && mode != PBBFMM_TC_F16 && mode != PBBFMM_TC_TF32) {
+    set_error("tensor-core mode must be PBBFMM_TC_OFF, PBBFMM_TC_F16 or PBBFMM_TC_TF32");
+    return PBBFMM_ERR_ARG;
+  }
+  t->use_tc = mode != PBBFMM_TC_OFF;
+  if (mode != PBBFMM_TC_OFF) t->tc_fmt = mode;
   return PBBFMM_OK;
 }
 
-int pbbfmm_tensor_core_m2l(const pbbfmm_tree* t) { return t && tc_eligible(t) ? 1 : 0; }
+int pbbfmm_tensor_core_m2l(const pbbfmm_tree* t) {
+  return t && tc_eligible(t) ? t->tc_fmt : PBBFMM_TC_OFF;
+}
 
 int pbbfmm_debug_copy(pbbfmm_tree* t, int what, int level, double* host, int64_t count,
                       int64_t* written) {

@@ -66,6 +66,21 @@ struct LevelLists {
   int ntyp[kMaxLevel + 1][9];       // type boundaries within the typed list
 };
 
+// Operands of the tensor-core Chebyshev M2L: for each level and operator o,
+// E_o^T as np rows (rf padded to 16), split hi / lo, zero padded:
+//   TF32: rows of kp floats (rs padded to 32);
+//   F16 : rows of kp16 halves (rs padded to 64), each operator scaled by
+//         2^eexp[lvl * 316 + o].
+// Null when np exceeds the tensor-core limit.
+struct TcOps {
+  float* eth = nullptr;
+  float* etl = nullptr;
+  uint16_t* eh16 = nullptr;
+  uint16_t* el16 = nullptr;
+  int* eexp = nullptr;
+  int np = 0, kp = 0, kp16 = 0;
+};
+
 }  // namespace pbbfmm
 
 struct pbbfmm_tree {
@@ -100,12 +115,11 @@ struct pbbfmm_tree {
   float* f_VT = nullptr;
   float* f_op = nullptr;  // nlev x nk x 343 complex (float2)
   float* f_twid = nullptr;
-  // tensor-core Chebyshev M2L (mixed path): hi / lo TF32 parts of E_o^T,
-  // nlev x 316 x tc_np x tc_kp (rf padded to 16, rs padded to 32)
+  // tensor-core Chebyshev M2L (mixed path); tc_fmt: PBBFMM_TC_F16 (scaled
+  // F16 operands, default) or PBBFMM_TC_TF32
   bool use_tc = true;
-  int tc_np = 0, tc_kp = 0;
-  float* f_Eth = nullptr;
-  float* f_Etl = nullptr;
+  int tc_fmt = PBBFMM_TC_F16;
+  pbbfmm::TcOps tc;
   int* h_tc_err = nullptr;  // mapped pinned flag: a tensor-core wait timed out
   int* d_tc_err = nullptr;  // its device address
   // Adjoint (transposed) Chebyshev operators: U' = VT^T, E'_p = E_{-p}^T,
@@ -113,8 +127,9 @@ struct pbbfmm_tree {
   // (swap_adjoint_ops) for the duration of an adjoint pass.
   struct OpSet {
     double *E = nullptr, *U = nullptr, *VT = nullptr;
-    float *fE = nullptr, *fU = nullptr, *fVT = nullptr, *fEth = nullptr, *fEtl = nullptr;
-    int rf = 0, rs = 0, np = 0, kp = 0;
+    float *fE = nullptr, *fU = nullptr, *fVT = nullptr;
+    pbbfmm::TcOps tc;
+    int rf = 0, rs = 0;
   } adj;
   bool adj_ready = false;
   // pass settings (set by the adjoint / gradient entry points, cleared after)

@@ -1,12 +1,21 @@
 // Chebyshev M2L of the mixed-precision path on the 5th-generation tensor
-// cores (tcgen05 with TMEM accumulators), split precision 3xTF32:
+// cores (tcgen05 with TMEM accumulators), in split precision:
 //     D += A_lo B_hi + A_hi B_lo + A_hi B_hi,
-// with x = hi + lo, hi = tf32(x), lo = tf32(x - hi), accumulated in float32.
-// The dropped A_lo B_lo term and the splitting leave a relative error near
-// 2^-21 per product, against 2^-11 for a single TF32 product.  The float32
-// accumulation inside the tensor pipe loses about one unit in the last place
-// per accumulation step, so accumulators are drained into pf every few
-// offsets (see `group`), which keeps the result within ~1e-6 of float64.
+// with x = hi + lo, accumulated in float32.  Two operand formats:
+//   F16  (default): x scaled by a power of two 2^e (one e per proxy row and
+//        one per operator, so that the largest magnitude lies in
+//        [2^14, 2^15)), hi = fp16(x 2^e), lo = fp16(x 2^e - hi);
+//        kind::f16, K = 16 per instruction.  Elements down to 2^-17 of their
+//        row's largest keep 22 significant bits; smaller ones an absolute
+//        error below 2^-39 of it.  Each offset's accumulator is unscaled by
+//        2^-(e_row + e_op) (exact) when it is drained.
+//   TF32: hi = tf32(x), lo = tf32(x - hi); kind::tf32, K = 8 per instruction.
+// Either way the dropped A_lo B_lo term and the splitting leave a relative
+// error near 2^-21 per product.  F16 moves half the bytes and issues half the
+// instructions per useful product.  The float32 accumulation inside the
+// tensor pipe loses about one unit in the last place per accumulation step,
+// so accumulators are drained into a running sum every few offsets (every
+// offset for F16, see `group`), which keeps the result within ~1e-6 of float64.
 //
 // Same product as k_m2l_cheb (reference: FarFieldInteractions / Moment2Local,
 // include/compute.hpp:402-508 and 881-914): for a tile of targets of one
@@ -16,12 +25,13 @@
 //   M = 128 rows (target, col) of one child type,  N = rf padded to 16,
 //   K = (offsets with a source in the tile) x (rs padded to 32).
 //
-// Operands are K-major, 128-byte-swizzled tiles (rows of 32 floats, groups of
-// 8 rows 1024 bytes apart), filled with cp.async (zero-fill for absent
-// sources) in NST stages.  Every wait is bounded: on timeout the kernel sets
+// Operands are K-major, 128-byte-swizzled tiles (rows of 128 bytes: 32 TF32 or
+// 64 F16 values; groups of 8 rows 1024 bytes apart), A filled with cp.async
+// (zero-fill for absent sources) and B by TMA, in NST stages.  Every wait is bounded: on timeout the kernel sets
 // *err, waits (bounded) for its last MMAs, frees its TMEM and returns.
 #include <cuda.h>
 #include <cudaTypedefs.h>
+#include <cuda_fp16.h>
 
 #include <cstdlib>
 #include <mutex>
@@ -31,7 +41,7 @@
 namespace pbbfmm {
 
 constexpr int TC_M = 128;
-constexpr int TC_KC = 32;          // K per stage: one 128-byte swizzle row of float32
+constexpr int TC_ROWB = 128;       // bytes of K per stage: one 128-byte swizzle row
 constexpr int TC_PRODUCERS = 128;  // warps 0-3: operand loads
 constexpr int TC_MMA_WARP = 4;     // warp 4: TMEM allocation, MMA issue (one thread)
 constexpr int TC_THREADS = 288;    // + warps 5-8: accumulator drains
@@ -58,6 +68,10 @@ __device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
 __host__ __device__ constexpr uint32_t tf32_idesc(int M, int N) {
   return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) |
          ((uint32_t)(M >> 4) << 24);
+}
+// kind::f16 with A and B F16 (format 0 in bits 7-9, 10-12), D float32.
+__host__ __device__ constexpr uint32_t f16_idesc(int M, int N) {
+  return (1u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
 // Byte offset of (row r, 16-byte chunk j) in a K-major SWIZZLE_128B tile.
@@ -144,6 +158,14 @@ __device__ __forceinline__ void tc_mma_tf32(uint32_t d_tmem, uint64_t a, uint64_
       "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
       : "memory");
 }
+__device__ __forceinline__ void tc_mma_f16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc,
+                                           uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
+      "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
 
 // Arrive on `bar` once every tcgen05.mma issued so far by this thread is done.
 __device__ __forceinline__ void tc_commit(uint64_t* bar) {
@@ -211,8 +233,12 @@ __host__ __device__ constexpr int tc_acc_stride(int NP) { return NP <= 160 ? (NP
 __host__ __device__ constexpr bool tc_sum_in_tmem(int NP) { return NP <= 160; }
 
 // One CTA per tile of 128 (target, col) rows of one child type; NST stages.
-//   Eh, El : [316][NP][KP] hi / lo of E_o^T (row f holds E_o[f][s] over s), zero padded
-//   Ph, Pl : proxy hi / lo, row (cell * C + col) of KP floats, zero padded
+//   tm_eh, tm_el : [nlev][316][NP] rows of hi / lo of E_o^T (row f holds
+//                  E_o[f][s] over s), zero padded to rowb bytes
+//   Ph, Pl : proxy hi / lo, row (cell * C + col) of rowb bytes, zero padded
+//   pexp   : F16 only: the scale exponent of each proxy row (any value for
+//            rows of empty cells: their A rows are zero-filled)
+//   eexp   : F16 only: the scale exponent of each operator of this level
 //   pf     : output rows (cell * C + col) of rf floats
 // Warp roles:
 //   warps 0-3  producers: each warp gathers its 32 rows of A with cp.async and
@@ -231,13 +257,14 @@ __host__ __device__ constexpr bool tc_sum_in_tmem(int NP) { return NP <= 160; }
 //   s_empty[s] : MMAs reading stage s done (tcgen05.commit)
 //   s_accf[b]  : MMAs of accumulator b's group done (tcgen05.commit)
 //   s_acce[b]  : accumulator b drained (128 drainer arrivals)
-template <int NST>
+template <int NST, bool F16>
 __global__ void __launch_bounds__(TC_THREADS, 1)
-    k_m2l_cheb_tc(int rf, int NP, int KP, const __grid_constant__ CUtensorMap tm_eh,
+    k_m2l_cheb_tc(int rf, int NP, int rowb, const __grid_constant__ CUtensorMap tm_eh,
                   const __grid_constant__ CUtensorMap tm_el, int lvl,
                   const int* __restrict__ typed, TcTiles tt, int C,
                   int lev, const int* __restrict__ sstart, int span, const int* __restrict__ offs,
-                  const float* __restrict__ Ph, const float* __restrict__ Pl,
+                  const unsigned char* __restrict__ Ph, const unsigned char* __restrict__ Pl,
+                  const int* __restrict__ pexp, const int* __restrict__ eexp,
                   float* __restrict__ pf, int group, int* __restrict__ err) {
   extern __shared__ unsigned char smraw[];
   const int bbytes = NP * 128;
@@ -324,7 +351,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   tc_fence_after();
   const uint32_t tmem = s_tmem;
   const int nvalid = s_nvalid;
-  const int kchunks = KP / TC_KC;
+  const int kchunks = rowb / TC_ROWB;
   const int niter = nvalid * kchunks;
   const int group_iters = max(group, 1) * kchunks;
   const int ngroups = (niter + group_iters - 1) / group_iters;
@@ -371,7 +398,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       const int q = j / kchunks, kc = j - q * kchunks;
       if (q != cur_q) {
         if (pre_q != q) start_lookup(q);
-        cur_row = (pre_in && pre_b > pre_a) ? ((long long)pre_bm * C + ocol) * KP : -1;
+        cur_row = (pre_in && pre_b > pre_a) ? ((long long)pre_bm * C + ocol) * rowb : -1;
         cur_q = q;
         start_lookup(q + 1);
       }
@@ -380,16 +407,18 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       for (int i = 0; i < 8; ++i) {
         const long long rr = __shfl_sync(0xffffffffu, cur_row, (lane >> 3) | (i << 2));
         const bool ok = rr >= 0;
-        const int64_t off = ok ? rr + kc * TC_KC + 4 * ch : 0;
+        const int64_t off = ok ? rr + kc * TC_ROWB + 16 * ch : 0;
         cp_async16(st + soff0 + 2048 * i, Ph + off, ok ? 16 : 0);
         cp_async16(st + 16384 + soff0 + 2048 * i, Pl + off, ok ? 16 : 0);
       }
       if (tid == 0) {
-        // the operator tile (NP rows x 32 floats, hi and lo) by TMA
+        // the operator tile (NP rows x 128 bytes, hi and lo) by TMA; x in
+        // elements: 64 per 128 bytes for F16, 32 for TF32
         const int y = (lvl * 316 + s_off[q].w) * NP;
+        const int x = kc * (F16 ? 64 : 32);
         mbar_arrive_expect_tx(&s_tfull[s], 2u * NP * 128u);
-        tma_load_2d(st + 32768, &tm_eh, kc * TC_KC, y, &s_tfull[s]);
-        tma_load_2d(st + 32768 + bbytes, &tm_el, kc * TC_KC, y, &s_tfull[s]);
+        tma_load_2d(st + 32768, &tm_eh, x, y, &s_tfull[s]);
+        tma_load_2d(st + 32768 + bbytes, &tm_el, x, y, &s_tfull[s]);
         tma_last[s] = j;
       }
       cp_async_arrive(&s_full[s]);
@@ -404,7 +433,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   } else if (warp == TC_MMA_WARP) {
     // ---------------------------------------------------------------- MMA issue
     if (lane == 0) {
-      const uint32_t idesc = tf32_idesc(TC_M, NP);
+      const uint32_t idesc = F16 ? f16_idesc(TC_M, NP) : tf32_idesc(TC_M, NP);
       const int astride = tc_acc_stride(NP);
       int last = -1;  // last iteration whose MMAs were committed
       for (int it = 0; it < niter; ++it) {
@@ -426,13 +455,21 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         const uint32_t a_hi = smem_u32(base + s * stage_bytes), a_lo = a_hi + 16384;
         const uint32_t b_hi = a_hi + 32768, b_lo = b_hi + bbytes;
         const uint32_t d = tmem + (uint32_t)((g & 1) * astride);
+        // four K steps of 32 bytes (16 F16 or 8 TF32 values) per 128-byte row
 #pragma unroll
-        for (int k = 0; k < TC_KC / 8; ++k) {
+        for (int k = 0; k < 4; ++k) {
           const uint32_t off = k * 32;
-          tc_mma_tf32(d, sw128_desc(a_lo + off), sw128_desc(b_hi + off), idesc,
-                      (fresh && k == 0) ? 0u : 1u);
-          tc_mma_tf32(d, sw128_desc(a_hi + off), sw128_desc(b_lo + off), idesc, 1u);
-          tc_mma_tf32(d, sw128_desc(a_hi + off), sw128_desc(b_hi + off), idesc, 1u);
+          if constexpr (F16) {
+            tc_mma_f16(d, sw128_desc(a_lo + off), sw128_desc(b_hi + off), idesc,
+                       (fresh && k == 0) ? 0u : 1u);
+            tc_mma_f16(d, sw128_desc(a_hi + off), sw128_desc(b_lo + off), idesc, 1u);
+            tc_mma_f16(d, sw128_desc(a_hi + off), sw128_desc(b_hi + off), idesc, 1u);
+          } else {
+            tc_mma_tf32(d, sw128_desc(a_lo + off), sw128_desc(b_hi + off), idesc,
+                        (fresh && k == 0) ? 0u : 1u);
+            tc_mma_tf32(d, sw128_desc(a_hi + off), sw128_desc(b_lo + off), idesc, 1u);
+            tc_mma_tf32(d, sw128_desc(a_hi + off), sw128_desc(b_hi + off), idesc, 1u);
+          }
         }
         tc_commit(&s_empty[s]);
         if (it + 1 == niter || it + 1 == (g + 1) * group_iters) tc_commit(&s_accf[g & 1]);
@@ -452,8 +489,28 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     const int astride = tc_acc_stride(NP);
     const bool tsum = tc_sum_in_tmem(NP);
     const uint32_t sum_base = lane_base + (uint32_t)(2 * astride);
+    // F16 (one offset per group): the unscaling exponent of this row at offset
+    // q, e_op + e_row of its source, clamped so that 2^-e is a normal float
+    // (rows without a source are zero, and stay zero under any finite scale)
+    const int rcol = row % C;
+    const int rx = s_xyz[row] >> 20, ry = (s_xyz[row] >> 10) & 1023, rz = s_xyz[row] & 1023;
+    auto row_exp = [&](int q) -> int {
+      if (!F16 || q >= nvalid || cell < 0) return 0;
+      const int4 o = s_off[q];
+      const int x = rx + o.x, y = ry + o.y, z = rz + o.z;
+      int e = eexp[o.w];
+      if (x >= 0 && y >= 0 && z >= 0 && x < nside && y < nside && z < nside)
+        e += min(max(pexp[(int64_t)morton_encode(x, y, z) * C + rcol], -256), 256);
+      return min(max(e, -252), 252);
+    };
+    int e_next = row_exp(0);
     for (int g = 0; g < ngroups; ++g) {
       const int b = g & 1;
+      const int e_cur = e_next;
+      e_next = row_exp(g + 1);  // loaded while this group's MMAs run
+      // 2^-e_cur as two normal powers of two (|e_cur| <= 252)
+      const float sc1 = __int_as_float((127 - (e_cur >> 1)) << 23);
+      const float sc2 = __int_as_float((127 - (e_cur - (e_cur >> 1))) << 23);
       if (!mbar_wait(&s_accf[b], (g >> 1) & 1, s_abort)) {
         *s_abort = 1;
         break;
@@ -463,6 +520,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       float v[16], u[16];
       for (int n0 = 0; n0 < NP; n0 += 16) {
         tc_ld16(lane_base + (uint32_t)(b * astride + n0), v);
+        if constexpr (F16) {
+#pragma unroll
+          for (int i = 0; i < 16; ++i) v[i] = v[i] * sc1 * sc2;  // exact: powers of two
+        }
         if (tsum) {
           if (g > 0) {
             tc_ld16(sum_base + (uint32_t)n0, u);
@@ -501,7 +562,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 }
 
 // Split the proxies of the listed source cells into TF32 hi / lo rows of KP
-// floats (zero padded from rs): thread per (row, k).
+// floats (zero padded from rs): thread per (row, k).  (TF32 operands.)
 __global__ void k_split_proxy(const int* __restrict__ cells, int64_t nrows, int C, int rs, int KP,
                               const float* __restrict__ proxy, float* __restrict__ ph,
                               float* __restrict__ pl) {
@@ -514,6 +575,37 @@ __global__ void k_split_proxy(const int* __restrict__ cells, int64_t nrows, int 
   const float h = to_tf32(v);
   ph[row * KP + k] = h;
   pl[row * KP + k] = to_tf32(v - h);
+}
+
+// F16 operands: split the proxies of the listed source cells into scaled F16
+// hi / lo rows of KP values (zero padded from rs) and the row's exponent e,
+// chosen so that the row's largest |x| 2^e lies in [2^14, 2^15) (e = 0 for a
+// zero row): one warp per row.
+__global__ void k_split_proxy_f16(const int* __restrict__ cells, int64_t nrows, int C, int rs,
+                                  int KP, const float* __restrict__ proxy, __half* __restrict__ ph,
+                                  __half* __restrict__ pl, int* __restrict__ pexp) {
+  const int64_t r = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (r >= nrows) return;  // uniform over the warp
+  const int64_t row = (int64_t)cells[r / C] * C + r % C;
+  const float* x = proxy + row * rs;
+  float m = 0.f;
+  for (int k = lane; k < rs; k += 32) m = fmaxf(m, fabsf(x[k]));
+#pragma unroll
+  for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+  int e = 0;
+  if (m > 0.f) {
+    int k2;
+    frexpf(m, &k2);  // m in [2^(k2-1), 2^k2)
+    e = 15 - k2;
+  }
+  for (int k = lane; k < KP; k += 32) {
+    const float v = k < rs ? ldexpf(x[k], e) : 0.f;
+    const __half h = __float2half_rn(v);
+    ph[row * KP + k] = h;
+    pl[row * KP + k] = __float2half_rn(v - __half2float(h));
+  }
+  if (lane == 0) pexp[row] = e;
 }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (the
@@ -532,19 +624,23 @@ static PFN_cuTensorMapEncodeTiled_v12000 tensor_map_encoder() {
   return fn;
 }
 
-// Tensor map over an operator half (rows of KP floats, nrows rows): boxes of
-// 32 x NP floats, 128-byte swizzle (the layout the MMA descriptors read).
-static int operator_tensor_map(CUtensorMap* m, const float* base, int NP, int KP, int64_t nrows) {
+// Tensor map over an operator half (rows of KP values, nrows rows): boxes of
+// NP rows x 128 bytes (32 TF32 or 64 F16 values), 128-byte swizzle (the
+// layout the MMA descriptors read).
+static int operator_tensor_map(CUtensorMap* m, const void* base, bool f16, int NP, int KP,
+                               int64_t nrows) {
   PFN_cuTensorMapEncodeTiled_v12000 enc = tensor_map_encoder();
   if (!enc) {
     set_error("cuTensorMapEncodeTiled is not available from the driver");
     return PBBFMM_ERR_CUDA;
   }
+  const int esize = f16 ? 2 : 4;
   const cuuint64_t dims[2] = {(cuuint64_t)KP, (cuuint64_t)nrows};
-  const cuuint64_t strides[1] = {(cuuint64_t)KP * sizeof(float)};
-  const cuuint32_t box[2] = {(cuuint32_t)TC_KC, (cuuint32_t)NP};
+  const cuuint64_t strides[1] = {(cuuint64_t)KP * esize};
+  const cuuint32_t box[2] = {(cuuint32_t)(TC_ROWB / esize), (cuuint32_t)NP};
   const cuuint32_t estr[2] = {1, 1};
-  const CUresult r = enc(m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(base), dims,
+  const CUresult r = enc(m, f16 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32,
+                         2, const_cast<void*>(base), dims,
                          strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                          CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                          CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -555,17 +651,34 @@ static int operator_tensor_map(CUtensorMap* m, const float* base, int NP, int KP
   return PBBFMM_OK;
 }
 
-// Offsets per TMEM accumulation chain (PBBFMM_TC_GROUP overrides the
+// Offsets per TMEM accumulation chain (PBBFMM_TC_GROUP overrides the TF32
 // default): one offset when the running sum stays in TMEM (drains then cost
-// nothing measurable), four when drains add into pf in global memory.
-static int tc_group(int NP) {
+// nothing measurable), four when drains add into pf in global memory.  F16
+// operands always drain every offset (each has its own scale).
+static int tc_group(int NP, bool f16) {
+  if (f16) return 1;
   const char* e = getenv("PBBFMM_TC_GROUP");
   const int g = e ? atoi(e) : (tc_sum_in_tmem(NP) ? 1 : 4);
   return g < 1 ? 1 : (g > 189 ? 189 : g);
 }
 
 bool tc_eligible(const pbbfmm_tree* t) {
-  return t->p.use_chebyshev && t->use_tc && t->f_Eth && t->tc_np > 0 && t->tc_np <= kTcMaxN;
+  return t->p.use_chebyshev && t->use_tc && t->tc.eth && t->tc.eh16 && t->tc.np > 0 &&
+         t->tc.np <= kTcMaxN;
+}
+
+template <int NST, bool F16>
+static int launch_tc(const pbbfmm_tree* t, unsigned tiles, int smem, int rf, int NP, int rowb,
+                     const CUtensorMap& tm_h, const CUtensorMap& tm_l, int lvl, const int* typed,
+                     const TcTiles& tt, int C, int l, int span, const unsigned char* ph,
+                     const unsigned char* pl, const int* pexp, float* pf, cudaStream_t st) {
+  PB_CUDA(cudaFuncSetAttribute(k_m2l_cheb_tc<NST, F16>,
+                               cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+  k_m2l_cheb_tc<NST, F16><<<tiles, TC_THREADS, smem, st>>>(
+      rf, NP, rowb, tm_h, tm_l, lvl, typed, tt, C, l, t->ws.sstart.as<int>(), span, t->d_offs,
+      ph, pl, pexp, t->tc.eexp + (int64_t)lvl * 316, pf, tc_group(NP, F16), t->d_tc_err);
+  PB_LAUNCH("m2l_cheb_tc");
+  return PBBFMM_OK;
 }
 
 // Level l of the tensor-core M2L: split the proxies, then the MMA kernel.
@@ -573,23 +686,33 @@ bool tc_eligible(const pbbfmm_tree* t) {
 int run_m2l_cheb_tc_level(pbbfmm_tree* t, int C, int l, int lvl, const float* proxy, float* pf,
                           cudaStream_t st) {
   const int L = t->p.tree_level, rf = t->ops.rf, rs = t->ops.rs;
-  const int NP = t->tc_np, KP = t->tc_kp;
+  const bool f16 = t->tc_fmt == PBBFMM_TC_F16;
+  const int NP = t->tc.np, KP = f16 ? t->tc.kp16 : t->tc.kp, esize = f16 ? 2 : 4;
+  const int rowb = KP * esize;  // a multiple of 128
   Workspace& ws = t->ws;
   const int* lists = ws.lists.as<int>();
   if (C > TC_M) {
     set_error("tensor-core M2L takes at most 128 columns per block");
     return PBBFMM_ERR_UNSUPPORTED;
   }
-  const int64_t per = cells_at(l) * C * KP;
-  if (int rc = grow(ws.tc_proxy, 2 * sizeof(float) * per)) return rc;
-  float* ph = ws.tc_proxy.as<float>();
-  float* pl = ph + per;
+  // hi rows | lo rows | (F16) row exponents, every cell of the level
+  const int64_t rows = cells_at(l) * C, pbytes = rows * rowb;
+  if (int rc = grow(ws.tc_proxy, 2 * pbytes + (f16 ? rows * (int64_t)sizeof(int) : 0))) return rc;
+  unsigned char* ph = ws.tc_proxy.as<unsigned char>();
+  unsigned char* pl = ph + pbytes;
+  int* pexp = f16 ? reinterpret_cast<int*>(pl + pbytes) : nullptr;
   const int ns = t->lists.nsrc[l];
   if (ns > 0) {
     const int64_t nrows = (int64_t)ns * C;
     if (int rc = kt_begin(t, KS_M2L_SPLIT, st)) return rc;
-    k_split_proxy<<<(unsigned)((nrows * KP + 255) / 256), 256, 0, st>>>(
-        lists + t->lists.src_off[l], nrows, C, rs, KP, proxy, ph, pl);
+    if (f16)
+      k_split_proxy_f16<<<(unsigned)((nrows * 32 + 255) / 256), 256, 0, st>>>(
+          lists + t->lists.src_off[l], nrows, C, rs, KP, proxy, reinterpret_cast<__half*>(ph),
+          reinterpret_cast<__half*>(pl), pexp);
+    else
+      k_split_proxy<<<(unsigned)((nrows * KP + 255) / 256), 256, 0, st>>>(
+          lists + t->lists.src_off[l], nrows, C, rs, KP, proxy, reinterpret_cast<float*>(ph),
+          reinterpret_cast<float*>(pl));
     PB_LAUNCH("m2l_split");
     if (int rc = kt_end(t, st)) return rc;
   }
@@ -609,23 +732,25 @@ int run_m2l_cheb_tc_level(pbbfmm_tree* t, int C, int l, int lvl, const float* pr
   const int smem = tc_smem_bytes(NP, nst);
   CUtensorMap tm_h, tm_l;
   const int64_t nrows = (int64_t)t->ops.nlev * 316 * NP;
-  if (int rc = operator_tensor_map(&tm_h, t->f_Eth, NP, KP, nrows)) return rc;
-  if (int rc = operator_tensor_map(&tm_l, t->f_Etl, NP, KP, nrows)) return rc;
+  const void* eh = f16 ? (const void*)t->tc.eh16 : (const void*)t->tc.eth;
+  const void* el = f16 ? (const void*)t->tc.el16 : (const void*)t->tc.etl;
+  if (int rc = operator_tensor_map(&tm_h, eh, f16, NP, KP, nrows)) return rc;
+  if (int rc = operator_tensor_map(&tm_l, el, f16, NP, KP, nrows)) return rc;
   if (int rc = kt_begin(t, KS_M2L, st)) return rc;
-  if (nst == 3) {
-    PB_CUDA(cudaFuncSetAttribute(k_m2l_cheb_tc<3>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 smem));
-    k_m2l_cheb_tc<3><<<(unsigned)tiles, TC_THREADS, smem, st>>>(
-        rf, NP, KP, tm_h, tm_l, lvl, lists + t->lists.typ_off[l], tt, C, l, ws.sstart.as<int>(), (int)cells_at(L - l), t->d_offs, ph, pl, pf, tc_group(NP),
-        t->d_tc_err);
-  } else {
-    PB_CUDA(cudaFuncSetAttribute(k_m2l_cheb_tc<2>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 smem));
-    k_m2l_cheb_tc<2><<<(unsigned)tiles, TC_THREADS, smem, st>>>(
-        rf, NP, KP, tm_h, tm_l, lvl, lists + t->lists.typ_off[l], tt, C, l, ws.sstart.as<int>(), (int)cells_at(L - l), t->d_offs, ph, pl, pf, tc_group(NP),
-        t->d_tc_err);
-  }
-  PB_LAUNCH("m2l_cheb_tc");
+  const int* typed = lists + t->lists.typ_off[l];
+  const int span = (int)cells_at(L - l);
+  int rc;
+  if (f16)
+    rc = nst == 3 ? launch_tc<3, true>(t, tiles, smem, rf, NP, rowb, tm_h, tm_l, lvl, typed, tt, C,
+                                       l, span, ph, pl, pexp, pf, st)
+                  : launch_tc<2, true>(t, tiles, smem, rf, NP, rowb, tm_h, tm_l, lvl, typed, tt, C,
+                                       l, span, ph, pl, pexp, pf, st);
+  else
+    rc = nst == 3 ? launch_tc<3, false>(t, tiles, smem, rf, NP, rowb, tm_h, tm_l, lvl, typed, tt,
+                                        C, l, span, ph, pl, pexp, pf, st)
+                  : launch_tc<2, false>(t, tiles, smem, rf, NP, rowb, tm_h, tm_l, lvl, typed, tt,
+                                        C, l, span, ph, pl, pexp, pf, st);
+  if (rc) return rc;
   return kt_end(t, st);
 }
 

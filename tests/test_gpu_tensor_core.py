@@ -1,10 +1,12 @@
-"""The Chebyshev M2L of the mixed path on the tensor cores (tcgen05, 3xTF32,
-float32 accumulation) against the float64 path and against the CUDA-core
-float32 kernel, through the C-ABI.
+"""The Chebyshev M2L of the mixed path on the tensor cores (tcgen05, split
+hi + lo operands with three products, float32 accumulation) in both operand
+formats -- power-of-two scaled F16 (the default) and TF32 -- against the
+float64 path and against the CUDA-core float32 kernel, through the C-ABI.
 
 Tolerance: 2e-6 relative L2 against float64 -- the bound the mixed path
-keeps everywhere (test_gpu_parity); 3xTF32 products carry ~2^-21 relative
-error each, and the TMEM accumulators are drained every few offsets."""
+keeps everywhere (test_gpu_parity); the split products carry ~2^-21 relative
+error each, and the TMEM accumulators are drained every offset (F16) or
+every few offsets (TF32)."""
 import numpy as np
 import pytest
 
@@ -21,9 +23,12 @@ def _tree(kernel, param, level, order, eps):
     return t
 
 
-def _run(t, p, w, ncols, precision, tc=True):
+FORMATS = ("f16", "tf32")
+
+
+def _run(t, p, w, ncols, precision, tc=True, fmt="f16"):
     t.set_precision(precision)
-    t.set_tensor_cores(tc)
+    t.set_tensor_cores(tc, fmt)
     out = np.zeros(p.shape[0] * ncols)
     fmm.H2_3D_Compute(t, p, p, w, ncols, out)
     return out
@@ -49,8 +54,9 @@ CASES = [
 ]
 
 
+@pytest.mark.parametrize("fmt", FORMATS)
 @pytest.mark.parametrize("case", CASES, ids=[f"{c[0]}n{c[3]}C{c[5]}" for c in CASES])
-def test_tensor_core_m2l_matches_fp64(case):
+def test_tensor_core_m2l_matches_fp64(case, fmt):
     kernel, param, level, order, eps, C, clustered = case
     rng = np.random.default_rng(31)
     N = 40000 if C < 8 else 3000
@@ -58,15 +64,18 @@ def test_tensor_core_m2l_matches_fp64(case):
     w = rng.uniform(-1, 1, N * C)
     t = _tree(kernel, param, level, order, eps)
     o64 = _run(t, p, w, C, fmm.PREC_FP64)
-    o_tc = _run(t, p, w, C, fmm.PREC_MIXED, tc=True)
-    assert t.tensor_core_m2l() == (t.get_operators()["rf"] <= 256)
+    o_tc = _run(t, p, w, C, fmm.PREC_MIXED, tc=True, fmt=fmt)
+    on_tc = t.get_operators()["rf"] <= 256
+    assert t.tensor_core_m2l() == on_tc
+    assert t.tensor_core_format() == (fmt if on_tc else None)
     o_cc = _run(t, p, w, C, fmm.PREC_MIXED, tc=False)
     assert rel(o_tc, o64) < 2e-6, rel(o_tc, o64)
     assert rel(o_cc, o64) < 2e-6
     assert rel(o_tc, o_cc) < 2e-6
 
 
-def test_tensor_core_locals_every_level():
+@pytest.mark.parametrize("fmt", FORMATS)
+def test_tensor_core_locals_every_level(fmt):
     """Locals F after the far field and L2L, level by level, mixed (tensor
     cores) against float64."""
     rng = np.random.default_rng(8)
@@ -76,7 +85,7 @@ def test_tensor_core_locals_every_level():
     t = _tree("Laplacian", 0.0, level, n, 1e-7)
     _run(t, p, w, C, fmm.PREC_FP64)
     F64 = {l: t.debug_copy(1, l) for l in range(2, level + 1)}
-    _run(t, p, w, C, fmm.PREC_MIXED, tc=True)
+    _run(t, p, w, C, fmm.PREC_MIXED, tc=True, fmt=fmt)
     cnt = np.diff(t.debug_copy(2).astype(np.int64))  # points per leaf
     n3 = n ** 3
     for l in range(2, level + 1):
@@ -102,6 +111,24 @@ def test_tensor_core_accuracy_against_direct_sum():
     assert etc < 1.05 * e64 + 1e-6, (etc, e64)
 
 
+@pytest.mark.parametrize("fmt", FORMATS)
+def test_tensor_core_scale_invariance(fmt):
+    """Weights scaled by 2^60 or 2^-60 scale the mixed result by exactly that
+    factor: the F16 operands carry a power-of-two scale per proxy row and per
+    operator (unscaled, 2^-60 x O(1) lies below the smallest F16 subnormal
+    and 2^60 above the largest F16), and every float32 step scales exactly."""
+    rng = np.random.default_rng(12)
+    N = 20000
+    p = _clustered(rng, N)
+    w = rng.uniform(-1, 1, N)
+    t = _tree("Laplacian", 0.0, 4, 5, 1e-7)
+    o = _run(t, p, w, 1, fmm.PREC_MIXED, fmt=fmt)
+    assert t.tensor_core_format() == fmt
+    for s in (2.0 ** 60, 2.0 ** -60):
+        os_ = _run(t, p, w * s, 1, fmm.PREC_MIXED, fmt=fmt)
+        assert rel(os_, o * s) < 1e-12, (s, rel(os_, o * s))
+
+
 def test_tensor_core_kernel_times_and_switch():
     rng = np.random.default_rng(3)
     p = rng.uniform(-0.5, 0.5, (5000, 3))
@@ -117,6 +144,12 @@ def test_tensor_core_kernel_times_and_switch():
     kt = t.kernel_times()
     assert kt["m2l_split"][1] == 0 and kt["m2l"][1] > 0
     t.set_tensor_cores(True)
-    assert t.tensor_core_m2l()
+    assert t.tensor_core_m2l() and t.tensor_core_format() == "f16"
+    t.set_tensor_cores(True, "tf32")
+    assert t.tensor_core_format() == "tf32"
     t.set_tensor_cores(False)
-    assert not t.tensor_core_m2l()
+    assert not t.tensor_core_m2l() and t.tensor_core_format() is None
+    with pytest.raises(ValueError):
+        t.set_tensor_cores(True, "bf16")
+    # the C-ABI refuses unknown modes
+    assert fmm._lib.lib().pbbfmm_set_tensor_cores(t._h, 7) == fmm._lib.ERR_ARG
