@@ -236,8 +236,8 @@ __host__ __device__ constexpr bool tc_sum_in_tmem(int NP) { return NP <= 160; }
 //   tm_eh, tm_el : [nlev][316][NP] rows of hi / lo of E_o^T (row f holds
 //                  E_o[f][s] over s), zero padded to rowb bytes
 //   Ph, Pl : proxy hi / lo, row (cell * C + col) of rowb bytes, zero padded
-//   pexp   : F16 only: the scale exponent of each proxy row (any value for
-//            rows of empty cells: their A rows are zero-filled)
+//   pexp   : F16 only: the scale exponent of each proxy row (read for
+//            nonempty source cells only, like Ph / Pl)
 //   eexp   : F16 only: the scale exponent of each operator of this level
 //   pf     : output rows (cell * C + col) of rf floats
 // Warp roles:
@@ -275,7 +275,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   __shared__ int s_cell[TC_M];     // target cell of each row, or -1
   __shared__ int s_xyz[TC_M];      // target coordinates, x << 20 | y << 10 | z
   __shared__ uint32_t s_valid[6];  // bit o: some target of the tile has a source at offset o
+  __shared__ uint32_t s_tmask[TC_M][6];  // per target of the tile: bit o = source at offset o
   __shared__ int4 s_off[189];      // valid offsets: (ox, oy, oz, operator index)
+  __shared__ uint8_t s_oidx[189];  // valid offset q: its index o in the type's list
   __shared__ int s_nvalid;
   __shared__ int s_abort_flag;
   volatile int* s_abort = &s_abort_flag;
@@ -305,6 +307,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     s_xyz[tid] = (x << 20) | (y << 10) | z;
   }
   if (tid < 6) s_valid[tid] = 0;
+  for (int i = tid; i < TC_M * 6; i += TC_THREADS) (&s_tmask[0][0])[i] = 0;
   if (warp == TC_MMA_WARP) {  // 128 lanes x 512 float32 columns
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
                      smem_u32(&s_tmem)),
@@ -326,24 +329,30 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
   }
   __syncthreads();
-  // offsets with at least one source cell for some target of the tile
-  if (tid < TC_M && s_cell[tid] >= 0 && tid % C == 0) {
-    const int x = s_xyz[tid] >> 20, y = (s_xyz[tid] >> 10) & 1023, z = s_xyz[tid] & 1023;
-    for (int o = 0; o < 189; ++o) {
-      const int bx = x + my_offs[4 * o], by = y + my_offs[4 * o + 1], bz = z + my_offs[4 * o + 2];
-      if (bx < 0 || by < 0 || bz < 0 || bx >= nside || by >= nside || bz >= nside) continue;
-      const uint32_t bm = morton_encode(bx, by, bz);
-      if (sstart[(int64_t)(bm + 1) * span] > sstart[(int64_t)bm * span])
-        atomicOr(&s_valid[o >> 5], 1u << (o & 31));
+  // which (target, offset) pairs of the tile have a source cell: all threads,
+  // one pair per item, independent loads
+#pragma unroll 4
+  for (int i = tid; i < ntile * 189; i += TC_THREADS) {
+    const int tg = i / 189, o = i - tg * 189;
+    const int xyz = s_xyz[tg * C];
+    const int bx = (xyz >> 20) + my_offs[4 * o], by = ((xyz >> 10) & 1023) + my_offs[4 * o + 1],
+              bz = (xyz & 1023) + my_offs[4 * o + 2];
+    if (bx < 0 || by < 0 || bz < 0 || bx >= nside || by >= nside || bz >= nside) continue;
+    const uint32_t bm = morton_encode(bx, by, bz);
+    if (sstart[(int64_t)(bm + 1) * span] > sstart[(int64_t)bm * span]) {
+      atomicOr(&s_tmask[tg][o >> 5], 1u << (o & 31));
+      atomicOr(&s_valid[o >> 5], 1u << (o & 31));
     }
   }
   __syncthreads();
   if (tid == 0) {
     int nv = 0;
     for (int o = 0; o < 189; ++o)
-      if ((s_valid[o >> 5] >> (o & 31)) & 1)
+      if ((s_valid[o >> 5] >> (o & 31)) & 1) {
+        s_oidx[nv] = (uint8_t)o;
         s_off[nv++] = make_int4(my_offs[4 * o], my_offs[4 * o + 1], my_offs[4 * o + 2],
                                 my_offs[4 * o + 3]);
+      }
     s_nvalid = nv;
   }
   tc_fence_before();
@@ -360,35 +369,19 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     // ---------------------------------------------------------------- producers
     // Lane l copies 16-byte chunk (l & 7) of rows 4 warp + (l >> 3) + 16 i of
     // A (i < 8) and B (i < NP / 16): four 128-byte rows per warp instruction.
-    // Lane l also owns A row 4 warp + (l & 3) + 16 (l >> 2): it looks up that
-    // row's source once per offset (one offset ahead) and the lanes copying
-    // the row fetch the result by shuffle.
+    // Lane l also owns A row 4 warp + (l & 3) + 16 (l >> 2): it finds that
+    // row's source once per offset (from the tile's source mask: no global
+    // load) and the lanes copying the row fetch the result by shuffle.
     const int own = 4 * warp + (lane & 3) + 16 * (lane >> 2);
-    const int ocell = s_cell[own], ocol = own % C;
+    const int ocell = s_cell[own], ocol = own % C, otg = own / C;
     const int ox = s_xyz[own] >> 20, oy = (s_xyz[own] >> 10) & 1023, oz = s_xyz[own] & 1023;
     const int ch = lane & 7, r0 = 4 * warp + (lane >> 3);
     const uint32_t soff0 = sw128_off(r0, ch);  // row r0 + 16 i lies 2048 i bytes further
-    int pre_q = -1, pre_a = 0, pre_b = 0;
-    uint32_t pre_bm = 0;
-    bool pre_in = false;
-    auto start_lookup = [&](int q) {
-      pre_q = q;
-      pre_in = false;
-      if (q >= nvalid || ocell < 0) return;
-      const int4 o = s_off[q];
-      const int x = ox + o.x, y = oy + o.y, z = oz + o.z;
-      if (x < 0 || y < 0 || z < 0 || x >= nside || y >= nside || z >= nside) return;
-      pre_bm = morton_encode(x, y, z);
-      pre_a = sstart[(int64_t)pre_bm * span];
-      pre_b = sstart[(int64_t)(pre_bm + 1) * span];
-      pre_in = true;
-    };
     int cur_q = -1;
     long long cur_row = -1;  // this lane's own row: source row offset or -1
     int tma_last[NST];       // thread 0: last iteration whose TMA went into each stage
 #pragma unroll
     for (int i = 0; i < NST; ++i) tma_last[i] = -1;
-    start_lookup(0);
     for (int j = 0; j < niter; ++j) {
       const int s = j % NST;
       if (j >= NST && !mbar_wait(&s_empty[s], (j / NST - 1) & 1, s_abort)) {
@@ -397,10 +390,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       }
       const int q = j / kchunks, kc = j - q * kchunks;
       if (q != cur_q) {
-        if (pre_q != q) start_lookup(q);
-        cur_row = (pre_in && pre_b > pre_a) ? ((long long)pre_bm * C + ocol) * rowb : -1;
+        const int o = s_oidx[q];
+        cur_row = -1;
+        if (ocell >= 0 && ((s_tmask[otg][o >> 5] >> (o & 31)) & 1)) {
+          const int4 d = s_off[q];
+          cur_row = ((long long)morton_encode(ox + d.x, oy + d.y, oz + d.z) * C + ocol) * rowb;
+        }
         cur_q = q;
-        start_lookup(q + 1);
       }
       unsigned char* st = base + s * stage_bytes;
 #pragma unroll
@@ -494,13 +490,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     // (rows without a source are zero, and stay zero under any finite scale)
     const int rcol = row % C;
     const int rx = s_xyz[row] >> 20, ry = (s_xyz[row] >> 10) & 1023, rz = s_xyz[row] & 1023;
+    const int rtg = row / C;
     auto row_exp = [&](int q) -> int {
       if (!F16 || q >= nvalid || cell < 0) return 0;
+      const int oi = s_oidx[q];
+      if (!((s_tmask[rtg][oi >> 5] >> (oi & 31)) & 1)) return 0;  // no source: a zero row
       const int4 o = s_off[q];
-      const int x = rx + o.x, y = ry + o.y, z = rz + o.z;
-      int e = eexp[o.w];
-      if (x >= 0 && y >= 0 && z >= 0 && x < nside && y < nside && z < nside)
-        e += min(max(pexp[(int64_t)morton_encode(x, y, z) * C + rcol], -256), 256);
+      const int e = eexp[o.w] + min(max(pexp[(int64_t)morton_encode(rx + o.x, ry + o.y, rz + o.z) *
+                                                 C + rcol], -256), 256);
       return min(max(e, -252), 252);
     };
     int e_next = row_exp(0);
