@@ -46,7 +46,7 @@ constexpr int TC_PRODUCERS = 128;  // warps 0-3: operand loads
 constexpr int TC_MMA_WARP = 4;     // warp 4: TMEM allocation, MMA issue (one thread)
 constexpr int TC_THREADS = 288;    // + warps 5-8: accumulator drains
 constexpr int TC_TMEM_COLS = 512;  // columns allocated (accumulators and running sum)
-constexpr unsigned long long kWaitNs = 1000000000ull;  // 1 s
+constexpr long long kWaitCycles = 2000000000ll;  // about 1 s of SM clock
 constexpr long long kWaitIters = 1ll << 26;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -84,28 +84,28 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, int count) {
                : "memory");
 }
 
-__device__ __forceinline__ unsigned long long global_ns() {
-  unsigned long long t;
-  asm volatile("mov.u64 %0, %%globaltimer;\n" : "=l"(t));
-  return t;
+__device__ __forceinline__ bool mbar_try(uint32_t a, int parity) {
+  uint32_t done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(done)
+      : "r"(a), "r"(parity)
+      : "memory");
+  return done != 0;
 }
 
 // Wait for the completion of the phase with parity `parity`; false after
-// about a second (or kWaitIters polls) without it, or once *abort is set
-// (abort may be null).
+// about a second of SM clock (or kWaitIters polls) without it, or once *abort
+// is set (abort may be null).  The first poll reads no clock: a wait that is
+// already satisfied costs one try_wait.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, int parity, const volatile int* abort) {
   const uint32_t a = smem_u32(bar);
-  const unsigned long long t0 = global_ns();
+  if (mbar_try(a, parity)) return true;
+  const long long t0 = clock64();
   for (long long it = 0; it < kWaitIters; ++it) {
-    uint32_t done;
-    asm volatile(
-        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-        " selp.u32 %0, 1, 0, p;\n}\n"
-        : "=r"(done)
-        : "r"(a), "r"(parity)
-        : "memory");
-    if (done) return true;
-    if ((it & 255) == 255 && ((abort && *abort) || global_ns() - t0 > kWaitNs)) return false;
+    if (mbar_try(a, parity)) return true;
+    if ((it & 255) == 255 && ((abort && *abort) || clock64() - t0 > kWaitCycles)) return false;
   }
   return false;
 }
@@ -190,6 +190,18 @@ __device__ __forceinline__ void tc_ld16(uint32_t taddr, float* v) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// 16 consecutive float32 columns of this thread's TMEM lane, loaded and waited
+// for in one asm statement (so that no use of r can precede the wait).
+__device__ __forceinline__ void tc_ld16_wait(uint32_t taddr, uint32_t* r) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];\n"
+      "tcgen05.wait::ld.sync.aligned;\n"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr)
+      : "memory");
+}
+
 // Store 16 consecutive float32 columns of this thread's TMEM lane.
 __device__ __forceinline__ void tc_st16(uint32_t taddr, const float* v) {
   asm volatile(
@@ -226,11 +238,16 @@ __host__ __device__ constexpr int tc_smem_bytes(int NP, int nst) {
   return nst * tc_stage_bytes(NP) + 1024;
 }
 
-// TMEM columns (512 allocated): accumulator b at b * stride; when three
-// regions fit (N <= 160), a running sum at 2 * stride that the drains update
-// inside TMEM, so that pf is written once; otherwise drains add into pf.
+// TMEM columns (512 allocated): accumulator b at b * stride.  With the
+// running sum in registers (N <= TC_REG_SUM) four accumulators take turns;
+// otherwise two, and when a third region fits (N <= 160) a running sum at
+// 2 * stride that the drains update inside TMEM, so that pf is written once;
+// beyond that drains add into pf.
 __host__ __device__ constexpr int tc_acc_stride(int NP) { return NP <= 160 ? (NP + 31) / 32 * 32 : 256; }
 __host__ __device__ constexpr bool tc_sum_in_tmem(int NP) { return NP <= 160; }
+// Up to this many columns the running sum lives in the drain threads'
+// registers (the CTA is alone on its SM, so they cost no occupancy).
+constexpr int TC_REG_SUM = 128;
 
 // One CTA per tile of 128 (target, col) rows of one child type; NST stages.
 //   tm_eh, tm_el : [nlev][316][NP] rows of hi / lo of E_o^T (row f holds
@@ -249,15 +266,18 @@ __host__ __device__ constexpr bool tc_sum_in_tmem(int NP) { return NP <= 160; }
 //              MMAs and commits them to the stage's empty barrier;
 //   warps 5-8  drain accumulators into the running sum (TMEM lane quadrant
 //              warp % 4).
-// Two TMEM accumulators take turns, one per group of `group` consecutive
-// offsets, so every float32 accumulation chain inside the tensor pipe spans
-// at most `group` offsets.
+// NACC TMEM accumulators (four with the register running sum, else two) take
+// turns, one per group of `group` consecutive offsets, so every float32
+// accumulation chain inside the tensor pipe spans at most `group` offsets;
+// an accumulator is reused NACC groups later, once drained (the commit that
+// releases a group's accumulator to the drains arrives well after its MMAs
+// are issued, so two accumulators left the MMA thread waiting for drains).
 //   s_full[s]  : 128 producer arrivals, one per thread, when its copies land
 //   s_tfull[s] : the operator tile's TMA bytes (thread 0's expect_tx)
 //   s_empty[s] : MMAs reading stage s done (tcgen05.commit)
 //   s_accf[b]  : MMAs of accumulator b's group done (tcgen05.commit)
 //   s_acce[b]  : accumulator b drained (128 drainer arrivals)
-template <int NST, bool F16>
+template <int NST, bool F16, bool RSUM>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     k_m2l_cheb_tc(int rf, int NP, int rowb, const __grid_constant__ CUtensorMap tm_eh,
                   const __grid_constant__ CUtensorMap tm_el, int lvl,
@@ -270,7 +290,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   const int bbytes = NP * 128;
   const int stage_bytes = tc_stage_bytes(NP);
   unsigned char* base = smraw + ((1024 - (smem_u32(smraw) & 1023)) & 1023);
-  __shared__ uint64_t s_full[NST], s_tfull[NST], s_empty[NST], s_accf[2], s_acce[2];
+  constexpr int NACC = RSUM ? 4 : 2;  // TMEM accumulators (4 x 128 columns at most)
+  __shared__ uint64_t s_full[NST], s_tfull[NST], s_empty[NST], s_accf[NACC], s_acce[NACC];
   __shared__ uint32_t s_tmem;
   __shared__ int s_cell[TC_M];     // target cell of each row, or -1
   __shared__ int s_xyz[TC_M];      // target coordinates, x << 20 | y << 10 | z
@@ -278,6 +299,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   __shared__ uint32_t s_tmask[TC_M][6];  // per target of the tile: bit o = source at offset o
   __shared__ int4 s_off[189];      // valid offsets: (ox, oy, oz, operator index)
   __shared__ uint8_t s_oidx[189];  // valid offset q: its index o in the type's list
+  __shared__ int s_oexp[189];      // F16: valid offset q: its operator's scale exponent
   __shared__ int s_nvalid;
   __shared__ int s_abort_flag;
   volatile int* s_abort = &s_abort_flag;
@@ -321,7 +343,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       mbar_init(&s_tfull[i], 1);
       mbar_init(&s_empty[i], 1);
     }
-    for (int b = 0; b < 2; ++b) {
+    for (int b = 0; b < NACC; ++b) {
       mbar_init(&s_accf[b], 1);
       mbar_init(&s_acce[b], TC_M);
     }
@@ -355,6 +377,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       }
     s_nvalid = nv;
   }
+  __syncthreads();
+  if constexpr (F16)
+    for (int q = tid; q < s_nvalid; q += TC_THREADS) s_oexp[q] = eexp[s_off[q].w];
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
@@ -436,8 +461,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         const int s = it % NST;
         const int g = it / group_iters;
         const bool fresh = it == g * group_iters;
-        // accumulator g & 1 is free once the drain of group g - 2 is done
-        if (fresh && g >= 2 && !mbar_wait(&s_acce[g & 1], ((g - 2) >> 1) & 1, s_abort)) {
+        // accumulator g % NACC is free once the drain of group g - NACC is done
+        const int ab = g % NACC;
+        if (fresh && g >= NACC && !mbar_wait(&s_acce[ab], ((g - NACC) / NACC) & 1, s_abort)) {
           *s_abort = 1;
           break;
         }
@@ -450,7 +476,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         tc_fence_after();
         const uint32_t a_hi = smem_u32(base + s * stage_bytes), a_lo = a_hi + 16384;
         const uint32_t b_hi = a_hi + 32768, b_lo = b_hi + bbytes;
-        const uint32_t d = tmem + (uint32_t)((g & 1) * astride);
+        const uint32_t d = tmem + (uint32_t)(ab * astride);
         // four K steps of 32 bytes (16 F16 or 8 TF32 values) per 128-byte row
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
@@ -468,7 +494,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
           }
         }
         tc_commit(&s_empty[s]);
-        if (it + 1 == niter || it + 1 == (g + 1) * group_iters) tc_commit(&s_accf[g & 1]);
+        if (it + 1 == niter || it + 1 == (g + 1) * group_iters) tc_commit(&s_accf[ab]);
         last = it;
       }
       // Before the TMEM is freed: MMAs complete in order, so the last commit
@@ -486,40 +512,71 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     const bool tsum = tc_sum_in_tmem(NP);
     const uint32_t sum_base = lane_base + (uint32_t)(2 * astride);
     // F16 (one offset per group): the unscaling exponent of this row at offset
-    // q, e_op + e_row of its source, clamped so that 2^-e is a normal float
-    // (rows without a source are zero, and stay zero under any finite scale)
+    // q is e_op + e_row of its source.  The row's exponent is loaded two
+    // offsets ahead, unconditionally (index 0 when the row has no source at q,
+    // the flag then marks it unused), so that no instruction waits for the
+    // load before the offset's drain.
     const int rcol = row % C;
     const int rx = s_xyz[row] >> 20, ry = (s_xyz[row] >> 10) & 1023, rz = s_xyz[row] & 1023;
     const int rtg = row / C;
-    auto row_exp = [&](int q) -> int {
-      if (!F16 || q >= nvalid || cell < 0) return 0;
+    auto has_src = [&](int q) -> bool {
+      if (!F16 || q >= nvalid || cell < 0) return false;
       const int oi = s_oidx[q];
-      if (!((s_tmask[rtg][oi >> 5] >> (oi & 31)) & 1)) return 0;  // no source: a zero row
-      const int4 o = s_off[q];
-      const int e = eexp[o.w] + min(max(pexp[(int64_t)morton_encode(rx + o.x, ry + o.y, rz + o.z) *
-                                                 C + rcol], -256), 256);
-      return min(max(e, -252), 252);
+      return (s_tmask[rtg][oi >> 5] >> (oi & 31)) & 1;
     };
-    int e_next = row_exp(0);
+    auto src_row = [&](int q, bool ok) -> int64_t {
+      if (!ok) return 0;
+      const int4 o = s_off[q];
+      return (int64_t)morton_encode(rx + o.x, ry + o.y, rz + o.z) * C + rcol;
+    };
+    bool v1 = has_src(0), v2 = has_src(1);
+    int x1 = F16 ? pexp[src_row(0, v1)] : 0, x2 = F16 && nvalid > 1 ? pexp[src_row(1, v2)] : 0;
+    float rsum[RSUM ? TC_REG_SUM : 1];  // running sum (RSUM: NP <= TC_REG_SUM)
+#pragma unroll
+    for (int i = 0; i < (RSUM ? TC_REG_SUM : 1); ++i) rsum[i] = 0.f;
     for (int g = 0; g < ngroups; ++g) {
-      const int b = g & 1;
-      const int e_cur = e_next;
-      e_next = row_exp(g + 1);  // loaded while this group's MMAs run
-      // 2^-e_cur as two normal powers of two (|e_cur| <= 252)
-      const float sc1 = __int_as_float((127 - (e_cur >> 1)) << 23);
-      const float sc2 = __int_as_float((127 - (e_cur - (e_cur >> 1))) << 23);
-      if (!mbar_wait(&s_accf[b], (g >> 1) & 1, s_abort)) {
+      const int b = g % NACC;
+      // 2^-e exactly (a normal or subnormal power of two), e = e_op + e_row
+      // clamped to [-126, 149]; rows without a source are zero (any scale)
+      int e = v1 ? s_oexp[g] + min(max(x1, -256), 256) : 0;
+      e = min(max(e, -126), 149);
+      const float sc = e <= 126 ? __int_as_float((127 - e) << 23) : __int_as_float(1 << (149 - e));
+      v1 = v2;
+      x1 = x2;
+      v2 = has_src(g + 2);
+      if (F16 && g + 2 < nvalid) x2 = pexp[src_row(g + 2, v2)];
+      if (!mbar_wait(&s_accf[b], (g / NACC) & 1, s_abort)) {
         *s_abort = 1;
         break;
       }
       tc_fence_after();
+      if constexpr (RSUM) {
+        // batches of 16 columns (one wait each) added into the register sum;
+        // the accumulator is released once its last batch is in registers
+#pragma unroll
+        for (int c = 0; c < TC_REG_SUM / 16; ++c) {
+          if (c * 16 >= NP) break;
+          uint32_t r[16];
+          tc_ld16_wait(lane_base + (uint32_t)(b * astride + c * 16), r);
+          if ((c + 1) * 16 >= NP) {
+            tc_fence_before();
+            mbar_arrive(&s_acce[b]);
+          }
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            const float x = __uint_as_float(r[i]);
+            rsum[c * 16 + i] = F16 ? fmaf(x, sc, rsum[c * 16 + i]) : rsum[c * 16 + i] + x;
+          }
+        }
+        continue;
+      } else {
       const bool final_group = g + 1 == ngroups;
       float v[16], u[16];
       for (int n0 = 0; n0 < NP; n0 += 16) {
         tc_ld16(lane_base + (uint32_t)(b * astride + n0), v);
         if constexpr (F16) {
 #pragma unroll
-          for (int i = 0; i < 16; ++i) v[i] = v[i] * sc1 * sc2;  // exact: powers of two
+          for (int i = 0; i < 16; ++i) v[i] *= sc;  // exact unless the product is subnormal
         }
         if (tsum) {
           if (g > 0) {
@@ -543,9 +600,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       if (tsum && !final_group) tc_wait_st();
       tc_fence_before();
       mbar_arrive(&s_acce[b]);
+      }
     }
-    if (ngroups == 0 && dst)  // no source in any interaction list of the tile
+    if constexpr (RSUM) {
+      if (dst)
+#pragma unroll
+        for (int i = 0; i < TC_REG_SUM; ++i)
+          if (i < rf) dst[i] = rsum[i];
+    } else if (ngroups == 0 && dst) {  // no source in any interaction list of the tile
       for (int n = 0; n < rf; ++n) dst[n] = 0.f;
+    }
   }
   tc_fence_before();
   __syncthreads();
@@ -664,14 +728,14 @@ bool tc_eligible(const pbbfmm_tree* t) {
          t->tc.np <= kTcMaxN;
 }
 
-template <int NST, bool F16>
+template <int NST, bool F16, bool RSUM>
 static int launch_tc(const pbbfmm_tree* t, unsigned tiles, int smem, int rf, int NP, int rowb,
                      const CUtensorMap& tm_h, const CUtensorMap& tm_l, int lvl, const int* typed,
                      const TcTiles& tt, int C, int l, int span, const unsigned char* ph,
                      const unsigned char* pl, const int* pexp, float* pf, cudaStream_t st) {
-  PB_CUDA(cudaFuncSetAttribute(k_m2l_cheb_tc<NST, F16>,
+  PB_CUDA(cudaFuncSetAttribute(k_m2l_cheb_tc<NST, F16, RSUM>,
                                cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-  k_m2l_cheb_tc<NST, F16><<<tiles, TC_THREADS, smem, st>>>(
+  k_m2l_cheb_tc<NST, F16, RSUM><<<tiles, TC_THREADS, smem, st>>>(
       rf, NP, rowb, tm_h, tm_l, lvl, typed, tt, C, l, t->ws.sstart.as<int>(), span, t->d_offs,
       ph, pl, pexp, t->tc.eexp + (int64_t)lvl * 316, pf, tc_group(NP, F16), t->d_tc_err);
   PB_LAUNCH("m2l_cheb_tc");
@@ -736,17 +800,19 @@ int run_m2l_cheb_tc_level(pbbfmm_tree* t, int C, int l, int lvl, const float* pr
   if (int rc = kt_begin(t, KS_M2L, st)) return rc;
   const int* typed = lists + t->lists.typ_off[l];
   const int span = (int)cells_at(L - l);
+  // register running sum up to TC_REG_SUM columns (three stages always fit there)
+  const bool rsum = NP <= TC_REG_SUM && nst == 3;
+#define PB_TC_LAUNCH(NSTV, F, R)                                                              \
+  launch_tc<NSTV, F, R>(t, tiles, smem, rf, NP, rowb, tm_h, tm_l, lvl, typed, tt, C, l, span, \
+                        ph, pl, pexp, pf, st)
   int rc;
   if (f16)
-    rc = nst == 3 ? launch_tc<3, true>(t, tiles, smem, rf, NP, rowb, tm_h, tm_l, lvl, typed, tt, C,
-                                       l, span, ph, pl, pexp, pf, st)
-                  : launch_tc<2, true>(t, tiles, smem, rf, NP, rowb, tm_h, tm_l, lvl, typed, tt, C,
-                                       l, span, ph, pl, pexp, pf, st);
+    rc = rsum ? PB_TC_LAUNCH(3, true, true)
+              : (nst == 3 ? PB_TC_LAUNCH(3, true, false) : PB_TC_LAUNCH(2, true, false));
   else
-    rc = nst == 3 ? launch_tc<3, false>(t, tiles, smem, rf, NP, rowb, tm_h, tm_l, lvl, typed, tt,
-                                        C, l, span, ph, pl, pexp, pf, st)
-                  : launch_tc<2, false>(t, tiles, smem, rf, NP, rowb, tm_h, tm_l, lvl, typed, tt,
-                                        C, l, span, ph, pl, pexp, pf, st);
+    rc = rsum ? PB_TC_LAUNCH(3, false, true)
+              : (nst == 3 ? PB_TC_LAUNCH(3, false, false) : PB_TC_LAUNCH(2, false, false));
+#undef PB_TC_LAUNCH
   if (rc) return rc;
   return kt_end(t, st);
 }

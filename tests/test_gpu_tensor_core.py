@@ -6,7 +6,8 @@ float64 path and against the CUDA-core float32 kernel, through the C-ABI.
 Tolerance: 2e-6 relative L2 against float64 -- the bound the mixed path
 keeps everywhere (test_gpu_parity); the split products carry ~2^-21 relative
 error each, and the TMEM accumulators are drained every offset (F16) or
-every few offsets (TF32)."""
+every few offsets (TF32), into a running sum kept in registers (r_f <= 128),
+in TMEM (r_f <= 160) or in the output."""
 import numpy as np
 import pytest
 
@@ -51,6 +52,7 @@ CASES = [
     ("OneOverR2", 0.0, 4, 4, 1e-5, 3, True),     # 42 targets x 3 columns per tile
     ("Laplacian", 0.0, 3, 4, 1e-5, 64, False),   # two targets per tile
     ("Laplacian", 0.0, 3, 7, 1e-9, 1, False),    # r_f near 256: two stages, N up to 256
+    ("Laplacian", 0.0, 3, 6, 1e-8, 1, False),    # r_f 150: running sum in TMEM
 ]
 
 
