@@ -115,7 +115,7 @@ static float tf32_round(float x) {
 }
 
 static void free_tc_ops(TcOps* o) {
-  void* b[] = {o->eth, o->etl, o->eh16, o->el16, o->eexp};
+  void* b[] = {o->eth, o->etl, o->eh16, o->el16, o->eexp, o->vth, o->vtl, o->uh, o->ul};
   for (void* p : b)
     if (p) cudaFree(p);
   *o = TcOps{};
@@ -189,8 +189,68 @@ static int upload_tc_split(const double* K, int nlev, int rf, int rs, TcOps* o) 
   return PBBFMM_OK;
 }
 
+// Scaled F16 hi / lo rows of a level's matrix W (rows x cols, read through
+// at(level, m, k)), [level][mp][kp] zero padded; exp[level] makes max |W|
+// 2^exp lie in [2^14, 2^15).
+template <typename At>
+static void split_f16_rows(int nlev, int rows, int cols, int mp, int kp, At at,
+                           std::vector<uint16_t>* hi, std::vector<uint16_t>* lo, int* exps) {
+  hi->assign((size_t)nlev * mp * kp, 0);
+  lo->assign((size_t)nlev * mp * kp, 0);
+  for (int lv = 0; lv < nlev; ++lv) {
+    float m = 0.f;
+    for (int r = 0; r < rows; ++r)
+      for (int k = 0; k < cols; ++k) m = std::max(m, std::fabs((float)at(lv, r, k)));
+    int e = 0;
+    if (m > 0.f) {
+      int k2;
+      std::frexp(m, &k2);
+      e = 15 - k2;
+    }
+    exps[lv] = e;
+    for (int r = 0; r < rows; ++r)
+      for (int k = 0; k < cols; ++k) {
+        const float x = std::ldexp((float)at(lv, r, k), e);
+        const __half xh = __float2half_rn(x);
+        const __half xl = __float2half_rn(x - __half2float(xh));
+        const size_t i = ((size_t)lv * mp + r) * kp + k;
+        memcpy(&(*hi)[i], &xh, 2);
+        memcpy(&(*lo)[i], &xl, 2);
+      }
+  }
+}
+
+// The M2L pre / post transforms' matrices for the tensor cores (see TcOps):
+// VT (column-major rs x n3 per level) and U (column-major n3 x rf per level).
+static int upload_tc_uvt(const double* U, const double* VT, int nlev, int n3, int rf, int rs,
+                         TcOps* o) {
+  if (nlev > 32) return PBBFMM_OK;  // more levels than the exponent tables: CUDA cores
+  o->vt_mp = (rs + 15) / 16 * 16;
+  o->vt_kp = (n3 + 63) / 64 * 64;
+  o->u_mp = (n3 + 15) / 16 * 16;
+  o->u_kp = (rf + 63) / 64 * 64;
+  std::vector<uint16_t> h, l;
+  int rc;
+  if (o->vt_mp <= 256) {
+    split_f16_rows(nlev, rs, n3, o->vt_mp, o->vt_kp,
+                   [&](int lv, int m, int k) { return VT[(size_t)lv * rs * n3 + m + (size_t)rs * k]; },
+                   &h, &l, o->vt_exp);
+    if ((rc = upload_vec(&o->vth, h)) || (rc = upload_vec(&o->vtl, l))) return rc;
+  }
+  if (o->u_mp <= 256) {
+    split_f16_rows(nlev, n3, rf, o->u_mp, o->u_kp,
+                   [&](int lv, int m, int k) { return U[(size_t)lv * n3 * rf + m + (size_t)n3 * k]; },
+                   &h, &l, o->u_exp);
+    if ((rc = upload_vec(&o->uh, h)) || (rc = upload_vec(&o->ul, l))) return rc;
+  }
+  return PBBFMM_OK;
+}
+
 static int upload_tc_operators(pbbfmm_tree* t) {
   if (int rc = upload_tc_split(t->ops.K.data(), t->ops.nlev, t->ops.rf, t->ops.rs, &t->tc))
+    return rc;
+  if (int rc = upload_tc_uvt(t->ops.U.data(), t->ops.VT.data(), t->ops.nlev, t->n3, t->ops.rf,
+                             t->ops.rs, &t->tc))
     return rc;
   if (!t->h_tc_err) {
     PB_CUDA(cudaHostAlloc(&t->h_tc_err, sizeof(int), cudaHostAllocMapped));
@@ -354,6 +414,8 @@ static int build_adjoint_ops(pbbfmm_tree* t) {
   if ((rc = upload_f32(&t->adj.fU, U.data(), U.size()))) return rc;
   if ((rc = upload_f32(&t->adj.fVT, VT.data(), VT.size()))) return rc;
   if ((rc = upload_tc_split(E.data(), nlev, rs, rf, &t->adj.tc))) return rc;
+  // adjoint: U' (n3 x rs) = VT^T and VT' (rf x n3) = U^T, so r_f' = rs, r_s' = rf
+  if ((rc = upload_tc_uvt(U.data(), VT.data(), nlev, n3, rs, rf, &t->adj.tc))) return rc;
   t->adj.rf = rs;
   t->adj.rs = rf;
   t->adj_ready = true;

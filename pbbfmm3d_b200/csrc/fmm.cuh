@@ -79,6 +79,13 @@ struct TcOps {
   uint16_t* el16 = nullptr;
   int* eexp = nullptr;
   int np = 0, kp = 0, kp16 = 0;
+  // M2L pre / post transforms on the tensor cores: W = VT (rs x n^3) and
+  // U (n^3 x r_f) as [level][mp][kp] F16 hi / lo rows (row m holds W[m][k]
+  // over k, zero padded; mp = rows padded to 16, kp = K padded to 64), each
+  // level's matrix scaled by 2^exp[level].  Null when mp exceeds 256.
+  uint16_t *vth = nullptr, *vtl = nullptr, *uh = nullptr, *ul = nullptr;
+  int vt_mp = 0, vt_kp = 0, u_mp = 0, u_kp = 0;
+  int vt_exp[32] = {}, u_exp[32] = {};
 };
 
 }  // namespace pbbfmm
@@ -202,6 +209,13 @@ int run_m2l_cheb(pbbfmm_tree* t, int C, cudaStream_t st);
 // tensor-core Chebyshev M2L (float path): N = rf padded to 16 must fit TMEM
 constexpr int kTcMaxN = 256;
 bool tc_eligible(const pbbfmm_tree* t);
+// M2L pre (post = false: proxy = VT (Kw o S)) or post (post = true:
+// F = alpha Kw o (U Pf)) transform of level l on the tensor cores, for the
+// ncols = (cells x C) columns listed; false from colgemm_tc_eligible when the
+// CUDA-core kernel must run instead.
+bool colgemm_tc_eligible(const pbbfmm_tree* t, bool post);
+int run_colgemm_tc(pbbfmm_tree* t, bool post, int lvl, const int* cells, int ncols, int C,
+                   const float* X, float* Out, float alpha, cudaStream_t st);
 int run_m2l_cheb_tc_level(pbbfmm_tree* t, int C, int l, int lvl, const float* proxy, float* pf,
                           cudaStream_t st);
 int run_m2l_unif(pbbfmm_tree* t, int C, cudaStream_t st);

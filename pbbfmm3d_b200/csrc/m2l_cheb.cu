@@ -278,12 +278,24 @@ static int run_m2l_cheb_t(pbbfmm_tree* t, int C, cudaStream_t st) {
     if (ns > 0) {
       dim3 g((unsigned)((ns * (int64_t)C + GBN - 1) / GBN), (unsigned)((rs + GBM - 1) / GBM));
       if (int rc_ = kt_begin(t, KS_M2L_PRE, st)) return rc_;
-      k_colgemm<T><<<g, kGemmThreads, 0, st>>>(rs, n3, ov.VT + (int64_t)lvl * rs * n3,
-                                            lists + t->lists.src_off[l], ns * C, C,
-                                            S + level_offset(l, (int64_t)C * n3), ov.Kw,
-                                            proxy + level_offset(l, (int64_t)C * rs), nullptr,
-                                            T(1));
-      PB_LAUNCH("m2l_pre");
+      bool pre_tc = false;  // float path: tcgen05 (scaled F16 hi / lo) when W fits
+      if constexpr (std::is_same<T, float>::value) {
+        if (colgemm_tc_eligible(t, false)) {
+          if (int rc_ = run_colgemm_tc(t, false, lvl, lists + t->lists.src_off[l], ns * C, C,
+                                       S + level_offset(l, (int64_t)C * n3),
+                                       proxy + level_offset(l, (int64_t)C * rs), 1.f, st))
+            return rc_;
+          pre_tc = true;
+        }
+      }
+      if (!pre_tc) {
+        k_colgemm<T><<<g, kGemmThreads, 0, st>>>(rs, n3, ov.VT + (int64_t)lvl * rs * n3,
+                                              lists + t->lists.src_off[l], ns * C, C,
+                                              S + level_offset(l, (int64_t)C * n3), ov.Kw,
+                                              proxy + level_offset(l, (int64_t)C * rs), nullptr,
+                                              T(1));
+        PB_LAUNCH("m2l_pre");
+      }
       if (int rc_ = kt_end(t, st)) return rc_;
     }
   }
@@ -328,12 +340,24 @@ static int run_m2l_cheb_t(pbbfmm_tree* t, int C, cudaStream_t st) {
     const double scale = pow(1.0 / len, t->homogen_neg);
     dim3 g2((unsigned)((nt * (int64_t)C + GBN - 1) / GBN), (unsigned)((n3 + GBM - 1) / GBM));
     if (int rc_ = kt_begin(t, KS_M2L_POST, st)) return rc_;
-    k_colgemm<T><<<g2, kGemmThreads, 0, st>>>(n3, rf, ov.U + (int64_t)lvl * n3 * rf,
-                                           lists + t->lists.tgt_off[l], nt * C, C,
-                                           pf + level_offset(l, (int64_t)C * rf), nullptr,
-                                           F + level_offset(l, (int64_t)C * n3), ov.Kw,
-                                           (T)scale);
-    PB_LAUNCH("m2l_post");
+    bool post_tc = false;
+    if constexpr (std::is_same<T, float>::value) {
+      if (colgemm_tc_eligible(t, true)) {
+        if (int rc_ = run_colgemm_tc(t, true, lvl, lists + t->lists.tgt_off[l], nt * C, C,
+                                     pf + level_offset(l, (int64_t)C * rf),
+                                     F + level_offset(l, (int64_t)C * n3), (float)scale, st))
+          return rc_;
+        post_tc = true;
+      }
+    }
+    if (!post_tc) {
+      k_colgemm<T><<<g2, kGemmThreads, 0, st>>>(n3, rf, ov.U + (int64_t)lvl * n3 * rf,
+                                             lists + t->lists.tgt_off[l], nt * C, C,
+                                             pf + level_offset(l, (int64_t)C * rf), nullptr,
+                                             F + level_offset(l, (int64_t)C * n3), ov.Kw,
+                                             (T)scale);
+      PB_LAUNCH("m2l_post");
+    }
     if (int rc_ = kt_end(t, st)) return rc_;
   }
   return PBBFMM_OK;

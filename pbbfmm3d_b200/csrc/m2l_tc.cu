@@ -33,6 +33,7 @@
 #include <cudaTypedefs.h>
 #include <cuda_fp16.h>
 
+#include <algorithm>
 #include <cstdlib>
 #include <mutex>
 
@@ -545,7 +546,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       x1 = x2;
       v2 = has_src(g + 2);
       if (F16 && g + 2 < nvalid) x2 = pexp[src_row(g + 2, v2)];
-      if (!mbar_wait(&s_accf[b], (g / NACC) & 1, s_abort)) {
+      // warp-uniform: the TMEM loads below are warp-collective
+      if (!__all_sync(0xffffffffu, mbar_wait(&s_accf[b], (g / NACC) & 1, s_abort))) {
         *s_abort = 1;
         break;
       }
@@ -816,5 +818,239 @@ int run_m2l_cheb_tc_level(pbbfmm_tree* t, int C, int l, int lvl, const float* pr
   if (rc) return rc;
   return kt_end(t, st);
 }
+
+// ------------------------------------------------------------------------
+// M2L pre / post transforms on the tensor cores, same split as the F16 M2L:
+//   Out[row_n][m] = alpha oscale[m] sum_k W[m][k] bscale[k] X[row_n][k],  m < M,
+// for the columns n < ncols, row_n = cells[n / C] * C + n % C (reference:
+// UpwardPass tail, include/compute.hpp:373-396, and the Moment2Local
+// post-transform, include/compute.hpp:881-914).  One CTA of 128 threads per
+// 128 columns; thread t owns column n = 128 blockIdx.x + t:
+//   A = its row of X (times bscale), scaled by its own power of two and split
+//       into F16 hi / lo, written to shared memory (SW128 K-major) one K chunk
+//       of 64 at a time;
+//   B = W (mp rows, pre-split with one exponent per level), by TMA;
+//   D[n][m] (128 lanes x mp columns, TMEM) accumulates three products per
+//       K step; thread t drains lane t, unscales and writes row_n of Out.
+// Chunks run one after another (one stage); two CTAs share an SM.  When
+// mp <= 128 each chunk's accumulator is drained into a register sum (the
+// tensor pipe's float32 accumulation loses about one ulp per step, so chains
+// stay 12 steps long); otherwise the chunks accumulate in TMEM.
+constexpr int CG_TC_THREADS = 128;
+
+template <bool BSCALE, bool OSCALE>
+__global__ void __launch_bounds__(CG_TC_THREADS)
+    k_colgemm_tc(int M, int mp, int K, int kp, const __grid_constant__ CUtensorMap tm_wh,
+                 const __grid_constant__ CUtensorMap tm_wl, int wrow0, int wexp,
+                 const int* __restrict__ cells, int ncols, int C, const float* __restrict__ X,
+                 const float* __restrict__ bscale, float* __restrict__ Out,
+                 const float* __restrict__ oscale, float alpha, int* __restrict__ err) {
+  extern __shared__ unsigned char smraw[];
+  unsigned char* base = smraw + ((1024 - (smem_u32(smraw) & 1023)) & 1023);
+  unsigned char* a_hi = base;
+  unsigned char* a_lo = base + 16384;
+  unsigned char* b_hi = base + 32768;
+  unsigned char* b_lo = b_hi + mp * 128;
+  __shared__ uint64_t s_tma, s_mma;
+  __shared__ uint32_t s_tmem;
+  __shared__ int s_fail;
+  const int tid = threadIdx.x, warp = tid >> 5;
+  const int n = blockIdx.x * CG_TC_THREADS + tid;
+  const bool valid = n < ncols;
+  const int64_t row = valid ? (int64_t)cells[n / C] * C + n % C : 0;
+  const float* xr = X + row * K;
+  // this column's exponent: max |bscale x| 2^e in [2^14, 2^15)
+  float mx = 0.f;
+  if (valid)
+    for (int k = 0; k < K; ++k) mx = fmaxf(mx, fabsf(BSCALE ? xr[k] * bscale[k] : xr[k]));
+  int e = 0;
+  if (mx > 0.f) {
+    int k2;
+    frexpf(mx, &k2);
+    e = 15 - k2;
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 256;\n" ::"r"(
+                     smem_u32(&s_tmem))
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
+  }
+  if (tid == 0) {
+    mbar_init(&s_tma, 1);
+    mbar_init(&s_mma, 1);
+    s_fail = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = s_tmem;
+  const uint32_t idesc = f16_idesc(TC_M, mp);
+  const int nchunks = kp / 64;
+  const bool rdrain = mp <= 128;  // uniform
+  const uint32_t lane_base = tmem + ((uint32_t)(32 * warp) << 16);
+  float racc[128];  // register sum of the drained chunks (rdrain)
+#pragma unroll
+  for (int i = 0; i < 128; ++i) racc[i] = 0.f;
+  int last_tma = -1;  // thread 0: the last chunk whose TMA was issued
+  for (int c = 0; c < nchunks; ++c) {
+    // A chunk: this column's 64 values (zero past K), scaled and split
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      uint32_t h[4], l[4];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        float v[2];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const int k = c * 64 + j * 8 + 2 * i + u;
+          v[u] = (valid && k < K) ? ldexpf(BSCALE ? xr[k] * bscale[k] : xr[k], e) : 0.f;
+        }
+        const __half2 vh = __floats2half2_rn(v[0], v[1]);
+        const float2 vf = __half22float2(vh);
+        const __half2 vl = __floats2half2_rn(v[0] - vf.x, v[1] - vf.y);
+        h[i] = *reinterpret_cast<const uint32_t*>(&vh);
+        l[i] = *reinterpret_cast<const uint32_t*>(&vl);
+      }
+      *reinterpret_cast<uint4*>(a_hi + sw128_off(tid, j)) = make_uint4(h[0], h[1], h[2], h[3]);
+      *reinterpret_cast<uint4*>(a_lo + sw128_off(tid, j)) = make_uint4(l[0], l[1], l[2], l[3]);
+    }
+    asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // to the tensor pipe
+    if (tid == 0) {
+      mbar_arrive_expect_tx(&s_tma, 2u * (uint32_t)mp * 128u);
+      tma_load_2d(b_hi, &tm_wh, c * 64, wrow0, &s_tma);
+      tma_load_2d(b_lo, &tm_wl, c * 64, wrow0, &s_tma);
+      last_tma = c;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      if (mbar_wait(&s_tma, c & 1, nullptr)) {
+        tc_fence_after();
+        const uint32_t ah = smem_u32(a_hi), al = smem_u32(a_lo);
+        const uint32_t bh = smem_u32(b_hi), bl = smem_u32(b_lo);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const uint32_t off = k * 32;
+          tc_mma_f16(tmem, sw128_desc(al + off), sw128_desc(bh + off), idesc,
+                     ((c > 0 && !rdrain) || k > 0) ? 1u : 0u);
+          tc_mma_f16(tmem, sw128_desc(ah + off), sw128_desc(bl + off), idesc, 1u);
+          tc_mma_f16(tmem, sw128_desc(ah + off), sw128_desc(bh + off), idesc, 1u);
+        }
+        tc_commit(&s_mma);
+      } else {
+        s_fail = 1;
+        mbar_arrive(&s_mma);  // release the others; the result is not used
+      }
+    }
+    // the chunk's MMAs (or the failure) before its shared memory is rewritten
+    if (!mbar_wait(&s_mma, c & 1, nullptr)) s_fail = 1;
+    __syncthreads();
+    if (s_fail) break;
+    if (rdrain) {
+      // all lanes (warp-collective loads); done before the next chunk's MMAs
+      // are issued (the barrier at the top of the next chunk orders them)
+      tc_fence_after();
+#pragma unroll
+      for (int q = 0; q < 8; ++q) {
+        if (q * 16 >= mp) break;
+        uint32_t r[16];
+        tc_ld16_wait(lane_base + (uint32_t)(q * 16), r);
+#pragma unroll
+        for (int i = 0; i < 16; ++i) racc[q * 16 + i] += __uint_as_float(r[i]);
+      }
+      tc_fence_before();
+    }
+  }
+  if (s_fail) {
+    // no copy or MMA may still be running when the CTA ends: wait (bounded)
+    // once more for the last chunk's
+    if (tid == 0 && last_tma >= 0) {
+      mbar_wait(&s_tma, last_tma & 1, nullptr);
+      mbar_wait(&s_mma, last_tma & 1, nullptr);
+    }
+    if (tid == 0) atomicExch(err, 1);
+  } else {
+    // every lane of the warp takes part in the (warp-collective) TMEM loads;
+    // only valid columns store
+    tc_fence_after();
+    // 2^-(e + wexp) as two exact powers of two (|e|, |wexp| < 170)
+    const float sc = alpha * ldexpf(1.f, -e) * ldexpf(1.f, -wexp);
+    float* o = valid ? Out + row * M : nullptr;
+    if (rdrain) {
+      if (o) {
+#pragma unroll
+        for (int m = 0; m < 128; ++m)
+          if (m < M) o[m] = racc[m] * sc * (OSCALE ? oscale[m] : 1.f);
+      }
+    } else {
+      for (int m0 = 0; m0 < mp; m0 += 16) {
+        uint32_t r[16];
+        tc_ld16_wait(lane_base + (uint32_t)m0, r);
+        if (o) {
+#pragma unroll
+          for (int i = 0; i < 16; ++i) {
+            const int m = m0 + i;
+            if (m < M) o[m] = __uint_as_float(r[i]) * sc * (OSCALE ? oscale[m] : 1.f);
+          }
+        }
+      }
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 0) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;\n" ::"r"(tmem)
+                 : "memory");
+  }
+}
+
+// Tensor cores when the output width fits one MMA (mp <= 256) and no TMEM
+// accumulation chain is longer than two K chunks (24 steps): either the
+// chunks are drained into registers (mp <= 128) or there are at most two
+// (K <= 128).  Longer chains would add ~1e-6 of accumulation error.
+bool colgemm_tc_eligible(const pbbfmm_tree* t, bool post) {
+  if (!t->p.use_chebyshev || !t->use_tc || t->ops.nlev > 32) return false;
+  const TcOps& o = t->tc;
+  const int mp = post ? o.u_mp : o.vt_mp, kp = post ? o.u_kp : o.vt_kp;
+  if (!(post ? o.uh : o.vth) || mp > 256) return false;
+  return mp <= 128 || kp <= 128;
+}
+
+int run_colgemm_tc(pbbfmm_tree* t, bool post, int lvl, const int* cells, int ncols, int C,
+                   const float* X, float* Out, float alpha, cudaStream_t st) {
+  if (ncols <= 0) return PBBFMM_OK;
+  const TcOps& o = t->tc;
+  const int M = post ? t->n3 : t->ops.rs, K = post ? t->ops.rf : t->n3;
+  const int mp = post ? o.u_mp : o.vt_mp, kp = post ? o.u_kp : o.vt_kp;
+  const uint16_t* wh = post ? o.uh : o.vth;
+  const uint16_t* wl = post ? o.ul : o.vtl;
+  const int wexp = post ? o.u_exp[lvl] : o.vt_exp[lvl];
+  CUtensorMap tm_h, tm_l;
+  const int64_t nrows = (int64_t)t->ops.nlev * mp;
+  if (int rc = operator_tensor_map(&tm_h, wh, true, mp, kp, nrows)) return rc;
+  if (int rc = operator_tensor_map(&tm_l, wl, true, mp, kp, nrows)) return rc;
+  // at least 78 KB, so that at most two CTAs share an SM: their 2 x 256 TMEM
+  // columns then always fit and no allocation waits for another CTA
+  const int smem = std::max(32768 + 2 * mp * 128 + 1024, 78 * 1024);
+  const unsigned grid = (unsigned)((ncols + CG_TC_THREADS - 1) / CG_TC_THREADS);
+  const float* Kw = t->f_Kw;
+  if (post) {
+    PB_CUDA(cudaFuncSetAttribute(k_colgemm_tc<false, true>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    k_colgemm_tc<false, true><<<grid, CG_TC_THREADS, smem, st>>>(
+        M, mp, K, kp, tm_h, tm_l, lvl * mp, wexp, cells, ncols, C, X, nullptr, Out, Kw, alpha,
+        t->d_tc_err);
+  } else {
+    PB_CUDA(cudaFuncSetAttribute(k_colgemm_tc<true, false>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    k_colgemm_tc<true, false><<<grid, CG_TC_THREADS, smem, st>>>(
+        M, mp, K, kp, tm_h, tm_l, lvl * mp, wexp, cells, ncols, C, X, Kw, Out, nullptr, alpha,
+        t->d_tc_err);
+  }
+  PB_LAUNCH(post ? "m2l_post_tc" : "m2l_pre_tc");
+  return PBBFMM_OK;
+}
+
 
 }  // namespace pbbfmm
