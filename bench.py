@@ -358,6 +358,11 @@ def per_step(kt, steps):
     return {k: v[0] / steps for k, v in kt.items() if v[1]}
 
 
+# DRAM bytes per (cell, frequency, column) of k_m2l_unif_mac<float>, from
+# the ncu capture in profiles/k_m2l_unif_mac_expcov0.3_unif5_N262144_C8_L5.md
+MAC_DRAM_BYTES_PER_UNIT = (852.425728e6 + 816.260608e6) / (32768 * 405 * 8)
+
+
 def unif_roofline(fmm, tree, wl, results, steps, local_rank):
     """Frequency-domain M2L (k_m2l_unif_mac): one complex MAC (8 flops) per
     (M2L pair, frequency, column); float32 FMA throughput bounds it."""
@@ -380,7 +385,15 @@ def unif_roofline(fmm, tree, wl, results, steps, local_rank):
     return {
         "kernel": "k_m2l_unif_mac<float> (frequency-domain M2L, mixed path)",
         "bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
-        "frac": achieved / fp32_peak, "traffic": None,
+        "frac": achieved / fp32_peak,
+        # DRAM bytes per step, scaled from one ncu capture of the same kernel
+        # (profiles/k_m2l_unif_mac_expcov0.3_unif5_N262144_C8_L5.md: 1.669 GB
+        # read + written for 32,768 cells x 405 frequencies x 8 columns, i.e.
+        # 15.7 B per (cell, frequency, column) against 16 B algorithmic)
+        "traffic": sum(nonempty.values()) * nk * C * MAC_DRAM_BYTES_PER_UNIT,
+        "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the level-5 "
+                          "launch of bench.py --workload profile, scaled per (cell, frequency, "
+                          "column); bytes per step",
         "peak_source": "measured in this run: float32 FMA loop on every SM "
                        "(pbbfmm_measure_fma_peak); the kernel runs on the CUDA cores, so neither "
                        "the HBM copy nor the bf16 tensor figure of MEASURED_PEAKS.json bounds it",

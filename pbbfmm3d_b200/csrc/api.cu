@@ -225,19 +225,22 @@ static void split_f16_rows(int nlev, int rows, int cols, int mp, int kp, At at,
 static int upload_tc_uvt(const double* U, const double* VT, int nlev, int n3, int rf, int rs,
                          TcOps* o) {
   if (nlev > 32) return PBBFMM_OK;  // more levels than the exponent tables: CUDA cores
-  o->vt_mp = (rs + 15) / 16 * 16;
+  // rows padded to 16, or to 32 above 256 (two MMAs of mp / 2, each a
+  // multiple of 16)
+  auto pad_rows = [](int r) { return r <= 256 ? (r + 15) / 16 * 16 : (r + 31) / 32 * 32; };
+  o->vt_mp = pad_rows(rs);
   o->vt_kp = (n3 + 63) / 64 * 64;
-  o->u_mp = (n3 + 15) / 16 * 16;
+  o->u_mp = pad_rows(n3);
   o->u_kp = (rf + 63) / 64 * 64;
   std::vector<uint16_t> h, l;
   int rc;
-  if (o->vt_mp <= 256) {
+  if (o->vt_mp <= 512) {
     split_f16_rows(nlev, rs, n3, o->vt_mp, o->vt_kp,
                    [&](int lv, int m, int k) { return VT[(size_t)lv * rs * n3 + m + (size_t)rs * k]; },
                    &h, &l, o->vt_exp);
     if ((rc = upload_vec(&o->vth, h)) || (rc = upload_vec(&o->vtl, l))) return rc;
   }
-  if (o->u_mp <= 256) {
+  if (o->u_mp <= 512) {
     split_f16_rows(nlev, n3, rf, o->u_mp, o->u_kp,
                    [&](int lv, int m, int k) { return U[(size_t)lv * n3 * rf + m + (size_t)n3 * k]; },
                    &h, &l, o->u_exp);

@@ -81,8 +81,9 @@ struct TcOps {
   int np = 0, kp = 0, kp16 = 0;
   // M2L pre / post transforms on the tensor cores: W = VT (rs x n^3) and
   // U (n^3 x r_f) as [level][mp][kp] F16 hi / lo rows (row m holds W[m][k]
-  // over k, zero padded; mp = rows padded to 16, kp = K padded to 64), each
-  // level's matrix scaled by 2^exp[level].  Null when mp exceeds 256.
+  // over k, zero padded; mp = rows padded to 16 (32 above 256), kp = K
+  // padded to 64), each level's matrix scaled by 2^exp[level].  Null when mp
+  // exceeds 512.
   uint16_t *vth = nullptr, *vtl = nullptr, *uh = nullptr, *ul = nullptr;
   int vt_mp = 0, vt_kp = 0, u_mp = 0, u_kp = 0;
   int vt_exp[32] = {}, u_exp[32] = {};

@@ -832,7 +832,9 @@ int run_m2l_cheb_tc_level(pbbfmm_tree* t, int C, int l, int lvl, const float* pr
 //   B = W (mp rows, pre-split with one exponent per level), by TMA;
 //   D[n][m] (128 lanes x mp columns, TMEM) accumulates three products per
 //       K step; thread t drains lane t, unscales and writes row_n of Out.
-// Chunks run one after another (one stage); two CTAs share an SM.  When
+// Chunks run one after another (one stage); two CTAs share an SM (one when
+// mp > 256: then each product is two MMAs of N = mp / 2 and the CTA holds all
+// 512 TMEM columns).  When
 // mp <= 128 each chunk's accumulator is drained into a register sum (the
 // tensor pipe's float32 accumulation loses about one ulp per step, so chains
 // stay 12 steps long); otherwise the chunks accumulate in TMEM.
@@ -847,6 +849,9 @@ __global__ void __launch_bounds__(CG_TC_THREADS)
                  const float* __restrict__ oscale, float alpha, int* __restrict__ err) {
   extern __shared__ unsigned char smraw[];
   unsigned char* base = smraw + ((1024 - (smem_u32(smraw) & 1023)) & 1023);
+  const int nh = mp > 256 ? 2 : 1;             // MMAs (and TMA boxes) per product
+  const int hn = mp / nh;                      // their N (a multiple of 16)
+  const uint32_t tcols = mp > 256 ? 512 : 256;  // TMEM columns
   unsigned char* a_hi = base;
   unsigned char* a_lo = base + 16384;
   unsigned char* b_hi = base + 32768;
@@ -870,8 +875,9 @@ __global__ void __launch_bounds__(CG_TC_THREADS)
     e = 15 - k2;
   }
   if (warp == 0) {
-    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], 256;\n" ::"r"(
-                     smem_u32(&s_tmem))
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
+                     smem_u32(&s_tmem)),
+                 "r"(tcols)
                  : "memory");
     asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::: "memory");
   }
@@ -885,7 +891,7 @@ __global__ void __launch_bounds__(CG_TC_THREADS)
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = s_tmem;
-  const uint32_t idesc = f16_idesc(TC_M, mp);
+  const uint32_t idesc = f16_idesc(TC_M, hn);
   const int nchunks = kp / 64;
   const bool rdrain = mp <= 128;  // uniform
   const uint32_t lane_base = tmem + ((uint32_t)(32 * warp) << 16);
@@ -918,8 +924,10 @@ __global__ void __launch_bounds__(CG_TC_THREADS)
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");  // to the tensor pipe
     if (tid == 0) {
       mbar_arrive_expect_tx(&s_tma, 2u * (uint32_t)mp * 128u);
-      tma_load_2d(b_hi, &tm_wh, c * 64, wrow0, &s_tma);
-      tma_load_2d(b_lo, &tm_wl, c * 64, wrow0, &s_tma);
+      for (int h = 0; h < nh; ++h) {  // boxes of hn rows
+        tma_load_2d(b_hi + h * hn * 128, &tm_wh, c * 64, wrow0 + h * hn, &s_tma);
+        tma_load_2d(b_lo + h * hn * 128, &tm_wl, c * 64, wrow0 + h * hn, &s_tma);
+      }
       last_tma = c;
     }
     __syncthreads();
@@ -928,13 +936,16 @@ __global__ void __launch_bounds__(CG_TC_THREADS)
         tc_fence_after();
         const uint32_t ah = smem_u32(a_hi), al = smem_u32(a_lo);
         const uint32_t bh = smem_u32(b_hi), bl = smem_u32(b_lo);
+        for (int h = 0; h < nh; ++h) {  // D columns [h hn, (h + 1) hn)
+          const uint32_t d = tmem + (uint32_t)(h * hn), bo = (uint32_t)(h * hn * 128);
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          const uint32_t off = k * 32;
-          tc_mma_f16(tmem, sw128_desc(al + off), sw128_desc(bh + off), idesc,
-                     ((c > 0 && !rdrain) || k > 0) ? 1u : 0u);
-          tc_mma_f16(tmem, sw128_desc(ah + off), sw128_desc(bl + off), idesc, 1u);
-          tc_mma_f16(tmem, sw128_desc(ah + off), sw128_desc(bh + off), idesc, 1u);
+          for (int k = 0; k < 4; ++k) {
+            const uint32_t off = k * 32;
+            tc_mma_f16(d, sw128_desc(al + off), sw128_desc(bh + bo + off), idesc,
+                       ((c > 0 && !rdrain) || k > 0) ? 1u : 0u);
+            tc_mma_f16(d, sw128_desc(ah + off), sw128_desc(bl + bo + off), idesc, 1u);
+            tc_mma_f16(d, sw128_desc(ah + off), sw128_desc(bh + bo + off), idesc, 1u);
+          }
         }
         tc_commit(&s_mma);
       } else {
@@ -1000,12 +1011,13 @@ __global__ void __launch_bounds__(CG_TC_THREADS)
   __syncthreads();
   if (warp == 0) {
     tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, 256;\n" ::"r"(tmem)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem),
+                 "r"(tcols)
                  : "memory");
   }
 }
 
-// Tensor cores when the output width fits one MMA (mp <= 256) and no TMEM
+// Tensor cores when the output width fits two MMAs (mp <= 512) and no TMEM
 // accumulation chain is longer than two K chunks (24 steps): either the
 // chunks are drained into registers (mp <= 128) or there are at most two
 // (K <= 128).  Longer chains would add ~1e-6 of accumulation error.
@@ -1013,7 +1025,7 @@ bool colgemm_tc_eligible(const pbbfmm_tree* t, bool post) {
   if (!t->p.use_chebyshev || !t->use_tc || t->ops.nlev > 32) return false;
   const TcOps& o = t->tc;
   const int mp = post ? o.u_mp : o.vt_mp, kp = post ? o.u_kp : o.vt_kp;
-  if (!(post ? o.uh : o.vth) || mp > 256) return false;
+  if (!(post ? o.uh : o.vth) || mp > 512) return false;
   return mp <= 128 || kp <= 128;
 }
 
@@ -1028,11 +1040,13 @@ int run_colgemm_tc(pbbfmm_tree* t, bool post, int lvl, const int* cells, int nco
   const int wexp = post ? o.u_exp[lvl] : o.vt_exp[lvl];
   CUtensorMap tm_h, tm_l;
   const int64_t nrows = (int64_t)t->ops.nlev * mp;
-  if (int rc = operator_tensor_map(&tm_h, wh, true, mp, kp, nrows)) return rc;
-  if (int rc = operator_tensor_map(&tm_l, wl, true, mp, kp, nrows)) return rc;
-  // at least 78 KB, so that at most two CTAs share an SM: their 2 x 256 TMEM
-  // columns then always fit and no allocation waits for another CTA
-  const int smem = std::max(32768 + 2 * mp * 128 + 1024, 78 * 1024);
+  const int hn = mp > 256 ? mp / 2 : mp;  // rows per TMA box
+  if (int rc = operator_tensor_map(&tm_h, wh, true, hn, kp, nrows)) return rc;
+  if (int rc = operator_tensor_map(&tm_l, wl, true, hn, kp, nrows)) return rc;
+  // at least 78 KB (114 KB when a CTA takes all 512 TMEM columns), so that
+  // the CTAs sharing an SM always find their TMEM columns free and no
+  // allocation waits for another CTA
+  const int smem = std::max(32768 + 2 * mp * 128 + 1024, (mp > 256 ? 114 : 78) * 1024);
   const unsigned grid = (unsigned)((ncols + CG_TC_THREADS - 1) / CG_TC_THREADS);
   const float* Kw = t->f_Kw;
   if (post) {

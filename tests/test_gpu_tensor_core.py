@@ -53,6 +53,7 @@ CASES = [
     ("Laplacian", 0.0, 3, 4, 1e-5, 64, False),   # two targets per tile
     ("Laplacian", 0.0, 3, 7, 1e-9, 1, False),    # r_f near 256: two stages, N up to 256
     ("Laplacian", 0.0, 3, 6, 1e-8, 1, False),    # r_f 150: running sum in TMEM
+    ("Laplacian", 0.0, 3, 7, 1e-7, 1, False),    # n^3 = 343: post-transform as two MMAs
 ]
 
 
