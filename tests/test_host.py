@@ -131,3 +131,26 @@ def test_bad_arguments_return_status():
         _lib.check(
             _lib.lib().pbbfmm_tree_set_operators(t._h, 27, 27, 5, fmm._dp(z), fmm._dp(z), fmm._dp(z)))
     assert e.value.code == _lib.ERR_ARG
+
+
+def test_tensor_core_mode_switch_on_host_tree():
+    """pbbfmm_set_tensor_cores takes PBBFMM_TC_OFF / _F16 / _TF32 (1 still
+    means on) and refuses other values; a host-only tree has no tensor-core
+    operators, so the query reports the CUDA-core path."""
+    t = fmm.kernel_Laplacian(1.0, 3, 4, 1e-5, 1, device=-1)
+    t.buildFMMTree()
+    L = _lib.lib()
+    for mode in (_lib.TC_OFF, _lib.TC_F16, _lib.TC_TF32, 1):
+        assert L.pbbfmm_set_tensor_cores(t._h, mode) == _lib.OK
+    for mode in (-1, 3, 7):
+        assert L.pbbfmm_set_tensor_cores(t._h, mode) == _lib.ERR_ARG
+    t.set_tensor_cores(True, "tf32")
+    t.set_tensor_cores(True, "f16")
+    with pytest.raises(ValueError):
+        t.set_tensor_cores(True, "bf16")
+    assert not t.tensor_core_m2l() and t.tensor_core_format() is None
+    # the header's constants are the binding's
+    hdr = open(os.path.join(os.path.dirname(__file__), "..", "include", "pbbfmm3d_b200.h")).read()
+    for name, val in (("PBBFMM_TC_OFF", _lib.TC_OFF), ("PBBFMM_TC_F16", _lib.TC_F16),
+                      ("PBBFMM_TC_TF32", _lib.TC_TF32)):
+        assert "#define %s %d" % (name, val) in hdr
