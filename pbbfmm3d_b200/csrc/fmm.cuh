@@ -44,7 +44,7 @@ struct Workspace {
   DevBuf proxy;  // Cheb: sum_l 8^l * C * rs ;  Unif: spectra sum_l 8^l * nk * C (complex)
   DevBuf pf;     // Cheb: sum_l 8^l * C * rf ;  Unif: accumulated spectra
   DevBuf halo;   // Unif M2L: per parent block 512 halo + 64 target cells
-  DevBuf tc_proxy;  // tensor-core Cheb M2L: TF32 hi then lo proxies of one level
+  DevBuf tc_proxy;  // tensor-core Cheb M2L: hi then lo proxies of one level (+ F16 exponents)
   DevBuf leafpart;  // leaf phase: target leaves partitioned dense-first, then their count
   // staging for the host-pointer entry point
   DevBuf io_tgt, io_src, io_w, io_out;

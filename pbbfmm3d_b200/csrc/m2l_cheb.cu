@@ -303,7 +303,7 @@ static int run_m2l_cheb_t(pbbfmm_tree* t, int C, cudaStream_t st) {
     const int lvl = t->homog ? 0 : l - 2;
     const int nt = t->lists.ntgt[l];
     if (nt == 0) continue;
-    bool on_tc = false;  // float path: tcgen05 3xTF32 kernel when rf fits TMEM
+    bool on_tc = false;  // float path: the tcgen05 kernel (split F16 or TF32) when rf fits TMEM
     if constexpr (std::is_same<T, float>::value) {
       if (tc_eligible(t)) {
         if (int rc_ = run_m2l_cheb_tc_level(t, C, l, lvl, proxy + level_offset(l, (int64_t)C * rs),
