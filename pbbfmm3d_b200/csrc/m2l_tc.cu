@@ -841,7 +841,7 @@ int run_m2l_cheb_tc_level(pbbfmm_tree* t, int C, int l, int lvl, const float* pr
 constexpr int CG_TC_THREADS = 128;
 
 template <bool BSCALE, bool OSCALE>
-__global__ void __launch_bounds__(CG_TC_THREADS)
+__global__ void __launch_bounds__(CG_TC_THREADS, 1)
     k_colgemm_tc(int M, int mp, int K, int kp, const __grid_constant__ CUtensorMap tm_wh,
                  const __grid_constant__ CUtensorMap tm_wl, int wrow0, int wexp,
                  const int* __restrict__ cells, int ncols, int C, const float* __restrict__ X,
@@ -864,10 +864,27 @@ __global__ void __launch_bounds__(CG_TC_THREADS)
   const bool valid = n < ncols;
   const int64_t row = valid ? (int64_t)cells[n / C] * C + n % C : 0;
   const float* xr = X + row * K;
+  // 16-byte loads when rows (K floats, from 16-byte aligned level bases) are
+  // 16-byte aligned
+  const bool vec4 = (K & 3) == 0;
   // this column's exponent: max |bscale x| 2^e in [2^14, 2^15)
   float mx = 0.f;
-  if (valid)
-    for (int k = 0; k < K; ++k) mx = fmaxf(mx, fabsf(BSCALE ? xr[k] * bscale[k] : xr[k]));
+  if (valid) {
+    if (vec4) {
+      const float4* x4 = reinterpret_cast<const float4*>(xr);
+#pragma unroll 4
+      for (int k4 = 0; k4 < K / 4; ++k4) {
+        float4 v = x4[k4];
+        if (BSCALE) {
+          const float4 b = reinterpret_cast<const float4*>(bscale)[k4];
+          v.x *= b.x, v.y *= b.y, v.z *= b.z, v.w *= b.w;
+        }
+        mx = fmaxf(mx, fmaxf(fmaxf(fabsf(v.x), fabsf(v.y)), fmaxf(fabsf(v.z), fabsf(v.w))));
+      }
+    } else {
+      for (int k = 0; k < K; ++k) mx = fmaxf(mx, fabsf(BSCALE ? xr[k] * bscale[k] : xr[k]));
+    }
+  }
   int e = 0;
   if (mx > 0.f) {
     int k2;
@@ -904,14 +921,33 @@ __global__ void __launch_bounds__(CG_TC_THREADS)
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
       uint32_t h[4], l[4];
+      float v8[8];
+      const int kb = c * 64 + j * 8;
+      if (vec4) {  // two 16-byte loads; a block of 4 lies wholly below or above K
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+          const int k = kb + 4 * q;
+          float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
+          if (valid && k < K) {
+            x = *reinterpret_cast<const float4*>(xr + k);
+            if (BSCALE) {
+              const float4 b = *reinterpret_cast<const float4*>(bscale + k);
+              x.x *= b.x, x.y *= b.y, x.z *= b.z, x.w *= b.w;
+            }
+          }
+          v8[4 * q] = ldexpf(x.x, e), v8[4 * q + 1] = ldexpf(x.y, e);
+          v8[4 * q + 2] = ldexpf(x.z, e), v8[4 * q + 3] = ldexpf(x.w, e);
+        }
+      } else {
+#pragma unroll
+        for (int u = 0; u < 8; ++u) {
+          const int k = kb + u;
+          v8[u] = (valid && k < K) ? ldexpf(BSCALE ? xr[k] * bscale[k] : xr[k], e) : 0.f;
+        }
+      }
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
-        float v[2];
-#pragma unroll
-        for (int u = 0; u < 2; ++u) {
-          const int k = c * 64 + j * 8 + 2 * i + u;
-          v[u] = (valid && k < K) ? ldexpf(BSCALE ? xr[k] * bscale[k] : xr[k], e) : 0.f;
-        }
+        const float v[2] = {v8[2 * i], v8[2 * i + 1]};
         const __half2 vh = __floats2half2_rn(v[0], v[1]);
         const float2 vf = __half22float2(vh);
         const __half2 vl = __floats2half2_rn(v[0] - vf.x, v[1] - vf.y);
