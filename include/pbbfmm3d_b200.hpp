@@ -63,6 +63,10 @@ class H2_3D_Tree {
   void buildFMMTree(const char* cache_dir = nullptr) { check(pbbfmm_tree_build(h_, cache_dir)); }
   // PBBFMM_PREC_FP64 (default) or PBBFMM_PREC_MIXED.
   void set_precision(int precision) { check(pbbfmm_set_precision(h_, precision)); }
+  // Mixed Chebyshev M2L operands: PBBFMM_TC_F16 (default), PBBFMM_TC_TF32, or
+  // PBBFMM_TC_OFF for the CUDA cores; tensor_core_m2l() reports the one in use.
+  void set_tensor_cores(int mode) { check(pbbfmm_set_tensor_cores(h_, mode)); }
+  int tensor_core_m2l() const { return pbbfmm_tensor_core_m2l(h_); }
   pbbfmm_tree* handle() const { return h_; }
 
  private:

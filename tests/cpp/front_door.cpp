@@ -59,6 +59,12 @@ int main(int argc, char** argv) {
     for (auto& v : w1) v = u(rng) + 0.5;
     fmm::H2_3D_Compute(t1, pts, pts, w1, 1, o1);
     const double e1 = direct_rel_err(pts, pts, w1, 1, o1, lap);
+    // the same tree in mixed precision: Chebyshev M2L on the tensor cores
+    t1.set_precision(PBBFMM_PREC_MIXED);
+    const bool on_tc = t1.tensor_core_m2l() == PBBFMM_TC_F16;
+    std::vector<double> o1m(N, 0.0);
+    fmm::H2_3D_Compute(t1, pts, pts, w1, 1, o1m);
+    const double e1m = direct_rel_err(pts, pts, w1, 1, o1m, lap);
     // exp(-r/0.3), uniform interpolation with FFT M2L, mixed precision, 3 columns
     fmm::kernel_ExpCov t2(1.0, 4, 5, 1e-5, 0, 0.3);
     t2.buildFMMTree();
@@ -74,9 +80,11 @@ int main(int argc, char** argv) {
     } catch (const fmm::Error& e) {
       threw = e.status == PBBFMM_ERR_ARG;
     }
-    std::printf("laplace_cheb rel %.3e  expcov_unif_mixed rel %.3e  bad-args threw %d\n", e1, e2,
-                (int)threw);
-    if (e1 < 1e-4 && e2 < 1e-4 && threw) {
+    std::printf(
+        "laplace_cheb rel %.3e  laplace_cheb_mixed (tensor cores %d) rel %.3e  "
+        "expcov_unif_mixed rel %.3e  bad-args threw %d\n",
+        e1, (int)on_tc, e1m, e2, (int)threw);
+    if (e1 < 1e-4 && on_tc && e1m < 1e-4 && e2 < 1e-4 && threw) {
       std::printf("OK\n");
       return 0;
     }
