@@ -154,3 +154,20 @@ def test_tensor_core_mode_switch_on_host_tree():
     for name, val in (("PBBFMM_TC_OFF", _lib.TC_OFF), ("PBBFMM_TC_F16", _lib.TC_F16),
                       ("PBBFMM_TC_TF32", _lib.TC_TF32)):
         assert "#define %s %d" % (name, val) in hdr
+
+
+def test_operator_cache_failures_return_io_status(tmp_path):
+    """The reference exits on operator-file errors (H2_3D_Tree.hpp READ_CHECK);
+    here they are statuses: an unwritable cache directory and a truncated
+    cache file both give PBBFMM_ERR_IO, and the tree stays usable."""
+    t = fmm.kernel_Laplacian(1.0, 3, 3, 1e-4, 1, device=-1)
+    with pytest.raises(fmm.FMMError) as e:
+        t.buildFMMTree(str(tmp_path / "missing" / "dir"))
+    assert e.value.code == _lib.ERR_IO
+    (tmp_path / "LaplacianChebK3.bin").write_bytes(b"\x00\x01")  # truncated
+    t2 = fmm.kernel_Laplacian(1.0, 3, 3, 1e-4, 1, device=-1)
+    with pytest.raises(fmm.FMMError) as e:
+        t2.buildFMMTree(str(tmp_path))
+    assert e.value.code == _lib.ERR_IO
+    t2.buildFMMTree()  # without the cache: computed
+    assert t2.get_operators()["rf"] > 0
