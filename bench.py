@@ -22,8 +22,10 @@ One JSON line on rank 0.  Multi-GPU (torchrun): every rank runs its own
 matvec over its own block of 8 right-hand sides on the same points (columns
 are independent; no data-path collective), weak scaling, value = all ranks'
 N*nCols / max-over-ranks time.  ``--impl reference`` times the reference's own
-CPU code (oracle/_ref, built from the reference sources) on a bounded sample of
-the same workload with every host core.
+CPU code (oracle/_ref, built from the reference sources) with every host core,
+each step on one octant of the workload (N = 125,000 at tree_level 5: the same
+points per leaf, kernel, order and columns); ``--reference-full`` adds one run
+on the whole workload for comparison.
 """
 from __future__ import annotations
 
@@ -68,8 +70,12 @@ WORKLOADS = {
 }
 KERNEL_TEXT = {"ExpCov": "exp(-r/%g)", "Laplacian": "1/r (0 at r=0)",
                "GaussSigma": "exp(-r^2/(2*%g^2))"}
-# bounded CPU sample: same kernel, order, columns and points per leaf (N / 8^L)
-CPU_SAMPLE = dict(N=15_625, L=4)
+# bounded CPU sample of the workload: one octant of it -- the same kernel,
+# order, columns and points per leaf (N / 8^L), one level less.  Its
+# throughput on the reference's CPU code is within about 20 % of the full
+# workload's (measured: 67k vs 80k N*nCols/s on 8 cores), while a sample as
+# small as N = 15,625 at L = 4 runs 3x faster per point (it fits in cache).
+CPU_SAMPLE = dict(N=125_000, L=5)
 N_SAMPLED_TARGETS = 4096
 METRIC = "FMM matvec N*nCols/s (rel-L2 vs FP64 direct sum on 4096 sampled targets)"
 
@@ -248,19 +254,27 @@ def load_peaks():
 
 
 # ------------------------------------------------------------ reference arm
-def cpu_sample_run(wl, steps, warmup, threads):
-    """Time the reference's own CPU matvec (oracle/_ref) on the bounded sample."""
+def cpu_sample_run(wl, steps, warmup, threads, full=False):
+    """Time the reference's own CPU matvec (oracle/_ref) on the bounded sample
+    (full=True: on the whole workload)."""
     import oracle
 
     rng = np.random.default_rng(wl["seed"])
-    Ns = CPU_SAMPLE["N"]
+    Ns, L = (wl["N"], wl["L"]) if full else (CPU_SAMPLE["N"], CPU_SAMPLE["L"])
     pts = rng.uniform(0.0, 1.0, (Ns, 3))
     w = rng.standard_normal(Ns * wl["C"])
-    out, timing, wd = oracle.run_reference(wl["kernel"], wl["param"], wl["box"], CPU_SAMPLE["L"],
+    out, timing, wd = oracle.run_reference(wl["kernel"], wl["param"], wl["box"], L,
                                            wl["n"], wl["eps"], wl["cheb"], pts, w, wl["C"],
                                            repeat=warmup + steps, threads=threads)
     times = timing["matvec_s"][warmup:]
     return Ns * wl["C"] / (sum(times) / len(times)), times, timing["threads"]
+
+
+def workload_config(wl):
+    """The workload as both arms name it (the bench line's "config")."""
+    return {"workload": wl["name"], "N": wl["N"], "nCols": wl["C"], "tree_level": wl["L"],
+            "interpolation_order": wl["n"], "use_chebyshev": wl["cheb"], "epsilon": wl["eps"],
+            "kernel": kernel_text(wl), "points": wl["dist"]}
 
 
 def reference_arm(args, rank):
@@ -268,10 +282,10 @@ def reference_arm(args, rank):
         return 0
     wl = WORKLOADS[args.workload]
     threads = os.cpu_count() or 1
-    sample = ("reference CPU H2_3D_Compute (oracle/_ref, built from the reference sources) on "
-              "N=%d points at tree_level %d (same %.2f points/leaf, kernel, order, nCols as the "
-              "workload); per-step time of the ctor" % (CPU_SAMPLE["N"], CPU_SAMPLE["L"],
-                                                         wl["N"] / 8 ** wl["L"]))
+    sample = ("each step one reference CPU H2_3D_Compute (oracle/_ref, built from the reference "
+              "sources; the ctor timed) on one octant of the workload: N=%d points at tree_level "
+              "%d, the same %.2f points/leaf, kernel, order and nCols" % (
+                  CPU_SAMPLE["N"], CPU_SAMPLE["L"], wl["N"] / 8 ** wl["L"]))
     try:
         value, times, th = cpu_sample_run(wl, args.steps, args.warmup, threads)
     except Exception as e:  # noqa: BLE001
@@ -283,14 +297,19 @@ def reference_arm(args, rank):
         "unit": "N*nCols/s", "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded uniform points, N(0,1) weights)",
-        "config": {"workload": wl["name"], "sample_N": CPU_SAMPLE["N"],
-                   "sample_tree_level": CPU_SAMPLE["L"], "kernel": kernel_text(wl),
-                   "interpolation_order": wl["n"], "use_chebyshev": wl["cheb"], "nCols": wl["C"]},
+        "config": workload_config(wl),
+        "sample_config": {"N": CPU_SAMPLE["N"], "tree_level": CPU_SAMPLE["L"]},
         "cpu_baseline": {"value": value, "unit": "N*nCols/s", "cores": th, "kind": "reference",
                          "sample": sample},
         "e2e": {"value": value, "unit": "N*nCols/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
+    if args.reference_full:
+        # one run of the reference on the whole workload, for comparison with
+        # the sample's throughput (not part of value)
+        v_full, t_full, _ = cpu_sample_run(wl, 1, 0, threads, full=True)
+        line["full_config_check"] = {"value": v_full, "unit": "N*nCols/s", "ms": 1e3 * t_full[0],
+                                     "N": wl["N"], "tree_level": wl["L"]}
     print(json.dumps(line))
     return 0
 
@@ -514,18 +533,16 @@ def run_workload(wl, args, rank, world, local_rank, e2e_wanted):
         "roofline": roof, "e2e": e2e,
         "gpu_launches": int(r["launches"]), "gpu_launches_per_step": r["launches"] / args.steps,
         "clocks": r["clocks"],
-        "config": {"workload": wl["name"], "N": N, "nCols": C, "tree_level": wl["L"],
-                   "interpolation_order": wl["n"], "use_chebyshev": wl["cheb"],
-                   "epsilon": wl["eps"], "kernel": kernel_text(wl), "points": wl["dist"],
-                   "precision": "mixed: float32 interpolation and near field with compensated "
+        "config": workload_config(wl),
+        "precision_detail": ("mixed: float32 interpolation and near field with compensated "
                                 "sums, %s, float64 positions, operators and output" % (
                                     {"f16": "tensor-core M2L with scaled F16 hi/lo operands "
                                              "(3 products, float32 accumulation)",
                                      "tf32": "3xTF32 tensor-core M2L"}.get(
                                         tree.tensor_core_format(), "float32 CUDA-core M2L")
-                                    if wl["cheb"] else "float32 FFT M2L"),
-                   "l2": "256 MB buffer written between timed steps",
-                   "parallelism": "independent column blocks per rank" if world > 1 else "1 GPU"},
+                                    if wl["cheb"] else "float32 FFT M2L")),
+        "l2_flush": "256 MB buffer written between timed steps",
+        "parallelism": "independent column blocks per rank" if world > 1 else "1 GPU",
     }
     tree.close()
     return out
@@ -645,7 +662,8 @@ def our_arm(args, rank, world, local_rank):
         # (the order at which the FMM itself meets rel-L2 1e-6)
         for key, wname in (("target_config", "clustered"), ("target_config_order7", "clustered7")):
             t = run_workload(WORKLOADS[wname], args, rank, world, local_rank, False)
-            blk = {k: t[k] for k in ("config", "value", "ms_per_step", "rel_l2_err", "fp64",
+            blk = {k: t[k] for k in ("config", "precision_detail", "value", "ms_per_step",
+                                     "rel_l2_err", "fp64",
                                      "mixed_over_fp64", "phase_ms_per_step", "dominant_kernel",
                                      "roofline", "gpu_launches_per_step", "clocks")}
             blk["unit"] = "N*nCols/s"
@@ -656,10 +674,11 @@ def our_arm(args, rank, world, local_rank):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            v, times, th = cpu_sample_run(wl, 6, 1, os.cpu_count() or 1)
+            v, times, th = cpu_sample_run(wl, 2, 1, os.cpu_count() or 1)
             cpu = {"value": v, "unit": "N*nCols/s", "cores": th, "kind": "reference",
-                   "sample": "reference CPU H2_3D_Compute (oracle/_ref) on N=%d at tree_level %d "
-                             "(same points/leaf, kernel, order, nCols); mean of 6 runs %.2fs" % (
+                   "sample": "reference CPU H2_3D_Compute (oracle/_ref) on one octant of the "
+                             "workload, N=%d at tree_level %d (same points/leaf, kernel, order, "
+                             "nCols); mean of 2 runs after 1, %.2fs each" % (
                                  CPU_SAMPLE["N"], CPU_SAMPLE["L"], sum(times) / len(times))}
         except Exception as e:  # noqa: BLE001
             cpu = {"value": None, "unit": "N*nCols/s", "cores": 0, "kind": "reference",
@@ -674,6 +693,8 @@ def our_arm(args, rank, world, local_rank):
         "data": "synthetic: seeded %s points in the unit cube, %s weights" % (
             wl["dist"], "N(0,1)" if wl["weights"] == "normal" else "U[-1,1]"),
         "config": head["config"],
+        "precision_detail": head["precision_detail"], "l2_flush": head["l2_flush"],
+        "parallelism": head["parallelism"],
         "rel_l2_err": head["rel_l2_err"], "fp64": head["fp64"],
         "mixed_over_fp64": head["mixed_over_fp64"],
         "phase_ms_per_step": head["phase_ms_per_step"],
@@ -705,6 +726,8 @@ def main():
     ap.add_argument("--no-target", action="store_true",
                     help="skip the clustered Chebyshev (tensor-core) workload block")
     ap.add_argument("--workload", default="bench", choices=sorted(WORKLOADS))
+    ap.add_argument("--reference-full", action="store_true",
+                    help="reference arm: also time one run on the whole workload")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))

@@ -80,6 +80,67 @@ typedef struct {
  * accessors work without a GPU, computes return PBBFMM_ERR_STATE. */
 int pbbfmm_tree_create(const pbbfmm_tree_params *params, int device, pbbfmm_tree **tree);
 
+/* ---- user-defined kernels ----
+ * The reference's user kernels subclass H2_3D_Tree and define
+ * SetKernelProperty (homogen, symmetry, kernelType) and
+ * EvaluateKernel(target, source) (README.md:178-227, include/H2_3D_Tree.hpp:
+ * 93-95).  Here a user kernel is a __device__ functor compiled by the user's
+ * nvcc: include/pbbfmm3d_b200_kernel.cuh turns a class with a
+ * __host__ __device__ EvaluateKernel into a pbbfmm_user_kernel whose
+ * launch_leaf instantiates this library's leaf kernels (L2P + P2P,
+ * include/pbbfmm3d_b200_leaf.cuh) for it.  Everything else in a compute is
+ * kernel-independent once the operators exist. */
+
+/* Everything the leaf-phase kernels read, prepared by the library for one
+ * compute (device pointers unless noted). */
+typedef struct {
+  int precision;             /* PBBFMM_PREC_FP64: F_leaf / Tkz are double; MIXED: float */
+  int gradient;              /* 0: potentials (L2P + P2P);  1: potentials and gradients */
+  const int *leaves;         /* nonempty target leaves (values: dense ones first) */
+  int nleaves;
+  const int *ndense;         /* values: number of dense leaves (device scalar) */
+  const int *chunk_prefix;   /* values: first 32-target chunk of each dense leaf */
+  int64_t max_chunks;        /* values: upper bound of the dense chunks (host) */
+  const int *tstart, *sstart;  /* leaf offsets of the sorted targets / sources */
+  const int *tperm;            /* sorted target -> original index */
+  const double *tpos, *spos;   /* recentred sorted positions, SoA 3 x N */
+  const double *wsorted;       /* sorted weights, point-major [j][col] */
+  int Nf, Ns, C;
+  const void *F_leaf;        /* leaf-level local coefficients [cell][col][n^3] */
+  int n, cheb;               /* interpolation order, 1 = Chebyshev */
+  const void *Tkz;           /* Chebyshev polynomial table n x n */
+  double box;                /* side of the computational box (host) */
+  int L;                     /* tree level (host) */
+  const double *kparam;      /* 4 kernel parameters */
+  double *out;               /* output [col * Nf + i] += potentials (may be NULL in gradient mode) */
+  const double *contract;    /* gradient: weights of each target's gradient [col * Nf + i] */
+  double *grad_out;          /* gradient: [i * 3 + d] += sum_col contract * d phi / d x_d */
+} pbbfmm_leaf_args;
+
+typedef struct {
+  const char *kernel_type; /* kernelType: names the operator-cache files */
+  double homogen;          /* degree of homogeneity as SetKernelProperty sets it (0: none) */
+  int symmetry;            /* 1 symmetric, -1 antisymmetric, 0 neither */
+  /* EvaluateKernel(target, source) in float64 on the host: the operator
+   * precompute (src/H2_3D_Tree.cpp:251-648) */
+  double (*evaluate)(const double *target, const double *source, void *ctx);
+  /* the leaf kernels instantiated for the device functor, launched on
+   * `stream` (a cudaStream_t): 0, a cudaError_t code, or -1 when a gradient
+   * pass is asked of a kernel without a gradient */
+  int (*launch_leaf)(const pbbfmm_leaf_args *args, void *stream);
+  int has_gradient;        /* launch_leaf supports gradient mode */
+  void *ctx;               /* passed to evaluate */
+} pbbfmm_user_kernel;
+
+#define PBBFMM_KERNEL_USER 64
+
+/* A tree over a user-defined kernel (the constructor + SetKernelProperty of
+ * a user subclass of H2_3D_Tree).  params->kernel and kernel_param are
+ * ignored; *kernel is copied (kernel_type included) and its functions must
+ * stay valid for the tree's lifetime. */
+int pbbfmm_tree_create_user(const pbbfmm_tree_params *params, const pbbfmm_user_kernel *kernel,
+                            int device, pbbfmm_tree **tree);
+
 /* buildFMMTree (src/H2_3D_Tree.cpp:40-66): computes the interpolation
  * weights and the M2L operators in float64 on the host and uploads them.
  * If cache_dir is non-NULL, operator files in the reference's format and
@@ -156,6 +217,16 @@ int pbbfmm_set_precision(pbbfmm_tree *tree, int precision);
 #define PBBFMM_TC_TF32 2
 int pbbfmm_set_tensor_cores(pbbfmm_tree *tree, int mode);
 int pbbfmm_tensor_core_m2l(const pbbfmm_tree *tree);
+
+/* Test access to the timeout path (no reference counterpart).  Sets the poll
+ * limit of the tensor-core Chebyshev M2L's pipeline waits on `device` (-1:
+ * the current device); polls <= 0 restores the default (about a second).
+ * With a limit of a few polls those waits run out, the kernel stops, waits
+ * with the full bound for the copies and MMAs it has already issued, frees
+ * its TMEM and reports through the timeout flag: the compute returns
+ * PBBFMM_ERR_TIMEOUT (pbbfmm_compute leaves the output untouched) and the
+ * next compute runs normally once the limit is restored. */
+int pbbfmm_debug_set_pipeline_wait_limit(int device, long long polls);
 
 /* Per-phase device times (ms) of the last compute, when timing is enabled
  * with pbbfmm_set_timing(tree, 1).  names: comma-separated phase names. */

@@ -14,6 +14,8 @@
  * Kernels are the library's compiled-in functors: the reference's built-ins
  * plus exp(-r/l) (kernel_ExpCov), exp(-r^2/2s^2) (kernel_GaussSigma) and the
  * anisotropic exponential of the reference's python example (kernel_AnisoExp).
+ * User-defined kernels (the reference's subclasses with SetKernelProperty and
+ * EvaluateKernel) are __device__ functors: include/pbbfmm3d_b200_kernel.cuh.
  */
 #ifndef PBBFMM3D_B200_HPP
 #define PBBFMM3D_B200_HPP
@@ -60,14 +62,39 @@ class H2_3D_Tree {
   H2_3D_Tree& operator=(const H2_3D_Tree&) = delete;
 
   // Operator precompute (or the reference-format cache in cache_dir).
-  void buildFMMTree(const char* cache_dir = nullptr) { check(pbbfmm_tree_build(h_, cache_dir)); }
+  void buildFMMTree(const char* cache_dir = nullptr) { check(pbbfmm_tree_build(live(), cache_dir)); }
   // PBBFMM_PREC_FP64 (default) or PBBFMM_PREC_MIXED.
-  void set_precision(int precision) { check(pbbfmm_set_precision(h_, precision)); }
+  void set_precision(int precision) { check(pbbfmm_set_precision(live(), precision)); }
   // Mixed Chebyshev M2L operands: PBBFMM_TC_F16 (default), PBBFMM_TC_TF32, or
   // PBBFMM_TC_OFF for the CUDA cores; tensor_core_m2l() reports the one in use.
-  void set_tensor_cores(int mode) { check(pbbfmm_set_tensor_cores(h_, mode)); }
+  void set_tensor_cores(int mode) { check(pbbfmm_set_tensor_cores(live(), mode)); }
   int tensor_core_m2l() const { return pbbfmm_tensor_core_m2l(h_); }
   pbbfmm_tree* handle() const { return h_; }
+
+ protected:
+  // For trees whose kernel is known only at buildFMMTree (user kernels, whose
+  // SetKernelProperty runs there as in the reference): parameters are kept
+  // and the library tree is created later by adopt().
+  struct deferred {};
+  H2_3D_Tree(deferred, double L, int tree_level, int interpolation_order, double epsilon,
+             int use_chebyshev, int device)
+      : device_(device) {
+    params_.L = L;
+    params_.tree_level = tree_level;
+    params_.interpolation_order = interpolation_order;
+    params_.epsilon = epsilon;
+    params_.use_chebyshev = use_chebyshev;
+  }
+  void adopt(pbbfmm_tree* h) {
+    if (h_) pbbfmm_tree_destroy(h_);
+    h_ = h;
+  }
+  pbbfmm_tree* live() const {
+    if (!h_) throw Error(PBBFMM_ERR_STATE, "call buildFMMTree() first");
+    return h_;
+  }
+  pbbfmm_tree_params params_{};
+  int device_ = 0;
 
  private:
   pbbfmm_tree* h_ = nullptr;

@@ -1,0 +1,636 @@
+/*
+ * pbbfmm3d_b200 -- device code shared by the library and by translation units
+ * that instantiate the leaf phase for their own kernel functor.
+ *
+ * Holds the Morton codes of the leaf numbering, the interpolation basis, the
+ * compensated sums, and the leaf-phase kernels (L2P + P2P + scatter to the
+ * output, reference include/compute.hpp:591-785) templated on the kernel
+ * functor KF, with their launcher launch_leaf_kernels<KF>().  The library
+ * instantiates them for its built-in kernels; include/pbbfmm3d_b200_kernel.cuh
+ * instantiates them for a user's kernel.  Everything the kernels read comes
+ * in a pbbfmm_leaf_args (include/pbbfmm3d_b200.h).
+ *
+ * A kernel functor KF provides
+ *   template <typename T> __device__ static T eval(T dx, T dy, T dz, const double* p);
+ * the kernel K(t, s) at d = s - t (p: up to four parameters), +inf where it
+ * is singular (set to 0, as the reference does, include/compute.hpp:767); and
+ * for the gradient passes (adjoint with position gradients) also
+ *   template <typename T> __device__ static T grad(T dx, T dy, T dz, const double* p, T* g);
+ * returning K and setting g = dK/dd (0 at d = 0), with
+ *   static constexpr bool has_gradient = true;
+ * Requires nvcc.
+ */
+#ifndef PBBFMM3D_B200_LEAF_CUH
+#define PBBFMM3D_B200_LEAF_CUH
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <type_traits>
+
+#include "pbbfmm3d_b200.h"
+
+namespace pbbfmm {
+
+constexpr int kMaxOrder = 10;
+
+// ------------------------------------------------------------ Morton codes
+// Leaf index of the reference: sum_l j_l 8^(L-1-l), j = 4 bx + 2 by + bz
+// (src/H2_3D_Tree.cpp:939-971) -- x in the most significant bit of each
+// octal digit.  Coordinate bit k sits at bit 3k+2 (x), 3k+1 (y), 3k (z).
+__host__ __device__ inline uint32_t spread3(uint32_t v) {
+  v &= 0x3ff;
+  v = (v | (v << 16)) & 0x030000ff;
+  v = (v | (v << 8)) & 0x0300f00f;
+  v = (v | (v << 4)) & 0x030c30c3;
+  v = (v | (v << 2)) & 0x09249249;
+  return v;
+}
+__host__ __device__ inline uint32_t compact3(uint32_t v) {
+  v &= 0x09249249;
+  v = (v | (v >> 2)) & 0x030c30c3;
+  v = (v | (v >> 4)) & 0x0300f00f;
+  v = (v | (v >> 8)) & 0x030000ff;
+  v = (v | (v >> 16)) & 0x000003ff;
+  return v;
+}
+__host__ __device__ inline uint32_t morton_encode(int x, int y, int z) {
+  return (spread3((uint32_t)x) << 2) | (spread3((uint32_t)y) << 1) | spread3((uint32_t)z);
+}
+__host__ __device__ inline void morton_decode(uint32_t m, int* x, int* y, int* z) {
+  *x = (int)compact3(m >> 2);
+  *y = (int)compact3(m >> 1);
+  *z = (int)compact3(m);
+}
+
+// Compensated (Kahan) sum: s holds the sum, c the running low-order error.
+template <typename T>
+struct Kahan {
+  T s = 0, c = 0;
+  __device__ __forceinline__ void add(T x) {
+    const T y = x - c;
+    const T t = s + y;
+    c = (t - s) - y;
+    s = t;
+  }
+  __device__ __forceinline__ double value() const { return (double)s - (double)c; }
+};
+
+// ------------------------------------------------------------ basis
+// S_m(x) per coordinate (ComputeSn, src/H2_3D_Tree.cpp:830-892).
+// Chebyshev: (2/n) * Clenshaw sum of T_k(node_m) T_k(x); uniform: Lagrange.
+template <typename T>
+__device__ __forceinline__ T basis_one(int n, int cheb, T x, const T* Tkz, int m) {
+  if (cheb) {
+    const T* Tk = Tkz + m * n;
+    T d0 = 0, d1 = 0, d2;
+    for (int j = n - 1; j > 0; j--) {
+      d2 = d0;
+      d0 = T(2) * x * d0 - d1 + Tk[j];
+      d1 = d2;
+    }
+    return (T(2) / T(n)) * (x * d0 - d1 + T(0.5) * Tk[0]);
+  }
+  T num = 1, den = 1;
+  for (int j = 0; j < n; j++)
+    if (m != j) {
+      num *= x - (T(1) - T(2) * T(j) / T(n - 1));
+      den *= T(-2) * (T(m) - T(j)) / T(n - 1);
+    }
+  return num / den;
+}
+
+// dS_m/dx on [-1, 1].  Chebyshev: S_m(x) = (2/n) (1/2 + sum_{k>=1} T_k(x_m)
+// T_k(x)), so S_m'(x) = (2/n) sum_{k>=1} T_k(x_m) k U_{k-1}(x) with U the
+// Chebyshev polynomials of the second kind.  Uniform: the derivative of the
+// Lagrange polynomial, sum over i != m of prod_{j != m, i} (x - x_j) / den.
+template <typename T>
+__device__ __forceinline__ T basis_deriv(int n, int cheb, T x, const T* Tkz, int m) {
+  if (cheb) {
+    const T* Tk = Tkz + m * n;
+    T u0 = 1, u1 = T(2) * x, s = 0;  // U_{k-1}, U_k
+    for (int k = 1; k < n; ++k) {
+      s += Tk[k] * T(k) * u0;
+      const T u2 = T(2) * x * u1 - u0;
+      u0 = u1;
+      u1 = u2;
+    }
+    return (T(2) / T(n)) * s;
+  }
+  T den = 1;
+  for (int j = 0; j < n; j++)
+    if (m != j) den *= T(-2) * (T(m) - T(j)) / T(n - 1);
+  T sum = 0;
+  for (int i = 0; i < n; ++i) {
+    if (i == m) continue;
+    T prod = 1;
+    for (int j = 0; j < n; ++j)
+      if (j != m && j != i) prod *= x - (T(1) - T(2) * T(j) / T(n - 1));
+    sum += prod;
+  }
+  return sum / den;
+}
+
+// out[m * stride] = S_m(x), m < n
+template <typename T>
+__device__ __forceinline__ void basis_all(int n, int cheb, T x, const T* Tkz, T* out,
+                                          int stride = 1) {
+  for (int m = 0; m < n; ++m) out[m * stride] = basis_one<T>(n, cheb, x, Tkz, m);
+}
+
+// Centre of cell m of level l (the reference's +-quarter-length steps from
+// the root, src/H2_3D_Tree.cpp:927-961, in the same rounding).
+__device__ __forceinline__ void cell_center_d(uint32_t m, int l, double box, double* c) {
+  int x, y, z;
+  morton_decode(m, &x, &y, &z);
+  double cx = 0, cy = 0, cz = 0, len = box;
+  for (int i = l - 1; i >= 0; --i) {
+    const double q = 0.25 * len;
+    cx = ((x >> i) & 1) ? __dadd_rn(cx, q) : __dsub_rn(cx, q);
+    cy = ((y >> i) & 1) ? __dadd_rn(cy, q) : __dsub_rn(cy, q);
+    cz = ((z >> i) & 1) ? __dadd_rn(cz, q) : __dsub_rn(cz, q);
+    len = 0.5 * len;
+  }
+  c[0] = cx;
+  c[1] = cy;
+  c[2] = cz;
+}
+
+// Leaf phase (L2P + P2P): one warp per nonempty target leaf.  Dense leaves
+// (kLaneLeafMin targets or more): one lane per target, 32 targets per pass;
+// the sources of the 27 neighbour leaves are staged through a per-warp
+// shared-memory tile of 32 (coalesced loads) that every lane sweeps by
+// broadcast reads, and the far field evaluates the n^3 local coefficients
+// (broadcast loads) against the lane's own basis.  Sparse leaves: one target
+// at a time, lanes over its sources and coefficients, warp shuffle reduction.
+// Reference: Local2Particle / DirectInteractions, include/compute.hpp:692-778.
+constexpr int kLeafWarps = 4;
+constexpr int kLeafCols = 8;  // columns per pass (registers)
+constexpr int kLaneLeafMin = 12;  // leaves with fewer targets take the warp-per-target path
+
+// Source coordinates relative to the target leaf's centre.  float (mixed
+// path): hi = float(d), lo = float(d - hi), so that differences of nearby
+// points keep ~48 bits; double: the offsets themselves.
+template <typename T>
+struct RelPos;
+template <>
+struct RelPos<float> {
+  float h[3], l[3];
+  __device__ void set(double dx, double dy, double dz) {
+    h[0] = (float)dx, h[1] = (float)dy, h[2] = (float)dz;
+    l[0] = (float)(dx - h[0]), l[1] = (float)(dy - h[1]), l[2] = (float)(dz - h[2]);
+  }
+  // source minus target
+  __device__ void diff(const float4& sh, const float4& sl, float* d) const {
+    d[0] = (sh.x - h[0]) + (sl.x - l[0]);
+    d[1] = (sh.y - h[1]) + (sl.y - l[1]);
+    d[2] = (sh.z - h[2]) + (sl.z - l[2]);
+  }
+};
+template <>
+struct RelPos<double> {
+  double h[3];
+  __device__ void set(double dx, double dy, double dz) { h[0] = dx, h[1] = dy, h[2] = dz; }
+  __device__ void diff(const double4& sh, const double4&, double* d) const {
+    d[0] = sh.x - h[0];
+    d[1] = sh.y - h[1];
+    d[2] = sh.z - h[2];
+  }
+};
+template <typename T>
+using vec4_t = typename std::conditional<sizeof(T) == 4, float4, double4>::type;
+
+// Running sum of the float64 path (plain; the mixed path uses Kahan<float>).
+template <typename T>
+struct PlainSum {
+  T s = 0;
+  __device__ __forceinline__ void add(T x) { s += x; }
+  __device__ __forceinline__ double value() const { return (double)s; }
+};
+template <typename T>
+using LeafAcc = typename std::conditional<sizeof(T) == 4, Kahan<T>, PlainSum<T>>::type;
+
+// T = float (mixed path): kernel values, interpolation and per-tile partial
+// sums in float32, each lane's running sums compensated (Kahan), the output
+// update in float64.  T = double: everything in float64.
+template <class KF, typename T, int KC, bool DENSE>
+__global__ void __launch_bounds__(32 * kLeafWarps, DENSE ? 4 : 6)
+    k_leaf(const int* __restrict__ leaves, int nleaves, const int* __restrict__ part_count,
+           const int* __restrict__ chunk_prefix, const int* __restrict__ tstart,
+           const int* __restrict__ sstart, const int* __restrict__ tperm,
+           const double* __restrict__ tpos, const double* __restrict__ spos,
+           const double* __restrict__ wsorted, int Nf, int Ns, int C,
+           const T* __restrict__ F_L, int n, int cheb, const T* __restrict__ Tkz_g,
+           double box, int L, const double* __restrict__ kparam_g, double* __restrict__ out) {
+  constexpr bool kMixed = sizeof(T) == 4;
+  using V4 = vec4_t<T>;
+  __shared__ T sTkz[kMaxOrder * kMaxOrder];
+  __shared__ double kp[4];
+  __shared__ int s_nb[kLeafWarps][27][2];  // neighbour source ranges
+  __shared__ int s_pre[kLeafWarps][28];    // exclusive prefix of their lengths
+  __shared__ V4 s_sh[kLeafWarps][DENSE ? 32 : 1];              // staged sources: position (hi)
+  __shared__ V4 s_sl[kLeafWarps][DENSE && kMixed ? 32 : 1];    // position (lo), mixed path
+  __shared__ T s_w[kLeafWarps][DENSE ? 32 : 1][KC];            // staged weights
+  // basis values of each lane's target, [warp][dim][m < n][lane] (dynamic, sized by n)
+  extern __shared__ __align__(16) unsigned char leaf_dyn[];
+  T* s_bw = reinterpret_cast<T*>(leaf_dyn) + (threadIdx.x >> 5) * 3 * n * 32;
+  __shared__ T s_bs[kLeafWarps][DENSE ? 1 : 3 * kMaxOrder];  // sparse path: the warp's target
+  for (int i = threadIdx.x; i < n * n; i += blockDim.x) sTkz[i] = Tkz_g[i];
+  if (threadIdx.x < 4) kp[threadIdx.x] = kparam_g[threadIdx.x];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+  const int wid = blockIdx.x * kLeafWarps + wl;
+  // leaves are partitioned: the dense ones first, the sparse ones after
+  const int nd = *part_count;
+  int leaf, ta, te, tc0 = 0;
+  if constexpr (DENSE) {
+    // warp = one 32-target chunk of a dense leaf; chunk_prefix[i] is the first
+    // chunk of dense leaf i (exclusive scan), chunk_prefix[nd] the total
+    if (wid >= chunk_prefix[nd]) return;
+    int lo = 0, hi = nd - 1;
+    while (lo < hi) {  // last i with chunk_prefix[i] <= wid
+      const int mid = (lo + hi + 1) >> 1;
+      if (chunk_prefix[mid] <= wid) lo = mid;
+      else hi = mid - 1;
+    }
+    leaf = leaves[lo];
+    ta = tstart[leaf];
+    te = tstart[leaf + 1];
+    tc0 = ta + 32 * (wid - chunk_prefix[lo]);
+  } else {
+    if (wid >= nleaves - nd) return;
+    leaf = leaves[nd + wid];
+    ta = tstart[leaf];
+    te = tstart[leaf + 1];
+  }
+  if ((te - ta >= kLaneLeafMin) != DENSE) return;  // the other instantiation's leaf
+  const int n3 = n * n * n;
+  double c[3];
+  cell_center_d((uint32_t)leaf, L, box, c);
+  double len = box;
+  for (int i = 0; i < L; ++i) len = 0.5 * len;
+  const double ihalfL = 2. / len;
+  int ax, ay, az;
+  morton_decode((uint32_t)leaf, &ax, &ay, &az);
+  const int nside = 1 << L;
+  // neighbour source ranges, slot 9(x+1)+3(y+1)+(z+1)
+  if (lane < 27) {
+    const int q = lane;
+    const int bx = ax + q / 9 - 1, by = ay + (q / 3) % 3 - 1, bz = az + q % 3 - 1;
+    int a = 0, e = 0;
+    if (bx >= 0 && by >= 0 && bz >= 0 && bx < nside && by < nside && bz < nside) {
+      const uint32_t bm = morton_encode(bx, by, bz);
+      a = sstart[bm];
+      e = sstart[bm + 1];
+    }
+    s_nb[wl][q][0] = a;
+    s_nb[wl][q][1] = e;
+  }
+  __syncwarp();
+  if (lane == 0) {
+    int acc = 0;
+    for (int q = 0; q < 27; ++q) {
+      s_pre[wl][q] = acc;
+      acc += s_nb[wl][q][1] - s_nb[wl][q][0];
+    }
+    s_pre[wl][27] = acc;
+  }
+  __syncwarp();
+  const int nsrc_total = s_pre[wl][27];
+  if constexpr (!DENSE) {
+    // Sparse leaf: one target at a time, lanes over its sources and over the
+    // n^3 local coefficients, warp-reduced in float64.
+    for (int c0 = 0; c0 < C; c0 += KC) {
+      const int cg = min(KC, C - c0);
+      for (int i = ta; i < te; ++i) {
+        const double x = tpos[i], y = tpos[(int64_t)Nf + i], z = tpos[2 * (int64_t)Nf + i];
+        LeafAcc<T> acc[KC];
+        __syncwarp();
+        if (lane < 3 * n) {
+          const int d = lane / n, mm = lane % n;
+          const T u = (T)(ihalfL * ((d == 0 ? x : d == 1 ? y : z) - c[d]));
+          s_bs[wl][d * n + mm] = basis_one<T>(n, cheb, u, sTkz, mm);
+        }
+        __syncwarp();
+        const T* Fl = F_L + ((int64_t)leaf * C + c0) * n3;
+        for (int l = lane; l < n3; l += 32) {
+          const int l1 = l / (n * n), l2 = (l / n) % n, l3 = l % n;
+          const T v = s_bs[wl][l1] * s_bs[wl][n + l2] * s_bs[wl][2 * n + l3];
+#pragma unroll
+          for (int cc = 0; cc < KC; ++cc)
+            if (cc < cg) acc[cc].add(Fl[cc * n3 + l] * v);
+        }
+        int q = 0;
+        for (int v = lane; v < nsrc_total; v += 32) {
+          while (v >= s_pre[wl][q + 1]) ++q;
+          const int j = s_nb[wl][q][0] + (v - s_pre[wl][q]);
+          const T dx = (T)(spos[j] - x), dy = (T)(spos[(int64_t)Ns + j] - y),
+                  dz = (T)(spos[2 * (int64_t)Ns + j] - z);
+          T kv = KF::template eval<T>(dx, dy, dz, kp);
+          if (isinf(kv)) kv = 0;  // coincident points (include/compute.hpp:767)
+          const double* wj = wsorted + (int64_t)j * C + c0;
+#pragma unroll
+          for (int cc = 0; cc < KC; ++cc)
+            if (cc < cg) acc[cc].add(kv * (T)wj[cc]);
+        }
+        double tot[KC];
+#pragma unroll
+        for (int cc = 0; cc < KC; ++cc) {
+          double v = acc[cc].value();
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+          tot[cc] = v;
+        }
+        if (lane == 0) {
+          const int64_t oi = tperm[i];
+#pragma unroll
+          for (int cc = 0; cc < KC; ++cc)
+            if (cc < cg) out[(int64_t)(c0 + cc) * Nf + oi] += tot[cc];
+        }
+      }
+    }
+  } else {
+  // Dense leaf: one target per lane, sources through shared-memory tiles.
+  for (int c0 = 0; c0 < C; c0 += KC) {
+    const int cg = min(KC, C - c0);
+    for (int t0 = tc0; t0 < te && t0 < tc0 + 32; t0 += 32) {  // this warp's chunk
+      const int i = t0 + lane;
+      const bool active = i < te;
+      double x = c[0], y = c[1], z = c[2];
+      if (active) x = tpos[i], y = tpos[(int64_t)Nf + i], z = tpos[2 * (int64_t)Nf + i];
+      RelPos<T> tp;
+      tp.set(x - c[0], y - c[1], z - c[2]);
+      LeafAcc<T> acc[KC];
+      // far field: phi += sum_l F[l] Sx[l1] Sy[l2] Sz[l3]
+      if (active) {
+        T* b = s_bw + lane;  // b[(d n + m) 32]: conflict-free, no local memory
+        for (int m = 0; m < n; ++m) {
+          b[m * 32] = basis_one<T>(n, cheb, (T)(ihalfL * (x - c[0])), sTkz, m);
+          b[(n + m) * 32] = basis_one<T>(n, cheb, (T)(ihalfL * (y - c[1])), sTkz, m);
+          b[(2 * n + m) * 32] = basis_one<T>(n, cheb, (T)(ihalfL * (z - c[2])), sTkz, m);
+        }
+        const T* Fl = F_L + ((int64_t)leaf * C + c0) * n3;
+        int l = 0;
+        for (int l1 = 0; l1 < n; ++l1)
+          for (int l2 = 0; l2 < n; ++l2) {
+            const T b12 = b[l1 * 32] * b[(n + l2) * 32];
+            for (int l3 = 0; l3 < n; ++l3, ++l) {
+              const T v = b12 * b[(2 * n + l3) * 32];
+#pragma unroll
+              for (int cc = 0; cc < KC; ++cc)
+                if (cc < cg) acc[cc].add(Fl[cc * n3 + l] * v);
+            }
+          }
+      }
+      // near field: the 27 neighbours' source ranges, concatenated, in tiles of 32
+      int q = 0;
+      for (int v0 = 0; v0 < nsrc_total; v0 += 32) {
+        const int v = v0 + lane;
+        if (v < nsrc_total) {
+          while (v >= s_pre[wl][q + 1]) ++q;
+          const int j = s_nb[wl][q][0] + (v - s_pre[wl][q]);
+          RelPos<T> sp;
+          sp.set(spos[j] - c[0], spos[(int64_t)Ns + j] - c[1], spos[2 * (int64_t)Ns + j] - c[2]);
+          V4 h;
+          h.x = sp.h[0], h.y = sp.h[1], h.z = sp.h[2], h.w = 0;
+          s_sh[wl][lane] = h;
+          if constexpr (kMixed) {
+            V4 lo;
+            lo.x = sp.l[0], lo.y = sp.l[1], lo.z = sp.l[2], lo.w = 0;
+            s_sl[wl][lane] = lo;
+          }
+          const double* wj = wsorted + (int64_t)j * C + c0;
+#pragma unroll
+          for (int cc = 0; cc < KC; ++cc) s_w[wl][lane][cc] = cc < cg ? (T)wj[cc] : T(0);
+        }
+        __syncwarp();
+        if (active) {
+          const int m = min(32, nsrc_total - v0);
+          T part[KC];
+#pragma unroll
+          for (int cc = 0; cc < KC; ++cc) part[cc] = 0;
+#pragma unroll 4
+          for (int jj = 0; jj < m; ++jj) {
+            T d[3];
+            tp.diff(s_sh[wl][jj], s_sl[wl][kMixed ? jj : 0], d);
+            T kv = KF::template eval<T>(d[0], d[1], d[2], kp);
+            if (isinf(kv)) kv = 0;  // coincident points (include/compute.hpp:767)
+#pragma unroll
+            for (int cc = 0; cc < KC; ++cc)
+              if (cc < cg) part[cc] = fma(kv, s_w[wl][jj][cc], part[cc]);
+          }
+#pragma unroll
+          for (int cc = 0; cc < KC; ++cc)
+            if (cc < cg) acc[cc].add(part[cc]);
+        }
+        __syncwarp();
+      }
+      if (active) {
+        const int64_t oi = tperm[i];
+#pragma unroll
+        for (int cc = 0; cc < KC; ++cc)
+          if (cc < cg) out[(int64_t)(c0 + cc) * Nf + oi] += (double)acc[cc].value();
+      }
+    }
+  }
+  }
+}
+
+// Gradient leaf phase (adjoint and position gradients): for each target x
+// and column c, phi_c(x) = sum_l F_lc S_l(x) + sum_j w_jc K(x, y_j) and its
+// gradient, from the differentiated interpolation basis (chain factor
+// 2 / cell length) and the kernel gradient.  grad_out[i*3 + d] gets
+// sum_c contract[c*Nf + i] d phi_c / d x_d; out[c*Nf + i] gets phi_c when
+// non-null.  One warp per target leaf, one target at a time, lanes over its
+// sources and coefficients.
+constexpr int kGradCols = 4;  // columns per pass (4 accumulators each)
+
+template <class KF, typename T>
+__global__ void __launch_bounds__(32 * kLeafWarps)
+    k_leaf_grad(const int* __restrict__ leaves, int nleaves, const int* __restrict__ tstart,
+                const int* __restrict__ sstart, const int* __restrict__ tperm,
+                const double* __restrict__ tpos, const double* __restrict__ spos,
+                const double* __restrict__ wsorted, int Nf, int Ns, int C,
+                const T* __restrict__ F_L, int n, int cheb, const T* __restrict__ Tkz_g,
+                double box, int L, const double* __restrict__ kparam_g, double* __restrict__ out,
+                const double* __restrict__ contract, double* __restrict__ grad_out) {
+  __shared__ T sTkz[kMaxOrder * kMaxOrder];
+  __shared__ double kp[4];
+  __shared__ int s_nb[kLeafWarps][27][2];
+  __shared__ int s_pre[kLeafWarps][28];
+  __shared__ T s_b[kLeafWarps][6 * kMaxOrder];  // S_m per dimension, then dS_m/dx
+  for (int i = threadIdx.x; i < n * n; i += blockDim.x) sTkz[i] = Tkz_g[i];
+  if (threadIdx.x < 4) kp[threadIdx.x] = kparam_g[threadIdx.x];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+  const int wid = blockIdx.x * kLeafWarps + wl;
+  if (wid >= nleaves) return;
+  const int leaf = leaves[wid];
+  const int ta = tstart[leaf], te = tstart[leaf + 1];
+  const int n3 = n * n * n;
+  double c[3];
+  cell_center_d((uint32_t)leaf, L, box, c);
+  double len = box;
+  for (int i = 0; i < L; ++i) len = 0.5 * len;
+  const double ihalfL = 2. / len;
+  int ax, ay, az;
+  morton_decode((uint32_t)leaf, &ax, &ay, &az);
+  const int nside = 1 << L;
+  if (lane < 27) {
+    const int q = lane;
+    const int bx = ax + q / 9 - 1, by = ay + (q / 3) % 3 - 1, bz = az + q % 3 - 1;
+    int a = 0, e = 0;
+    if (bx >= 0 && by >= 0 && bz >= 0 && bx < nside && by < nside && bz < nside) {
+      const uint32_t bm = morton_encode(bx, by, bz);
+      a = sstart[bm];
+      e = sstart[bm + 1];
+    }
+    s_nb[wl][q][0] = a;
+    s_nb[wl][q][1] = e;
+  }
+  __syncwarp();
+  if (lane == 0) {
+    int acc = 0;
+    for (int q = 0; q < 27; ++q) {
+      s_pre[wl][q] = acc;
+      acc += s_nb[wl][q][1] - s_nb[wl][q][0];
+    }
+    s_pre[wl][27] = acc;
+  }
+  __syncwarp();
+  const int nsrc_total = s_pre[wl][27];
+  const T* Sb = s_b[wl];
+  const T* Db = s_b[wl] + 3 * n;
+  for (int c0 = 0; c0 < C; c0 += kGradCols) {
+    const int cg = min(kGradCols, C - c0);
+    for (int i = ta; i < te; ++i) {
+      const double x = tpos[i], y = tpos[(int64_t)Nf + i], z = tpos[2 * (int64_t)Nf + i];
+      __syncwarp();
+      if (lane < 3 * n) {
+        const int d = lane / n, mm = lane % n;
+        const T u = (T)(ihalfL * ((d == 0 ? x : d == 1 ? y : z) - c[d]));
+        s_b[wl][d * n + mm] = basis_one<T>(n, cheb, u, sTkz, mm);
+        s_b[wl][3 * n + d * n + mm] = basis_deriv<T>(n, cheb, u, sTkz, mm) * (T)ihalfL;
+      }
+      __syncwarp();
+      LeafAcc<T> v[kGradCols], g[kGradCols][3];
+      const T* Fl = F_L + ((int64_t)leaf * C + c0) * n3;
+      for (int l = lane; l < n3; l += 32) {
+        const int l1 = l / (n * n), l2 = (l / n) % n, l3 = l % n;
+        const T b1 = Sb[l1], b2 = Sb[n + l2], b3 = Sb[2 * n + l3];
+        const T e0 = Db[l1] * b2 * b3, e1 = b1 * Db[n + l2] * b3, e2 = b1 * b2 * Db[2 * n + l3];
+        const T val = b1 * b2 * b3;
+#pragma unroll
+        for (int cc = 0; cc < kGradCols; ++cc)
+          if (cc < cg) {
+            const T f = Fl[cc * n3 + l];
+            v[cc].add(f * val);
+            g[cc][0].add(f * e0);
+            g[cc][1].add(f * e1);
+            g[cc][2].add(f * e2);
+          }
+      }
+      int q = 0;
+      for (int vv = lane; vv < nsrc_total; vv += 32) {
+        while (vv >= s_pre[wl][q + 1]) ++q;
+        const int j = s_nb[wl][q][0] + (vv - s_pre[wl][q]);
+        const T dx = (T)(spos[j] - x), dy = (T)(spos[(int64_t)Ns + j] - y),
+                dz = (T)(spos[2 * (int64_t)Ns + j] - z);
+        T gk[3];
+        T kv = KF::template grad<T>(dx, dy, dz, kp, gk);
+        if (isinf(kv)) kv = 0;  // coincident points (include/compute.hpp:767)
+        const double* wj = wsorted + (int64_t)j * C + c0;
+#pragma unroll
+        for (int cc = 0; cc < kGradCols; ++cc)
+          if (cc < cg) {
+            const T w = (T)wj[cc];
+            v[cc].add(kv * w);
+            // d K(x, y_j) / d x = -dK/dd with d = y_j - x
+            g[cc][0].add(-gk[0] * w);
+            g[cc][1].add(-gk[1] * w);
+            g[cc][2].add(-gk[2] * w);
+          }
+      }
+      double tv[kGradCols], tg[kGradCols][3];
+#pragma unroll
+      for (int cc = 0; cc < kGradCols; ++cc) {
+        double a = v[cc].value(), b0 = g[cc][0].value(), b1 = g[cc][1].value(),
+               b2 = g[cc][2].value();
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+          a += __shfl_xor_sync(0xffffffffu, a, o);
+          b0 += __shfl_xor_sync(0xffffffffu, b0, o);
+          b1 += __shfl_xor_sync(0xffffffffu, b1, o);
+          b2 += __shfl_xor_sync(0xffffffffu, b2, o);
+        }
+        tv[cc] = a, tg[cc][0] = b0, tg[cc][1] = b1, tg[cc][2] = b2;
+      }
+      if (lane == 0) {
+        const int64_t oi = tperm[i];
+        double gs[3] = {0, 0, 0};
+#pragma unroll
+        for (int cc = 0; cc < kGradCols; ++cc)
+          if (cc < cg) {
+            if (out) out[(int64_t)(c0 + cc) * Nf + oi] += tv[cc];
+            if (grad_out) {
+              const double wc = contract[(int64_t)(c0 + cc) * Nf + oi];
+              gs[0] += wc * tg[cc][0], gs[1] += wc * tg[cc][1], gs[2] += wc * tg[cc][2];
+            }
+          }
+        if (grad_out)
+          for (int d = 0; d < 3; ++d) grad_out[oi * 3 + d] += gs[d];
+      }
+    }
+  }
+}
+
+// Whether a kernel functor provides the gradient (KF::has_gradient).
+template <class KF, class = void>
+struct kf_has_gradient : std::false_type {};
+template <class KF>
+struct kf_has_gradient<KF, typename std::enable_if<KF::has_gradient>::type> : std::true_type {};
+
+template <class KF, typename T>
+inline int launch_leaf_kernels_t(const pbbfmm_leaf_args& a, cudaStream_t st) {
+  const T* F = static_cast<const T*>(a.F_leaf);
+  const T* Tkz = static_cast<const T*>(a.Tkz);
+  if (a.gradient) {
+    if constexpr (kf_has_gradient<KF>::value) {
+      k_leaf_grad<KF, T><<<(a.nleaves + kLeafWarps - 1) / kLeafWarps, 32 * kLeafWarps, 0, st>>>(
+          a.leaves, a.nleaves, a.tstart, a.sstart, a.tperm, a.tpos, a.spos, a.wsorted, a.Nf, a.Ns,
+          a.C, F, a.n, a.cheb, Tkz, a.box, a.L, a.kparam, a.out, a.contract, a.grad_out);
+      return (int)cudaGetLastError();
+    } else {
+      return -1;  // no gradient: the caller reports PBBFMM_ERR_UNSUPPORTED
+    }
+  }
+  // dense leaves (32-target chunks, one warp each), then the sparse ones; one
+  // column: registers for one, otherwise columns in passes of kLeafCols
+  const size_t dyn = sizeof(T) * kLeafWarps * 3 * a.n * 32;
+  for (int dense = 1; dense >= 0; --dense) {
+    auto kern = a.C == 1
+                    ? (dense ? k_leaf<KF, T, 1, true> : k_leaf<KF, T, 1, false>)
+                    : (dense ? k_leaf<KF, T, kLeafCols, true> : k_leaf<KF, T, kLeafCols, false>);
+    const int64_t warps = dense ? a.max_chunks : a.nleaves;
+    kern<<<(unsigned)((warps + kLeafWarps - 1) / kLeafWarps), 32 * kLeafWarps, dense ? dyn : 0,
+           st>>>(a.leaves, a.nleaves, a.ndense, a.chunk_prefix, a.tstart, a.sstart, a.tperm,
+                 a.tpos, a.spos, a.wsorted, a.Nf, a.Ns, a.C, F, a.n, a.cheb, Tkz, a.box, a.L,
+                 a.kparam, a.out);
+    if (const cudaError_t e = cudaGetLastError()) return (int)e;
+  }
+  return 0;
+}
+
+// Launch the leaf phase described by `a` for the kernel functor KF on
+// `stream`: 0 on success, a cudaError_t code if a launch failed, -1 when a
+// gradient pass is asked of a functor without gradient.  Launches 2 kernels
+// (values) or 1 (gradient).
+template <class KF>
+inline int launch_leaf_kernels(const pbbfmm_leaf_args& a, cudaStream_t st) {
+  return a.precision == PBBFMM_PREC_FP64 ? launch_leaf_kernels_t<KF, double>(a, st)
+                                         : launch_leaf_kernels_t<KF, float>(a, st);
+}
+
+}  // namespace pbbfmm
+
+#endif  // PBBFMM3D_B200_LEAF_CUH

@@ -83,8 +83,9 @@ def build() -> None:
     """Compile the C restatement (and, where the reference tree is present,
     the reference itself).  Building the checker is not using it."""
     subprocess.run(["make", "-s", "-C", HERE], check=True)
-    if os.path.isdir("/root/reference"):
-        subprocess.run(["make", "-s", "-C", os.path.join(HERE, "ref")], check=True)
+    ref = os.environ.get("PBBFMM_REF_DIR")
+    if ref and os.path.isdir(ref):
+        subprocess.run(["make", "-s", "-C", os.path.join(HERE, "ref"), "REF=" + ref], check=True)
 
 
 def lib():

@@ -80,6 +80,26 @@ class kernel_AnisoExp : public H2_3D_Tree {  // python/mykernel_python.hpp:10-18
   }
 };
 
+// The softened Laplacian 1/sqrt(r^2 + delta^2): a kernel outside the
+// library's built-in set, used to check user-defined device kernels.
+class kernel_SoftLap : public H2_3D_Tree {
+ public:
+  double delta;
+  kernel_SoftLap(double L, int lv, int n, double eps, int cheb, double d)
+      : H2_3D_Tree(L, lv, n, eps, cheb), delta(d) {}
+  void SetKernelProperty() override {
+    homogen = 0;
+    symmetry = 1;
+    char buf[32];
+    snprintf(buf, sizeof buf, "SoftLap%g", delta);
+    kernelType = buf;
+  }
+  double EvaluateKernel(const vector3& t, const vector3& s) override {
+    double dx = s.x - t.x, dy = s.y - t.y, dz = s.z - t.z;
+    return 1. / sqrt(dx * dx + dy * dy + dz * dz + delta * delta);
+  }
+};
+
 struct Args {
   std::string kernel = "Laplacian";
   double param = 0.0;
@@ -216,6 +236,9 @@ int main(int argc, char** argv) {
   else if (a.kernel == "GaussSigma") run<kernel_GaussSigma>(
       a, [&]() { return new kernel_GaussSigma(L, lv, n, eps, ch, prm); }, target, source,
       weight, output, times, tpre);
+  else if (a.kernel == "SoftLap") run<kernel_SoftLap>(
+      a, [&]() { return new kernel_SoftLap(L, lv, n, eps, ch, prm); }, target, source, weight,
+      output, times, tpre);
   else die(("unknown kernel " + a.kernel).c_str());
 #undef RUN_BUILTIN
 

@@ -46,6 +46,8 @@ _i64 = ctypes.c_int64
 
 EXPORTS = {
     "pbbfmm_tree_create": ([ctypes.POINTER(TreeParams), ctypes.c_int, ctypes.POINTER(_vp)], ctypes.c_int),
+    "pbbfmm_tree_create_user": ([ctypes.POINTER(TreeParams), _vp, ctypes.c_int, ctypes.POINTER(_vp)],
+                                ctypes.c_int),
     "pbbfmm_tree_build": ([_vp, ctypes.c_char_p], ctypes.c_int),
     "pbbfmm_tree_set_operators": ([_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int, _dp, _dp, _dp], ctypes.c_int),
     "pbbfmm_tree_get_operators": ([_vp, _ip, _ip, _ip, _dp, _dp, _dp], ctypes.c_int),
@@ -71,6 +73,7 @@ EXPORTS = {
     "pbbfmm_bin_points_noalloc": ([_vp, _i64, ctypes.c_double, ctypes.c_int, _vp, _vp, _vp, _vp],
                                   ctypes.c_int),
     "pbbfmm_measure_fma_peak": ([ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_double)], ctypes.c_int),
+    "pbbfmm_debug_set_pipeline_wait_limit": ([ctypes.c_int, ctypes.c_longlong], ctypes.c_int),
 }
 
 

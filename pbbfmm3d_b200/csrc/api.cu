@@ -635,13 +635,18 @@ const char* pbbfmm_version(void) { return "pbbfmm3d_b200 0.1 (sm_100a)"; }
 
 long long pbbfmm_launch_count(void) { return g_launches.load(); }
 
-int pbbfmm_tree_create(const pbbfmm_tree_params* params, int device, pbbfmm_tree** out) {
+static int create_tree(const pbbfmm_tree_params* params, const pbbfmm_user_kernel* uk,
+                       int device, pbbfmm_tree** out) {
   if (!params || !out) {
     set_error("null argument");
     return PBBFMM_ERR_ARG;
   }
   *out = nullptr;
-  const pbbfmm_tree_params& p = *params;
+  pbbfmm_tree_params p = *params;
+  if (uk) {
+    p.kernel = PBBFMM_KERNEL_USER;
+    for (double& x : p.kernel_param) x = 0.0;
+  }
   if (!(p.L > 0) || !std::isfinite(p.L)) {
     set_error("box length L must be positive");
     return PBBFMM_ERR_ARG;
@@ -654,8 +659,14 @@ int pbbfmm_tree_create(const pbbfmm_tree_params* params, int device, pbbfmm_tree
     set_error("interpolation_order must be in [2, 10]");
     return PBBFMM_ERR_ARG;
   }
-  if (p.kernel < 0 || p.kernel >= PBBFMM_KERNEL_COUNT) {
+  if (!uk && (p.kernel < 0 || p.kernel >= PBBFMM_KERNEL_COUNT)) {
     set_error("unknown kernel id");
+    return PBBFMM_ERR_ARG;
+  }
+  if (uk && (!uk->evaluate || !uk->launch_leaf || !uk->kernel_type || !uk->kernel_type[0] ||
+             uk->symmetry < -1 || uk->symmetry > 1 || !std::isfinite(uk->homogen))) {
+    set_error("user kernel needs evaluate, launch_leaf, a kernel_type name, symmetry in "
+              "{-1, 0, 1} and a finite homogen");
     return PBBFMM_ERR_ARG;
   }
   if (p.use_chebyshev && !(p.epsilon > 0)) {
@@ -685,6 +696,15 @@ int pbbfmm_tree_create(const pbbfmm_tree_params* params, int device, pbbfmm_tree
   t->p = p;
   t->device = device;
   t->kspec = kernel_spec(p.kernel, p.kernel_param);
+  if (uk) {  // SetKernelProperty of the user's subclass
+    t->user = *uk;
+    t->kspec.homogen = uk->homogen;
+    t->kspec.symmetry = uk->symmetry;
+    t->kspec.user_type = uk->kernel_type;
+    t->kspec.user_eval = uk->evaluate;
+    t->kspec.user_ctx = uk->ctx;
+    t->user.kernel_type = nullptr;  // the copy in kspec.user_type is the one used
+  }
   t->n = p.interpolation_order;
   t->n3 = t->n * t->n * t->n;
   t->m = 2 * t->n - 1;
@@ -734,6 +754,19 @@ int pbbfmm_tree_create(const pbbfmm_tree_params* params, int device, pbbfmm_tree
   }
   *out = t;
   return PBBFMM_OK;
+}
+
+int pbbfmm_tree_create(const pbbfmm_tree_params* params, int device, pbbfmm_tree** out) {
+  return create_tree(params, nullptr, device, out);
+}
+
+int pbbfmm_tree_create_user(const pbbfmm_tree_params* params, const pbbfmm_user_kernel* kernel,
+                            int device, pbbfmm_tree** out) {
+  if (!kernel) {
+    set_error("null user kernel");
+    return PBBFMM_ERR_ARG;
+  }
+  return create_tree(params, kernel, device, out);
 }
 
 int pbbfmm_tree_build(pbbfmm_tree* t, const char* cache_dir) {
@@ -1066,6 +1099,13 @@ int pbbfmm_compute(pbbfmm_tree* t, const double* target, int64_t Nf, const doubl
   int rc;
   if (!ws.io_stream) PB_CUDA(cudaStreamCreateWithFlags(&ws.io_stream, cudaStreamNonBlocking));
   cudaStream_t st = ws.io_stream;
+  // Every exit waits for the stream: no copy queued here may still read the
+  // pinned staging (which the next call overwrites) or write the caller's
+  // result after this call returns.  On success the stream is already idle.
+  struct StreamDrain {
+    cudaStream_t s;
+    ~StreamDrain() { cudaStreamSynchronize(s); }
+  } drain{st};
   const bool same = (source == target && Ns == Nf);
   const size_t bt = sizeof(double) * 3 * Nf, bs = same ? 0 : sizeof(double) * 3 * Ns;
   const size_t bw = sizeof(double) * (size_t)Ns * nCols, bo = sizeof(double) * (size_t)Nf * nCols;
@@ -1119,11 +1159,14 @@ int pbbfmm_compute(pbbfmm_tree* t, const double* target, int64_t Nf, const doubl
     const size_t n = total_d - c < chunk_d ? total_d - c : chunk_d;
     cudaError_t e = cudaEventSynchronize(evs[k]);
     if (e != cudaSuccess && status == PBBFMM_OK) status = cuda_status(e, "result copy");
+    // The compute's kernels finished before the first result chunk landed,
+    // so a timed-out tensor-core wait has set its flag by now: nothing is
+    // added to the caller's output from an invalid compute.
+    if (k == 0 && status == PBBFMM_OK) status = take_tc_timeout(t);
     if (status == PBBFMM_OK) host_add_mt(output + c, hout + c, n);
   }
   for (cudaEvent_t e : evs) cudaEventDestroy(e);
-  if (status) return status;
-  return take_tc_timeout(t);
+  return status;
 }
 
 int pbbfmm_set_tensor_cores(pbbfmm_tree* t, int mode) {

@@ -1,42 +1,14 @@
-// Shared device utilities: kernel functors, interpolation basis, Morton codes.
+// Shared device utilities: the built-in kernel functors, dispatch helpers,
+// complex types and asynchronous copies (Morton codes, the interpolation basis
+// and the leaf kernels are in include/pbbfmm3d_b200_leaf.cuh).
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
 
 #include "../../include/pbbfmm3d_b200.h"
+#include "../../include/pbbfmm3d_b200_leaf.cuh"
 
 namespace pbbfmm {
-
-constexpr int kMaxOrder = 10;
-
-// ------------------------------------------------------------ Morton codes
-// Leaf index of the reference: sum_l j_l 8^(L-1-l), j = 4 bx + 2 by + bz
-// (src/H2_3D_Tree.cpp:939-971) -- x in the most significant bit of each
-// octal digit.  Coordinate bit k sits at bit 3k+2 (x), 3k+1 (y), 3k (z).
-__host__ __device__ inline uint32_t spread3(uint32_t v) {
-  v &= 0x3ff;
-  v = (v | (v << 16)) & 0x030000ff;
-  v = (v | (v << 8)) & 0x0300f00f;
-  v = (v | (v << 4)) & 0x030c30c3;
-  v = (v | (v << 2)) & 0x09249249;
-  return v;
-}
-__host__ __device__ inline uint32_t compact3(uint32_t v) {
-  v &= 0x09249249;
-  v = (v | (v >> 2)) & 0x030c30c3;
-  v = (v | (v >> 4)) & 0x0300f00f;
-  v = (v | (v >> 8)) & 0x030000ff;
-  v = (v | (v >> 16)) & 0x000003ff;
-  return v;
-}
-__host__ __device__ inline uint32_t morton_encode(int x, int y, int z) {
-  return (spread3((uint32_t)x) << 2) | (spread3((uint32_t)y) << 1) | spread3((uint32_t)z);
-}
-__host__ __device__ inline void morton_decode(uint32_t m, int* x, int* y, int* z) {
-  *x = (int)compact3(m >> 2);
-  *y = (int)compact3(m >> 1);
-  *z = (int)compact3(m);
-}
 
 // ------------------------------------------------------------ kernels
 // K(t, s) with d = s - t, the arithmetic of src/kernel_Types.cpp (float64;
@@ -50,6 +22,7 @@ struct Kern;
 
 template <>
 struct Kern<PBBFMM_KERNEL_LAPLACIAN> {
+  static constexpr bool has_gradient = true;
   template <typename T>
   __device__ static T eval(T dx, T dy, T dz, const double*) {
     return inv_sqrt(dx * dx + dy * dy + dz * dz);
@@ -65,6 +38,7 @@ struct Kern<PBBFMM_KERNEL_LAPLACIAN> {
 };
 template <>
 struct Kern<PBBFMM_KERNEL_ONEOVERR2> {
+  static constexpr bool has_gradient = true;
   template <typename T>
   __device__ static T eval(T dx, T dy, T dz, const double*) {
     T ri = inv_sqrt(dx * dx + dy * dy + dz * dz);
@@ -81,6 +55,7 @@ struct Kern<PBBFMM_KERNEL_ONEOVERR2> {
 };
 template <>
 struct Kern<PBBFMM_KERNEL_ONEOVERR4> {
+  static constexpr bool has_gradient = true;
   template <typename T>
   __device__ static T eval(T dx, T dy, T dz, const double*) {
     T ri = inv_sqrt(dx * dx + dy * dy + dz * dz);
@@ -97,6 +72,7 @@ struct Kern<PBBFMM_KERNEL_ONEOVERR4> {
 };
 template <>
 struct Kern<PBBFMM_KERNEL_GAUSSIAN> {
+  static constexpr bool has_gradient = true;
   template <typename T>
   __device__ static T eval(T dx, T dy, T dz, const double*) {
     T r = sqrt(dx * dx + dy * dy + dz * dz);
@@ -112,6 +88,7 @@ struct Kern<PBBFMM_KERNEL_GAUSSIAN> {
 };
 template <>
 struct Kern<PBBFMM_KERNEL_LOGARITHM> {
+  static constexpr bool has_gradient = true;
   template <typename T>
   __device__ static T eval(T dx, T dy, T dz, const double*) {
     T r2 = dx * dx + dy * dy + dz * dz;
@@ -128,6 +105,7 @@ struct Kern<PBBFMM_KERNEL_LOGARITHM> {
 };
 template <>
 struct Kern<PBBFMM_KERNEL_QUADRIC> {
+  static constexpr bool has_gradient = true;
   template <typename T>
   __device__ static T eval(T dx, T dy, T dz, const double*) {
     return T(1) + (dx * dx + dy * dy + dz * dz);
@@ -141,6 +119,7 @@ struct Kern<PBBFMM_KERNEL_QUADRIC> {
 };
 template <>
 struct Kern<PBBFMM_KERNEL_INVQUADRIC> {
+  static constexpr bool has_gradient = true;
   template <typename T>
   __device__ static T eval(T dx, T dy, T dz, const double*) {
     return T(1) / (T(1) + (dx * dx + dy * dy + dz * dz));
@@ -155,6 +134,7 @@ struct Kern<PBBFMM_KERNEL_INVQUADRIC> {
 };
 template <>
 struct Kern<PBBFMM_KERNEL_THINPLATESPLINE> {
+  static constexpr bool has_gradient = true;
   template <typename T>
   __device__ static T eval(T dx, T dy, T dz, const double*) {
     T r2 = dx * dx + dy * dy + dz * dz;
@@ -171,6 +151,7 @@ struct Kern<PBBFMM_KERNEL_THINPLATESPLINE> {
 };
 template <>
 struct Kern<PBBFMM_KERNEL_EXPCOV> {
+  static constexpr bool has_gradient = true;
   template <typename T>
   __device__ static T eval(T dx, T dy, T dz, const double* p) {
     return exp(-sqrt(dx * dx + dy * dy + dz * dz) / T(p[0]));
@@ -186,6 +167,7 @@ struct Kern<PBBFMM_KERNEL_EXPCOV> {
 };
 template <>
 struct Kern<PBBFMM_KERNEL_GAUSSSIGMA> {
+  static constexpr bool has_gradient = true;
   template <typename T>
   __device__ static T eval(T dx, T dy, T dz, const double* p) {
     return exp(-(dx * dx + dy * dy + dz * dz) / (T(2) * T(p[0]) * T(p[0])));
@@ -201,6 +183,7 @@ struct Kern<PBBFMM_KERNEL_GAUSSSIGMA> {
 };
 template <>
 struct Kern<PBBFMM_KERNEL_ANISOEXP> {
+  static constexpr bool has_gradient = true;
   template <typename T>
   __device__ static T eval(T dx, T dy, T dz, const double*) {
     return T(0.75) * exp(-sqrt(dx * dx / T(100) + dy * dy / T(100) + dz * dz / T(2.25)));
@@ -256,19 +239,6 @@ __host__ __device__ __forceinline__ cplx_t<T> make_cplx(T re, T im) {
   v.y = im;
   return v;
 }
-
-// Compensated (Kahan) sum: s holds the sum, c the running low-order error.
-template <typename T>
-struct Kahan {
-  T s = 0, c = 0;
-  __device__ __forceinline__ void add(T x) {
-    const T y = x - c;
-    const T t = s + y;
-    c = (t - s) - y;
-    s = t;
-  }
-  __device__ __forceinline__ double value() const { return (double)s - (double)c; }
-};
 
 // ------------------------------------------------------------ async copies
 // 16-byte global -> shared copy that bypasses registers (cp.async, L2 only);
@@ -337,68 +307,6 @@ inline int dispatch_order(int n, F&& f) {
     case 10: return f.template run<10>();
     default: return PBBFMM_ERR_ARG;
   }
-}
-
-// ------------------------------------------------------------ basis
-// S_m(x) per coordinate (ComputeSn, src/H2_3D_Tree.cpp:830-892).
-// Chebyshev: (2/n) * Clenshaw sum of T_k(node_m) T_k(x); uniform: Lagrange.
-template <typename T>
-__device__ __forceinline__ T basis_one(int n, int cheb, T x, const T* Tkz, int m) {
-  if (cheb) {
-    const T* Tk = Tkz + m * n;
-    T d0 = 0, d1 = 0, d2;
-    for (int j = n - 1; j > 0; j--) {
-      d2 = d0;
-      d0 = T(2) * x * d0 - d1 + Tk[j];
-      d1 = d2;
-    }
-    return (T(2) / T(n)) * (x * d0 - d1 + T(0.5) * Tk[0]);
-  }
-  T num = 1, den = 1;
-  for (int j = 0; j < n; j++)
-    if (m != j) {
-      num *= x - (T(1) - T(2) * T(j) / T(n - 1));
-      den *= T(-2) * (T(m) - T(j)) / T(n - 1);
-    }
-  return num / den;
-}
-
-// dS_m/dx on [-1, 1].  Chebyshev: S_m(x) = (2/n) (1/2 + sum_{k>=1} T_k(x_m)
-// T_k(x)), so S_m'(x) = (2/n) sum_{k>=1} T_k(x_m) k U_{k-1}(x) with U the
-// Chebyshev polynomials of the second kind.  Uniform: the derivative of the
-// Lagrange polynomial, sum over i != m of prod_{j != m, i} (x - x_j) / den.
-template <typename T>
-__device__ __forceinline__ T basis_deriv(int n, int cheb, T x, const T* Tkz, int m) {
-  if (cheb) {
-    const T* Tk = Tkz + m * n;
-    T u0 = 1, u1 = T(2) * x, s = 0;  // U_{k-1}, U_k
-    for (int k = 1; k < n; ++k) {
-      s += Tk[k] * T(k) * u0;
-      const T u2 = T(2) * x * u1 - u0;
-      u0 = u1;
-      u1 = u2;
-    }
-    return (T(2) / T(n)) * s;
-  }
-  T den = 1;
-  for (int j = 0; j < n; j++)
-    if (m != j) den *= T(-2) * (T(m) - T(j)) / T(n - 1);
-  T sum = 0;
-  for (int i = 0; i < n; ++i) {
-    if (i == m) continue;
-    T prod = 1;
-    for (int j = 0; j < n; ++j)
-      if (j != m && j != i) prod *= x - (T(1) - T(2) * T(j) / T(n - 1));
-    sum += prod;
-  }
-  return sum / den;
-}
-
-// out[m * stride] = S_m(x), m < n
-template <typename T>
-__device__ __forceinline__ void basis_all(int n, int cheb, T x, const T* Tkz, T* out,
-                                          int stride = 1) {
-  for (int m = 0; m < n; ++m) out[m * stride] = basis_one<T>(n, cheb, x, Tkz, m);
 }
 
 }  // namespace pbbfmm

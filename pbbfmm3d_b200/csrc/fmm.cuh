@@ -94,6 +94,7 @@ struct TcOps {
 struct pbbfmm_tree {
   pbbfmm_tree_params p{};
   pbbfmm::KernelSpec kspec;
+  pbbfmm_user_kernel user{};  // user-defined kernel (p.kernel == PBBFMM_KERNEL_USER)
   pbbfmm::Weights w;
   pbbfmm::Operators ops;
   int device = 0;

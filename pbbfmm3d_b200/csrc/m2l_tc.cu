@@ -49,6 +49,12 @@ constexpr int TC_THREADS = 288;    // + warps 5-8: accumulator drains
 constexpr int TC_TMEM_COLS = 512;  // columns allocated (accumulators and running sum)
 constexpr long long kWaitCycles = 2000000000ll;  // about 1 s of SM clock
 constexpr long long kWaitIters = 1ll << 26;
+// Poll limit of the M2L kernel's pipeline waits (stage and accumulator
+// barriers inside its main loops), per device; kWaitIters unless a test
+// lowers it through pbbfmm_debug_set_pipeline_wait_limit to make those waits
+// run out.  The waits for committed copies and MMAs before a CTA exits always
+// keep the full bound.
+__device__ long long g_pipe_wait_iters = kWaitIters;
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -100,11 +106,12 @@ __device__ __forceinline__ bool mbar_try(uint32_t a, int parity) {
 // about a second of SM clock (or kWaitIters polls) without it, or once *abort
 // is set (abort may be null).  The first poll reads no clock: a wait that is
 // already satisfied costs one try_wait.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, int parity, const volatile int* abort) {
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, int parity, const volatile int* abort,
+                                          long long iters = kWaitIters) {
   const uint32_t a = smem_u32(bar);
   if (mbar_try(a, parity)) return true;
   const long long t0 = clock64();
-  for (long long it = 0; it < kWaitIters; ++it) {
+  for (long long it = 0; it < iters; ++it) {
     if (mbar_try(a, parity)) return true;
     if ((it & 255) == 255 && ((abort && *abort) || clock64() - t0 > kWaitCycles)) return false;
   }
@@ -220,6 +227,34 @@ __device__ __forceinline__ void tc_wait_st() {
   asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory");
 }
 
+// 2^k as a float, exactly, for k in [-149, 127].
+__device__ __forceinline__ float exp2i(int k) {
+  return k >= -126 ? __int_as_float((k + 127) << 23) : __int_as_float(1 << (k + 149));
+}
+
+// x 2^k with every step an exact power-of-two product: k is split into
+// factors inside the float exponent range, so the result is exact whenever
+// it is a normal number (whatever k), and correctly rounded otherwise.
+__device__ __forceinline__ float scale2(float x, int k) {
+  k = min(max(k, -400), 400);
+  while (k > 127) {
+    x *= exp2i(127);
+    k -= 127;
+  }
+  while (k < -126) {
+    x *= exp2i(-126);
+    k += 126;
+  }
+  return x * exp2i(k);
+}
+
+// k2 with |x| in [2^(k2-1), 2^k2) for finite x != 0 (frexp's exponent).
+__device__ __forceinline__ int exponent_of(float x) {
+  const uint32_t b = __float_as_uint(x) & 0x7fffffffu;
+  if (b >= 0x00800000u) return (int)(b >> 23) - 126;
+  return 32 - __clz(b) - 149;  // subnormal: b 2^-149, b in [2^(j-1), 2^j)
+}
+
 __device__ __forceinline__ float to_tf32(float x) {
   uint32_t r;
   asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
@@ -305,6 +340,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   __shared__ int s_abort_flag;
   volatile int* s_abort = &s_abort_flag;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const long long piters = g_pipe_wait_iters;  // poll limit of the pipeline waits
 
   // child type of this tile (unrolled so the parameter arrays stay in registers)
   int type = 0, tstart = 0, tlist = 0, tcount = 0;
@@ -410,7 +446,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     for (int i = 0; i < NST; ++i) tma_last[i] = -1;
     for (int j = 0; j < niter; ++j) {
       const int s = j % NST;
-      if (j >= NST && !mbar_wait(&s_empty[s], (j / NST - 1) & 1, s_abort)) {
+      // warp-uniform: the shuffles below are warp-collective
+      if (j >= NST &&
+          !__all_sync(0xffffffffu, mbar_wait(&s_empty[s], (j / NST - 1) & 1, s_abort, piters))) {
         *s_abort = 1;
         break;
       }
@@ -464,12 +502,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         const bool fresh = it == g * group_iters;
         // accumulator g % NACC is free once the drain of group g - NACC is done
         const int ab = g % NACC;
-        if (fresh && g >= NACC && !mbar_wait(&s_acce[ab], ((g - NACC) / NACC) & 1, s_abort)) {
+        if (fresh && g >= NACC &&
+            !mbar_wait(&s_acce[ab], ((g - NACC) / NACC) & 1, s_abort, piters)) {
           *s_abort = 1;
           break;
         }
-        if (!mbar_wait(&s_full[s], (it / NST) & 1, s_abort) ||
-            !mbar_wait(&s_tfull[s], (it / NST) & 1, s_abort)) {
+        if (!mbar_wait(&s_full[s], (it / NST) & 1, s_abort, piters) ||
+            !mbar_wait(&s_tfull[s], (it / NST) & 1, s_abort, piters)) {
           *s_abort = 1;
           break;
         }
@@ -537,17 +576,21 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     for (int i = 0; i < (RSUM ? TC_REG_SUM : 1); ++i) rsum[i] = 0.f;
     for (int g = 0; g < ngroups; ++g) {
       const int b = g % NACC;
-      // 2^-e exactly (a normal or subnormal power of two), e = e_op + e_row
-      // clamped to [-126, 149]; rows without a source are zero (any scale)
-      int e = v1 ? s_oexp[g] + min(max(x1, -256), 256) : 0;
-      e = min(max(e, -126), 149);
-      const float sc = e <= 126 ? __int_as_float((127 - e) << 23) : __int_as_float(1 << (149 - e));
+      // the unscaling 2^-e, e = e_op + e_row, as two exact powers of two
+      // 2^-e1 2^-e2 with e1 in [-126, 126] (a normal number) and the rest in
+      // e2 (normal or subnormal): a sum beyond one float's exponent range
+      // still scales correctly as long as the result itself is a normal
+      // number; rows without a source are zero (any scale)
+      const int e = v1 ? s_oexp[g] + min(max(x1, -256), 256) : 0;
+      const int e1 = min(max(e, -126), 126), e2 = min(max(e - e1, -126), 149);
+      const float sc = __int_as_float((127 - e1) << 23);
+      const float sc2 = e2 <= 126 ? __int_as_float((127 - e2) << 23) : __int_as_float(1 << (149 - e2));
       v1 = v2;
       x1 = x2;
       v2 = has_src(g + 2);
       if (F16 && g + 2 < nvalid) x2 = pexp[src_row(g + 2, v2)];
       // warp-uniform: the TMEM loads below are warp-collective
-      if (!__all_sync(0xffffffffu, mbar_wait(&s_accf[b], (g / NACC) & 1, s_abort))) {
+      if (!__all_sync(0xffffffffu, mbar_wait(&s_accf[b], (g / NACC) & 1, s_abort, piters))) {
         *s_abort = 1;
         break;
       }
@@ -567,7 +610,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 #pragma unroll
           for (int i = 0; i < 16; ++i) {
             const float x = __uint_as_float(r[i]);
-            rsum[c * 16 + i] = F16 ? fmaf(x, sc, rsum[c * 16 + i]) : rsum[c * 16 + i] + x;
+            rsum[c * 16 + i] = F16 ? fmaf(x * sc, sc2, rsum[c * 16 + i]) : rsum[c * 16 + i] + x;
           }
         }
         continue;
@@ -578,7 +621,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         tc_ld16(lane_base + (uint32_t)(b * astride + n0), v);
         if constexpr (F16) {
 #pragma unroll
-          for (int i = 0; i < 16; ++i) v[i] *= sc;  // exact unless the product is subnormal
+          for (int i = 0; i < 16; ++i) v[i] = v[i] * sc * sc2;  // exact unless the result is subnormal
         }
         if (tsum) {
           if (g > 0) {
@@ -656,14 +699,9 @@ __global__ void k_split_proxy_f16(const int* __restrict__ cells, int64_t nrows, 
   for (int k = lane; k < rs; k += 32) m = fmaxf(m, fabsf(x[k]));
 #pragma unroll
   for (int o = 16; o; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
-  int e = 0;
-  if (m > 0.f) {
-    int k2;
-    frexpf(m, &k2);  // m in [2^(k2-1), 2^k2)
-    e = 15 - k2;
-  }
+  const int e = m > 0.f ? 15 - exponent_of(m) : 0;  // m in [2^(k2-1), 2^k2)
   for (int k = lane; k < KP; k += 32) {
-    const float v = k < rs ? ldexpf(x[k], e) : 0.f;
+    const float v = k < rs ? scale2(x[k], e) : 0.f;
     const __half h = __float2half_rn(v);
     ph[row * KP + k] = h;
     pl[row * KP + k] = __float2half_rn(v - __half2float(h));
@@ -885,12 +923,7 @@ __global__ void __launch_bounds__(CG_TC_THREADS, 1)
       for (int k = 0; k < K; ++k) mx = fmaxf(mx, fabsf(BSCALE ? xr[k] * bscale[k] : xr[k]));
     }
   }
-  int e = 0;
-  if (mx > 0.f) {
-    int k2;
-    frexpf(mx, &k2);
-    e = 15 - k2;
-  }
+  const int e = mx > 0.f ? 15 - exponent_of(mx) : 0;
   if (warp == 0) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
                      smem_u32(&s_tmem)),
@@ -935,14 +968,14 @@ __global__ void __launch_bounds__(CG_TC_THREADS, 1)
               x.x *= b.x, x.y *= b.y, x.z *= b.z, x.w *= b.w;
             }
           }
-          v8[4 * q] = ldexpf(x.x, e), v8[4 * q + 1] = ldexpf(x.y, e);
-          v8[4 * q + 2] = ldexpf(x.z, e), v8[4 * q + 3] = ldexpf(x.w, e);
+          v8[4 * q] = scale2(x.x, e), v8[4 * q + 1] = scale2(x.y, e);
+          v8[4 * q + 2] = scale2(x.z, e), v8[4 * q + 3] = scale2(x.w, e);
         }
       } else {
 #pragma unroll
         for (int u = 0; u < 8; ++u) {
           const int k = kb + u;
-          v8[u] = (valid && k < K) ? ldexpf(BSCALE ? xr[k] * bscale[k] : xr[k], e) : 0.f;
+          v8[u] = (valid && k < K) ? scale2(BSCALE ? xr[k] * bscale[k] : xr[k], e) : 0.f;
         }
       }
 #pragma unroll
@@ -1020,14 +1053,17 @@ __global__ void __launch_bounds__(CG_TC_THREADS, 1)
     // every lane of the warp takes part in the (warp-collective) TMEM loads;
     // only valid columns store
     tc_fence_after();
-    // 2^-(e + wexp) as two exact powers of two (|e|, |wexp| < 170)
-    const float sc = alpha * ldexpf(1.f, -e) * ldexpf(1.f, -wexp);
+    // the unscaling 2^-(e + wexp) as two exact power-of-two factors applied
+    // one after the other (never multiplied together, which could leave the
+    // float range although the result lies inside it), then alpha
+    const int kt = -(e + wexp), k1 = min(max(kt, -126), 127), k2 = min(max(kt - k1, -149), 127);
+    const float sc = exp2i(k1), sc2 = exp2i(k2);
     float* o = valid ? Out + row * M : nullptr;
     if (rdrain) {
       if (o) {
 #pragma unroll
         for (int m = 0; m < 128; ++m)
-          if (m < M) o[m] = racc[m] * sc * (OSCALE ? oscale[m] : 1.f);
+          if (m < M) o[m] = racc[m] * sc * sc2 * alpha * (OSCALE ? oscale[m] : 1.f);
       }
     } else {
       for (int m0 = 0; m0 < mp; m0 += 16) {
@@ -1037,7 +1073,7 @@ __global__ void __launch_bounds__(CG_TC_THREADS, 1)
 #pragma unroll
           for (int i = 0; i < 16; ++i) {
             const int m = m0 + i;
-            if (m < M) o[m] = __uint_as_float(r[i]) * sc * (OSCALE ? oscale[m] : 1.f);
+            if (m < M) o[m] = __uint_as_float(r[i]) * sc * sc2 * alpha * (OSCALE ? oscale[m] : 1.f);
           }
         }
       }
@@ -1104,3 +1140,15 @@ int run_colgemm_tc(pbbfmm_tree* t, bool post, int lvl, const int* cells, int nco
 
 
 }  // namespace pbbfmm
+
+extern "C" int pbbfmm_debug_set_pipeline_wait_limit(int device, long long polls) {
+  using namespace pbbfmm;
+  int cur = 0;
+  PB_CUDA(cudaGetDevice(&cur));
+  if (device >= 0 && device != cur) PB_CUDA(cudaSetDevice(device));
+  const long long v = polls > 0 ? polls : kWaitIters;
+  const cudaError_t e = cudaMemcpyToSymbol(g_pipe_wait_iters, &v, sizeof(v));
+  if (device >= 0 && device != cur) cudaSetDevice(cur);
+  if (e != cudaSuccess) return cuda_status(e, "set pipeline wait limit");
+  return PBBFMM_OK;
+}

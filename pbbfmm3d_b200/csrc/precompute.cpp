@@ -63,11 +63,13 @@ std::string kernel_type_name(const KernelSpec& k) {
     case PBBFMM_KERNEL_EXPCOV: snprintf(buf, sizeof buf, "ExpCov%g", k.param[0]); return buf;
     case PBBFMM_KERNEL_GAUSSSIGMA: snprintf(buf, sizeof buf, "GaussS%g", k.param[0]); return buf;
     case PBBFMM_KERNEL_ANISOEXP: return "AnisoExp";
+    case PBBFMM_KERNEL_USER: return k.user_type;
     default: return "Unknown";
   }
 }
 
 double eval_kernel_host(const KernelSpec& k, const double t[3], const double s[3]) {
+  if (k.id == PBBFMM_KERNEL_USER) return k.user_eval(t, s, k.user_ctx);
   const double dx = s[0] - t[0], dy = s[1] - t[1], dz = s[2] - t[2];
   switch (k.id) {
     case PBBFMM_KERNEL_LAPLACIAN: return 1. / sqrt(dx * dx + dy * dy + dz * dz);

@@ -13,6 +13,11 @@ struct KernelSpec {
   double param[4] = {0, 0, 0, 0};
   double homogen = 0;  // as set by SetKernelProperty (before the negation)
   int symmetry = 1;
+  // user-defined kernel (id PBBFMM_KERNEL_USER): its kernelType and its
+  // EvaluateKernel(target, source) on the host
+  std::string user_type;
+  double (*user_eval)(const double*, const double*, void*) = nullptr;
+  void* user_ctx = nullptr;
 };
 
 // Kernel metadata of the built-in kernels (src/kernel_Types.cpp).

@@ -32,7 +32,9 @@ sys.path.insert(0, os.path.dirname(os.path.dirname(HERE)))
 
 import oracle  # noqa: E402
 
-REF_INPUT = "/root/reference/input"
+# the reference checkout (read-only) is named by PBBFMM_REF_DIR; its input/
+# fixture is used when present
+REF_INPUT = os.path.join(os.environ.get("PBBFMM_REF_DIR", ""), "input")
 
 
 def run_case(name, kernel, param, box, level, order, eps, cheb, target, weight, ncols,

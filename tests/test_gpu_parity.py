@@ -76,6 +76,14 @@ def test_gpu_matches_oracle_phase_by_phase(meta):
     N = 6000
     p = _points(rng, N, meta["box"])
     w = rng.standard_normal(N * meta["ncols"])
+    phase_by_phase(meta, p, w)
+
+
+def phase_by_phase(meta, p, w):
+    """Run the GPU tree and the oracle on the same operators and points and
+    compare the leaf binning (bit-exact), S and F at every level and the
+    output (1e-12)."""
+    N = p.shape[0]
     ops = host_ops(meta["kernel"], meta["param"], meta["box"], meta["level"], meta["order"],
                    meta["eps"], meta["cheb"])
     t = gpu_tree(meta, ops)

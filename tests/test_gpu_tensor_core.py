@@ -156,3 +156,53 @@ def test_tensor_core_kernel_times_and_switch():
         t.set_tensor_cores(True, "bf16")
     # the C-ABI refuses unknown modes
     assert fmm._lib.lib().pbbfmm_set_tensor_cores(t._h, 7) == fmm._lib.ERR_ARG
+
+
+@pytest.mark.parametrize("kernel,param", [("Laplacian", 0.0), ("GaussSigma", 0.1)])
+def test_tensor_core_extreme_scales(kernel, param):
+    """Weights near 2^-110 (about 8e-34): proxy rows then carry exponents near
+    125 and, for the Gaussian, the coarse levels' operators near 30, so that
+    e_row + e_op passes the float exponent range, and the pre/post transforms'
+    column exponents pass 126.  Every unscaling is applied as exact powers of
+    two, so the result scales by 2^-110 up to the float32 subnormal rounding
+    of terms far below the result (measured 6e-9; a mis-scaled factor shows
+    as 2e-6 or more)."""
+    rng = np.random.default_rng(19)
+    N = 20000
+    p = _clustered(rng, N)
+    w = rng.uniform(-1, 1, N)
+    t = _tree(kernel, param, 4, 4, 1e-6)
+    o = _run(t, p, w, 1, fmm.PREC_MIXED, fmt="f16")
+    assert t.tensor_core_format() == "f16"
+    s = 2.0 ** -110
+    os_ = _run(t, p, w * s, 1, fmm.PREC_MIXED, fmt="f16")
+    assert rel(os_, o * s) < 1e-7, rel(os_, o * s)
+
+
+def test_tensor_core_timeout_reports_and_recovers():
+    """The bounded-wait path.  With the M2L pipeline waits limited to one
+    poll they run out; each CTA stops, waits with the full bound for the
+    copies and MMAs it has already issued, frees its TMEM and sets the
+    timeout flag.  The host entry returns PBBFMM_ERR_TIMEOUT and leaves the
+    caller's output untouched; once the limit is restored the next compute
+    is correct again."""
+    lib = fmm._lib.lib()
+    rng = np.random.default_rng(23)
+    N = 60000
+    p = _clustered(rng, N)
+    w = rng.uniform(-1, 1, N)
+    t = _tree("Laplacian", 0.0, 5, 5, 1e-7)
+    o64 = _run(t, p, w, 1, fmm.PREC_FP64)
+    t.set_precision(fmm.PREC_MIXED)
+    t.set_tensor_cores(True, "f16")
+    out = np.full(N, 7.0)
+    assert lib.pbbfmm_debug_set_pipeline_wait_limit(0, 1) == fmm._lib.OK
+    try:
+        with pytest.raises(fmm.FMMError) as ei:
+            fmm.H2_3D_Compute(t, p, p, w, 1, out)
+        assert ei.value.code == fmm._lib.ERR_TIMEOUT
+    finally:
+        assert lib.pbbfmm_debug_set_pipeline_wait_limit(0, 0) == fmm._lib.OK
+    assert np.all(out == 7.0)
+    o = _run(t, p, w, 1, fmm.PREC_MIXED, fmt="f16")
+    assert rel(o, o64) < 2e-6, rel(o, o64)

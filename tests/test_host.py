@@ -2,6 +2,7 @@
 every declared symbol, the float64 operator precompute reproduces the
 reference's, the reference cache format round-trips, and bad arguments are
 rejected with status codes instead of crashing."""
+import ctypes
 import os
 import re
 
@@ -171,3 +172,82 @@ def test_operator_cache_failures_return_io_status(tmp_path):
     assert e.value.code == _lib.ERR_IO
     t2.buildFMMTree()  # without the cache: computed
     assert t2.get_operators()["rf"] > 0
+
+
+_EVAL = ctypes.CFUNCTYPE(ctypes.c_double, ctypes.POINTER(ctypes.c_double),
+                         ctypes.POINTER(ctypes.c_double), ctypes.c_void_p)
+_LAUNCH = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p)
+
+
+class _UserKernel(ctypes.Structure):
+    """pbbfmm_user_kernel (include/pbbfmm3d_b200.h)."""
+    _fields_ = [
+        ("kernel_type", ctypes.c_char_p),
+        ("homogen", ctypes.c_double),
+        ("symmetry", ctypes.c_int),
+        ("evaluate", _EVAL),
+        ("launch_leaf", _LAUNCH),
+        ("has_gradient", ctypes.c_int),
+        ("ctx", ctypes.c_void_p),
+    ]
+
+
+def _user_tree(kernel, homogen, L=1.0, level=3, order=4, eps=1e-5, cheb=1):
+    p = _lib.TreeParams()
+    p.L, p.tree_level, p.interpolation_order, p.epsilon, p.use_chebyshev = L, level, order, eps, cheb
+    h = ctypes.c_void_p()
+    rc = _lib.lib().pbbfmm_tree_create_user(ctypes.byref(p), ctypes.cast(ctypes.byref(kernel),
+                                                                        ctypes.c_void_p),
+                                            -1, ctypes.byref(h))
+    return rc, h
+
+
+def test_user_kernel_host_precompute_equals_builtin():
+    """A user-defined kernel's float64 operators come from its host
+    EvaluateKernel (here the Laplacian written in Python through the C ABI's
+    evaluate callback): on a host-only tree they equal the built-in
+    Laplacian's, since homogen, symmetry and the kernel values agree."""
+    import math
+
+    calls = [0]
+
+    def lap(t, s, ctx):
+        calls[0] += 1
+        dx, dy, dz = s[0] - t[0], s[1] - t[1], s[2] - t[2]
+        r = math.sqrt(dx * dx + dy * dy + dz * dz)
+        return 1.0 / r if r > 0 else math.inf
+
+    k = _UserKernel()
+    k.kernel_type = b"myLaplacian"
+    k.homogen, k.symmetry = -1.0, 1
+    k.evaluate = _EVAL(lap)
+    k.launch_leaf = _LAUNCH(lambda a, s: 0)
+    k.has_gradient = 0
+    for cheb in (1, 0):
+        rc, h = _user_tree(k, -1.0, cheb=cheb)
+        assert rc == _lib.OK
+        _lib.check(_lib.lib().pbbfmm_tree_build(h, None))
+        b = fmm.kernel_Laplacian(1.0, 3, 4, 1e-5, cheb, device=-1)
+        b.buildFMMTree()
+        ref = b.get_operators()
+        u = fmm.H2_3D_Tree.__new__(fmm.H2_3D_Tree)
+        u._h, u.interpolation_order, u.use_chebyshev = h, 4, cheb
+        ops = u.get_operators()
+        assert ops["rf"] == ref["rf"] and ops["nlev_ops"] == ref["nlev_ops"] == 1
+        assert np.array_equal(ops["K"], ref["K"])
+        u.close()
+        b.close()
+    assert calls[0] > 0
+
+
+def test_user_kernel_rejected_without_its_functions():
+    k = _UserKernel()
+    k.kernel_type = b"x"
+    k.homogen, k.symmetry = 0.0, 1
+    rc, _ = _user_tree(k, 0.0)  # no evaluate / launch_leaf
+    assert rc == _lib.ERR_ARG
+    k.evaluate = _EVAL(lambda t, s, c: 1.0)
+    k.launch_leaf = _LAUNCH(lambda a, s: 0)
+    k.symmetry = 2
+    rc, _ = _user_tree(k, 0.0)
+    assert rc == _lib.ERR_ARG
