@@ -255,6 +255,13 @@ static int upload_tc_operators(pbbfmm_tree* t) {
   if (int rc = upload_tc_uvt(t->ops.U.data(), t->ops.VT.data(), t->ops.nlev, t->n3, t->ops.rf,
                              t->ops.rs, &t->tc))
     return rc;
+  return PBBFMM_OK;
+}
+
+// The timeout flag of the tensor-core kernels (mapped pinned memory), for
+// every tree that computes: the Chebyshev and the uniform M2L both have
+// tensor-core kernels that report through it.
+static int ensure_tc_err_flag(pbbfmm_tree* t) {
   if (!t->h_tc_err) {
     PB_CUDA(cudaHostAlloc(&t->h_tc_err, sizeof(int), cudaHostAllocMapped));
     *t->h_tc_err = 0;
@@ -446,6 +453,7 @@ static int upload_operators(pbbfmm_tree* t) {
   PB_CUDA(cudaSetDevice(t->device));
   free_adjoint_ops(t);  // rebuilt from the new operators on the next adjoint
   int rc;
+  if ((rc = ensure_tc_err_flag(t))) return rc;
   if (t->p.use_chebyshev) {
     if ((rc = upload(&t->d_E, t->ops.K.data(), t->ops.K.size()))) return rc;
     if ((rc = upload(&t->d_U, t->ops.U.data(), t->ops.U.size()))) return rc;
@@ -459,6 +467,11 @@ static int upload_operators(pbbfmm_tree* t) {
     unif_spectra(t->n, t->ops.stencil, t->ops.nlev, &op);
     if ((rc = upload(&t->d_op, op.data(), op.size()))) return rc;
     if ((rc = upload_f32(&t->f_op, op.data(), op.size()))) return rc;
+    std::vector<float> tiles;
+    unif_tc_tiles(t->n, op, t->ops.nlev, &tiles);
+    if (t->f_unif_tiles) cudaFree(t->f_unif_tiles);
+    t->f_unif_tiles = nullptr;
+    if ((rc = upload_vec(&t->f_unif_tiles, tiles))) return rc;
   }
   t->ops_ready = true;
   return PBBFMM_OK;
@@ -471,7 +484,8 @@ static void free_tree_device(pbbfmm_tree* t) {
     if (*b) cudaFree(*b);
     *b = nullptr;
   }
-  float** fbufs[] = {&t->f_Tkz, &t->f_Kw, &t->f_Cw, &t->f_E, &t->f_U, &t->f_VT, &t->f_op, &t->f_twid};
+  float** fbufs[] = {&t->f_Tkz, &t->f_Kw, &t->f_Cw, &t->f_E,    &t->f_U,
+                     &t->f_VT,  &t->f_op, &t->f_twid, &t->f_unif_tiles};
   for (float** b : fbufs) {
     if (*b) cudaFree(*b);
     *b = nullptr;
@@ -487,7 +501,8 @@ static void free_tree_device(pbbfmm_tree* t) {
                    &ws.tperm,     &ws.sperm, &ws.tstart,  &ws.sstart,     &ws.tpos,
                    &ws.spos,      &ws.wsorted, &ws.cub_temp, &ws.lists,    &ws.dcounts,
                    &ws.S,         &ws.F,     &ws.proxy,   &ws.pf,         &ws.io_tgt,
-                   &ws.io_src,    &ws.io_w,  &ws.io_out, &ws.halo, &ws.tc_proxy, &ws.leafpart};
+                   &ws.io_src,    &ws.io_w,  &ws.io_out, &ws.halo, &ws.tc_proxy, &ws.leafpart,
+                   &ws.occ};
   for (DevBuf* b : all) release(*b);
   if (ws.h_in) cudaFreeHost(ws.h_in);
   if (ws.h_out) cudaFreeHost(ws.h_out);

@@ -46,6 +46,7 @@ struct Workspace {
   DevBuf halo;   // Unif M2L: per parent block 512 halo + 64 target cells
   DevBuf tc_proxy;  // tensor-core Cheb M2L: hi then lo proxies of one level (+ F16 exponents)
   DevBuf leafpart;  // leaf phase: target leaves partitioned dense-first, then their count
+  DevBuf occ;       // tensor-core uniform M2L: per-cell source / target occupancy of a level
   // staging for the host-pointer entry point
   DevBuf io_tgt, io_src, io_w, io_out;
   // pinned host staging of the host-buffer entry point (cudaHostAlloc)
@@ -123,6 +124,9 @@ struct pbbfmm_tree {
   float* f_U = nullptr;
   float* f_VT = nullptr;
   float* f_op = nullptr;  // nlev x nk x 343 complex (float2)
+  // tensor-core uniform M2L: per level and frequency the operator tiles of
+  // the block product (m2l_unif_tc.cu), TF32 hi / lo
+  float* f_unif_tiles = nullptr;
   float* f_twid = nullptr;
   // tensor-core Chebyshev M2L (mixed path); tc_fmt: PBBFMM_TC_F16 (scaled
   // F16 operands, default) or PBBFMM_TC_TF32
@@ -221,6 +225,13 @@ int run_colgemm_tc(pbbfmm_tree* t, bool post, int lvl, const int* cells, int nco
 int run_m2l_cheb_tc_level(pbbfmm_tree* t, int C, int l, int lvl, const float* proxy, float* pf,
                           cudaStream_t st);
 int run_m2l_unif(pbbfmm_tree* t, int C, cudaStream_t st);
+// tensor-core uniform M2L (float path): levels with >= 16 parents per side,
+// columns in groups of 8
+bool unif_tc_eligible(const pbbfmm_tree* t, int l, int C);
+int run_m2l_unif_tc_level(pbbfmm_tree* t, int C, int l, int lvl, const float2* X, float2* Y,
+                          cudaStream_t st);
+void unif_tc_tiles(int n, const std::vector<double>& op, int nlev, std::vector<float>* tiles);
+int set_unif_tc_wait_limit(long long polls);
 int run_downward(pbbfmm_tree* t, int C, cudaStream_t st);
 int run_leaves(pbbfmm_tree* t, int64_t Nf, int64_t Ns, int C, double* d_out, cudaStream_t st);
 // operator spectra for the uniform path (host, float64) from the stencils

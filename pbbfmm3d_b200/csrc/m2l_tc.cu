@@ -38,6 +38,7 @@
 #include <mutex>
 
 #include "fmm.cuh"
+#include "tcgen05.cuh"
 
 namespace pbbfmm {
 
@@ -47,219 +48,12 @@ constexpr int TC_PRODUCERS = 128;  // warps 0-3: operand loads
 constexpr int TC_MMA_WARP = 4;     // warp 4: TMEM allocation, MMA issue (one thread)
 constexpr int TC_THREADS = 288;    // + warps 5-8: accumulator drains
 constexpr int TC_TMEM_COLS = 512;  // columns allocated (accumulators and running sum)
-constexpr long long kWaitCycles = 2000000000ll;  // about 1 s of SM clock
-constexpr long long kWaitIters = 1ll << 26;
 // Poll limit of the M2L kernel's pipeline waits (stage and accumulator
 // barriers inside its main loops), per device; kWaitIters unless a test
 // lowers it through pbbfmm_debug_set_pipeline_wait_limit to make those waits
 // run out.  The waits for committed copies and MMAs before a CTA exits always
 // keep the full bound.
 __device__ long long g_pipe_wait_iters = kWaitIters;
-
-__device__ __forceinline__ uint32_t smem_u32(const void* p) {
-  return (uint32_t)__cvta_generic_to_shared(p);
-}
-
-// K-major SWIZZLE_128B shared-memory matrix descriptor (sm100 format:
-// start>>4 in [0,14), LBO>>4 in [16,30) (unused for this layout, 1), SBO>>4 in
-// [32,46) = 1024 bytes between 8-row groups, version 1 in [46,48), layout
-// type 2 = SWIZZLE_128B in [61,64)).  Tile bases are 1024-byte aligned; a K
-// step of 8 float32 inside the 128-byte row advances the start by 32 bytes.
-__device__ __forceinline__ uint64_t sw128_desc(uint32_t addr) {
-  return (uint64_t)((addr >> 4) & 0x3FFF) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
-         ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
-}
-
-// Instruction descriptor for kind::tf32: D float32 (bits 4-5 = 1), A and B
-// TF32 (bits 7-9, 10-12 = 2), both K-major, N>>3 in bits 17-22, M>>4 in 24-28.
-__host__ __device__ constexpr uint32_t tf32_idesc(int M, int N) {
-  return (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(N >> 3) << 17) |
-         ((uint32_t)(M >> 4) << 24);
-}
-// kind::f16 with A and B F16 (format 0 in bits 7-9, 10-12), D float32.
-__host__ __device__ constexpr uint32_t f16_idesc(int M, int N) {
-  return (1u << 4) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
-}
-
-// Byte offset of (row r, 16-byte chunk j) in a K-major SWIZZLE_128B tile.
-__device__ __forceinline__ uint32_t sw128_off(int r, int j) {
-  return (uint32_t)((r >> 3) * 1024 + (r & 7) * 128 + ((j ^ (r & 7)) << 4));
-}
-
-__device__ __forceinline__ void mbar_init(uint64_t* bar, int count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_u32(bar)), "r"(count)
-               : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try(uint32_t a, int parity) {
-  uint32_t done;
-  asm volatile(
-      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
-      " selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(done)
-      : "r"(a), "r"(parity)
-      : "memory");
-  return done != 0;
-}
-
-// Wait for the completion of the phase with parity `parity`; false after
-// about a second of SM clock (or kWaitIters polls) without it, or once *abort
-// is set (abort may be null).  The first poll reads no clock: a wait that is
-// already satisfied costs one try_wait.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, int parity, const volatile int* abort,
-                                          long long iters = kWaitIters) {
-  const uint32_t a = smem_u32(bar);
-  if (mbar_try(a, parity)) return true;
-  const long long t0 = clock64();
-  for (long long it = 0; it < iters; ++it) {
-    if (mbar_try(a, parity)) return true;
-    if ((it & 255) == 255 && ((abort && *abort) || clock64() - t0 > kWaitCycles)) return false;
-  }
-  return false;
-}
-
-__device__ __forceinline__ void mbar_arrive(uint64_t* bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_u32(bar)) : "memory");
-}
-
-// Arrive on `bar` and add `bytes` to the transaction count it waits for.
-__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_u32(bar)),
-               "r"(bytes)
-               : "memory");
-}
-
-// 2-D tiled TMA load (no multicast) into this CTA's shared memory, completing
-// `bytes` of the transaction count of `bar`; x (the innermost coordinate)
-// is a multiple of 32 floats (128 bytes).
-__device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, int x, int y,
-                                            uint64_t* bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, "
-      "%4}], [%2];\n" ::"r"(smem_u32(dst)),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(smem_u32(bar)), "r"(x), "r"(y)
-      : "memory");
-}
-
-// Arrive on `bar` once every cp.async issued so far by this thread has
-// landed (the barrier's expected count includes this arrival).
-__device__ __forceinline__ void cp_async_arrive(uint64_t* bar) {
-  asm volatile("cp.async.mbarrier.arrive.noinc.shared::cta.b64 [%0];\n" ::"r"(smem_u32(bar))
-               : "memory");
-}
-
-__device__ __forceinline__ void fence_async_smem() {
-  asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_before() {
-  asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
-}
-__device__ __forceinline__ void tc_fence_after() {
-  asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
-}
-
-__device__ __forceinline__ void tc_mma_tf32(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc,
-                                            uint32_t accumulate) {
-  asm volatile(
-      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-      " tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
-      "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
-      : "memory");
-}
-__device__ __forceinline__ void tc_mma_f16(uint32_t d_tmem, uint64_t a, uint64_t b, uint32_t idesc,
-                                           uint32_t accumulate) {
-  asm volatile(
-      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(d_tmem),
-      "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
-      : "memory");
-}
-
-// Arrive on `bar` once every tcgen05.mma issued so far by this thread is done.
-__device__ __forceinline__ void tc_commit(uint64_t* bar) {
-  asm volatile(
-      "tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
-          smem_u32(bar))
-      : "memory");
-}
-
-// 16 consecutive float32 columns of this thread's TMEM lane.
-__device__ __forceinline__ void tc_ld16(uint32_t taddr, float* v) {
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, "
-      "%12, %13, %14, %15}, [%16];\n"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-        "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-        "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
-}
-
-// 16 consecutive float32 columns of this thread's TMEM lane, loaded and waited
-// for in one asm statement (so that no use of r can precede the wait).
-__device__ __forceinline__ void tc_ld16_wait(uint32_t taddr, uint32_t* r) {
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];\n"
-      "tcgen05.wait::ld.sync.aligned;\n"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr)
-      : "memory");
-}
-
-// Store 16 consecutive float32 columns of this thread's TMEM lane.
-__device__ __forceinline__ void tc_st16(uint32_t taddr, const float* v) {
-  asm volatile(
-      "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1, %2, %3, %4, %5, %6, %7, %8, %9, %10, "
-      "%11, %12, %13, %14, %15, %16};\n" ::"r"(taddr),
-      "r"(__float_as_uint(v[0])), "r"(__float_as_uint(v[1])), "r"(__float_as_uint(v[2])),
-      "r"(__float_as_uint(v[3])), "r"(__float_as_uint(v[4])), "r"(__float_as_uint(v[5])),
-      "r"(__float_as_uint(v[6])), "r"(__float_as_uint(v[7])), "r"(__float_as_uint(v[8])),
-      "r"(__float_as_uint(v[9])), "r"(__float_as_uint(v[10])), "r"(__float_as_uint(v[11])),
-      "r"(__float_as_uint(v[12])), "r"(__float_as_uint(v[13])), "r"(__float_as_uint(v[14])),
-      "r"(__float_as_uint(v[15]))
-      : "memory");
-}
-__device__ __forceinline__ void tc_wait_st() {
-  asm volatile("tcgen05.wait::st.sync.aligned;\n" ::: "memory");
-}
-
-// 2^k as a float, exactly, for k in [-149, 127].
-__device__ __forceinline__ float exp2i(int k) {
-  return k >= -126 ? __int_as_float((k + 127) << 23) : __int_as_float(1 << (k + 149));
-}
-
-// x 2^k with every step an exact power-of-two product: k is split into
-// factors inside the float exponent range, so the result is exact whenever
-// it is a normal number (whatever k), and correctly rounded otherwise.
-__device__ __forceinline__ float scale2(float x, int k) {
-  k = min(max(k, -400), 400);
-  while (k > 127) {
-    x *= exp2i(127);
-    k -= 127;
-  }
-  while (k < -126) {
-    x *= exp2i(-126);
-    k += 126;
-  }
-  return x * exp2i(k);
-}
-
-// k2 with |x| in [2^(k2-1), 2^k2) for finite x != 0 (frexp's exponent).
-__device__ __forceinline__ int exponent_of(float x) {
-  const uint32_t b = __float_as_uint(x) & 0x7fffffffu;
-  if (b >= 0x00800000u) return (int)(b >> 23) - 126;
-  return 32 - __clz(b) - 149;  // subnormal: b 2^-149, b in [2^(j-1), 2^j)
-}
-
-__device__ __forceinline__ float to_tf32(float x) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;\n" : "=r"(r) : "f"(x));
-  return __uint_as_float(r);
-}
 
 struct TcTiles {
   int start[9];  // first tile of each child type; start[8] = total tiles
@@ -658,7 +452,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
   }
   tc_fence_before();
   __syncthreads();
-  if (tid == 0 && *s_abort) atomicExch(err, 1);
+  if (tid == 0 && *s_abort && err) atomicExch(err, 1);
   if (warp == TC_MMA_WARP) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem),
@@ -1048,7 +842,7 @@ __global__ void __launch_bounds__(CG_TC_THREADS, 1)
       mbar_wait(&s_tma, last_tma & 1, nullptr);
       mbar_wait(&s_mma, last_tma & 1, nullptr);
     }
-    if (tid == 0) atomicExch(err, 1);
+    if (tid == 0 && err) atomicExch(err, 1);
   } else {
     // every lane of the warp takes part in the (warp-collective) TMEM loads;
     // only valid columns store
@@ -1148,7 +942,8 @@ extern "C" int pbbfmm_debug_set_pipeline_wait_limit(int device, long long polls)
   if (device >= 0 && device != cur) PB_CUDA(cudaSetDevice(device));
   const long long v = polls > 0 ? polls : kWaitIters;
   const cudaError_t e = cudaMemcpyToSymbol(g_pipe_wait_iters, &v, sizeof(v));
+  const int rc = e == cudaSuccess ? set_unif_tc_wait_limit(v) : PBBFMM_OK;
   if (device >= 0 && device != cur) cudaSetDevice(cur);
   if (e != cudaSuccess) return cuda_status(e, "set pipeline wait limit");
-  return PBBFMM_OK;
+  return rc;
 }

@@ -557,8 +557,13 @@ static int run_m2l_unif_t(pbbfmm_tree* t, int C, cudaStream_t st) {
     if ((rc = kt_begin(t, KS_MAC, st))) return rc;
     const C2* Xl = X + level_offset(l, perX);
     C2* Yl = Y + level_offset(l, perX);
-    // 4x2x2 parent blocks from level 3 up (level 2 has 2 parents per side)
-    if (l >= 3)
+    // float32, 16 parents per side or more, columns in groups of 8: the
+    // tensor cores (m2l_unif_tc.cu); otherwise 4x2x2 parent blocks on the
+    // CUDA cores from level 3 up (level 2 has 2 parents per side)
+    if (sizeof(T) == 4 && unif_tc_eligible(t, l, C))
+      rc = run_m2l_unif_tc_level(t, C, l, lvl, reinterpret_cast<const float2*>(Xl),
+                                 reinterpret_cast<float2*>(Yl), st);
+    else if (l >= 3)
       rc = launch_mac_cols<4, T>(Xl, Yl, op, halo, sstart, tstart, span, l, C, nk, st);
     else
       rc = launch_mac_cols<2, T>(Xl, Yl, op, halo, sstart, tstart, span, l, C, nk, st);
