@@ -27,10 +27,10 @@
 // float32 operands at about 2^-21 relative error per product (3xTF32 plus
 // the lo x lo term), accumulated in float32.
 //
-// Roles (288 threads): warps 0-3 stage source lines (cp.async of the raw
+// Roles (416 threads): warps 0-7 stage source lines (cp.async of the raw
 // float32 spectra, zero-filled for empty or out-of-domain cells, then a split
 // into the hi / lo A layout) and load each frequency's operator tiles by a
-// bulk copy; one thread of warp 4 issues the MMAs; warps 5-8 drain the
+// bulk copy; one thread of warp 8 issues the MMAs; warps 9-12 drain the
 // accumulators (two TMEM sets, alternating by frequency), write the target
 // spectra and zero the accumulators.  Every wait is bounded; on timeout the
 // kernel sets *err, waits (bounded) for its issued copies and MMAs, frees its
@@ -55,15 +55,18 @@ constexpr int UT_APLANE = UT_ROWS * 16;    // bytes of one K core plane of A
 constexpr int UT_APART = 4 * UT_APLANE;    // hi or lo part of a stage (K = 16 floats)
 constexpr int UT_ASTAGE = 2 * UT_APART;
 constexpr int UT_NST = 3;                  // A stages
-constexpr int UT_RAWLINE = UT_SRCZ * 512;  // raw float32 spectra of one source line
+constexpr int UT_RAWZ = 576;               // bytes per parent in a raw line (512 + bank padding)
+constexpr int UT_RAWLINE = UT_SRCZ * UT_RAWZ;  // raw float32 spectra of one source line
 constexpr int UT_PREFETCH = 4;             // lines whose raw copies run ahead of the split
 constexpr int UT_NRAW = UT_PREFETCH + 2;   // raw slots
 constexpr int UT_BROWS = 96;               // B rows of one (D_x, D_z) tile
 constexpr int UT_BPLANE = UT_BROWS * 16;
 constexpr int UT_BTILE = 4 * UT_BPLANE;
 constexpr int UT_BFREQ = 9 * UT_BTILE;     // operator tiles of one frequency (bytes)
-constexpr int UT_THREADS = 288;
-constexpr int UT_PRODUCERS = 128;
+constexpr int UT_PRODUCERS = 256;          // warps 0-7
+constexpr int UT_MMA_WARP = UT_PRODUCERS / 32;  // warp 8
+constexpr int UT_DRAIN0 = UT_PRODUCERS + 32;    // first drain thread (warps 9-12)
+constexpr int UT_THREADS = UT_DRAIN0 + 128;
 constexpr int UT_TMEM_COLS = 512;          // two sets of UT_BY x 32 columns
 constexpr int UT_SMEM = UT_NST * UT_ASTAGE + UT_NRAW * UT_RAWLINE + 2 * UT_BFREQ + 1024;
 static_assert(2 * UT_BY * 32 == UT_TMEM_COLS, "two accumulator sets fill the TMEM");
@@ -75,18 +78,42 @@ constexpr int kUnifTcTileFloats = UT_BFREQ / 4;
 // Poll limit of the pipeline waits (see g_pipe_wait_iters in m2l_tc.cu).
 __device__ long long g_unif_wait_iters = kWaitIters;
 
-// OR of `v` over the 128 producer threads (warps 0-3), which also acts as
+// OR of `v` over the 256 producer threads (warps 0-7), which also acts as
 // their barrier (named barrier 1): every producer executes the same sequence
 // of these, so none waits for a thread that has left.
 __device__ __forceinline__ bool producers_any(bool v) {
   uint32_t r;
   asm volatile(
-      "{\n .reg .pred p, q;\n setp.ne.u32 q, %1, 0;\n bar.red.or.pred p, 1, 128, q;\n"
+      "{\n .reg .pred p, q;\n setp.ne.u32 q, %1, 0;\n bar.red.or.pred p, 1, 256, q;\n"
       " selp.u32 %0, 1, 0, p;\n}\n"
       : "=r"(r)
       : "r"((uint32_t)v)
       : "memory");
   return r != 0;
+}
+
+// Barrier among the `n` threads of a role group (named barrier `id`).
+__device__ __forceinline__ void group_sync(int id, int n) {
+  asm volatile("bar.sync %0, %1;\n" ::"r"(id), "r"(n) : "memory");
+}
+
+// OR of `v` over the 128 drain threads (warps 9-12, named barrier 2).
+__device__ __forceinline__ bool drains_any(bool v) {
+  uint32_t r;
+  asm volatile(
+      "{\n .reg .pred p, q;\n setp.ne.u32 q, %1, 0;\n bar.red.or.pred p, 2, 128, q;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(r)
+      : "r"((uint32_t)v)
+      : "memory");
+  return r != 0;
+}
+
+// x rounded to TF32 (10 explicit mantissa bits), to nearest with ties away
+// from zero, by integer operations on its bits: the value cvt.rna.tf32.f32
+// gives for finite x (no conversion instruction on the producers' path).
+__device__ __forceinline__ float tf32_rna_bits(float x) {
+  return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xffffe000u);
 }
 
 __global__ void k_occupancy(const int* __restrict__ start, int span, int64_t ncells,
@@ -133,7 +160,7 @@ __global__ void __launch_bounds__(UT_THREADS, 1) k_m2l_unif_tc(const UnifTcArgs 
   const int64_t ncells = (int64_t)1 << (3 * a.lev);
   const int nitems = a.nblocks * a.nchunks;
 
-  if (warp == 4) {
+  if (warp == UT_MMA_WARP) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(
                      smem_u32(&s_tmem)),
                  "r"(UT_TMEM_COLS)
@@ -142,7 +169,7 @@ __global__ void __launch_bounds__(UT_THREADS, 1) k_m2l_unif_tc(const UnifTcArgs 
   }
   if (tid == 0) {
     for (int i = 0; i < UT_NST; ++i) {
-      mbar_init(&s_full[i], UT_PRODUCERS);
+      mbar_init(&s_full[i], 1);
       mbar_init(&s_empty[i], 1);
       s_nz[i] = 0;
     }
@@ -150,7 +177,7 @@ __global__ void __launch_bounds__(UT_THREADS, 1) k_m2l_unif_tc(const UnifTcArgs 
       mbar_init(&s_bfull[i], 1);
       mbar_init(&s_bempty[i], 1);
       mbar_init(&s_accf[i], 1);
-      mbar_init(&s_acce[i], 128);
+      mbar_init(&s_acce[i], 1);
     }
     s_abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
@@ -160,7 +187,7 @@ __global__ void __launch_bounds__(UT_THREADS, 1) k_m2l_unif_tc(const UnifTcArgs 
   tc_fence_after();
   const uint32_t tmem = s_tmem;
   // the drain warps zero both accumulator sets before the first MMA
-  if (warp >= 5) {
+  if (warp > UT_MMA_WARP) {
     const uint32_t lb = tmem + ((uint32_t)(32 * (warp & 3)) << 16);
     const float z[16] = {};
     for (int c = 0; c < UT_TMEM_COLS; c += 16) tc_st16(lb + (uint32_t)c, z);
@@ -170,7 +197,7 @@ __global__ void __launch_bounds__(UT_THREADS, 1) k_m2l_unif_tc(const UnifTcArgs 
   __syncthreads();
   tc_fence_after();
 
-  if (warp < 4) {
+  if (warp < UT_MMA_WARP) {
     // ------------------------------------------------------------ producers
     // The source lines of every frequency of every work item, in the order
     // the MMA thread consumes them: item (block, frequency chunk) round robin
@@ -190,40 +217,72 @@ __global__ void __launch_bounds__(UT_THREADS, 1) k_m2l_unif_tc(const UnifTcArgs 
       }
     };
     const int ptid = tid;
-    // raw copies (cp.async, 16-byte chunks) of one source line into raw slot
-    // `slot`; chunk q: parent zpos = q / 32, child j = (q / 4) % 8, columns
-    // 2 (q % 4) and 2 (q % 4) + 1; zero for empty or out-of-domain cells
-    auto issue_raw = [&](const Pos& p, int slot) {
-      int bx, y0, z0;
-      ut_block(p.item % a.nblocks, S, &bx, &y0, &z0);
-      const int xs = bx + p.sl / (UT_BY + 2) - 1, ys = y0 + p.sl % (UT_BY + 2) - 1;
-      const bool in = xs >= 0 && xs < S && ys >= 0 && ys < S;
-      unsigned char* dst = raw + slot * UT_RAWLINE;
-      // unrolled, so that the occupancy loads of all of this thread's chunks
-      // are in flight together before the first copy needs its answer
-      constexpr int kPer = (UT_SRCZ * 32 + UT_PRODUCERS - 1) / UT_PRODUCERS;
-      int64_t cell[kPer];
-      uint8_t occ[kPer];
+    // This thread's split tasks t = ptid + 256 i: K plane kc = t / 144 and
+    // row = t % 144 = (zpos, column); byte offsets in the raw line and in
+    // one part of an A stage (-1: no task)
+    constexpr int kSplit = (4 * UT_ROWS + UT_PRODUCERS - 1) / UT_PRODUCERS;
+    int split_src[kSplit], split_dst[kSplit];
+#pragma unroll
+    for (int i = 0; i < kSplit; ++i) {
+      const int t = ptid + i * UT_PRODUCERS;
+      const int kc = t / UT_ROWS, row = t - kc * UT_ROWS;
+      split_src[i] = t < 4 * UT_ROWS ? (row >> 3) * UT_RAWZ + (2 * kc) * 64 + (row & 7) * 8 : -1;
+      split_dst[i] = kc * UT_APLANE + row * 16;
+    }
+    // This thread's raw chunks: q_i = ptid + 256 i (16 bytes each): parent
+    // zpos = q / 32, child j = (q / 4) % 8, columns 2 (q % 4) and 2 (q % 4) + 1.
+    // The z part of their Morton codes is fixed per work item.
+    constexpr int kPer = (UT_SRCZ * 32 + UT_PRODUCERS - 1) / UT_PRODUCERS;
+    int item_ctx = -1, bx = 0, y0 = 0, z0 = 0;
+    uint32_t zsp[kPer];
+    auto set_item = [&](int item) {
+      if (item == item_ctx) return;
+      item_ctx = item;
+      ut_block(item % a.nblocks, S, &bx, &y0, &z0);
 #pragma unroll
       for (int i = 0; i < kPer; ++i) {
         const int q = ptid + i * UT_PRODUCERS;
-        const int zpos = q >> 5, j = (q >> 2) & 7;
-        const int z = z0 - 1 + zpos;
-        cell[i] = -1;
-        if (q < UT_SRCZ * 32 && in && z >= 0 && z < S)
-          cell[i] = 8 * (int64_t)morton_encode(xs, ys, z) + j;
-        occ[i] = cell[i] >= 0 ? a.socc[cell[i]] : 0;
+        const int z = z0 - 1 + (q >> 5);
+        zsp[i] = (q < UT_SRCZ * 32 && z >= 0 && z < S) ? spread3((uint32_t)z) : 0xffffffffu;
       }
+    };
+    // A line whose copies are about to be issued: its cells and their
+    // occupancy, loaded one iteration before the copies need them.
+    struct Pending {
+      int64_t cell[kPer];
+      uint8_t occ[kPer];
+      int k;
+    };
+    auto prepare = [&](const Pos& p, Pending& L) {
+      set_item(p.item);
+      const int xs = bx + p.sl / (UT_BY + 2) - 1, ys = y0 + p.sl % (UT_BY + 2) - 1;
+      const bool in = xs >= 0 && xs < S && ys >= 0 && ys < S;
+      const uint32_t xy = in ? (spread3((uint32_t)xs) << 2) | (spread3((uint32_t)ys) << 1) : 0u;
+#pragma unroll
+      for (int i = 0; i < kPer; ++i) {
+        const int q = ptid + i * UT_PRODUCERS;
+        L.cell[i] = (in && zsp[i] != 0xffffffffu) ? 8 * (int64_t)(xy | zsp[i]) + ((q >> 2) & 7) : -1;
+        L.occ[i] = L.cell[i] >= 0 ? a.socc[L.cell[i]] : 0;
+      }
+      L.k = p.k;
+    };
+    // raw copies (cp.async) of a prepared line into raw slot `slot`, zero for
+    // empty or out-of-domain cells; parent rows UT_RAWZ bytes apart
+    auto issue = [&](const Pending& L, int slot) -> bool {
+      unsigned char* dst = raw + slot * UT_RAWLINE;
+      const float2* xk = a.X + (int64_t)L.k * ncells * a.C + a.c0;
+      bool any = false;
 #pragma unroll
       for (int i = 0; i < kPer; ++i) {
         const int q = ptid + i * UT_PRODUCERS;
         if (q < UT_SRCZ * 32) {
-          const bool ok = occ[i] != 0;
-          const float2* src =
-              ok ? a.X + ((int64_t)p.k * ncells + cell[i]) * a.C + a.c0 + 2 * (q & 3) : a.X;
-          cp_async16(dst + q * 16, src, ok ? 16 : 0);
+          const bool ok = L.occ[i] != 0;
+          any |= ok;
+          cp_async16(dst + (q >> 5) * UT_RAWZ + (q & 31) * 16,
+                     ok ? xk + L.cell[i] * a.C + 2 * (q & 3) : a.X, ok ? 16 : 0);
         }
       }
+      return any;
     };
     Pos cur{(int)blockIdx.x, 0, 0};
     if (cur.item < nitems) cur.k = first_k(cur.item);
@@ -231,15 +290,23 @@ __global__ void __launch_bounds__(UT_THREADS, 1) k_m2l_unif_tc(const UnifTcArgs 
     // UT_PREFETCH + 2 slots (a slot is rewritten two iterations after its
     // split, so one barrier per line orders the reuse)
     Pos pf = cur;
+    Pending L;
+    bool have = pf.item < nitems;
+    if (have) prepare(pf, L);
     int issued = 0;
-    for (int i = 0; i < UT_PREFETCH; ++i) {
-      if (pf.item < nitems) {
-        issue_raw(pf, issued % UT_NRAW);
+    uint32_t anymask = 0;  // bit r: this thread's chunks of the line in raw slot r hold data
+    auto issue_next = [&]() {
+      if (have) {
+        const int slot = issued % UT_NRAW;
+        anymask = (anymask & ~(1u << slot)) | ((issue(L, slot) ? 1u : 0u) << slot);
         ++issued;
         advance(pf);
+        have = pf.item < nitems;
+        if (have) prepare(pf, L);
       }
-      cp_async_commit();
-    }
+      cp_async_commit();  // (possibly empty) keeps one group per line
+    };
+    for (int i = 0; i < UT_PREFETCH; ++i) issue_next();
     // operator tiles: frequency f goes to buffer f % 2; the load for f + 1 is
     // issued in the middle of frequency f (the MMAs of f - 1, the buffer's
     // previous user, are issued by then)
@@ -265,53 +332,45 @@ __global__ void __launch_bounds__(UT_THREADS, 1) k_m2l_unif_tc(const UnifTcArgs 
     if (ptid == 0 && cur.item < nitems) fail = !load_b();
     for (; cur.item < nitems; advance(cur)) {
       if (ptid == 0 && cur.sl == UT_SRC_LINES / 2 && !fail) fail = !load_b();
-      if (pf.item < nitems) {
-        issue_raw(pf, issued % UT_NRAW);
-        ++issued;
-        advance(pf);
-      }
-      cp_async_commit();  // (possibly empty) keeps one group per line
+      issue_next();
       asm volatile("cp.async.wait_group %0;\n" ::"n"(UT_PREFETCH) : "memory");
       const int s = li % UT_NST;
-      if (li >= UT_NST && !mbar_wait(&s_empty[s], (li / UT_NST - 1) & 1, s_abort, piters))
+      // one thread waits for the stage (its MMAs of UT_NST lines ago); the
+      // barrier-with-reduction then releases every producer, makes the raw
+      // line complete for all of them, and lets all leave together on failure
+      if (ptid == 0 && li >= UT_NST &&
+          !mbar_wait(&s_empty[s], (li / UT_NST - 1) & 1, s_abort, piters))
         fail = true;
-      // one barrier per line among the producers: the raw line is complete
-      // (every thread's copies) and all leave together on a failure
       if (producers_any(fail)) {
         *s_abort = 1;
         break;
       }
-      // split into the A layout: task (zpos, kc, column pair) -> rows c, c+1
+      // split into the A layout: task t = (kc, row), row = (zpos, column);
+      // a warp's stores fill 32 consecutive 16-byte rows of one K plane
       const unsigned char* rl = raw + (li % UT_NRAW) * UT_RAWLINE;
       unsigned char* ahi = astage + s * UT_ASTAGE;
       unsigned char* alo = ahi + UT_APART;
-      bool any = false;
-      for (int q = ptid; q < UT_SRCZ * 16; q += UT_PRODUCERS) {
-        const int zpos = q >> 4, kc = (q >> 2) & 3, cp = q & 3;
-        const float4 u =
-            *reinterpret_cast<const float4*>(rl + zpos * 512 + (2 * kc) * 64 + cp * 16);
-        const float4 v =
-            *reinterpret_cast<const float4*>(rl + zpos * 512 + (2 * kc + 1) * 64 + cp * 16);
-        // row c = 2 cp: (u.x, u.y, v.x, v.y); row c + 1: (u.z, u.w, v.z, v.w)
-        const float r0[4] = {u.x, u.y, v.x, v.y}, r1[4] = {u.z, u.w, v.z, v.w};
-        float h0[4], l0[4], h1[4], l1[4];
 #pragma unroll
-        for (int e = 0; e < 4; ++e) {
-          h0[e] = to_tf32(r0[e]);
-          l0[e] = to_tf32(r0[e] - h0[e]);
-          h1[e] = to_tf32(r1[e]);
-          l1[e] = to_tf32(r1[e] - h1[e]);
-          any |= r0[e] != 0.f || r1[e] != 0.f;
+      for (int i = 0; i < kSplit; ++i) {
+        if (split_src[i] >= 0) {
+          const unsigned char* src = rl + split_src[i];
+          const float2 u = *reinterpret_cast<const float2*>(src);
+          const float2 v = *reinterpret_cast<const float2*>(src + 64);
+          const float r[4] = {u.x, u.y, v.x, v.y};
+          float h[4], l[4];
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            h[e] = tf32_rna_bits(r[e]);
+            l[e] = tf32_rna_bits(r[e] - h[e]);
+          }
+          *reinterpret_cast<float4*>(ahi + split_dst[i]) = make_float4(h[0], h[1], h[2], h[3]);
+          *reinterpret_cast<float4*>(alo + split_dst[i]) = make_float4(l[0], l[1], l[2], l[3]);
         }
-        const int off = kc * UT_APLANE + (zpos * 8 + 2 * cp) * 16;
-        *reinterpret_cast<float4*>(ahi + off) = make_float4(h0[0], h0[1], h0[2], h0[3]);
-        *reinterpret_cast<float4*>(ahi + off + 16) = make_float4(h1[0], h1[1], h1[2], h1[3]);
-        *reinterpret_cast<float4*>(alo + off) = make_float4(l0[0], l0[1], l0[2], l0[3]);
-        *reinterpret_cast<float4*>(alo + off + 16) = make_float4(l1[0], l1[1], l1[2], l1[3]);
       }
-      if (any) s_nz[s] = li + 1;
-      fence_async_smem();  // the generic-proxy stores, to the tensor pipe
-      mbar_arrive(&s_full[s]);
+      if ((anymask >> (li % UT_NRAW)) & 1u) s_nz[s] = li + 1;
+      fence_async_smem();  // this thread's generic-proxy stores, to the tensor pipe
+      group_sync(1, UT_PRODUCERS);  // every producer's stores and fence
+      if (ptid == 0) mbar_arrive(&s_full[s]);
       ++li;
       if (cur.sl == UT_SRC_LINES - 1) ++fi;
     }
@@ -321,7 +380,7 @@ __global__ void __launch_bounds__(UT_THREADS, 1) k_m2l_unif_tc(const UnifTcArgs 
         !mbar_wait(&s_bfull[last_b & 1], (last_b >> 1) & 1, nullptr))
       *s_abort = 1;
     (void)fi;
-  } else if (warp == 4) {
+  } else if (warp == UT_MMA_WARP) {
     // ------------------------------------------------------------ MMA issue
     if (lane == 0) {
       int fi = 0, li = 0;
@@ -347,7 +406,6 @@ __global__ void __launch_bounds__(UT_THREADS, 1) k_m2l_unif_tc(const UnifTcArgs 
               stop = true;
               break;
             }
-            fence_async_smem();
             tc_fence_after();
             if (s_nz[s] == li + 1) {
               const int dxi = sl / (UT_BY + 2), sy = sl % (UT_BY + 2) - 1;
@@ -355,19 +413,22 @@ __global__ void __launch_bounds__(UT_THREADS, 1) k_m2l_unif_tc(const UnifTcArgs 
               const int dyi_lo = ty_lo - sy + 1, nl = ty_hi - ty_lo + 1;
               const uint32_t idesc = tf32_idesc(128, 32 * nl);
               const uint32_t d = dset + (uint32_t)(32 * ty_lo);
-              const uint32_t ahi = smem_u32(astage + s * UT_ASTAGE), alo = ahi + UT_APART;
+              // descriptors of the line's first A and B tiles; the others
+              // differ only in their start address (16-byte units, no carry:
+              // shared memory is below 256 KB), by compile-time offsets
+              const uint64_t a0 = kmajor_desc(smem_u32(astage + s * UT_ASTAGE), UT_APLANE, 128);
+              const uint64_t b0 =
+                  kmajor_desc(bb + (uint32_t)(dxi * 3 * UT_BTILE + dyi_lo * 32 * 16), UT_BPLANE, 128);
 #pragma unroll
-              for (int dzi = 0; dzi < 3; ++dzi) {
-                const uint32_t bt = bb + (uint32_t)((dxi * 3 + dzi) * UT_BTILE + dyi_lo * 32 * 16);
-                const uint32_t aw = (uint32_t)(dzi * 8 * 16);  // window: D_z + 1 parents down
+              for (int dzi = 0; dzi < 3; ++dzi)
 #pragma unroll
                 for (int ks = 0; ks < 2; ++ks) {
-                  const uint64_t bd = kmajor_desc(bt + ks * 2 * UT_BPLANE, UT_BPLANE, 128);
-                  const uint32_t ao = aw + ks * 2 * UT_APLANE;
-                  tc_mma_tf32(d, kmajor_desc(ahi + ao, UT_APLANE, 128), bd, idesc, 1u);
-                  tc_mma_tf32(d, kmajor_desc(alo + ao, UT_APLANE, 128), bd, idesc, 1u);
+                  // A window D_z + 1 parents down; K step ks = planes 2 ks, 2 ks + 1
+                  const uint64_t ah = a0 + ((dzi * 8 * 16 + ks * 2 * UT_APLANE) >> 4);
+                  const uint64_t bd = b0 + ((dzi * UT_BTILE + ks * 2 * UT_BPLANE) >> 4);
+                  tc_mma_tf32(d, ah, bd, idesc, 1u);
+                  tc_mma_tf32(d, ah + (UT_APART >> 4), bd, idesc, 1u);
                 }
-              }
             }
             tc_commit(&s_empty[s]);
             committed = true;
@@ -396,8 +457,12 @@ __global__ void __launch_bounds__(UT_THREADS, 1) k_m2l_unif_tc(const UnifTcArgs 
       const int k0 = (item / a.nblocks) * a.kchunk, k1 = min(a.nk, k0 + a.kchunk);
       for (int k = k0; k < k1; ++k, ++fi) {
         const int fb = fi & 1;
-        // warp-uniform: the TMEM loads below are warp-collective
-        if (!__all_sync(0xffffffffu, mbar_wait(&s_accf[fb], (fi >> 1) & 1, s_abort, piters))) {
+        // one thread waits for the accumulators; the barrier-with-reduction
+        // releases the other drain threads (uniformly: the TMEM loads below
+        // are warp-collective)
+        bool bad = false;
+        if (tid == UT_DRAIN0 && !mbar_wait(&s_accf[fb], (fi >> 1) & 1, s_abort, piters)) bad = true;
+        if (drains_any(bad)) {
           *s_abort = 1;
           stop = true;
           break;
@@ -422,14 +487,15 @@ __global__ void __launch_bounds__(UT_THREADS, 1) k_m2l_unif_tc(const UnifTcArgs 
         }
         tc_wait_st();
         tc_fence_before();
-        mbar_arrive(&s_acce[fb]);
+        group_sync(2, 128);  // every drain thread's loads and stores
+        if (tid == UT_DRAIN0) mbar_arrive(&s_acce[fb]);
       }
     }
   }
   tc_fence_before();
   __syncthreads();
   if (tid == 0 && *s_abort && a.err) atomicExch(a.err, 1);
-  if (warp == 4) {
+  if (warp == UT_MMA_WARP) {
     tc_fence_after();
     asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem),
                  "r"(UT_TMEM_COLS)
