@@ -209,6 +209,76 @@ def direct_sum_sampled(pts, w, C, rows, wl, device):
     return out.cpu().numpy()
 
 
+def leaf_grid(tstart, L):
+    """Points per leaf as a (side, side, side) grid (the reference's leaf
+    numbering is Morton with x most significant)."""
+    cnt = np.diff(tstart)
+    side = 1 << L
+    idx = np.arange(8 ** L)
+    x = np.zeros_like(idx)
+    y = np.zeros_like(idx)
+    z = np.zeros_like(idx)
+    for b in range(L):
+        x |= ((idx >> (3 * b + 2)) & 1) << b
+        y |= ((idx >> (3 * b + 1)) & 1) << b
+        z |= ((idx >> (3 * b)) & 1) << b
+    grid = np.zeros((side, side, side), dtype=np.int64)
+    grid[x, y, z] = cnt
+    return grid
+
+
+def near_field_pairs(tstart, L):
+    """Ordered (target, source) pairs of the near field, sources = targets:
+    the sum over leaves of (targets in the leaf) x (sources in its 27
+    neighbour leaves, itself included), counted from the built tree."""
+    g = leaf_grid(tstart, L)
+    p = np.pad(g, 1)
+    side = g.shape[0]
+    nb = np.zeros_like(g)
+    for dx in range(3):
+        for dy in range(3):
+            for dz in range(3):
+                nb += p[dx:dx + side, dy:dy + side, dz:dz + side]
+    return int((g * nb).sum())
+
+
+# special-function operations per near-field pair (rsqrt, sqrt, exp)
+SFU_PER_PAIR = {"Laplacian": 1, "ExpCov": 2, "GaussSigma": 1}
+FLOPS_PER_INTERACTION = 20  # the counting convention for one kernel evaluation + FMA
+
+
+def near_field(fmm, tree, wl, results, steps, local_rank):
+    """Leaf phase (L2P + P2P, k_leaf / k_leaf_sparse) of the mixed path:
+    near-field interactions (ordered pairs x columns) per second, against the
+    measured float32 FMA and reciprocal-square-root peaks of this GPU."""
+    tstart = tree.debug_copy(2).astype(np.int64)
+    pairs = near_field_pairs(tstart, wl["L"])
+    C = wl["C"]
+    ms = results["mixed"]["ktimes"]["leaf"][0] / steps
+    ms64 = results["fp64"]["ktimes"]["leaf"][0] / steps
+    fp32 = fmm.measure_fma_peak(local_rank, fmm.PREC_MIXED)
+    sfu = fmm.measure_fma_peak(local_rank, 2)
+    inter = pairs * C
+    flops = inter * FLOPS_PER_INTERACTION
+    sfu_ops = pairs * SFU_PER_PAIR.get(wl["kernel"], 1)
+    return {
+        "pairs": pairs, "interactions_per_step": inter,
+        "ms_per_step": ms, "interactions_per_s": inter / (ms * 1e-3),
+        "fp32": {"achieved": flops / (ms * 1e-3) / 1e12, "peak": fp32, "unit": "TFLOP/s",
+                 "frac": flops / (ms * 1e-3) / 1e12 / fp32,
+                 "convention": "%d flops per interaction (one kernel evaluation and its "
+                               "multiply-add per column)" % FLOPS_PER_INTERACTION},
+        "sfu": {"achieved": sfu_ops / (ms * 1e-3) / 1e12, "peak": sfu, "unit": "1e12 ops/s",
+                "frac": sfu_ops / (ms * 1e-3) / 1e12 / sfu,
+                "convention": "%d special-function operation(s) per pair, independent of the "
+                              "columns" % SFU_PER_PAIR.get(wl["kernel"], 1)},
+        "peak_source": "measured in this run: float32 FMA and rsqrtf loops on every SM "
+                       "(pbbfmm_measure_fma_peak precision 1 and 2)",
+        "includes": "the leaf phase's L2P and its leaf partitioning, which the time also covers",
+        "fp64_path_ms_per_step": ms64,
+    }
+
+
 def interaction_pairs(tstart, L):
     """Number of (target cell, source cell) M2L pairs per level, counted from
     the built tree (sources = targets)."""
@@ -377,14 +447,34 @@ def per_step(kt, steps):
     return {k: v[0] / steps for k, v in kt.items() if v[1]}
 
 
-# DRAM bytes per (cell, frequency, column) of k_m2l_unif_mac<float>, from
-# the ncu capture in profiles/k_m2l_unif_mac_expcov0.3_unif5_N262144_C8_L5.md
-MAC_DRAM_BYTES_PER_UNIT = (852.425728e6 + 816.260608e6) / (32768 * 405 * 8)
+# DRAM bytes per (cell, frequency, column) of the frequency-domain M2L, from
+# the ncu capture in profiles/k_m2l_unif_tc_expcov0.3_unif5_N262144_C8_L5.md
+# (the level-5 launch of k_m2l_unif_tc: 891.98 MB read + 810.80 MB written
+# for 32,768 cells x 405 frequencies x 8 columns)
+MAC_DRAM_BYTES_PER_UNIT = (891.978752e6 + 810.800896e6) / (32768 * 405 * 8)
+# tensor-core MAC tiling (csrc/m2l_unif_tc.cu): 8 target lines of 16 parents
+# per CTA, 3 x 10 source lines per frequency, 12 MMAs (M = 128, K = 8) per
+# source line with N = 32 x (target lines it serves)
+UT_BY, UT_LINE = 8, 16
+
+
+def unif_tc_issued_flops(L, nk):
+    """Tensor-pipe flops the MMAs of k_m2l_unif_tc issue per step (empty
+    source lines skipped at run time are counted: an upper bound)."""
+    nl = [min(UT_BY - 1, sy + 1) - max(0, sy - 1) + 1 for sy in range(-1, UT_BY + 1)]
+    per_cta_freq = 3 * sum(12 * 128 * 32 * k * 8 * 2 for k in nl)
+    total = 0
+    for l in range(5, L + 1):
+        S = 1 << (l - 1)
+        total += S * (S // UT_BY) * (S // UT_LINE) * nk * per_cta_freq
+    return float(total)
 
 
 def unif_roofline(fmm, tree, wl, results, steps, local_rank):
-    """Frequency-domain M2L (k_m2l_unif_mac): one complex MAC (8 flops) per
-    (M2L pair, frequency, column); float32 FMA throughput bounds it."""
+    """Frequency-domain M2L: one complex MAC (8 useful flops) per (M2L pair,
+    frequency, column).  Levels with >= 16 parents per side run on the tensor
+    cores (k_m2l_unif_tc, kind::tf32, hi/lo splits of both operands), the
+    coarser ones on the CUDA cores (k_m2l_unif_mac<float>)."""
     kt = results["mixed"]["ktimes"]
     tstart = tree.debug_copy(2).astype(np.int64)
     pairs = interaction_pairs(tstart, wl["L"])
@@ -397,29 +487,30 @@ def unif_roofline(fmm, tree, wl, results, steps, local_rank):
     nbytes = sum(2 * nonempty[l] * nk * C * 8 for l in nonempty)  # float2: read X^, write Y^
     peaks, peak_kind = load_peaks()
     fp64_peak = fmm.measure_fma_peak(local_rank, fmm.PREC_FP64)
-    fp32_peak = fmm.measure_fma_peak(local_rank, fmm.PREC_MIXED)
+    tf32_peak = peaks["bf16_tflops"] / 2.0
     mac_ms = kt["m2l_mac"][0] / steps
     mac64_ms = results["fp64"]["ktimes"]["m2l_mac"][0] / steps
     achieved = flops / (mac_ms * 1e-3) / 1e12
+    issued = unif_tc_issued_flops(wl["L"], nk) * (C // 8) if C % 8 == 0 else 0.0
     return {
-        "kernel": "k_m2l_unif_mac<float> (frequency-domain M2L, mixed path)",
-        "bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
-        "frac": achieved / fp32_peak,
+        "kernel": "k_m2l_unif_tc (tcgen05 kind::tf32 block product, levels >= 5) + "
+                  "k_m2l_unif_mac<float> (levels 2-4), frequency-domain M2L, mixed path",
+        "bound": "tensor", "achieved": achieved, "peak": tf32_peak, "unit": "TFLOP/s",
+        "frac": achieved / tf32_peak,
+        "tensor_pipe_issued_frac": issued / (mac_ms * 1e-3) / 1e12 / tf32_peak,
+        "peak_source": "dense TF32 = half the %s bf16 tensor figure of MEASURED_PEAKS.json "
+                       "(%.0f TFLOP/s)" % (peak_kind, peaks["bf16_tflops"]),
         # DRAM bytes per step, scaled from one ncu capture of the same kernel
-        # (profiles/k_m2l_unif_mac_expcov0.3_unif5_N262144_C8_L5.md: 1.669 GB
-        # read + written for 32,768 cells x 405 frequencies x 8 columns, i.e.
-        # 15.7 B per (cell, frequency, column) against 16 B algorithmic)
         "traffic": sum(nonempty.values()) * nk * C * MAC_DRAM_BYTES_PER_UNIT,
         "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of the level-5 "
                           "launch of bench.py --workload profile, scaled per (cell, frequency, "
                           "column); bytes per step",
-        "peak_source": "measured in this run: float32 FMA loop on every SM "
-                       "(pbbfmm_measure_fma_peak); the kernel runs on the CUDA cores, so neither "
-                       "the HBM copy nor the bf16 tensor figure of MEASURED_PEAKS.json bounds it",
-        "fp64_path": {"achieved": flops / (mac64_ms * 1e-3) / 1e12, "peak": fp64_peak,
+        "fp64_path": {"kernel": "k_m2l_unif_mac<double> (CUDA cores)",
+                      "achieved": flops / (mac64_ms * 1e-3) / 1e12, "peak": fp64_peak,
                       "frac": flops / (mac64_ms * 1e-3) / 1e12 / fp64_peak, "unit": "TFLOP/s"},
-        "algorithmic": "%.4g flops per step = %d M2L pairs x %d freqs x %d cols x 8" % (
-            flops, sum(pairs.values()), nk, C),
+        "algorithmic": "%.4g useful flops per step = %d M2L pairs x %d freqs x %d cols x 8; "
+                       "the tensor pipe issues %.4g (dense 8x8 complex blocks, hi/lo splits, "
+                       "four products)" % (flops, sum(pairs.values()), nk, C, issued),
         "launches_per_step": kt["m2l_mac"][1] / steps,
         "hbm": {"achieved": nbytes / (mac_ms * 1e-3) / 1e9, "peak": peaks["hbm_gbs"],
                 "unit": "GB/s", "frac": nbytes / (mac_ms * 1e-3) / 1e9 / peaks["hbm_gbs"],
@@ -519,6 +610,7 @@ def run_workload(wl, args, rank, world, local_rank, e2e_wanted):
                       "stages them through pinned memory; output accumulated on the host)"}
     roof = (cheb_roofline if wl["cheb"] else unif_roofline)(fmm, tree, wl, results, args.steps,
                                                              local_rank)
+    nfield = near_field(fmm, tree, wl, results, args.steps, local_rank)
     r, r64 = results["mixed"], results["fp64"]
     value = job_throughput(world, N, C, args.steps, r["total_ms"])
     value64 = job_throughput(world, N, C, args.steps, r64["total_ms"])
@@ -530,7 +622,7 @@ def run_workload(wl, args, rank, world, local_rank, e2e_wanted):
         "mixed_over_fp64": value / value64,
         "phase_ms_per_step": per_step(kt, args.steps),
         "dominant_kernel": max(kt, key=lambda k: kt[k][0]),
-        "roofline": roof, "e2e": e2e,
+        "roofline": roof, "near_field": nfield, "e2e": e2e,
         "gpu_launches": int(r["launches"]), "gpu_launches_per_step": r["launches"] / args.steps,
         "clocks": r["clocks"],
         "config": workload_config(wl),
@@ -663,7 +755,7 @@ def our_arm(args, rank, world, local_rank):
         for key, wname in (("target_config", "clustered"), ("target_config_order7", "clustered7")):
             t = run_workload(WORKLOADS[wname], args, rank, world, local_rank, False)
             blk = {k: t[k] for k in ("config", "precision_detail", "value", "ms_per_step",
-                                     "rel_l2_err", "fp64",
+                                     "rel_l2_err", "fp64", "near_field",
                                      "mixed_over_fp64", "phase_ms_per_step", "dominant_kernel",
                                      "roofline", "gpu_launches_per_step", "clocks")}
             blk["unit"] = "N*nCols/s"
@@ -700,6 +792,7 @@ def our_arm(args, rank, world, local_rank):
         "phase_ms_per_step": head["phase_ms_per_step"],
         "dominant_kernel": head["dominant_kernel"],
         "roofline": head["roofline"],
+        "near_field": head["near_field"],
         "cpu_baseline": cpu,
         "e2e": head["e2e"],
         "gpu_launches": head["gpu_launches"],

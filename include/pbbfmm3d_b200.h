@@ -243,7 +243,9 @@ int pbbfmm_get_kernel_times(pbbfmm_tree *tree, float *ms, int *launches, int max
                             int *nslots, const char **names);
 
 /* Measured float64 (precision 0) or float32 (1) FMA throughput of `device`
- * in TFLOP/s (2 flops per FMA): the peak the CUDA-core kernels are held to. */
+ * in TFLOP/s (2 flops per FMA): the peak the CUDA-core kernels are held to;
+ * precision 2: float32 reciprocal square roots (the special-function pipe)
+ * in 1e12 per second. */
 int pbbfmm_measure_fma_peak(int device, int precision, double *tflops);
 
 /* Debug/test access to device arrays of the last compute (all as float64):

@@ -210,11 +210,13 @@ struct PlainSum {
 template <typename T>
 using LeafAcc = typename std::conditional<sizeof(T) == 4, Kahan<T>, PlainSum<T>>::type;
 
+// Dense leaves (at least kLaneLeafMin targets): warp = one 32-target chunk,
+// one target per lane, sources through shared-memory tiles of 32.
 // T = float (mixed path): kernel values, interpolation and per-tile partial
 // sums in float32, each lane's running sums compensated (Kahan), the output
 // update in float64.  T = double: everything in float64.
-template <class KF, typename T, int KC, bool DENSE>
-__global__ void __launch_bounds__(32 * kLeafWarps, DENSE ? 4 : 6)
+template <class KF, typename T, int KC>
+__global__ void __launch_bounds__(32 * kLeafWarps, 4)
     k_leaf(const int* __restrict__ leaves, int nleaves, const int* __restrict__ part_count,
            const int* __restrict__ chunk_prefix, const int* __restrict__ tstart,
            const int* __restrict__ sstart, const int* __restrict__ tperm,
@@ -228,42 +230,31 @@ __global__ void __launch_bounds__(32 * kLeafWarps, DENSE ? 4 : 6)
   __shared__ double kp[4];
   __shared__ int s_nb[kLeafWarps][27][2];  // neighbour source ranges
   __shared__ int s_pre[kLeafWarps][28];    // exclusive prefix of their lengths
-  __shared__ V4 s_sh[kLeafWarps][DENSE ? 32 : 1];              // staged sources: position (hi)
-  __shared__ V4 s_sl[kLeafWarps][DENSE && kMixed ? 32 : 1];    // position (lo), mixed path
-  __shared__ T s_w[kLeafWarps][DENSE ? 32 : 1][KC];            // staged weights
+  __shared__ V4 s_sh[kLeafWarps][32];               // staged sources: position (hi)
+  __shared__ V4 s_sl[kLeafWarps][kMixed ? 32 : 1];  // position (lo), mixed path
+  __shared__ T s_w[kLeafWarps][32][KC];             // staged weights
   // basis values of each lane's target, [warp][dim][m < n][lane] (dynamic, sized by n)
   extern __shared__ __align__(16) unsigned char leaf_dyn[];
   T* s_bw = reinterpret_cast<T*>(leaf_dyn) + (threadIdx.x >> 5) * 3 * n * 32;
-  __shared__ T s_bs[kLeafWarps][DENSE ? 1 : 3 * kMaxOrder];  // sparse path: the warp's target
   for (int i = threadIdx.x; i < n * n; i += blockDim.x) sTkz[i] = Tkz_g[i];
   if (threadIdx.x < 4) kp[threadIdx.x] = kparam_g[threadIdx.x];
   __syncthreads();
   const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
   const int wid = blockIdx.x * kLeafWarps + wl;
-  // leaves are partitioned: the dense ones first, the sparse ones after
+  // leaves are partitioned: the dense ones first, the sparse ones after;
+  // warp = one 32-target chunk of a dense leaf, chunk_prefix[i] the first
+  // chunk of dense leaf i (exclusive scan), chunk_prefix[nd] the total
   const int nd = *part_count;
-  int leaf, ta, te, tc0 = 0;
-  if constexpr (DENSE) {
-    // warp = one 32-target chunk of a dense leaf; chunk_prefix[i] is the first
-    // chunk of dense leaf i (exclusive scan), chunk_prefix[nd] the total
-    if (wid >= chunk_prefix[nd]) return;
-    int lo = 0, hi = nd - 1;
-    while (lo < hi) {  // last i with chunk_prefix[i] <= wid
-      const int mid = (lo + hi + 1) >> 1;
-      if (chunk_prefix[mid] <= wid) lo = mid;
-      else hi = mid - 1;
-    }
-    leaf = leaves[lo];
-    ta = tstart[leaf];
-    te = tstart[leaf + 1];
-    tc0 = ta + 32 * (wid - chunk_prefix[lo]);
-  } else {
-    if (wid >= nleaves - nd) return;
-    leaf = leaves[nd + wid];
-    ta = tstart[leaf];
-    te = tstart[leaf + 1];
+  if (wid >= chunk_prefix[nd]) return;
+  int lo = 0, hi = nd - 1;
+  while (lo < hi) {  // last i with chunk_prefix[i] <= wid
+    const int mid = (lo + hi + 1) >> 1;
+    if (chunk_prefix[mid] <= wid) lo = mid;
+    else hi = mid - 1;
   }
-  if ((te - ta >= kLaneLeafMin) != DENSE) return;  // the other instantiation's leaf
+  const int leaf = leaves[lo];
+  const int te = tstart[leaf + 1];
+  const int tc0 = tstart[leaf] + 32 * (wid - chunk_prefix[lo]);
   const int n3 = n * n * n;
   double c[3];
   cell_center_d((uint32_t)leaf, L, box, c);
@@ -297,60 +288,6 @@ __global__ void __launch_bounds__(32 * kLeafWarps, DENSE ? 4 : 6)
   }
   __syncwarp();
   const int nsrc_total = s_pre[wl][27];
-  if constexpr (!DENSE) {
-    // Sparse leaf: one target at a time, lanes over its sources and over the
-    // n^3 local coefficients, warp-reduced in float64.
-    for (int c0 = 0; c0 < C; c0 += KC) {
-      const int cg = min(KC, C - c0);
-      for (int i = ta; i < te; ++i) {
-        const double x = tpos[i], y = tpos[(int64_t)Nf + i], z = tpos[2 * (int64_t)Nf + i];
-        LeafAcc<T> acc[KC];
-        __syncwarp();
-        if (lane < 3 * n) {
-          const int d = lane / n, mm = lane % n;
-          const T u = (T)(ihalfL * ((d == 0 ? x : d == 1 ? y : z) - c[d]));
-          s_bs[wl][d * n + mm] = basis_one<T>(n, cheb, u, sTkz, mm);
-        }
-        __syncwarp();
-        const T* Fl = F_L + ((int64_t)leaf * C + c0) * n3;
-        for (int l = lane; l < n3; l += 32) {
-          const int l1 = l / (n * n), l2 = (l / n) % n, l3 = l % n;
-          const T v = s_bs[wl][l1] * s_bs[wl][n + l2] * s_bs[wl][2 * n + l3];
-#pragma unroll
-          for (int cc = 0; cc < KC; ++cc)
-            if (cc < cg) acc[cc].add(Fl[cc * n3 + l] * v);
-        }
-        int q = 0;
-        for (int v = lane; v < nsrc_total; v += 32) {
-          while (v >= s_pre[wl][q + 1]) ++q;
-          const int j = s_nb[wl][q][0] + (v - s_pre[wl][q]);
-          const T dx = (T)(spos[j] - x), dy = (T)(spos[(int64_t)Ns + j] - y),
-                  dz = (T)(spos[2 * (int64_t)Ns + j] - z);
-          T kv = KF::template eval<T>(dx, dy, dz, kp);
-          if (isinf(kv)) kv = 0;  // coincident points (include/compute.hpp:767)
-          const double* wj = wsorted + (int64_t)j * C + c0;
-#pragma unroll
-          for (int cc = 0; cc < KC; ++cc)
-            if (cc < cg) acc[cc].add(kv * (T)wj[cc]);
-        }
-        double tot[KC];
-#pragma unroll
-        for (int cc = 0; cc < KC; ++cc) {
-          double v = acc[cc].value();
-#pragma unroll
-          for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-          tot[cc] = v;
-        }
-        if (lane == 0) {
-          const int64_t oi = tperm[i];
-#pragma unroll
-          for (int cc = 0; cc < KC; ++cc)
-            if (cc < cg) out[(int64_t)(c0 + cc) * Nf + oi] += tot[cc];
-        }
-      }
-    }
-  } else {
-  // Dense leaf: one target per lane, sources through shared-memory tiles.
   for (int c0 = 0; c0 < C; c0 += KC) {
     const int cg = min(KC, C - c0);
     for (int t0 = tc0; t0 < te && t0 < tc0 + 32; t0 += 32) {  // this warp's chunk
@@ -433,6 +370,254 @@ __global__ void __launch_bounds__(32 * kLeafWarps, DENSE ? 4 : 6)
       }
     }
   }
+}
+
+// Sparse leaves (fewer than kLaneLeafMin targets): one warp per leaf, all its
+// targets at once, their positions and basis values computed once.  With few
+// (target, column) pairs (up to TA targets) the lanes run over the sources
+// of the 27 neighbour leaves and over the local coefficients, every lane
+// holds every pair's partial sum, and one warp reduction per pair ends the
+// leaf.  Otherwise the warp stages the sources 32 at a time in shared memory
+// (positions relative to the leaf centre and the weights of KC columns),
+// evaluates the kernel once per (target, source) pair with the lanes over
+// sources, and lane (t, c) -- target group member t, column c -- accumulates
+// its targets' sums over the tile from shared memory; its far field (L2P)
+// reads the leaf's local coefficients of column c against its target's basis.
+// T = float (mixed path): kernel values and per-tile partial sums in float32,
+// running sums compensated (Kahan), output update in float64.
+template <class KF, typename T, int KC>
+__global__ void __launch_bounds__(32 * kLeafWarps, 4)
+    k_leaf_sparse(const int* __restrict__ leaves, int nleaves, const int* __restrict__ part_count,
+                  const int* __restrict__ tstart, const int* __restrict__ sstart,
+                  const int* __restrict__ tperm, const double* __restrict__ tpos,
+                  const double* __restrict__ spos, const double* __restrict__ wsorted, int Nf,
+                  int Ns, int C, const T* __restrict__ F_L, int n, int cheb,
+                  const T* __restrict__ Tkz_g, double box, int L,
+                  const double* __restrict__ kparam_g, double* __restrict__ out) {
+  constexpr bool kMixed = sizeof(T) == 4;
+  constexpr int kMaxT = kLaneLeafMin - 1;             // targets of a sparse leaf
+  constexpr int G = KC == 1 ? kMaxT : 32 / KC;        // targets per lane group
+  constexpr int NG = (kMaxT + G - 1) / G;             // groups per leaf
+  // up to TA targets: every (target, column) sum in each lane instead
+  constexpr int TA = KC == 1 ? kMaxT : 2;
+  static_assert(G * KC <= 32, "a lane group fits the warp");
+  using V4 = vec4_t<T>;
+  __shared__ T sTkz[kMaxOrder * kMaxOrder];
+  __shared__ double kp[4];
+  __shared__ int s_nb[kLeafWarps][27][2];
+  __shared__ int s_pre[kLeafWarps][28];
+  __shared__ V4 s_th[kLeafWarps][kMaxT], s_tl[kLeafWarps][kMaxT];  // targets (hi, lo)
+  __shared__ T s_b[kLeafWarps][kMaxT][3 * kMaxOrder];              // their basis values
+  __shared__ V4 s_sh[kLeafWarps][32], s_sl[kLeafWarps][kMixed ? 32 : 1];  // source tile
+  __shared__ T s_w[kLeafWarps][32][KC];                            // its weights
+  __shared__ T s_k[kLeafWarps][kMaxT][32];                         // kernel values
+  for (int i = threadIdx.x; i < n * n; i += blockDim.x) sTkz[i] = Tkz_g[i];
+  if (threadIdx.x < 4) kp[threadIdx.x] = kparam_g[threadIdx.x];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, wl = threadIdx.x >> 5;
+  const int wid = blockIdx.x * kLeafWarps + wl;
+  const int nd = *part_count;  // dense leaves come first in the list
+  if (wid >= nleaves - nd) return;
+  const int leaf = leaves[nd + wid];
+  const int ta = tstart[leaf], te = tstart[leaf + 1], nt = te - ta;
+  if (nt >= kLaneLeafMin || nt <= 0) return;  // (dense leaves run elsewhere)
+  const int n3 = n * n * n;
+  double c[3];
+  cell_center_d((uint32_t)leaf, L, box, c);
+  double len = box;
+  for (int i = 0; i < L; ++i) len = 0.5 * len;
+  const double ihalfL = 2. / len;
+  int ax, ay, az;
+  morton_decode((uint32_t)leaf, &ax, &ay, &az);
+  const int nside = 1 << L;
+  if (lane < 27) {
+    const int q = lane;
+    const int bx = ax + q / 9 - 1, by = ay + (q / 3) % 3 - 1, bz = az + q % 3 - 1;
+    int a = 0, e = 0;
+    if (bx >= 0 && by >= 0 && bz >= 0 && bx < nside && by < nside && bz < nside) {
+      const uint32_t bm = morton_encode(bx, by, bz);
+      a = sstart[bm];
+      e = sstart[bm + 1];
+    }
+    s_nb[wl][q][0] = a;
+    s_nb[wl][q][1] = e;
+  }
+  // the targets, relative to the leaf centre, and their basis values
+  if (lane < nt) {
+    const int i = ta + lane;
+    const double x = tpos[i], y = tpos[(int64_t)Nf + i], z = tpos[2 * (int64_t)Nf + i];
+    RelPos<T> tp;
+    tp.set(x - c[0], y - c[1], z - c[2]);
+    V4 h, l;
+    h.x = tp.h[0], h.y = tp.h[1], h.z = tp.h[2], h.w = 0;
+    l.x = 0, l.y = 0, l.z = 0, l.w = 0;
+    if constexpr (kMixed) l.x = tp.l[0], l.y = tp.l[1], l.z = tp.l[2];
+    s_th[wl][lane] = h;
+    s_tl[wl][lane] = l;
+  }
+  for (int idx = lane; idx < nt * 3 * n; idx += 32) {
+    const int t = idx / (3 * n), d = (idx / n) % 3, m = idx % n;
+    const int i = ta + t;
+    const double xd = tpos[(int64_t)d * Nf + i];
+    s_b[wl][t][d * n + m] = basis_one<T>(n, cheb, (T)(ihalfL * (xd - c[d])), sTkz, m);
+  }
+  __syncwarp();
+  if (lane == 0) {
+    int acc = 0;
+    for (int q = 0; q < 27; ++q) {
+      s_pre[wl][q] = acc;
+      acc += s_nb[wl][q][1] - s_nb[wl][q][0];
+    }
+    s_pre[wl][27] = acc;
+  }
+  __syncwarp();
+  const int nsrc_total = s_pre[wl][27];
+  const int tl = lane / KC, cl = lane % KC;  // this lane's target-group member and column
+  for (int c0 = 0; c0 < C; c0 += KC) {
+    const int kce = min(KC, C - c0);  // columns of this pass
+    if (nt <= TA) {
+      // Few (target, column) pairs: lanes over sources (and over the
+      // coefficients), every pair's sum in each lane, one warp reduction
+      // per pair at the end.
+      LeafAcc<T> acc[TA][KC];
+      for (int l = lane; l < n3; l += 32) {
+        const int l1 = l / (n * n), l2 = (l / n) % n, l3 = l % n;
+#pragma unroll
+        for (int t = 0; t < TA; ++t)
+          if (t < nt) {
+            const T* b = s_b[wl][t];
+            const T v = b[l1] * b[n + l2] * b[2 * n + l3];
+#pragma unroll
+            for (int cc = 0; cc < KC; ++cc)
+              if (cc < kce) acc[t][cc].add(F_L[((int64_t)leaf * C + c0 + cc) * n3 + l] * v);
+          }
+      }
+      int q = 0;
+      for (int v = lane; v < nsrc_total; v += 32) {
+        while (v >= s_pre[wl][q + 1]) ++q;
+        const int j = s_nb[wl][q][0] + (v - s_pre[wl][q]);
+        RelPos<T> sp;
+        sp.set(spos[j] - c[0], spos[(int64_t)Ns + j] - c[1], spos[2 * (int64_t)Ns + j] - c[2]);
+        V4 sh, sl;
+        sh.x = sp.h[0], sh.y = sp.h[1], sh.z = sp.h[2], sh.w = 0;
+        sl.x = 0, sl.y = 0, sl.z = 0, sl.w = 0;
+        if constexpr (kMixed) sl.x = sp.l[0], sl.y = sp.l[1], sl.z = sp.l[2];
+        T w[KC];
+        const double* wj = wsorted + (int64_t)j * C + c0;
+#pragma unroll
+        for (int cc = 0; cc < KC; ++cc) w[cc] = cc < kce ? (T)wj[cc] : T(0);
+#pragma unroll
+        for (int t = 0; t < TA; ++t)
+          if (t < nt) {
+            RelPos<T> tp;
+            const V4 th = s_th[wl][t];
+            tp.h[0] = th.x, tp.h[1] = th.y, tp.h[2] = th.z;
+            if constexpr (kMixed) {
+              const V4 tlo = s_tl[wl][t];
+              tp.l[0] = tlo.x, tp.l[1] = tlo.y, tp.l[2] = tlo.z;
+            }
+            T d[3];
+            tp.diff(sh, sl, d);
+            T kv = KF::template eval<T>(d[0], d[1], d[2], kp);
+            if (isinf(kv)) kv = 0;  // coincident points (include/compute.hpp:767)
+#pragma unroll
+            for (int cc = 0; cc < KC; ++cc)
+              if (cc < kce) acc[t][cc].add(kv * w[cc]);
+          }
+      }
+#pragma unroll
+      for (int t = 0; t < TA; ++t)
+#pragma unroll
+        for (int cc = 0; cc < KC; ++cc) {
+          if (t >= nt || cc >= kce) continue;  // uniform over the warp
+          double v = acc[t][cc].value();
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+          if (lane == 0) out[(int64_t)(c0 + cc) * Nf + tperm[ta + t]] += v;
+        }
+      continue;
+    }
+    // Many pairs: lane (t, c) owns target group members t and column c; the
+    // sources are staged 32 at a time and the kernel evaluated once per pair.
+    const bool col_ok = tl < G && c0 + cl < C;
+    LeafAcc<T> acc[NG];
+    // far field: phi += sum_l F[l] Sx[l1] Sy[l2] Sz[l3]
+#pragma unroll
+    for (int g = 0; g < NG; ++g) {
+      const int t = g * G + tl;
+      if (col_ok && t < nt) {
+        const T* Fl = F_L + ((int64_t)leaf * C + c0 + cl) * n3;
+        const T* b = s_b[wl][t];
+        int l = 0;
+        for (int l1 = 0; l1 < n; ++l1)
+          for (int l2 = 0; l2 < n; ++l2) {
+            const T b12 = b[l1] * b[n + l2];
+            T part = 0;
+            for (int l3 = 0; l3 < n; ++l3, ++l) part = fma(Fl[l], b12 * b[2 * n + l3], part);
+            acc[g].add(part);
+          }
+      }
+    }
+    // near field: the neighbours' sources in tiles of 32
+    int q = 0;
+    for (int v0 = 0; v0 < nsrc_total; v0 += 32) {
+      const int v = v0 + lane, m = min(32, nsrc_total - v0);
+      __syncwarp();
+      if (v < nsrc_total) {
+        while (v >= s_pre[wl][q + 1]) ++q;
+        const int j = s_nb[wl][q][0] + (v - s_pre[wl][q]);
+        RelPos<T> sp;
+        sp.set(spos[j] - c[0], spos[(int64_t)Ns + j] - c[1], spos[2 * (int64_t)Ns + j] - c[2]);
+        V4 h;
+        h.x = sp.h[0], h.y = sp.h[1], h.z = sp.h[2], h.w = 0;
+        s_sh[wl][lane] = h;
+        if constexpr (kMixed) {
+          V4 lo;
+          lo.x = sp.l[0], lo.y = sp.l[1], lo.z = sp.l[2], lo.w = 0;
+          s_sl[wl][lane] = lo;
+        }
+        const double* wj = wsorted + (int64_t)j * C + c0;
+#pragma unroll
+        for (int cc = 0; cc < KC; ++cc) s_w[wl][lane][cc] = c0 + cc < C ? (T)wj[cc] : T(0);
+      }
+      __syncwarp();
+      // kernel values: lanes over the tile's sources, one target at a time
+      if (lane < m) {
+        const V4 sh = s_sh[wl][lane];
+        const V4 sl = s_sl[wl][kMixed ? lane : 0];
+        for (int t = 0; t < nt; ++t) {
+          RelPos<T> tp;
+          const V4 th = s_th[wl][t];
+          tp.h[0] = th.x, tp.h[1] = th.y, tp.h[2] = th.z;
+          if constexpr (kMixed) {
+            const V4 tlo = s_tl[wl][t];
+            tp.l[0] = tlo.x, tp.l[1] = tlo.y, tp.l[2] = tlo.z;
+          }
+          T d[3];
+          tp.diff(sh, sl, d);
+          T kv = KF::template eval<T>(d[0], d[1], d[2], kp);
+          if (isinf(kv)) kv = 0;  // coincident points (include/compute.hpp:767)
+          s_k[wl][t][lane] = kv;
+        }
+      }
+      __syncwarp();
+      // sums over the tile: lane (t, c)
+#pragma unroll
+      for (int g = 0; g < NG; ++g) {
+        const int t = g * G + tl;
+        if (col_ok && t < nt) {
+          T part = 0;
+          for (int jj = 0; jj < m; ++jj) part = fma(s_k[wl][t][jj], s_w[wl][jj][cl], part);
+          acc[g].add(part);
+        }
+      }
+    }
+#pragma unroll
+    for (int g = 0; g < NG; ++g) {
+      const int t = g * G + tl;
+      if (col_ok && t < nt)
+        out[(int64_t)(c0 + cl) * Nf + tperm[ta + t]] += (double)acc[g].value();
+    }
   }
 }
 
@@ -608,14 +793,17 @@ inline int launch_leaf_kernels_t(const pbbfmm_leaf_args& a, cudaStream_t st) {
   // column: registers for one, otherwise columns in passes of kLeafCols
   const size_t dyn = sizeof(T) * kLeafWarps * 3 * a.n * 32;
   for (int dense = 1; dense >= 0; --dense) {
-    auto kern = a.C == 1
-                    ? (dense ? k_leaf<KF, T, 1, true> : k_leaf<KF, T, 1, false>)
-                    : (dense ? k_leaf<KF, T, kLeafCols, true> : k_leaf<KF, T, kLeafCols, false>);
-    const int64_t warps = dense ? a.max_chunks : a.nleaves;
-    kern<<<(unsigned)((warps + kLeafWarps - 1) / kLeafWarps), 32 * kLeafWarps, dense ? dyn : 0,
-           st>>>(a.leaves, a.nleaves, a.ndense, a.chunk_prefix, a.tstart, a.sstart, a.tperm,
-                 a.tpos, a.spos, a.wsorted, a.Nf, a.Ns, a.C, F, a.n, a.cheb, Tkz, a.box, a.L,
-                 a.kparam, a.out);
+    if (dense) {
+      auto kern = a.C == 1 ? k_leaf<KF, T, 1> : k_leaf<KF, T, kLeafCols>;
+      kern<<<(unsigned)((a.max_chunks + kLeafWarps - 1) / kLeafWarps), 32 * kLeafWarps, dyn, st>>>(
+          a.leaves, a.nleaves, a.ndense, a.chunk_prefix, a.tstart, a.sstart, a.tperm, a.tpos,
+          a.spos, a.wsorted, a.Nf, a.Ns, a.C, F, a.n, a.cheb, Tkz, a.box, a.L, a.kparam, a.out);
+    } else {
+      auto kern = a.C == 1 ? k_leaf_sparse<KF, T, 1> : k_leaf_sparse<KF, T, kLeafCols>;
+      kern<<<(unsigned)((a.nleaves + kLeafWarps - 1) / kLeafWarps), 32 * kLeafWarps, 0, st>>>(
+          a.leaves, a.nleaves, a.ndense, a.tstart, a.sstart, a.tperm, a.tpos, a.spos, a.wsorted,
+          a.Nf, a.Ns, a.C, F, a.n, a.cheb, Tkz, a.box, a.L, a.kparam, a.out);
+    }
     if (const cudaError_t e = cudaGetLastError()) return (int)e;
   }
   return 0;
