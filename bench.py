@@ -453,7 +453,7 @@ def per_step(kt, steps):
 # for 32,768 cells x 405 frequencies x 8 columns)
 MAC_DRAM_BYTES_PER_UNIT = (891.978752e6 + 810.800896e6) / (32768 * 405 * 8)
 # tensor-core MAC tiling (csrc/m2l_unif_tc.cu): 8 target lines of 16 parents
-# per CTA, 3 x 10 source lines per frequency, 12 MMAs (M = 128, K = 8) per
+# per CTA, 3 x 10 source lines per frequency, 6 MMAs (M = 128, K = 16) per
 # source line with N = 32 x (target lines it serves)
 UT_BY, UT_LINE = 8, 16
 
@@ -462,7 +462,7 @@ def unif_tc_issued_flops(L, nk):
     """Tensor-pipe flops the MMAs of k_m2l_unif_tc issue per step (empty
     source lines skipped at run time are counted: an upper bound)."""
     nl = [min(UT_BY - 1, sy + 1) - max(0, sy - 1) + 1 for sy in range(-1, UT_BY + 1)]
-    per_cta_freq = 3 * sum(12 * 128 * 32 * k * 8 * 2 for k in nl)
+    per_cta_freq = 3 * sum(6 * 128 * 32 * k * 16 * 2 for k in nl)
     total = 0
     for l in range(5, L + 1):
         S = 1 << (l - 1)
@@ -473,8 +473,8 @@ def unif_tc_issued_flops(L, nk):
 def unif_roofline(fmm, tree, wl, results, steps, local_rank):
     """Frequency-domain M2L: one complex MAC (8 useful flops) per (M2L pair,
     frequency, column).  Levels with >= 16 parents per side run on the tensor
-    cores (k_m2l_unif_tc, kind::tf32, hi/lo splits of both operands), the
-    coarser ones on the CUDA cores (k_m2l_unif_mac<float>)."""
+    cores (k_m2l_unif_tc, kind::f16, power-of-two scaled hi/lo splits of both
+    operands), the coarser ones on the CUDA cores (k_m2l_unif_mac<float>)."""
     kt = results["mixed"]["ktimes"]
     tstart = tree.debug_copy(2).astype(np.int64)
     pairs = interaction_pairs(tstart, wl["L"])
@@ -487,18 +487,19 @@ def unif_roofline(fmm, tree, wl, results, steps, local_rank):
     nbytes = sum(2 * nonempty[l] * nk * C * 8 for l in nonempty)  # float2: read X^, write Y^
     peaks, peak_kind = load_peaks()
     fp64_peak = fmm.measure_fma_peak(local_rank, fmm.PREC_FP64)
-    tf32_peak = peaks["bf16_tflops"] / 2.0
+    f16_peak = peaks["bf16_tflops"]
     mac_ms = kt["m2l_mac"][0] / steps
     mac64_ms = results["fp64"]["ktimes"]["m2l_mac"][0] / steps
     achieved = flops / (mac_ms * 1e-3) / 1e12
     issued = unif_tc_issued_flops(wl["L"], nk) * (C // 8) if C % 8 == 0 else 0.0
     return {
-        "kernel": "k_m2l_unif_tc (tcgen05 kind::tf32 block product, levels >= 5) + "
-                  "k_m2l_unif_mac<float> (levels 2-4), frequency-domain M2L, mixed path",
-        "bound": "tensor", "achieved": achieved, "peak": tf32_peak, "unit": "TFLOP/s",
-        "frac": achieved / tf32_peak,
-        "tensor_pipe_issued_frac": issued / (mac_ms * 1e-3) / 1e12 / tf32_peak,
-        "peak_source": "dense TF32 = half the %s bf16 tensor figure of MEASURED_PEAKS.json "
+        "kernel": "k_m2l_unif_tc (tcgen05 kind::f16 block product on scaled F16 hi/lo "
+                  "splits, levels >= 5) + k_m2l_unif_mac<float> (levels 2-4), "
+                  "frequency-domain M2L, mixed path",
+        "bound": "tensor", "achieved": achieved, "peak": f16_peak, "unit": "TFLOP/s",
+        "frac": achieved / f16_peak,
+        "tensor_pipe_issued_frac": issued / (mac_ms * 1e-3) / 1e12 / f16_peak,
+        "peak_source": "dense F16 = the %s bf16 tensor figure of MEASURED_PEAKS.json "
                        "(%.0f TFLOP/s)" % (peak_kind, peaks["bf16_tflops"]),
         # DRAM bytes per step, scaled from one ncu capture of the same kernel
         "traffic": sum(nonempty.values()) * nk * C * MAC_DRAM_BYTES_PER_UNIT,

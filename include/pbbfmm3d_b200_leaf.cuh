@@ -167,6 +167,11 @@ __device__ __forceinline__ void cell_center_d(uint32_t m, int l, double box, dou
 constexpr int kLeafWarps = 4;
 constexpr int kLeafCols = 8;  // columns per pass (registers)
 constexpr int kLaneLeafMin = 12;  // leaves with fewer targets take the warp-per-target path
+// resident CTAs per SM the leaf kernels are compiled for: the float32
+// one-column kernels fit 64 registers (32 warps per SM, latency hiding for
+// the gathers); the others keep 128
+template <typename T, int KC>
+constexpr int kLeafBlocks = sizeof(T) == 4 && KC == 1 ? 6 : 4;
 
 // Source coordinates relative to the target leaf's centre.  float (mixed
 // path): hi = float(d), lo = float(d - hi), so that differences of nearby
@@ -216,7 +221,7 @@ using LeafAcc = typename std::conditional<sizeof(T) == 4, Kahan<T>, PlainSum<T>>
 // sums in float32, each lane's running sums compensated (Kahan), the output
 // update in float64.  T = double: everything in float64.
 template <class KF, typename T, int KC>
-__global__ void __launch_bounds__(32 * kLeafWarps, 4)
+__global__ void __launch_bounds__(32 * kLeafWarps, kLeafBlocks<T, KC>)
     k_leaf(const int* __restrict__ leaves, int nleaves, const int* __restrict__ part_count,
            const int* __restrict__ chunk_prefix, const int* __restrict__ tstart,
            const int* __restrict__ sstart, const int* __restrict__ tperm,
@@ -233,6 +238,7 @@ __global__ void __launch_bounds__(32 * kLeafWarps, 4)
   __shared__ V4 s_sh[kLeafWarps][32];               // staged sources: position (hi)
   __shared__ V4 s_sl[kLeafWarps][kMixed ? 32 : 1];  // position (lo), mixed path
   __shared__ T s_w[kLeafWarps][32][KC];             // staged weights
+  __shared__ T s_F[kLeafWarps][KC * 32];            // staged local coefficients (L2P)
   // basis values of each lane's target, [warp][dim][m < n][lane] (dynamic, sized by n)
   extern __shared__ __align__(16) unsigned char leaf_dyn[];
   T* s_bw = reinterpret_cast<T*>(leaf_dyn) + (threadIdx.x >> 5) * 3 * n * 32;
@@ -298,8 +304,11 @@ __global__ void __launch_bounds__(32 * kLeafWarps, 4)
       RelPos<T> tp;
       tp.set(x - c[0], y - c[1], z - c[2]);
       LeafAcc<T> acc[KC];
-      // far field: phi += sum_l F[l] Sx[l1] Sy[l2] Sz[l3]
-      if (active) {
+      // far field: phi += sum_l F[l] Sx[l1] Sy[l2] Sz[l3].  The leaf's
+      // coefficients are staged 32 at a time (coalesced loads, one round
+      // trip per chunk) and read by broadcast; every lane takes part,
+      // inactive ones on the leaf centre, writing nothing.
+      {
         T* b = s_bw + lane;  // b[(d n + m) 32]: conflict-free, no local memory
         for (int m = 0; m < n; ++m) {
           b[m * 32] = basis_one<T>(n, cheb, (T)(ihalfL * (x - c[0])), sTkz, m);
@@ -307,17 +316,30 @@ __global__ void __launch_bounds__(32 * kLeafWarps, 4)
           b[(2 * n + m) * 32] = basis_one<T>(n, cheb, (T)(ihalfL * (z - c[2])), sTkz, m);
         }
         const T* Fl = F_L + ((int64_t)leaf * C + c0) * n3;
-        int l = 0;
-        for (int l1 = 0; l1 < n; ++l1)
-          for (int l2 = 0; l2 < n; ++l2) {
-            const T b12 = b[l1 * 32] * b[(n + l2) * 32];
-            for (int l3 = 0; l3 < n; ++l3, ++l) {
-              const T v = b12 * b[(2 * n + l3) * 32];
+        T* sF = s_F[wl];
+        int l1 = 0, l2 = 0, l3 = 0;
+        T b12 = b[0] * b[n * 32];
+        for (int l0 = 0; l0 < n3; l0 += 32) {
+          __syncwarp();
+          if (l0 + lane < n3) {
 #pragma unroll
-              for (int cc = 0; cc < KC; ++cc)
-                if (cc < cg) acc[cc].add(Fl[cc * n3 + l] * v);
+            for (int cc = 0; cc < KC; ++cc)
+              sF[cc * 32 + lane] = cc < cg ? Fl[cc * n3 + l0 + lane] : T(0);
+          }
+          __syncwarp();
+          const int mm = min(32, n3 - l0);
+          for (int jj = 0; jj < mm; ++jj) {
+            const T v = b12 * b[(2 * n + l3) * 32];
+#pragma unroll
+            for (int cc = 0; cc < KC; ++cc)
+              if (cc < cg) acc[cc].add(sF[cc * 32 + jj] * v);
+            if (++l3 == n) {
+              l3 = 0;
+              if (++l2 == n) l2 = 0, ++l1;
+              if (l1 < n) b12 = b[l1 * 32] * b[(n + l2) * 32];
             }
           }
+        }
       }
       // near field: the 27 neighbours' source ranges, concatenated, in tiles of 32
       int q = 0;
@@ -386,7 +408,7 @@ __global__ void __launch_bounds__(32 * kLeafWarps, 4)
 // T = float (mixed path): kernel values and per-tile partial sums in float32,
 // running sums compensated (Kahan), output update in float64.
 template <class KF, typename T, int KC>
-__global__ void __launch_bounds__(32 * kLeafWarps, 4)
+__global__ void __launch_bounds__(32 * kLeafWarps, kLeafBlocks<T, KC>)
     k_leaf_sparse(const int* __restrict__ leaves, int nleaves, const int* __restrict__ part_count,
                   const int* __restrict__ tstart, const int* __restrict__ sstart,
                   const int* __restrict__ tperm, const double* __restrict__ tpos,
@@ -410,7 +432,10 @@ __global__ void __launch_bounds__(32 * kLeafWarps, 4)
   __shared__ T s_b[kLeafWarps][kMaxT][3 * kMaxOrder];              // their basis values
   __shared__ V4 s_sh[kLeafWarps][32], s_sl[kLeafWarps][kMixed ? 32 : 1];  // source tile
   __shared__ T s_w[kLeafWarps][32][KC];                            // its weights
-  __shared__ T s_k[kLeafWarps][kMaxT][32];                         // kernel values
+  // kernel values [target][source], or basis products [target][coefficient]
+  // (rows padded to 33: lanes of different targets read different banks)
+  __shared__ T s_k[kLeafWarps][kMaxT][33];
+  __shared__ T s_F[kLeafWarps][KC * 33];  // staged local coefficients [column][coefficient]
   for (int i = threadIdx.x; i < n * n; i += blockDim.x) sTkz[i] = Tkz_g[i];
   if (threadIdx.x < 4) kp[threadIdx.x] = kparam_g[threadIdx.x];
   __syncthreads();
@@ -541,21 +566,31 @@ __global__ void __launch_bounds__(32 * kLeafWarps, 4)
     // sources are staged 32 at a time and the kernel evaluated once per pair.
     const bool col_ok = tl < G && c0 + cl < C;
     LeafAcc<T> acc[NG];
-    // far field: phi += sum_l F[l] Sx[l1] Sy[l2] Sz[l3]
+    // far field: phi += sum_l F[l] Sx[l1] Sy[l2] Sz[l3], 32 coefficients at
+    // a time: lanes over coefficients load the KC columns (coalesced) and
+    // form every target's basis products, then lane (t, c) sums the chunk
+    for (int l0 = 0; l0 < n3; l0 += 32) {
+      const int l = l0 + lane, mm = min(32, n3 - l0);
+      __syncwarp();
+      if (l < n3) {
+        const int l1 = l / (n * n), l2 = (l / n) % n, l3 = l % n;
 #pragma unroll
-    for (int g = 0; g < NG; ++g) {
-      const int t = g * G + tl;
-      if (col_ok && t < nt) {
-        const T* Fl = F_L + ((int64_t)leaf * C + c0 + cl) * n3;
-        const T* b = s_b[wl][t];
-        int l = 0;
-        for (int l1 = 0; l1 < n; ++l1)
-          for (int l2 = 0; l2 < n; ++l2) {
-            const T b12 = b[l1] * b[n + l2];
-            T part = 0;
-            for (int l3 = 0; l3 < n; ++l3, ++l) part = fma(Fl[l], b12 * b[2 * n + l3], part);
-            acc[g].add(part);
-          }
+        for (int cc = 0; cc < KC; ++cc)
+          s_F[wl][cc * 33 + lane] = cc < kce ? F_L[((int64_t)leaf * C + c0 + cc) * n3 + l] : T(0);
+        for (int t = 0; t < nt; ++t) {
+          const T* b = s_b[wl][t];
+          s_k[wl][t][lane] = b[l1] * b[n + l2] * b[2 * n + l3];
+        }
+      }
+      __syncwarp();
+#pragma unroll
+      for (int g = 0; g < NG; ++g) {
+        const int t = g * G + tl;
+        if (col_ok && t < nt) {
+          T part = 0;
+          for (int jj = 0; jj < mm; ++jj) part = fma(s_F[wl][cl * 33 + jj], s_k[wl][t][jj], part);
+          acc[g].add(part);
+        }
       }
     }
     // near field: the neighbours' sources in tiles of 32

@@ -467,11 +467,15 @@ static int upload_operators(pbbfmm_tree* t) {
     unif_spectra(t->n, t->ops.stencil, t->ops.nlev, &op);
     if ((rc = upload(&t->d_op, op.data(), op.size()))) return rc;
     if ((rc = upload_f32(&t->f_op, op.data(), op.size()))) return rc;
-    std::vector<float> tiles;
-    unif_tc_tiles(t->n, op, t->ops.nlev, &tiles);
+    std::vector<uint16_t> tiles;
+    std::vector<int> bexp;
+    unif_tc_tiles(t->n, op, t->ops.nlev, &tiles, &bexp);
     if (t->f_unif_tiles) cudaFree(t->f_unif_tiles);
+    if (t->f_unif_bexp) cudaFree(t->f_unif_bexp);
     t->f_unif_tiles = nullptr;
+    t->f_unif_bexp = nullptr;
     if ((rc = upload_vec(&t->f_unif_tiles, tiles))) return rc;
+    if ((rc = upload_vec(&t->f_unif_bexp, bexp))) return rc;
   }
   t->ops_ready = true;
   return PBBFMM_OK;
@@ -485,11 +489,15 @@ static void free_tree_device(pbbfmm_tree* t) {
     *b = nullptr;
   }
   float** fbufs[] = {&t->f_Tkz, &t->f_Kw, &t->f_Cw, &t->f_E,    &t->f_U,
-                     &t->f_VT,  &t->f_op, &t->f_twid, &t->f_unif_tiles};
+                     &t->f_VT,  &t->f_op, &t->f_twid};
   for (float** b : fbufs) {
     if (*b) cudaFree(*b);
     *b = nullptr;
   }
+  if (t->f_unif_tiles) cudaFree(t->f_unif_tiles);
+  if (t->f_unif_bexp) cudaFree(t->f_unif_bexp);
+  t->f_unif_tiles = nullptr;
+  t->f_unif_bexp = nullptr;
   if (t->d_offs) cudaFree(t->d_offs);
   t->d_offs = nullptr;
   free_tc_ops(&t->tc);
@@ -502,7 +510,7 @@ static void free_tree_device(pbbfmm_tree* t) {
                    &ws.spos,      &ws.wsorted, &ws.cub_temp, &ws.lists,    &ws.dcounts,
                    &ws.S,         &ws.F,     &ws.proxy,   &ws.pf,         &ws.io_tgt,
                    &ws.io_src,    &ws.io_w,  &ws.io_out, &ws.halo, &ws.tc_proxy, &ws.leafpart,
-                   &ws.occ};
+                   &ws.occ,       &ws.amax};
   for (DevBuf* b : all) release(*b);
   if (ws.h_in) cudaFreeHost(ws.h_in);
   if (ws.h_out) cudaFreeHost(ws.h_out);

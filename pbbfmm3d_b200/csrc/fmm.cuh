@@ -47,6 +47,7 @@ struct Workspace {
   DevBuf tc_proxy;  // tensor-core Cheb M2L: hi then lo proxies of one level (+ F16 exponents)
   DevBuf leafpart;  // leaf phase: target leaves partitioned dense-first, then their count
   DevBuf occ;       // tensor-core uniform M2L: per-cell source / target occupancy of a level
+  DevBuf amax;      // tensor-core uniform M2L: per level, largest |spectra| per (k23, column mod 8)
   // staging for the host-pointer entry point
   DevBuf io_tgt, io_src, io_w, io_out;
   // pinned host staging of the host-buffer entry point (cudaHostAlloc)
@@ -125,8 +126,10 @@ struct pbbfmm_tree {
   float* f_VT = nullptr;
   float* f_op = nullptr;  // nlev x nk x 343 complex (float2)
   // tensor-core uniform M2L: per level and frequency the operator tiles of
-  // the block product (m2l_unif_tc.cu), TF32 hi / lo
-  float* f_unif_tiles = nullptr;
+  // the block product (m2l_unif_tc.cu), scaled F16 hi / lo, and their
+  // power-of-two exponents
+  uint16_t* f_unif_tiles = nullptr;
+  int* f_unif_bexp = nullptr;
   float* f_twid = nullptr;
   // tensor-core Chebyshev M2L (mixed path); tc_fmt: PBBFMM_TC_F16 (scaled
   // F16 operands, default) or PBBFMM_TC_TF32
@@ -229,8 +232,9 @@ int run_m2l_unif(pbbfmm_tree* t, int C, cudaStream_t st);
 // columns in groups of 8
 bool unif_tc_eligible(const pbbfmm_tree* t, int l, int C);
 int run_m2l_unif_tc_level(pbbfmm_tree* t, int C, int l, int lvl, const float2* X, float2* Y,
-                          cudaStream_t st);
-void unif_tc_tiles(int n, const std::vector<double>& op, int nlev, std::vector<float>* tiles);
+                          const uint32_t* amax, cudaStream_t st);
+void unif_tc_tiles(int n, const std::vector<double>& op, int nlev, std::vector<uint16_t>* tiles,
+                   std::vector<int>* bexp);
 int set_unif_tc_wait_limit(long long polls);
 int run_downward(pbbfmm_tree* t, int C, cudaStream_t st);
 int run_leaves(pbbfmm_tree* t, int64_t Nf, int64_t Ns, int C, double* d_out, cudaStream_t st);

@@ -15,6 +15,7 @@
 // the operator spectra stored as conj(DFT3(A)).  Only the k3 < n half of each
 // spectrum is kept (Hermitian symmetry), nk = m*m*n complex values per cell
 // and column.  Same sums as the reference, different rounding.
+#include <algorithm>
 #include <cmath>
 #include <mutex>
 
@@ -80,12 +81,16 @@ int init_fft_twiddles() {
 // Spectra of a level are stored frequency-major: X[(k * ncells + cell) * C + col]
 // (ncells = 8^level), so that one frequency plane of a level is contiguous.
 
-// Forward: one CTA per nonempty source cell; columns in groups of CG.
+// Forward: CTAs loop over the nonempty source cells (cells[0..ncl)), columns
+// in groups of CG.  With amax (float path, levels of the tensor-core MAC),
+// the largest |re| or |im| of the spectra per (k23, column mod 8), over the
+// level's cells and k1, as float bits: per CTA in shared memory, then one
+// atomicMax per slot into amax[k23][8] (zeroed by the caller).
 // w = e^{-2 pi i / m}; (a + ib) w^j = (a c + b s) + i (b c - a s).
 template <int n, typename T>
-__global__ void k_fft_fwd(const int* __restrict__ cells, const T* __restrict__ S_l,
+__global__ void k_fft_fwd(const int* __restrict__ cells, int ncl, const T* __restrict__ S_l,
                           cplx_t<T>* __restrict__ X_l, int64_t ncells, int C, int CG,
-                          const T* __restrict__ twid) {
+                          const T* __restrict__ twid, unsigned* __restrict__ amax) {
   using C2 = cplx_t<T>;
   using W = Tw<n, T>;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -94,9 +99,13 @@ __global__ void k_fft_fwd(const int* __restrict__ cells, const T* __restrict__ S
   T* sin_ = sm + 2 * m;                         // CG * n3 real moments
   C2* Z = (C2*)(sin_ + ((CG * n3 + 3) & ~3));  // CG * n * n * n   (l1, l2, k3)
   C2* Y = Z + CG * n3;                         // CG * n * m * n   (l1, k2, k3)
+  unsigned* s_amax = reinterpret_cast<unsigned*>(Y + CG * ny);  // [m n][8]
   (void)twid;
-  const int cell = cells[blockIdx.x];
   const int tid = threadIdx.x, bd = blockDim.x;
+  if (amax)
+    for (int i = tid; i < m * n * 8; i += bd) s_amax[i] = 0u;
+  for (int ci = blockIdx.x; ci < ncl; ci += gridDim.x) {
+  const int cell = cells[ci];
   for (int c0 = 0; c0 < C; c0 += CG) {
     const int cg = min(CG, C - c0);
     __syncthreads();
@@ -150,6 +159,8 @@ __global__ void k_fft_fwd(const int* __restrict__ cells, const T* __restrict__ S
 #pragma unroll
       for (int l = 0; l < n; ++l) v[l] = y[l * m * n];
       C2* out = X_l + ((int64_t)k23 * ncells + cell) * C + c0 + cc;
+      float amx = 0.f;
+      (void)amx;
 #pragma unroll
       for (int k = 0; k < m; ++k) {
         T re = 0, im = 0;
@@ -160,8 +171,17 @@ __global__ void k_fft_fwd(const int* __restrict__ cells, const T* __restrict__ S
           im = fma(v[l].y, c, fma(-v[l].x, s, im));
         }
         out[(int64_t)k * m * n * ncells * C] = make_cplx<T>(re, im);
+        if constexpr (sizeof(T) == 4) amx = fmaxf(amx, fmaxf(fabsf(re), fabsf(im)));
       }
+      if constexpr (sizeof(T) == 4)
+        if (amax) atomicMax(&s_amax[k23 * 8 + ((c0 + cc) & 7)], __float_as_uint(amx));
     }
+  }
+  }
+  if (amax) {
+    __syncthreads();
+    for (int i = tid; i < m * n * 8; i += bd)
+      if (s_amax[i]) atomicMax(&amax[i], s_amax[i]);
   }
 }
 
@@ -488,6 +508,7 @@ struct FftLaunch {
   int level = 2;
   bool inverse = false;
   double scale = 1.0;
+  unsigned* amax = nullptr;  // forward: spectra maxima of the level (tensor-core MAC)
   template <int N>
   int run() {
     const int n3 = N * N * N, nk = (2 * N - 1) * (2 * N - 1) * N;
@@ -499,9 +520,16 @@ struct FftLaunch {
     if (!inverse) {
       PB_CUDA(cudaFuncSetAttribute(k_fft_fwd<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)smem_f));
-      k_fft_fwd<N, T><<<t->lists.nsrc[l], 128, smem_f, st>>>(
-          lists + t->lists.src_off[l], ws.S.as<T>() + level_offset(l, perS),
-          ws.proxy.as<cplx_t<T>>() + level_offset(l, perX), cells_at(l), C, CGf, twid);
+      // CTAs loop over the cells: as many as fit on the GPU at once
+      int per_sm = 1, dev = 0, nsm = 148;
+      PB_CUDA(cudaGetDevice(&dev));
+      PB_CUDA(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev));
+      PB_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fft_fwd<N, T>, 128, smem_f));
+      const int ncl = t->lists.nsrc[l];
+      const int grid = std::max(1, std::min(ncl, std::max(1, per_sm) * nsm));
+      k_fft_fwd<N, T><<<grid, 128, smem_f, st>>>(
+          lists + t->lists.src_off[l], ncl, ws.S.as<T>() + level_offset(l, perS),
+          ws.proxy.as<cplx_t<T>>() + level_offset(l, perX), cells_at(l), C, CGf, twid, amax);
       PB_LAUNCH("fft_fwd");
     } else {
       PB_CUDA(cudaFuncSetAttribute(k_fft_inv<N, T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -532,17 +560,30 @@ static int run_m2l_unif_t(pbbfmm_tree* t, int C, cudaStream_t st) {
   const int fwd_col = n3 * ts + n3 * 2 * ts + n * m * n * 2 * ts;
   const int CGf = max(1, min(C, 60000 / fwd_col));
   const size_t smem_f = (size_t)ts * (2 * m + ((CGf * n3 + 3) & ~3)) +
-                        (size_t)2 * ts * (CGf * n3 + CGf * n * m * n);
+                        (size_t)2 * ts * (CGf * n3 + CGf * n * m * n) + (size_t)4 * m * n * 8;
   const int inv_col = (nk + n * m * n + n3) * 2 * ts;
   const int CGi = max(1, min(C, 60000 / inv_col));
   const size_t smem_i = (size_t)ts * ((2 * m + 3) & ~3) +
                         (size_t)2 * ts * (CGi * nk + CGi * n * m * n + CGi * n3);
   FftLaunch<T> fl{t, C, CGf, CGi, smem_f, smem_i, invP, st};
+  // spectra maxima per level for the tensor-core MAC's scaling (float path)
+  const size_t amax_per = (size_t)m * n * 8;
+  bool any_tc = false;
+  for (int l = 2; l <= L; ++l) any_tc |= sizeof(T) == 4 && unif_tc_eligible(t, l, C);
+  if (any_tc) {
+    if (int rc_ = grow(ws.amax, (size_t)(L + 1) * amax_per * sizeof(unsigned))) return rc_;
+    PB_CUDA(cudaMemsetAsync(ws.amax.p, 0, (size_t)(L + 1) * amax_per * sizeof(unsigned), st));
+  }
+  auto amax_at = [&](int l) -> unsigned* {
+    return sizeof(T) == 4 && unif_tc_eligible(t, l, C) ? ws.amax.as<unsigned>() + l * amax_per
+                                                       : nullptr;
+  };
   for (int l = 2; l <= L; ++l) {
     if (t->lists.nsrc[l] == 0) continue;
     if (int rc_ = kt_begin(t, KS_FFT_FWD, st)) return rc_;
     fl.level = l;
     fl.inverse = false;
+    fl.amax = amax_at(l);
     if (int rc_ = dispatch_order(n, fl)) return rc_;
     if (int rc_ = kt_end(t, st)) return rc_;
   }
@@ -562,7 +603,7 @@ static int run_m2l_unif_t(pbbfmm_tree* t, int C, cudaStream_t st) {
     // CUDA cores from level 3 up (level 2 has 2 parents per side)
     if (sizeof(T) == 4 && unif_tc_eligible(t, l, C))
       rc = run_m2l_unif_tc_level(t, C, l, lvl, reinterpret_cast<const float2*>(Xl),
-                                 reinterpret_cast<float2*>(Yl), st);
+                                 reinterpret_cast<float2*>(Yl), amax_at(l), st);
     else if (l >= 3)
       rc = launch_mac_cols<4, T>(Xl, Yl, op, halo, sstart, tstart, span, l, C, nk, st);
     else

@@ -16,26 +16,39 @@
 // y = y0..y0+7, z = z0..z0+15) and a chunk of frequencies.  For a frequency
 // it walks the 3 x 10 source lines (x = bx-1..bx+1, y = y0-1..y0+8) of 18
 // parents (z0-1..z0+16).  A source line is staged in shared memory as the
-// A operand, 144 rows (z, column) x K = 16 (child, re/im), split into TF32 hi
+// A operand, 144 rows (z, column) x K = 16 (child, re/im), split into F16 hi
 // and lo parts; a window of 128 of its rows, shifted by D_z parents, lines up
 // with the rows of the target lines.  The operator tiles B for one D_x and D_z
 // stack the three D_y in N (96 rows: D_y x (hi, lo) x (child, re/im)), so one
 // MMA serves the three target lines y - D_y at once; their TMEM accumulators
 // (32 columns per line: the products with B hi, then with B lo) are adjacent.
-// Each (line, D_x, D_z) issues four tcgen05.mma kind::tf32 (A hi and A lo, K
-// in two steps of 8); D = A_hi B + A_lo B = (A_hi + A_lo)(B_hi + B_lo), i.e.
-// float32 operands at about 2^-21 relative error per product (3xTF32 plus
-// the lo x lo term), accumulated in float32.
+// Each (line, D_z) issues two tcgen05.mma kind::f16 (A hi and A lo, K = 16):
+// D = A_hi B + A_lo B = (A_hi + A_lo)(B_hi + B_lo), accumulated in float32.
 //
-// Roles (416 threads): warps 0-7 stage source lines (cp.async of the raw
-// float32 spectra, zero-filled for empty or out-of-domain cells, then a split
-// into the hi / lo A layout) and load each frequency's operator tiles by a
-// bulk copy; one thread of warp 8 issues the MMAs; warps 9-12 drain the
+// Scaling.  F16 holds 11 significant bits between 2^-14 and 2^16, so both
+// operands are scaled by powers of two before the split: the spectra of
+// column c at frequencies (k1, k23) by 2^sA(k23, c mod 8), with sA chosen from
+// the largest magnitude over the level's cells and k1 (recorded by the forward
+// FFT) so that it lies in [2^14, 2^15); the operator tiles of a frequency by
+// 2^sB(k) from their largest entry.  hi = fp16(x 2^s), lo = fp16(x 2^s - hi)
+// keep 22 significant bits for values down to 2^-17 of the scale's maximum
+// and an absolute error below 2^-39 of it for smaller ones.  A TMEM row holds
+// one column only (source and target rows share the column), so one factor
+// 2^-(sA + sB) per drained row and frequency undoes the scaling exactly.
+//
+// Roles (448 threads): warps 0-8 produce the A operand, one (K plane, row)
+// task per thread: each thread loads its four spectra values and the
+// children's occupancy into a register ring six lines ahead (so the loads of
+// several lines are in flight), then scales, splits and stores them into an
+// A stage; thread 0 also loads each frequency's operator tiles by a bulk
+// copy.  One thread of warp 9 issues the MMAs; warps 10-13 drain the
 // accumulators (two TMEM sets, alternating by frequency), write the target
-// spectra and zero the accumulators.  Every wait is bounded; on timeout the
-// kernel sets *err, waits (bounded) for its issued copies and MMAs, frees its
-// TMEM and returns.
+// spectra and zero the accumulators.  Producer warps run on their own,
+// ordered by mbarriers only (no block-wide barrier per line).  Every wait is
+// bounded; on timeout the kernel sets *err, waits (bounded) for its issued
+// copies and MMAs, frees its TMEM and returns.
 #include <cuda.h>
+#include <cuda_fp16.h>
 
 #include <algorithm>
 #include <mutex>
@@ -51,46 +64,31 @@ constexpr int UT_LINE = 16;                // parents per target line (along z)
 constexpr int UT_SRCZ = UT_LINE + 2;       // parents per source line
 constexpr int UT_ROWS = UT_SRCZ * 8;       // A rows of a source line: (z, column)
 constexpr int UT_SRC_LINES = 3 * (UT_BY + 2);  // source lines per frequency
-constexpr int UT_APLANE = UT_ROWS * 16;    // bytes of one K core plane of A
-constexpr int UT_APART = 4 * UT_APLANE;    // hi or lo part of a stage (K = 16 floats)
+constexpr int UT_APLANE = UT_ROWS * 16;    // bytes of one K core plane (8 F16) of A
+constexpr int UT_APART = 2 * UT_APLANE;    // hi or lo part of a stage (K = 16)
 constexpr int UT_ASTAGE = 2 * UT_APART;
-constexpr int UT_NST = 3;                  // A stages
-constexpr int UT_RAWZ = 576;               // bytes per parent in a raw line (512 + bank padding)
-constexpr int UT_RAWLINE = UT_SRCZ * UT_RAWZ;  // raw float32 spectra of one source line
-constexpr int UT_PREFETCH = 4;             // lines whose raw copies run ahead of the split
-constexpr int UT_NRAW = UT_PREFETCH + 2;   // raw slots
+constexpr int UT_NST = 8;                  // A stages
+constexpr int UT_RING = 6;                 // lines whose loads run ahead of the split (registers)
 constexpr int UT_BROWS = 96;               // B rows of one (D_x, D_z) tile
 constexpr int UT_BPLANE = UT_BROWS * 16;
-constexpr int UT_BTILE = 4 * UT_BPLANE;
+constexpr int UT_BTILE = 2 * UT_BPLANE;
 constexpr int UT_BFREQ = 9 * UT_BTILE;     // operator tiles of one frequency (bytes)
-constexpr int UT_PRODUCERS = 256;          // warps 0-7
-constexpr int UT_MMA_WARP = UT_PRODUCERS / 32;  // warp 8
-constexpr int UT_DRAIN0 = UT_PRODUCERS + 32;    // first drain thread (warps 9-12)
+constexpr int UT_PWARPS = 9;               // producer warps 0-8: one task per thread
+constexpr int UT_PRODUCERS = 32 * UT_PWARPS;
+constexpr int UT_MMA_WARP = UT_PWARPS;     // warp 9
+constexpr int UT_DRAIN0 = UT_PRODUCERS + 32;    // first drain thread (warps 10-13)
 constexpr int UT_THREADS = UT_DRAIN0 + 128;
 constexpr int UT_TMEM_COLS = 512;          // two sets of UT_BY x 32 columns
-constexpr int UT_SMEM = UT_NST * UT_ASTAGE + UT_NRAW * UT_RAWLINE + 2 * UT_BFREQ + 1024;
+constexpr int UT_SMEM = UT_NST * UT_ASTAGE + 2 * UT_BFREQ + 1024;
 static_assert(2 * UT_BY * 32 == UT_TMEM_COLS, "two accumulator sets fill the TMEM");
+static_assert(UT_PRODUCERS == 2 * UT_ROWS, "one split task (K plane, row) per producer thread");
 static_assert(UT_SMEM <= 232448, "shared memory of one CTA");
 
-// Floats of the operator tiles per (level, frequency).
-constexpr int kUnifTcTileFloats = UT_BFREQ / 4;
+// F16 values (uint16 bit patterns) of the operator tiles per (level, frequency).
+constexpr int kUnifTcTileHalves = UT_BFREQ / 2;
 
 // Poll limit of the pipeline waits (see g_pipe_wait_iters in m2l_tc.cu).
 __device__ long long g_unif_wait_iters = kWaitIters;
-
-// OR of `v` over the 256 producer threads (warps 0-7), which also acts as
-// their barrier (named barrier 1): every producer executes the same sequence
-// of these, so none waits for a thread that has left.
-__device__ __forceinline__ bool producers_any(bool v) {
-  uint32_t r;
-  asm volatile(
-      "{\n .reg .pred p, q;\n setp.ne.u32 q, %1, 0;\n bar.red.or.pred p, 1, 256, q;\n"
-      " selp.u32 %0, 1, 0, p;\n}\n"
-      : "=r"(r)
-      : "r"((uint32_t)v)
-      : "memory");
-  return r != 0;
-}
 
 // Barrier among the `n` threads of a role group (named barrier `id`).
 __device__ __forceinline__ void group_sync(int id, int n) {
@@ -109,11 +107,12 @@ __device__ __forceinline__ bool drains_any(bool v) {
   return r != 0;
 }
 
-// x rounded to TF32 (10 explicit mantissa bits), to nearest with ties away
-// from zero, by integer operations on its bits: the value cvt.rna.tf32.f32
-// gives for finite x (no conversion instruction on the producers' path).
-__device__ __forceinline__ float tf32_rna_bits(float x) {
-  return __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xffffe000u);
+// 2^s as a float with s = 15 - e for the largest magnitude m = 2^(e-1).. of
+// a spectra scale slot (float bits, 0 if every value is zero), so that
+// m 2^s lies in [2^14, 2^15); s clamped to the float exponent range.
+__device__ __forceinline__ int unif_scale_exp(uint32_t mbits) {
+  if (mbits == 0u || (mbits & 0x7f800000u) == 0x7f800000u) return 0;
+  return max(-126, min(127, 15 - exponent_of(__uint_as_float(mbits))));
 }
 
 __global__ void k_occupancy(const int* __restrict__ start, int span, int64_t ncells,
@@ -125,12 +124,14 @@ __global__ void k_occupancy(const int* __restrict__ start, int span, int64_t nce
 struct UnifTcArgs {
   const float2* X;       // level spectra [k][cell][C]
   float2* Y;             // level target spectra [k][cell][C]
-  const float* tiles;    // [nk][kUnifTcTileFloats] operator tiles of this level
+  const uint16_t* tiles;  // [nk][kUnifTcTileHalves] operator tiles of this level (F16)
+  const int* bexp;        // [nk] exponent sB of each frequency's tiles
+  const uint32_t* amax;   // [nk23][8] largest |spectra| (float bits) per (k23, column mod 8)
   const uint8_t* socc;   // [cell] source cell nonempty
   const uint8_t* tocc;   // [cell] target cell nonempty
   int lev;               // cells 2^lev per side, parents S = 2^(lev-1)
   int C, c0;             // columns of the arrays; first of this group of 8
-  int nk, kchunk, nchunks, nblocks;
+  int nk, nk23, kchunk, nchunks, nblocks;  // frequencies k = k1 nk23 + k23
   int* err;
 };
 
@@ -146,8 +147,7 @@ __global__ void __launch_bounds__(UT_THREADS, 1) k_m2l_unif_tc(const UnifTcArgs 
   extern __shared__ unsigned char smraw[];
   unsigned char* base = smraw + ((1024 - (smem_u32(smraw) & 1023)) & 1023);
   unsigned char* astage = base;                               // UT_NST x (hi | lo)
-  unsigned char* raw = astage + UT_NST * UT_ASTAGE;           // UT_NRAW raw lines
-  unsigned char* bbuf = raw + UT_NRAW * UT_RAWLINE;           // 2 x operator tiles
+  unsigned char* bbuf = astage + UT_NST * UT_ASTAGE;          // 2 x operator tiles
   __shared__ uint64_t s_full[UT_NST], s_empty[UT_NST], s_bfull[2], s_bempty[2], s_accf[2],
       s_acce[2];
   __shared__ uint32_t s_tmem;
@@ -169,8 +169,8 @@ __global__ void __launch_bounds__(UT_THREADS, 1) k_m2l_unif_tc(const UnifTcArgs 
   }
   if (tid == 0) {
     for (int i = 0; i < UT_NST; ++i) {
-      mbar_init(&s_full[i], 1);
-      mbar_init(&s_empty[i], 1);
+      mbar_init(&s_full[i], UT_PWARPS);  // one arrival per producer warp
+      mbar_init(&s_empty[i], 1);         // the MMA commit
       s_nz[i] = 0;
     }
     for (int i = 0; i < 2; ++i) {
@@ -197,131 +197,87 @@ __global__ void __launch_bounds__(UT_THREADS, 1) k_m2l_unif_tc(const UnifTcArgs 
   __syncthreads();
   tc_fence_after();
 
-  if (warp < UT_MMA_WARP) {
-    // ------------------------------------------------------------ producers
-    // The source lines of every frequency of every work item, in the order
-    // the MMA thread consumes them: item (block, frequency chunk) round robin
-    // over the CTAs, then frequency, then line.
-    struct Pos {
-      int item, k, sl;
-    };
-    auto first_k = [&](int item) { return (item / a.nblocks) * a.kchunk; };
-    auto end_k = [&](int item) { return min(a.nk, (item / a.nblocks + 1) * a.kchunk); };
-    auto advance = [&](Pos& p) {
-      if (++p.sl == UT_SRC_LINES) {
-        p.sl = 0;
-        if (++p.k == end_k(p.item)) {
-          p.item += gridDim.x;
-          if (p.item < nitems) p.k = first_k(p.item);
-        }
+  // The source lines of every frequency of every work item, in the order the
+  // MMA thread consumes them: item (block, frequency chunk) round robin over
+  // the CTAs, then frequency, then line.
+  struct Pos {
+    int item, k, sl;
+  };
+  auto first_k = [&](int item) { return (item / a.nblocks) * a.kchunk; };
+  auto end_k = [&](int item) { return min(a.nk, (item / a.nblocks + 1) * a.kchunk); };
+  auto advance = [&](Pos& p) {
+    if (++p.sl == UT_SRC_LINES) {
+      p.sl = 0;
+      if (++p.k == end_k(p.item)) {
+        p.item += gridDim.x;
+        if (p.item < nitems) p.k = first_k(p.item);
       }
-    };
-    const int ptid = tid;
-    // This thread's split tasks t = ptid + 256 i: K plane kc = t / 144 and
-    // row = t % 144 = (zpos, column); byte offsets in the raw line and in
-    // one part of an A stage (-1: no task)
-    constexpr int kSplit = (4 * UT_ROWS + UT_PRODUCERS - 1) / UT_PRODUCERS;
-    int split_src[kSplit], split_dst[kSplit];
-#pragma unroll
-    for (int i = 0; i < kSplit; ++i) {
-      const int t = ptid + i * UT_PRODUCERS;
-      const int kc = t / UT_ROWS, row = t - kc * UT_ROWS;
-      split_src[i] = t < 4 * UT_ROWS ? (row >> 3) * UT_RAWZ + (2 * kc) * 64 + (row & 7) * 8 : -1;
-      split_dst[i] = kc * UT_APLANE + row * 16;
     }
-    // This thread's raw chunks: q_i = ptid + 256 i (16 bytes each): parent
-    // zpos = q / 32, child j = (q / 4) % 8, columns 2 (q % 4) and 2 (q % 4) + 1.
-    // The z part of their Morton codes is fixed per work item.
-    constexpr int kPer = (UT_SRCZ * 32 + UT_PRODUCERS - 1) / UT_PRODUCERS;
-    int item_ctx = -1, bx = 0, y0 = 0, z0 = 0;
-    uint32_t zsp[kPer];
-    auto set_item = [&](int item) {
-      if (item == item_ctx) return;
-      item_ctx = item;
-      ut_block(item % a.nblocks, S, &bx, &y0, &z0);
+  };
+  if (warp < UT_PWARPS) {
+    // ------------------------------------------------------------ producers
+    // Thread ptid's task: K plane kc = ptid / 144 (the children 4 kc ..
+    // 4 kc + 3) and row = ptid % 144 = (zpos, column) of every source line.
+    // Its four spectra values (8 bytes each; a warp's loads cover four
+    // parents x 64 contiguous bytes per child) and the children's occupancy
+    // are loaded into registers UT_RING lines ahead of their split, so the
+    // loads of several lines are in flight while the warp converts one.
+    // Each producer warp runs on its own, ordered by mbarriers: a line is
+    // stored once the MMAs of the stage's previous line completed
+    // (s_empty), and the MMA thread starts once every warp stored its part
+    // (s_full).
+    const int ptid = tid;
+    const int t_kc = ptid / UT_ROWS, t_row = ptid - t_kc * UT_ROWS;
+    const int t_z = t_row >> 3, t_col = t_row & 7;
+    const int split_dst = t_kc * UT_APLANE + t_row * 16;
+    struct Slot {
+      float2 v[4];    // children 4 kc + e, column c0 + t_col
+      uint32_t occ;   // their occupancy bytes (0 outside the domain)
+      uint32_t amax;  // the spectra maximum of (k23, t_col)
+    };
+    Slot ring[UT_RING];
+    Pos lp{(int)blockIdx.x, 0, 0};  // the next line to load
+    if (lp.item < nitems) lp.k = first_k(lp.item);
+    int item_ctx = -1, bx = 0, y0 = 0;
+    uint32_t zsp = 0xffffffffu;
+    auto load = [&](Slot& r) {
+      if (lp.item != item_ctx) {
+        int z0;
+        item_ctx = lp.item;
+        ut_block(lp.item % a.nblocks, S, &bx, &y0, &z0);
+        const int z = z0 - 1 + t_z;
+        zsp = (z >= 0 && z < S) ? spread3((uint32_t)z) : 0xffffffffu;
+      }
+      const int xs = bx + lp.sl / (UT_BY + 2) - 1, ys = y0 + lp.sl % (UT_BY + 2) - 1;
+      const bool in = xs >= 0 && xs < S && ys >= 0 && ys < S && zsp != 0xffffffffu;
+      r.amax = __ldg(a.amax + 8 * (lp.k % a.nk23) + t_col);
+      r.occ = 0;
+      if (in) {
+        const int64_t cell =
+            8 * (int64_t)((spread3((uint32_t)xs) << 2) | (spread3((uint32_t)ys) << 1) | zsp) +
+            4 * t_kc;
+        r.occ = __ldg(reinterpret_cast<const uint32_t*>(a.socc + cell));
+        const float2* src = a.X + ((int64_t)lp.k * ncells + cell) * a.C + a.c0 + t_col;
 #pragma unroll
-      for (int i = 0; i < kPer; ++i) {
-        const int q = ptid + i * UT_PRODUCERS;
-        const int z = z0 - 1 + (q >> 5);
-        zsp[i] = (q < UT_SRCZ * 32 && z >= 0 && z < S) ? spread3((uint32_t)z) : 0xffffffffu;
+        for (int e = 0; e < 4; ++e) r.v[e] = __ldg(src + (int64_t)e * a.C);
       }
+      advance(lp);
     };
-    // A line whose copies are about to be issued: its cells and their
-    // occupancy, loaded one iteration before the copies need them.
-    struct Pending {
-      int64_t cell[kPer];
-      uint8_t occ[kPer];
-      int k;
-    };
-    auto prepare = [&](const Pos& p, Pending& L) {
-      set_item(p.item);
-      const int xs = bx + p.sl / (UT_BY + 2) - 1, ys = y0 + p.sl % (UT_BY + 2) - 1;
-      const bool in = xs >= 0 && xs < S && ys >= 0 && ys < S;
-      const uint32_t xy = in ? (spread3((uint32_t)xs) << 2) | (spread3((uint32_t)ys) << 1) : 0u;
-#pragma unroll
-      for (int i = 0; i < kPer; ++i) {
-        const int q = ptid + i * UT_PRODUCERS;
-        L.cell[i] = (in && zsp[i] != 0xffffffffu) ? 8 * (int64_t)(xy | zsp[i]) + ((q >> 2) & 7) : -1;
-        L.occ[i] = L.cell[i] >= 0 ? a.socc[L.cell[i]] : 0;
-      }
-      L.k = p.k;
-    };
-    // raw copies (cp.async) of a prepared line into raw slot `slot`, zero for
-    // empty or out-of-domain cells; parent rows UT_RAWZ bytes apart
-    auto issue = [&](const Pending& L, int slot) -> bool {
-      unsigned char* dst = raw + slot * UT_RAWLINE;
-      const float2* xk = a.X + (int64_t)L.k * ncells * a.C + a.c0;
-      bool any = false;
-#pragma unroll
-      for (int i = 0; i < kPer; ++i) {
-        const int q = ptid + i * UT_PRODUCERS;
-        if (q < UT_SRCZ * 32) {
-          const bool ok = L.occ[i] != 0;
-          any |= ok;
-          cp_async16(dst + (q >> 5) * UT_RAWZ + (q & 31) * 16,
-                     ok ? xk + L.cell[i] * a.C + 2 * (q & 3) : a.X, ok ? 16 : 0);
-        }
-      }
-      return any;
-    };
-    Pos cur{(int)blockIdx.x, 0, 0};
-    if (cur.item < nitems) cur.k = first_k(cur.item);
-    // prefetch: the raw copies run UT_PREFETCH lines ahead of the split, in
-    // UT_PREFETCH + 2 slots (a slot is rewritten two iterations after its
-    // split, so one barrier per line orders the reuse)
-    Pos pf = cur;
-    Pending L;
-    bool have = pf.item < nitems;
-    if (have) prepare(pf, L);
-    int issued = 0;
-    uint32_t anymask = 0;  // bit r: this thread's chunks of the line in raw slot r hold data
-    auto issue_next = [&]() {
-      if (have) {
-        const int slot = issued % UT_NRAW;
-        anymask = (anymask & ~(1u << slot)) | ((issue(L, slot) ? 1u : 0u) << slot);
-        ++issued;
-        advance(pf);
-        have = pf.item < nitems;
-        if (have) prepare(pf, L);
-      }
-      cp_async_commit();  // (possibly empty) keeps one group per line
-    };
-    for (int i = 0; i < UT_PREFETCH; ++i) issue_next();
     // operator tiles: frequency f goes to buffer f % 2; the load for f + 1 is
-    // issued in the middle of frequency f (the MMAs of f - 1, the buffer's
-    // previous user, are issued by then)
-    Pos bnext = cur;  // the frequency whose tiles are loaded next
-    int fi = 0, li = 0, bissued = 0, last_b = -1;
+    // issued by thread 0 in the middle of frequency f (the MMAs of f - 1,
+    // the buffer's previous user, are issued by then)
+    Pos bnext{(int)blockIdx.x, 0, 0};
+    if (bnext.item < nitems) bnext.k = first_k(bnext.item);
+    int bissued = 0, last_b = -1;
     auto load_b = [&]() -> bool {  // ptid 0 only
       if (bnext.item >= nitems) return true;
       const int fb = bissued & 1;
       if (bissued >= 2 && !mbar_wait(&s_bempty[fb], ((bissued - 2) >> 1) & 1, s_abort, piters))
         return false;
       mbar_arrive_expect_tx(&s_bfull[fb], UT_BFREQ);
-      bulk_load(bbuf + fb * UT_BFREQ, a.tiles + (int64_t)bnext.k * kUnifTcTileFloats, UT_BFREQ,
+      bulk_load(bbuf + fb * UT_BFREQ, a.tiles + (int64_t)bnext.k * kUnifTcTileHalves, UT_BFREQ,
                 &s_bfull[fb]);
       last_b = bissued++;
-      // the following frequency
       if (++bnext.k == end_k(bnext.item)) {
         bnext.item += gridDim.x;
         if (bnext.item < nitems) bnext.k = first_k(bnext.item);
@@ -329,57 +285,62 @@ __global__ void __launch_bounds__(UT_THREADS, 1) k_m2l_unif_tc(const UnifTcArgs 
       return true;
     };
     bool fail = false;
-    if (ptid == 0 && cur.item < nitems) fail = !load_b();
-    for (; cur.item < nitems; advance(cur)) {
-      if (ptid == 0 && cur.sl == UT_SRC_LINES / 2 && !fail) fail = !load_b();
-      issue_next();
-      asm volatile("cp.async.wait_group %0;\n" ::"n"(UT_PREFETCH) : "memory");
-      const int s = li % UT_NST;
-      // one thread waits for the stage (its MMAs of UT_NST lines ago); the
-      // barrier-with-reduction then releases every producer, makes the raw
-      // line complete for all of them, and lets all leave together on failure
-      if (ptid == 0 && li >= UT_NST &&
-          !mbar_wait(&s_empty[s], (li / UT_NST - 1) & 1, s_abort, piters))
-        fail = true;
-      if (producers_any(fail)) {
-        *s_abort = 1;
-        break;
-      }
-      // split into the A layout: task t = (kc, row), row = (zpos, column);
-      // a warp's stores fill 32 consecutive 16-byte rows of one K plane
-      const unsigned char* rl = raw + (li % UT_NRAW) * UT_RAWLINE;
-      unsigned char* ahi = astage + s * UT_ASTAGE;
-      unsigned char* alo = ahi + UT_APART;
+    if (ptid == 0) fail = !load_b();
 #pragma unroll
-      for (int i = 0; i < kSplit; ++i) {
-        if (split_src[i] >= 0) {
-          const unsigned char* src = rl + split_src[i];
-          const float2 u = *reinterpret_cast<const float2*>(src);
-          const float2 v = *reinterpret_cast<const float2*>(src + 64);
-          const float r[4] = {u.x, u.y, v.x, v.y};
-          float h[4], l[4];
+    for (int d = 0; d < UT_RING; ++d)
+      if (lp.item < nitems) load(ring[d]);
+    Pos cur{(int)blockIdx.x, 0, 0};  // the line to store
+    if (cur.item < nitems) cur.k = first_k(cur.item);
+    int li = 0;
+    while (cur.item < nitems && !fail) {
 #pragma unroll
-          for (int e = 0; e < 4; ++e) {
-            h[e] = tf32_rna_bits(r[e]);
-            l[e] = tf32_rna_bits(r[e] - h[e]);
-          }
-          *reinterpret_cast<float4*>(ahi + split_dst[i]) = make_float4(h[0], h[1], h[2], h[3]);
-          *reinterpret_cast<float4*>(alo + split_dst[i]) = make_float4(l[0], l[1], l[2], l[3]);
+      for (int d = 0; d < UT_RING; ++d) {
+        if (cur.item >= nitems) break;
+        if (ptid == 0 && cur.sl == UT_SRC_LINES / 2 && !load_b()) fail = true;
+        const int s = li % UT_NST;
+        if (!fail && li >= UT_NST &&
+            !mbar_wait(&s_empty[s], (li / UT_NST - 1) & 1, s_abort, piters))
+          fail = true;
+        if (__any_sync(0xffffffffu, fail)) {
+          fail = true;
+          break;
         }
+        // scaled split into the A layout, zero for empty cells and parents
+        // outside the domain; a warp's stores fill 32 consecutive 16-byte
+        // rows of one K plane
+        {
+          const Slot& r = ring[d];
+          const float sc = exp2i(unif_scale_exp(r.amax));
+          uint32_t h[4], l[4];
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {  // child 4 kc + e: (re, im)
+            const bool ok = (r.occ >> (8 * e)) & 0xffu;
+            const float x0 = ok ? r.v[e].x * sc : 0.f, x1 = ok ? r.v[e].y * sc : 0.f;
+            const __half2 hh = __floats2half2_rn(x0, x1);
+            const float2 hf = __half22float2(hh);
+            const __half2 ll = __floats2half2_rn(x0 - hf.x, x1 - hf.y);
+            h[e] = *reinterpret_cast<const uint32_t*>(&hh);
+            l[e] = *reinterpret_cast<const uint32_t*>(&ll);
+          }
+          unsigned char* ahi = astage + s * UT_ASTAGE;
+          *reinterpret_cast<uint4*>(ahi + split_dst) = make_uint4(h[0], h[1], h[2], h[3]);
+          *reinterpret_cast<uint4*>(ahi + UT_APART + split_dst) =
+              make_uint4(l[0], l[1], l[2], l[3]);
+          if (r.occ) s_nz[s] = li + 1;
+        }
+        fence_async_smem();  // this thread's generic-proxy stores, to the tensor pipe
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&s_full[s]);
+        if (lp.item < nitems) load(ring[d]);
+        advance(cur);
+        ++li;
       }
-      if ((anymask >> (li % UT_NRAW)) & 1u) s_nz[s] = li + 1;
-      fence_async_smem();  // this thread's generic-proxy stores, to the tensor pipe
-      group_sync(1, UT_PRODUCERS);  // every producer's stores and fence
-      if (ptid == 0) mbar_arrive(&s_full[s]);
-      ++li;
-      if (cur.sl == UT_SRC_LINES - 1) ++fi;
     }
-    cp_async_wait_all();
+    if (fail) *s_abort = 1;
     // no bulk copy may still be writing when the CTA ends
     if (ptid == 0 && last_b >= 0 &&
         !mbar_wait(&s_bfull[last_b & 1], (last_b >> 1) & 1, nullptr))
       *s_abort = 1;
-    (void)fi;
   } else if (warp == UT_MMA_WARP) {
     // ------------------------------------------------------------ MMA issue
     if (lane == 0) {
@@ -411,7 +372,7 @@ __global__ void __launch_bounds__(UT_THREADS, 1) k_m2l_unif_tc(const UnifTcArgs 
               const int dxi = sl / (UT_BY + 2), sy = sl % (UT_BY + 2) - 1;
               const int ty_lo = max(0, sy - 1), ty_hi = min(UT_BY - 1, sy + 1);
               const int dyi_lo = ty_lo - sy + 1, nl = ty_hi - ty_lo + 1;
-              const uint32_t idesc = tf32_idesc(128, 32 * nl);
+              const uint32_t idesc = f16_idesc(128, 32 * nl);
               const uint32_t d = dset + (uint32_t)(32 * ty_lo);
               // descriptors of the line's first A and B tiles; the others
               // differ only in their start address (16-byte units, no carry:
@@ -420,15 +381,13 @@ __global__ void __launch_bounds__(UT_THREADS, 1) k_m2l_unif_tc(const UnifTcArgs 
               const uint64_t b0 =
                   kmajor_desc(bb + (uint32_t)(dxi * 3 * UT_BTILE + dyi_lo * 32 * 16), UT_BPLANE, 128);
 #pragma unroll
-              for (int dzi = 0; dzi < 3; ++dzi)
-#pragma unroll
-                for (int ks = 0; ks < 2; ++ks) {
-                  // A window D_z + 1 parents down; K step ks = planes 2 ks, 2 ks + 1
-                  const uint64_t ah = a0 + ((dzi * 8 * 16 + ks * 2 * UT_APLANE) >> 4);
-                  const uint64_t bd = b0 + ((dzi * UT_BTILE + ks * 2 * UT_BPLANE) >> 4);
-                  tc_mma_tf32(d, ah, bd, idesc, 1u);
-                  tc_mma_tf32(d, ah + (UT_APART >> 4), bd, idesc, 1u);
-                }
+              for (int dzi = 0; dzi < 3; ++dzi) {
+                // A window D_z + 1 parents down
+                const uint64_t ah = a0 + ((dzi * 8 * 16) >> 4);
+                const uint64_t bd = b0 + ((dzi * UT_BTILE) >> 4);
+                tc_mma_f16(d, ah, bd, idesc, 1u);
+                tc_mma_f16(d, ah + (UT_APART >> 4), bd, idesc, 1u);
+              }
             }
             tc_commit(&s_empty[s]);
             committed = true;
@@ -468,6 +427,9 @@ __global__ void __launch_bounds__(UT_THREADS, 1) k_m2l_unif_tc(const UnifTcArgs 
           break;
         }
         tc_fence_after();
+        // undo the scaling of this row's column and of the frequency's tiles
+        const float ua = exp2i(-unif_scale_exp(__ldg(a.amax + 8 * (k % a.nk23) + col)));
+        const float ub = exp2i(-__ldg(a.bexp + k));
         for (int ty = 0; ty < UT_BY; ++ty) {
           const uint32_t ta = lb + (uint32_t)(fb * UT_BY * 32 + 32 * ty);
           uint32_t h[16], l[16];
@@ -480,9 +442,9 @@ __global__ void __launch_bounds__(UT_THREADS, 1) k_m2l_unif_tc(const UnifTcArgs 
           for (int t = 0; t < 8; ++t) {
             const int64_t cell = 8 * p + t;
             if (a.tocc[cell])
-              a.Y[((int64_t)k * ncells + cell) * a.C + a.c0 + col] =
-                  make_float2(__uint_as_float(h[2 * t]) + __uint_as_float(l[2 * t]),
-                              __uint_as_float(h[2 * t + 1]) + __uint_as_float(l[2 * t + 1]));
+              a.Y[((int64_t)k * ncells + cell) * a.C + a.c0 + col] = make_float2(
+                  (__uint_as_float(h[2 * t]) + __uint_as_float(l[2 * t])) * ua * ub,
+                  (__uint_as_float(h[2 * t + 1]) + __uint_as_float(l[2 * t + 1])) * ua * ub);
           }
         }
         tc_wait_st();
@@ -505,49 +467,63 @@ __global__ void __launch_bounds__(UT_THREADS, 1) k_m2l_unif_tc(const UnifTcArgs 
 
 // Operator tiles of the tensor-core MAC from the spectra op[lvl][k][343]
 // (complex, lex-indexed offsets, inner 27 zero): for each level and frequency
-// nine tiles (D_x, D_z), each [kcore 4][row 96][4 floats], row = 32 dyi +
-// 16 part + 2 t + ri_out (D_y = 1 - dyi; part 0: TF32 hi, 1: lo), element
-// K = 4 kcore + e = 2 s + ri_in, value the real form of E[o] with
+// nine tiles (D_x, D_z), each [kcore 2][row 96][8 halves], row = 32 dyi +
+// 16 part + 2 t + ri_out (D_y = 1 - dyi; part 0: F16 hi, 1: lo), element
+// K = 8 kcore + e = 2 s + ri_in, value the real form of E[o] with
 // o = 2 D + bits(s) - bits(t):  (re, re) = a, (im, re) = -b, (re, im) = b,
-// (im, im) = a for E = a + i b, zero where o is near.
-void unif_tc_tiles(int n, const std::vector<double>& op, int nlev, std::vector<float>* tiles) {
+// (im, im) = a for E = a + i b, zero where o is near; every value of a
+// frequency scaled by 2^sB (bexp), sB putting the largest in [2^14, 2^15).
+void unif_tc_tiles(int n, const std::vector<double>& op, int nlev, std::vector<uint16_t>* tiles,
+                   std::vector<int>* bexp) {
   const int m = 2 * n - 1, nk = m * m * n;
-  tiles->assign((size_t)nlev * nk * kUnifTcTileFloats, 0.f);
-  auto tf32r = [](float x) {
-    uint32_t u;
-    memcpy(&u, &x, 4);
-    if ((u & 0x7f800000u) == 0x7f800000u) return x;
-    u = (u + 0x1000u) & 0xffffe000u;  // to nearest, ties away (cvt.rna.tf32.f32)
-    float r;
-    memcpy(&r, &u, 4);
-    return r;
-  };
+  tiles->assign((size_t)nlev * nk * kUnifTcTileHalves, 0);
+  bexp->assign((size_t)nlev * nk, 0);
   parallel_for((int64_t)nlev * nk, [&](int64_t b0, int64_t b1) {
+    std::vector<float> val(UT_BFREQ / 4);  // float32 values of the hi slots, tile order
     for (int64_t b = b0; b < b1; ++b) {
       const double* E = &op[(size_t)b * 343 * 2];
-      float* dst = tiles->data() + (size_t)b * kUnifTcTileFloats;
-      for (int dxi = 0; dxi < 3; ++dxi)
-        for (int dzi = 0; dzi < 3; ++dzi) {
-          float* tile = dst + (dxi * 3 + dzi) * (UT_BTILE / 4);
-          for (int row = 0; row < UT_BROWS; ++row) {
-            const int dyi = row / 32, part = (row / 16) & 1, t = (row & 15) >> 1, ro = row & 1;
-            const int D[3] = {dxi - 1, 1 - dyi, dzi - 1};
-            for (int kk = 0; kk < 16; ++kk) {
-              const int s = kk >> 1, ri = kk & 1;
-              int o[3], far = 0;
-              for (int d = 0; d < 3; ++d) {
-                o[d] = 2 * D[d] + ((s >> (2 - d)) & 1) - ((t >> (2 - d)) & 1);
-                far |= o[d] > 1 || o[d] < -1;
-              }
-              double v = 0;
-              if (far) {
-                const int lex = 49 * (o[0] + 3) + 7 * (o[1] + 3) + (o[2] + 3);
-                const double re = E[2 * lex], im = E[2 * lex + 1];
-                v = ri == ro ? re : (ri ? -im : im);
-              }
-              const float hi = tf32r((float)v), lo = tf32r((float)v - hi);
-              tile[((kk >> 2) * UT_BROWS + row) * 4 + (kk & 3)] = part ? lo : hi;
+      float vmax = 0.f;
+      for (int tile = 0; tile < 9; ++tile) {
+        const int dxi = tile / 3, dzi = tile % 3;
+        for (int row = 0; row < UT_BROWS; ++row) {
+          const int dyi = row / 32, part = (row / 16) & 1, t = (row & 15) >> 1, ro = row & 1;
+          if (part) continue;
+          const int D[3] = {dxi - 1, 1 - dyi, dzi - 1};
+          for (int kk = 0; kk < 16; ++kk) {
+            const int s = kk >> 1, ri = kk & 1;
+            int o[3], far = 0;
+            for (int d = 0; d < 3; ++d) {
+              o[d] = 2 * D[d] + ((s >> (2 - d)) & 1) - ((t >> (2 - d)) & 1);
+              far |= o[d] > 1 || o[d] < -1;
             }
+            float v = 0.f;
+            if (far) {
+              const int lex = 49 * (o[0] + 3) + 7 * (o[1] + 3) + (o[2] + 3);
+              const double re = E[2 * lex], im = E[2 * lex + 1];
+              v = (float)(ri == ro ? re : (ri ? -im : im));
+            }
+            val[(size_t)(tile * 48 + dyi * 16 + (row & 15)) * 16 + kk] = v;
+            vmax = std::max(vmax, std::fabs(v));
+          }
+        }
+      }
+      int e = 0;
+      if (vmax > 0.f && std::isfinite(vmax)) {
+        int k2;
+        std::frexp(vmax, &k2);
+        e = std::max(-126, std::min(127, 15 - k2));
+      }
+      (*bexp)[b] = e;
+      uint16_t* dst = tiles->data() + (size_t)b * kUnifTcTileHalves;
+      for (int tile = 0; tile < 9; ++tile)
+        for (int row = 0; row < UT_BROWS; ++row) {
+          const int dyi = row / 32, part = (row / 16) & 1;
+          for (int kk = 0; kk < 16; ++kk) {
+            const float x = std::ldexp(val[(size_t)(tile * 48 + dyi * 16 + (row & 15)) * 16 + kk], e);
+            const __half xh = __float2half_rn(x);
+            const __half xv = part ? __float2half_rn(x - __half2float(xh)) : xh;
+            memcpy(&dst[tile * (UT_BTILE / 2) + (kk >> 3) * (UT_BPLANE / 2) + row * 8 + (kk & 7)],
+                   &xv, 2);
           }
         }
     }
@@ -555,13 +531,13 @@ void unif_tc_tiles(int n, const std::vector<double>& op, int nlev, std::vector<f
 }
 
 bool unif_tc_eligible(const pbbfmm_tree* t, int l, int C) {
-  return t->use_tc && t->f_unif_tiles && (C % 8) == 0 && l >= 5 && l <= 10;
+  return t->use_tc && t->f_unif_tiles && t->f_unif_bexp && (C % 8) == 0 && l >= 5 && l <= 10;
 }
 
 // Level l of the tensor-core MAC (after the forward FFTs): Y = sum_D B X for
 // every column group of 8.
 int run_m2l_unif_tc_level(pbbfmm_tree* t, int C, int l, int lvl, const float2* X, float2* Y,
-                          cudaStream_t st) {
+                          const uint32_t* amax, cudaStream_t st) {
   if (!t->d_tc_err) {
     set_error("tensor-core uniform M2L: the tree has no timeout flag");
     return PBBFMM_ERR_STATE;
@@ -584,7 +560,10 @@ int run_m2l_unif_tc_level(pbbfmm_tree* t, int C, int l, int lvl, const float2* X
   UnifTcArgs a{};
   a.X = X;
   a.Y = Y;
-  a.tiles = t->f_unif_tiles + (size_t)lvl * nk * kUnifTcTileFloats;
+  a.tiles = t->f_unif_tiles + (size_t)lvl * nk * kUnifTcTileHalves;
+  a.bexp = t->f_unif_bexp + (size_t)lvl * nk;
+  a.amax = amax;
+  a.nk23 = (2 * t->n - 1) * t->n;
   a.socc = socc;
   a.tocc = tocc;
   a.lev = l;

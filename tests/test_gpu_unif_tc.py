@@ -1,7 +1,7 @@
 """The frequency-domain M2L of the mixed uniform path on the tensor cores
-(csrc/m2l_unif_tc.cu: tcgen05 kind::tf32 on hi / lo splits of both
-operands, float32 accumulation), through the C-ABI, against the CUDA-core
-float32 kernel it replaces and against the float64 path.
+(csrc/m2l_unif_tc.cu: tcgen05 kind::f16 on power-of-two scaled F16 hi / lo
+splits of both operands, float32 accumulation), through the C-ABI, against
+the CUDA-core float32 kernel it replaces and against the float64 path.
 
 It runs at levels with at least 16 parents per side and for column groups of
 8; other levels and column counts stay on the CUDA cores.  Tolerances: the
@@ -92,7 +92,7 @@ def test_unif_tensor_core_mac_not_used_for_other_column_counts():
 
 
 def test_unif_tensor_core_scale_invariance():
-    """No operand scaling is involved (TF32 keeps float32's exponent range):
+    """The operand scales are powers of two taken from the spectra's maxima:
     weights scaled by 2^60 and 2^-60 scale the result by exactly that."""
     rng = np.random.default_rng(57)
     N, C = 40000, 8
@@ -103,6 +103,24 @@ def test_unif_tensor_core_scale_invariance():
     o = _run(t, p, w, C, fmm.PREC_MIXED)
     for s in (2.0 ** 60, 2.0 ** -60):
         assert rel(_run(t, p, w * s, C, fmm.PREC_MIXED), o * s) < 1e-12
+    t.close()
+
+
+def test_unif_tensor_core_columns_of_any_magnitude():
+    """Each column (mod 8) has its own spectra scale: columns whose weights
+    differ by 2^-40 .. 2^30 each keep float32 accuracy on their own."""
+    rng = np.random.default_rng(59)
+    N, C = 60000, 8
+    p = rng.uniform(-0.5, 0.5, (N, 3))
+    w = rng.standard_normal((C, N))
+    w *= np.exp2(10.0 * (np.arange(C) - 4))[:, None]
+    w = w.ravel()
+    t = make_tree("ExpCov", 0.3, 1.0, 5, 4, 1e-6, 0)
+    t.buildFMMTree()
+    o64 = _run(t, p, w, C, fmm.PREC_FP64).reshape(C, N)
+    o_tc = _run(t, p, w, C, fmm.PREC_MIXED, tc=True).reshape(C, N)
+    for c in range(C):
+        assert rel(o_tc[c], o64[c]) < 2e-6, (c, rel(o_tc[c], o64[c]))
     t.close()
 
 
