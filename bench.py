@@ -61,6 +61,13 @@ WORKLOADS = {
     "grad": dict(name="gauss0.1_cheb5_S1e6_T1e6_C4_L6", kernel="GaussSigma", param=0.1,
                  N=1_000_000, C=4, L=6, n=5, cheb=1, eps=1e-6, box=1.0, seed=777,
                  dist="uniform", weights="normal"),
+    # kernel solve with gradient: GMRES on (K + 1e-2 I) x = b, 8 right-hand sides
+    "solve": dict(name="expcov0.2_unif5_N2e6_C8_L7_gmres", kernel="ExpCov", param=0.2,
+                  N=2_000_000, C=8, L=7, n=5, cheb=0, eps=1e-5, box=1.0, seed=2468,
+                  dist="uniform", weights="normal", lam=1e-2, tol=1e-6),
+    "solve_small": dict(name="expcov0.2_unif5_N2e5_C8_L6_gmres", kernel="ExpCov", param=0.2,
+                        N=200_000, C=8, L=6, n=5, cheb=0, eps=1e-5, box=1.0, seed=2468,
+                        dist="uniform", weights="normal", lam=1e-2, tol=1e-6),
     "profile": dict(name="expcov0.3_unif5_N262144_C8_L5", kernel="ExpCov", param=0.3, N=262_144,
                     C=8, L=5, n=5, cheb=0, eps=1e-5, box=1.0, seed=1234, dist="uniform",
                     weights="normal"),
@@ -743,6 +750,79 @@ def run_grad_workload(wl, args, local_rank):
     }
 
 
+def run_solve_workload(wl, args, local_rank, max_fast=120):
+    """GMRES solve of (K + lam I) x = b for 8 right-hand sides at once, mixed
+    precision (GMRES on the mixed-precision FMM inside float64 iterative
+    refinement, pbbfmm3d_b200.solve.kernel_solve), and its backward (the
+    adjoint solve plus the adjoint FMM for dL/d(points)) for L = sum(x * g).
+    The float64 matvecs run in two groups of 4 columns (the level-7 spectra
+    of 8 float64 columns would need ~220 GB).  Timed with CUDA events around
+    the whole solve; at most ``max_fast`` mixed-precision matvecs per solve."""
+    import torch
+
+    import pbbfmm3d_b200 as fmm
+    from pbbfmm3d_b200.solve import kernel_operator, kernel_solve
+
+    dev = torch.device("cuda", local_rank)
+    rng = np.random.default_rng(wl["seed"])
+    N, C = wl["N"], wl["C"]
+    P = torch.tensor(rng.uniform(0.0, 1.0, (N, 3)), device=dev)
+    b = torch.tensor(rng.standard_normal((C, N)), device=dev)
+    g = torch.tensor(rng.standard_normal((C, N)), device=dev)
+    tree = make_tree(fmm, wl, local_rank)
+    t0 = time.time()
+    tree.buildFMMTree()
+    pre_s = time.time() - t0
+    stream = torch.cuda.current_stream(dev)
+
+    def event_ms(fn):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1), r
+
+    fast = kernel_operator(tree, P, wl["lam"], fmm.PREC_MIXED)
+    exact = kernel_operator(tree, P, wl["lam"], fmm.PREC_FP64, max_cols=4)
+    fast(b)
+    exact(b)  # warm-up: workspace allocation
+    mv_fast, _ = event_ms(lambda: fast(b))
+    mv_exact, _ = event_ms(lambda: exact(b))
+    info = {}
+    bb = b.clone().requires_grad_(True)
+    Pg = P.clone().requires_grad_(True)
+    f_ms, x = event_ms(lambda: kernel_solve(tree, Pg, bb, wl["lam"], tol=wl["tol"],
+                                            precision=fmm.PREC_MIXED, restart=30,
+                                            maxiter=max_fast, exact_cols=4, info=info))
+    b_ms, _ = event_ms(lambda: (x * g).sum().backward())
+    res = exact(x.detach()) - b
+    rel = (torch.linalg.norm(res, dim=1) / torch.linalg.norm(b, dim=1)).cpu().numpy()
+    fi, ai = info["forward"], info.get("adjoint", {})
+    tree.close()
+    del tree
+    torch.cuda.empty_cache()
+    return {
+        "config": workload_config(wl), "lam": wl["lam"], "tol": wl["tol"],
+        "precision_detail": "GMRES(30) on the mixed-precision FMM (float32 near field, "
+                            "tensor-core frequency-domain M2L) inside float64 iterative "
+                            "refinement; float64 residuals",
+        "precompute_s": pre_s,
+        "matvec_ms": {"mixed_8cols": mv_fast, "fp64_8cols_as_2x4": mv_exact},
+        "solve": {"ms": f_ms, "mixed_matvecs": fi["matvecs"],
+                  "fp64_matvecs": fi["exact_matvecs"], "outer_refinements": fi["outer"],
+                  "rel_residual_max": float(np.max(rel)), "converged": bool(fi["converged"]),
+                  "matvec_cap": max_fast},
+        "adjoint_solve": {"ms_backward": b_ms, "mixed_matvecs": ai.get("matvecs"),
+                          "fp64_matvecs": ai.get("exact_matvecs"),
+                          "rel_residual_max": (float(np.max(ai["rel_residual"]))
+                                               if "rel_residual" in ai else None),
+                          "converged": bool(ai.get("converged", False)),
+                          "includes": "adjoint GMRES solve + adjoint FMM for dL/d(points)"},
+    }
+
+
 def our_arm(args, rank, world, local_rank):
     import torch
 
@@ -764,6 +844,9 @@ def our_arm(args, rank, world, local_rank):
     diff = None
     if args.workload == "bench" and not args.no_grad and world == 1:
         diff = run_grad_workload(WORKLOADS["grad"], args, local_rank)
+    solve = None
+    if args.workload == "bench" and not args.no_solve and world == 1:
+        solve = run_solve_workload(WORKLOADS[args.solve_workload], args, local_rank)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -803,6 +886,8 @@ def our_arm(args, rank, world, local_rank):
     line.update(targets)
     if diff is not None:
         line["differentiation"] = diff
+    if solve is not None:
+        line["kernel_solve"] = solve
     print(json.dumps(line))
     return 0
 
@@ -819,6 +904,9 @@ def main():
                     help="skip the forward+backward (adjoint) workload block")
     ap.add_argument("--no-target", action="store_true",
                     help="skip the clustered Chebyshev (tensor-core) workload block")
+    ap.add_argument("--no-solve", action="store_true",
+                    help="skip the kernel-solve (GMRES, 2M points) workload block")
+    ap.add_argument("--solve-workload", default="solve", choices=["solve", "solve_small"])
     ap.add_argument("--workload", default="bench", choices=sorted(WORKLOADS))
     ap.add_argument("--reference-full", action="store_true",
                     help="reference arm: also time one run on the whole workload")

@@ -242,7 +242,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       const int s = j % NST;
       // warp-uniform: the shuffles below are warp-collective
       if (j >= NST &&
-          !__all_sync(0xffffffffu, mbar_wait(&s_empty[s], (j / NST - 1) & 1, s_abort, piters))) {
+          !__all_sync(0xffffffffu, mbar_wait_sleep(&s_empty[s], (j / NST - 1) & 1, s_abort, piters))) {
         *s_abort = 1;
         break;
       }
@@ -297,12 +297,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         // accumulator g % NACC is free once the drain of group g - NACC is done
         const int ab = g % NACC;
         if (fresh && g >= NACC &&
-            !mbar_wait(&s_acce[ab], ((g - NACC) / NACC) & 1, s_abort, piters)) {
+            !mbar_wait_sleep(&s_acce[ab], ((g - NACC) / NACC) & 1, s_abort, piters)) {
           *s_abort = 1;
           break;
         }
-        if (!mbar_wait(&s_full[s], (it / NST) & 1, s_abort, piters) ||
-            !mbar_wait(&s_tfull[s], (it / NST) & 1, s_abort, piters)) {
+        if (!mbar_wait_sleep(&s_full[s], (it / NST) & 1, s_abort, piters) ||
+            !mbar_wait_sleep(&s_tfull[s], (it / NST) & 1, s_abort, piters)) {
           *s_abort = 1;
           break;
         }
@@ -384,7 +384,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
       v2 = has_src(g + 2);
       if (F16 && g + 2 < nvalid) x2 = pexp[src_row(g + 2, v2)];
       // warp-uniform: the TMEM loads below are warp-collective
-      if (!__all_sync(0xffffffffu, mbar_wait(&s_accf[b], (g / NACC) & 1, s_abort, piters))) {
+      if (!__all_sync(0xffffffffu, mbar_wait_sleep(&s_accf[b], (g / NACC) & 1, s_abort, piters))) {
         *s_abort = 1;
         break;
       }

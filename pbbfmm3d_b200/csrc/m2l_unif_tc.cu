@@ -238,8 +238,9 @@ __global__ void __launch_bounds__(UT_THREADS, 1) k_m2l_unif_tc(const UnifTcArgs 
     Slot ring[UT_RING];
     Pos lp{(int)blockIdx.x, 0, 0};  // the next line to load
     if (lp.item < nitems) lp.k = first_k(lp.item);
-    int item_ctx = -1, bx = 0, y0 = 0;
+    int item_ctx = -1, bx = 0, y0 = 0, k_ctx = -1;
     uint32_t zsp = 0xffffffffu;
+    const uint32_t* amax_k = a.amax;
     auto load = [&](Slot& r) {
       if (lp.item != item_ctx) {
         int z0;
@@ -250,7 +251,11 @@ __global__ void __launch_bounds__(UT_THREADS, 1) k_m2l_unif_tc(const UnifTcArgs 
       }
       const int xs = bx + lp.sl / (UT_BY + 2) - 1, ys = y0 + lp.sl % (UT_BY + 2) - 1;
       const bool in = xs >= 0 && xs < S && ys >= 0 && ys < S && zsp != 0xffffffffu;
-      r.amax = __ldg(a.amax + 8 * (lp.k % a.nk23) + t_col);
+      if (lp.k != k_ctx) {
+        k_ctx = lp.k;
+        amax_k = a.amax + 8 * (lp.k % a.nk23) + t_col;
+      }
+      r.amax = __ldg(amax_k);
       r.occ = 0;
       if (in) {
         const int64_t cell =
@@ -299,7 +304,7 @@ __global__ void __launch_bounds__(UT_THREADS, 1) k_m2l_unif_tc(const UnifTcArgs 
         if (ptid == 0 && cur.sl == UT_SRC_LINES / 2 && !load_b()) fail = true;
         const int s = li % UT_NST;
         if (!fail && li >= UT_NST &&
-            !mbar_wait(&s_empty[s], (li / UT_NST - 1) & 1, s_abort, piters))
+            !mbar_wait_sleep(&s_empty[s], (li / UT_NST - 1) & 1, s_abort, piters))
           fail = true;
         if (__any_sync(0xffffffffu, fail)) {
           fail = true;
@@ -351,8 +356,8 @@ __global__ void __launch_bounds__(UT_THREADS, 1) k_m2l_unif_tc(const UnifTcArgs 
         const int k0 = (item / a.nblocks) * a.kchunk, k1 = min(a.nk, k0 + a.kchunk);
         for (int k = k0; k < k1 && !stop; ++k, ++fi) {
           const int fb = fi & 1;
-          if (!mbar_wait(&s_bfull[fb], (fi >> 1) & 1, s_abort, piters) ||
-              (fi >= 2 && !mbar_wait(&s_acce[fb], ((fi - 2) >> 1) & 1, s_abort, piters))) {
+          if (!mbar_wait_sleep(&s_bfull[fb], (fi >> 1) & 1, s_abort, piters) ||
+              (fi >= 2 && !mbar_wait_sleep(&s_acce[fb], ((fi - 2) >> 1) & 1, s_abort, piters))) {
             *s_abort = 1;
             stop = true;
             break;
@@ -362,7 +367,7 @@ __global__ void __launch_bounds__(UT_THREADS, 1) k_m2l_unif_tc(const UnifTcArgs 
           const uint32_t dset = tmem + (uint32_t)(fb * UT_BY * 32);
           for (int sl = 0; sl < UT_SRC_LINES; ++sl, ++li) {
             const int s = li % UT_NST;
-            if (!mbar_wait(&s_full[s], (li / UT_NST) & 1, s_abort, piters)) {
+            if (!mbar_wait_sleep(&s_full[s], (li / UT_NST) & 1, s_abort, piters)) {
               *s_abort = 1;
               stop = true;
               break;
@@ -420,7 +425,8 @@ __global__ void __launch_bounds__(UT_THREADS, 1) k_m2l_unif_tc(const UnifTcArgs 
         // releases the other drain threads (uniformly: the TMEM loads below
         // are warp-collective)
         bool bad = false;
-        if (tid == UT_DRAIN0 && !mbar_wait(&s_accf[fb], (fi >> 1) & 1, s_abort, piters)) bad = true;
+        if (tid == UT_DRAIN0 && !mbar_wait_sleep(&s_accf[fb], (fi >> 1) & 1, s_abort, piters))
+          bad = true;
         if (drains_any(bad)) {
           *s_abort = 1;
           stop = true;

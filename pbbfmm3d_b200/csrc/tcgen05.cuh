@@ -58,6 +58,37 @@ __device__ __forceinline__ bool mbar_try(uint32_t a, int parity) {
   return done != 0;
 }
 
+// try_wait that may suspend the thread (not issuing) for up to `ns`
+// nanoseconds while the phase is incomplete; it returns as soon as the phase
+// completes.
+__device__ __forceinline__ bool mbar_try_sleep(uint32_t a, int parity, uint32_t ns) {
+  uint32_t done;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n"
+      " selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(done)
+      : "r"(a), "r"(parity), "r"(ns)
+      : "memory");
+  return done != 0;
+}
+
+// mbar_wait with suspending polls (see mbar_try_sleep): for waiters that
+// share their SM sub-partition with warps doing work.
+__device__ __forceinline__ bool mbar_wait_sleep(uint64_t* bar, int parity,
+                                                const volatile int* abort,
+                                                long long iters = kWaitIters) {
+  const uint32_t a = smem_u32(bar);
+  if (mbar_try(a, parity)) return true;
+  const long long t0 = clock64();
+  // (a poll limit below 1024, a test's forced timeout, polls without suspending)
+  const uint32_t ns = iters >= 1024 ? 20000u : 0u;
+  for (long long it = 0; it < iters; ++it) {
+    if (ns ? mbar_try_sleep(a, parity, ns) : mbar_try(a, parity)) return true;
+    if ((it & 15) == 15 && ((abort && *abort) || clock64() - t0 > kWaitCycles)) return false;
+  }
+  return false;
+}
+
 // Wait for the completion of the phase with parity `parity`; false after
 // about a second of SM clock (or kWaitIters polls) without it, or once *abort
 // is set (abort may be null).  The first poll reads no clock: a wait that is

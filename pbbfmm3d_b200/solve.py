@@ -131,12 +131,14 @@ def gmres_ir(apply_fast: Callable[[torch.Tensor], torch.Tensor],
 
 
 def kernel_operator(tree: H2_3D_Tree, points: torch.Tensor, lam: float,
-                    precision: int = PREC_FP64, adjoint: bool = False):
-    """v (C, N) -> (K + lam I) v, or its transpose (the adjoint FMM)."""
+                    precision: int = PREC_FP64, adjoint: bool = False,
+                    max_cols: Optional[int] = None):
+    """v (C, N) -> (K + lam I) v, or its transpose (the adjoint FMM).  With
+    ``max_cols`` the columns go through the FMM in groups of at most that
+    many (the tree's spectra workspace grows with the columns of a call)."""
     pts = points.contiguous()
 
-    def apply(v):
-        v = v.contiguous()
+    def apply_block(v):
         C = v.shape[0]
         out = torch.zeros_like(v)
         if adjoint:
@@ -144,15 +146,24 @@ def kernel_operator(tree: H2_3D_Tree, points: torch.Tensor, lam: float,
                                    precision=precision)
         else:
             compute_device(tree, pts, pts, v, C, out, precision=precision)
+        return out
+
+    def apply(v):
+        v = v.contiguous()
+        C = v.shape[0]
+        step = C if not max_cols else max(1, int(max_cols))
+        out = torch.cat([apply_block(v[c:c + step].contiguous()) for c in range(0, C, step)])
         return out + lam * v
 
     return apply
 
 
-def _solve(tree, points, b, lam, tol, precision, restart, maxiter, adjoint=False):
+def _solve(tree, points, b, lam, tol, precision, restart, maxiter, adjoint=False,
+           exact_cols=None):
     """float64: GMRES; mixed: GMRES on the mixed operator inside float64
-    iterative refinement."""
-    exact = kernel_operator(tree, points, lam, PREC_FP64, adjoint)
+    iterative refinement (float64 matvecs in groups of ``exact_cols``
+    columns when given)."""
+    exact = kernel_operator(tree, points, lam, PREC_FP64, adjoint, exact_cols)
     if precision == PREC_FP64:
         return gmres(exact, b, tol, restart, maxiter)
     fast = kernel_operator(tree, points, lam, precision, adjoint)
@@ -165,19 +176,25 @@ class KernelSolve(torch.autograd.Function):
     refinement, so the float64 residual meets ``tol``."""
 
     @staticmethod
-    def forward(ctx, points, b, tree, lam, tol, precision, restart, maxiter):
-        x, info = _solve(tree, points, b.contiguous(), lam, tol, precision, restart, maxiter)
+    def forward(ctx, points, b, tree, lam, tol, precision, restart, maxiter, exact_cols=None,
+                info_out=None):
+        x, info = _solve(tree, points, b.contiguous(), lam, tol, precision, restart, maxiter,
+                         exact_cols=exact_cols)
         ctx.save_for_backward(points, x)
-        ctx.cfg = (tree, lam, tol, precision, restart, maxiter)
+        ctx.cfg = (tree, lam, tol, precision, restart, maxiter, exact_cols, info_out)
         ctx.info = info
+        if info_out is not None:
+            info_out["forward"] = info
         return x
 
     @staticmethod
     def backward(ctx, gx):
         points, x = ctx.saved_tensors
-        tree, lam, tol, precision, restart, maxiter = ctx.cfg
-        mu, _ = _solve(tree, points, gx.contiguous(), lam, tol, precision, restart, maxiter,
-                       adjoint=True)
+        tree, lam, tol, precision, restart, maxiter, exact_cols, info_out = ctx.cfg
+        mu, ainfo = _solve(tree, points, gx.contiguous(), lam, tol, precision, restart, maxiter,
+                           adjoint=True, exact_cols=exact_cols)
+        if info_out is not None:
+            info_out["adjoint"] = ainfo
         grad_points = None
         if ctx.needs_input_grad[0]:
             gt = torch.zeros_like(points)
@@ -187,12 +204,16 @@ class KernelSolve(torch.autograd.Function):
                                    mu.contiguous(), C, grad_source=gs, grad_target=gt,
                                    precision=precision)
             grad_points = -(gt + gs)
-        return grad_points, mu, None, None, None, None, None, None
+        return grad_points, mu, None, None, None, None, None, None, None, None
 
 
 def kernel_solve(tree: H2_3D_Tree, points: torch.Tensor, b: torch.Tensor, lam: float,
                  tol: float = 1e-6, precision: Optional[int] = None, restart: int = 50,
-                 maxiter: int = 2000) -> torch.Tensor:
-    """(K + lam I)^{-1} b for b (C, N); differentiable in b and points (N, 3)."""
+                 maxiter: int = 2000, exact_cols: Optional[int] = None,
+                 info: Optional[dict] = None) -> torch.Tensor:
+    """(K + lam I)^{-1} b for b (C, N); differentiable in b and points (N, 3).
+    ``exact_cols`` bounds the columns of one float64 matvec (memory);
+    ``info``, if given, receives the solver statistics of the forward solve
+    ("forward") and, after backward, of the adjoint solve ("adjoint")."""
     prec = tree.precision if precision is None else int(precision)
-    return KernelSolve.apply(points, b, tree, lam, tol, prec, restart, maxiter)
+    return KernelSolve.apply(points, b, tree, lam, tol, prec, restart, maxiter, exact_cols, info)
