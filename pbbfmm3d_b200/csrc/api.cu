@@ -620,14 +620,16 @@ static int compute_chunk(pbbfmm_tree* t, const double* d_tgt, int64_t Nf, const 
   if ((rc = kt_end(t, st))) return rc;
   if (t->timing) PB_CUDA(cudaEventRecord(t->ev[1], st));
   const int64_t perS = (int64_t)C * n3;
-  if ((rc = grow(ws.S, sizeof(double) * level_total(L, perS)))) return rc;
-  if ((rc = grow(ws.F, sizeof(double) * level_total(L, perS)))) return rc;
+  // coefficient arrays in the precision of the pass (float32 on the mixed path)
+  const size_t es = precision == PBBFMM_PREC_FP64 ? sizeof(double) : sizeof(float);
+  if ((rc = grow(ws.S, es * level_total(L, perS)))) return rc;
+  if ((rc = grow(ws.F, es * level_total(L, perS)))) return rc;
   if (t->p.use_chebyshev) {
-    if ((rc = grow(ws.proxy, sizeof(double) * level_total(L, (int64_t)C * t->ops.rs)))) return rc;
-    if ((rc = grow(ws.pf, sizeof(double) * level_total(L, (int64_t)C * t->ops.rf)))) return rc;
+    if ((rc = grow(ws.proxy, es * level_total(L, (int64_t)C * t->ops.rs)))) return rc;
+    if ((rc = grow(ws.pf, es * level_total(L, (int64_t)C * t->ops.rf)))) return rc;
   } else {
-    if ((rc = grow(ws.proxy, 2 * sizeof(double) * level_total(L, (int64_t)C * t->nk)))) return rc;
-    if ((rc = grow(ws.pf, 2 * sizeof(double) * level_total(L, (int64_t)C * t->nk)))) return rc;
+    if ((rc = grow(ws.proxy, 2 * es * level_total(L, (int64_t)C * t->nk)))) return rc;
+    if ((rc = grow(ws.pf, 2 * es * level_total(L, (int64_t)C * t->nk)))) return rc;
     // halo tables: at most 8^(L-2) parent blocks x (region + target) entries
     if ((rc = grow(ws.halo, sizeof(int) * 576 * cells_at(L - 2)))) return rc;
   }

@@ -47,11 +47,36 @@ __global__ void __launch_bounds__(32 * L2LCfg<N>::warps)
   T* b1 = b0 + n3;
   const T* src = Fpar + ((int64_t)par * C + col) * n3;
   for (int i = lane; i < n3; i += 32) sp[i] = src[i];
+  // which children hold targets (lanes 0..8 read the 9 leaf-range bounds at
+  // once), and (float32, orders up to 5: the registers of order 6 cost more
+  // resident warps than the batched loads save) every child's current
+  // coefficients, loaded with all loads in flight before the passes
+  int bound = 0;
+  if (lane <= 8) bound = tstart[(int64_t)(par * 8 + lane) * span_child];
+  unsigned present = 0;
+#pragma unroll
+  for (int ch = 0; ch < 8; ++ch)
+    present |= (__shfl_sync(0xffffffffu, bound, ch + 1) != __shfl_sync(0xffffffffu, bound, ch))
+                   ? 1u << ch : 0u;
+  constexpr int PER = (n3 + 31) / 32;
+  constexpr bool kBatch = sizeof(T) == 4 && N <= 5;
+  T cur[kBatch ? 8 : 1][kBatch ? PER : 1];
+  if constexpr (kBatch) {
+#pragma unroll
+    for (int ch = 0; ch < 8; ++ch) {
+      const T* d = Fch + ((int64_t)(par * 8 + ch) * C + col) * n3;
+#pragma unroll
+      for (int r = 0; r < PER; ++r) {
+        const int i = lane + 32 * r;
+        cur[ch][r] = ((present >> ch) & 1) && i < n3 ? d[i] : T(0);
+      }
+    }
+  }
   __syncwarp();
+#pragma unroll
   for (int ch = 0; ch < 8; ++ch) {
     const int cell = par * 8 + ch;
-    const int64_t a = (int64_t)cell * span_child, b = (int64_t)(cell + 1) * span_child;
-    if (tstart[b] == tstart[a]) continue;  // child without targets
+    if (!((present >> ch) & 1)) continue;  // child without targets
     const T* wx = sCw + (((ch >> 2) & 1) ? n2 : 0);
     const T* wy = sCw + (((ch >> 1) & 1) ? n2 : 0);
     const T* wz = sCw + ((ch & 1) ? n2 : 0);
@@ -75,12 +100,17 @@ __global__ void __launch_bounds__(32 * L2LCfg<N>::warps)
     __syncwarp();
     // z: Fchild[l1 n + l3] += sum_k Fy[l1 n + k] wz[l3 + k n]   (l1 over n^2)
     T* dst = Fch + ((int64_t)cell * C + col) * n3;
-    for (int i = lane; i < n3; i += 32) {
-      const int l1 = i / N, l3 = i % N;
-      T v = 0;
 #pragma unroll
-      for (int k = 0; k < N; ++k) v += b1[l1 * N + k] * wz[l3 + k * N];
-      dst[i] += v;
+    for (int r = 0; r < PER; ++r) {
+      const int i = lane + 32 * r;
+      if (i < n3) {
+        const int l1 = i / N, l3 = i % N;
+        T v = 0;
+#pragma unroll
+        for (int k = 0; k < N; ++k) v += b1[l1 * N + k] * wz[l3 + k * N];
+        if constexpr (kBatch) dst[i] = cur[ch][r] + v;
+        else dst[i] += v;
+      }
     }
     __syncwarp();
   }

@@ -82,10 +82,12 @@ int init_fft_twiddles() {
 // (ncells = 8^level), so that one frequency plane of a level is contiguous.
 
 // Forward: CTAs loop over the nonempty source cells (cells[0..ncl)), columns
-// in groups of CG.  With amax (float path, levels of the tensor-core MAC),
-// the largest |re| or |im| of the spectra per (k23, column mod 8), over the
-// level's cells and k1, as float bits: per CTA in shared memory, then one
-// atomicMax per slot into amax[k23][8] (zeroed by the caller).
+// in groups of CG.  With amax (float path, levels of the tensor-core MAC), a
+// bound on |re| and |im| of the spectra per (k23, column mod 8), over the
+// level's cells and k1, as float bits: the sum of |re| + |im| of the last
+// transform's n inputs (a bound on every one of its m outputs), per CTA in
+// shared memory, then one atomicMax per slot into amax[k23][8] (zeroed by
+// the caller).
 // w = e^{-2 pi i / m}; (a + ib) w^j = (a c + b s) + i (b c - a s).
 template <int n, typename T>
 __global__ void k_fft_fwd(const int* __restrict__ cells, int ncl, const T* __restrict__ S_l,
@@ -159,8 +161,14 @@ __global__ void k_fft_fwd(const int* __restrict__ cells, int ncl, const T* __res
 #pragma unroll
       for (int l = 0; l < n; ++l) v[l] = y[l * m * n];
       C2* out = X_l + ((int64_t)k23 * ncells + cell) * C + c0 + cc;
-      float amx = 0.f;
-      (void)amx;
+      if constexpr (sizeof(T) == 4) {
+        if (amax) {  // |X_k1| <= sum_l |v_l| <= sum_l (|re| + |im|) for every k1
+          float bnd = 0.f;
+#pragma unroll
+          for (int l = 0; l < n; ++l) bnd += fabsf(v[l].x) + fabsf(v[l].y);
+          atomicMax(&s_amax[k23 * 8 + ((c0 + cc) & 7)], __float_as_uint(bnd));
+        }
+      }
 #pragma unroll
       for (int k = 0; k < m; ++k) {
         T re = 0, im = 0;
@@ -171,10 +179,7 @@ __global__ void k_fft_fwd(const int* __restrict__ cells, int ncl, const T* __res
           im = fma(v[l].y, c, fma(-v[l].x, s, im));
         }
         out[(int64_t)k * m * n * ncells * C] = make_cplx<T>(re, im);
-        if constexpr (sizeof(T) == 4) amx = fmaxf(amx, fmaxf(fabsf(re), fabsf(im)));
       }
-      if constexpr (sizeof(T) == 4)
-        if (amax) atomicMax(&s_amax[k23 * 8 + ((c0 + cc) & 7)], __float_as_uint(amx));
     }
   }
   }

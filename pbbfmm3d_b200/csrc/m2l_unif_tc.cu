@@ -28,9 +28,10 @@
 // Scaling.  F16 holds 11 significant bits between 2^-14 and 2^16, so both
 // operands are scaled by powers of two before the split: the spectra of
 // column c at frequencies (k1, k23) by 2^sA(k23, c mod 8), with sA chosen from
-// the largest magnitude over the level's cells and k1 (recorded by the forward
-// FFT) so that it lies in [2^14, 2^15); the operator tiles of a frequency by
-// 2^sB(k) from their largest entry.  hi = fp16(x 2^s), lo = fp16(x 2^s - hi)
+// a bound on their magnitude over the level's cells and k1 (recorded by the
+// forward FFT, within a small factor of the largest) so that it lies in
+// [2^14, 2^15); the operator tiles of a frequency by 2^sB(k) from their
+// largest entry.  hi = fp16(x 2^s), lo = fp16(x 2^s - hi)
 // keep 22 significant bits for values down to 2^-17 of the scale's maximum
 // and an absolute error below 2^-39 of it for smaller ones.  A TMEM row holds
 // one column only (source and target rows share the column), so one factor
@@ -233,7 +234,7 @@ __global__ void __launch_bounds__(UT_THREADS, 1) k_m2l_unif_tc(const UnifTcArgs 
     struct Slot {
       float2 v[4];    // children 4 kc + e, column c0 + t_col
       uint32_t occ;   // their occupancy bytes (0 outside the domain)
-      uint32_t amax;  // the spectra maximum of (k23, t_col)
+      uint32_t amax;  // the spectra bound of (k23, t_col)
     };
     Slot ring[UT_RING];
     Pos lp{(int)blockIdx.x, 0, 0};  // the next line to load

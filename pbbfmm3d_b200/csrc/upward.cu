@@ -35,7 +35,7 @@ constexpr int kP2MCols = 8;    // columns per pass
 // warps per CTA: static shared memory (basis + weights) stays under 48 KB
 template <int N, typename T>
 constexpr int p2m_warps() {
-  return (3 * N * kP2MChunk + kP2MChunk * kP2MCols) * (int)sizeof(T) * 8 <= 40 * 1024 ? 8 : 4;
+  return (3 * N * (kP2MChunk + 1) + kP2MChunk * kP2MCols) * (int)sizeof(T) * 8 <= 40 * 1024 ? 8 : 4;
 }
 
 // One warp per nonempty source leaf.  Lanes first evaluate the basis of up to
@@ -53,7 +53,9 @@ __global__ void __launch_bounds__(32 * kP2MWarps)
   constexpr int n3 = N * N * N;
   constexpr bool kKahan = sizeof(T) == 4;
   __shared__ T sTkz[N * N];
-  __shared__ T sB[kP2MWarps][3][N][kP2MChunk];
+  // basis values [dim][m][point], rows padded to 33 so that lanes reading
+  // different m of one point hit different banks
+  __shared__ T sB[kP2MWarps][3][N][kP2MChunk + 1];
   __shared__ T sW[kP2MWarps][kP2MChunk][kP2MCols];
   for (int i = threadIdx.x; i < N * N; i += blockDim.x) sTkz[i] = Tkz_g[i];
   __syncthreads();
@@ -154,17 +156,43 @@ __global__ void __launch_bounds__(32 * M2MCfg<N, T>::warps)
   T* sch = smd + wl * G::per_warp;  // 8 x n3
   T* b0 = sch + 8 * n3;
   T* b1 = b0 + n3;
+  // which children hold sources: lanes 0..8 read the 9 leaf-range bounds at
+  // once; then (float32, orders up to 6) every child's moments are loaded
+  // with all loads in flight (an empty child's moments are never read)
+  int bound = 0;
+  if (lane <= 8) bound = sstart[(int64_t)(par * 8 + lane) * span_child];
   unsigned present = 0;
-  for (int ch = 0; ch < 8; ++ch) {
-    const int cell = par * 8 + ch;
-    const int64_t a = (int64_t)cell * span_child, b = (int64_t)(cell + 1) * span_child;
-    if (sstart[b] == sstart[a]) continue;  // empty child: no moments
-    present |= 1u << ch;
-    const T* src = Schild + ((int64_t)cell * C + col) * n3;
-    for (int i = lane; i < n3; i += 32) sch[ch * n3 + i] = src[i];
+#pragma unroll
+  for (int ch = 0; ch < 8; ++ch)
+    present |= (__shfl_sync(0xffffffffu, bound, ch + 1) != __shfl_sync(0xffffffffu, bound, ch))
+                   ? 1u << ch : 0u;
+  constexpr int PER = (n3 + 31) / 32;
+  if constexpr (N > 6 || sizeof(T) == 8) {
+    for (int ch = 0; ch < 8; ++ch) {
+      if (!((present >> ch) & 1)) continue;
+      const T* src = Schild + ((int64_t)(par * 8 + ch) * C + col) * n3;
+      for (int i = lane; i < n3; i += 32) sch[ch * n3 + i] = src[i];
+    }
+  } else {
+    T v[8][PER];
+#pragma unroll
+    for (int ch = 0; ch < 8; ++ch) {
+      const T* src = Schild + ((int64_t)(par * 8 + ch) * C + col) * n3;
+#pragma unroll
+      for (int r = 0; r < PER; ++r) {
+        const int i = lane + 32 * r;
+        v[ch][r] = ((present >> ch) & 1) && i < n3 ? src[i] : T(0);
+      }
+    }
+#pragma unroll
+    for (int ch = 0; ch < 8; ++ch)
+#pragma unroll
+      for (int r = 0; r < PER; ++r) {
+        const int i = lane + 32 * r;
+        if (i < n3) sch[ch * n3 + i] = v[ch][r];
+      }
   }
   __syncwarp();
-  constexpr int PER = (n3 + 31) / 32;
   T acc[PER];
 #pragma unroll
   for (int r = 0; r < PER; ++r) acc[r] = 0;
