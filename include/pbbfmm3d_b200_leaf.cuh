@@ -172,6 +172,9 @@ constexpr int kLaneLeafMin = 12;  // leaves with fewer targets take the warp-per
 // the gathers); the others keep 128
 template <typename T, int KC>
 constexpr int kLeafBlocks = sizeof(T) == 4 && KC == 1 ? 6 : 4;
+// the sparse-leaf kernel: float32 at 6 CTAs per SM for any column count
+template <typename T>
+constexpr int kSparseBlocks = sizeof(T) == 4 ? 6 : 4;
 
 // Source coordinates relative to the target leaf's centre.  float (mixed
 // path): hi = float(d), lo = float(d - hi), so that differences of nearby
@@ -408,7 +411,7 @@ __global__ void __launch_bounds__(32 * kLeafWarps, kLeafBlocks<T, KC>)
 // T = float (mixed path): kernel values and per-tile partial sums in float32,
 // running sums compensated (Kahan), output update in float64.
 template <class KF, typename T, int KC>
-__global__ void __launch_bounds__(32 * kLeafWarps, kLeafBlocks<T, KC>)
+__global__ void __launch_bounds__(32 * kLeafWarps, kSparseBlocks<T>)
     k_leaf_sparse(const int* __restrict__ leaves, int nleaves, const int* __restrict__ part_count,
                   const int* __restrict__ tstart, const int* __restrict__ sstart,
                   const int* __restrict__ tperm, const double* __restrict__ tpos,
@@ -419,9 +422,10 @@ __global__ void __launch_bounds__(32 * kLeafWarps, kLeafBlocks<T, KC>)
   constexpr bool kMixed = sizeof(T) == 4;
   constexpr int kMaxT = kLaneLeafMin - 1;             // targets of a sparse leaf
   constexpr int G = KC == 1 ? kMaxT : 32 / KC;        // targets per lane group
-  constexpr int NG = (kMaxT + G - 1) / G;             // groups per leaf
-  // up to TA targets: every (target, column) sum in each lane instead
-  constexpr int TA = KC == 1 ? kMaxT : 2;
+  // up to TA targets: every (target, column) sum in each lane instead (one
+  // column only: with several, the per-lane sums and reductions cost more
+  // than the idle lanes of a short group)
+  constexpr int TA = KC == 1 ? kMaxT : 0;
   static_assert(G * KC <= 32, "a lane group fits the warp");
   using V4 = vec4_t<T>;
   __shared__ T sTkz[kMaxOrder * kMaxOrder];
@@ -500,6 +504,7 @@ __global__ void __launch_bounds__(32 * kLeafWarps, kLeafBlocks<T, KC>)
   const int tl = lane / KC, cl = lane % KC;  // this lane's target-group member and column
   for (int c0 = 0; c0 < C; c0 += KC) {
     const int kce = min(KC, C - c0);  // columns of this pass
+    if constexpr (TA > 0) {
     if (nt <= TA) {
       // Few (target, column) pairs: lanes over sources (and over the
       // coefficients), every pair's sum in each lane, one warp reduction
@@ -562,96 +567,95 @@ __global__ void __launch_bounds__(32 * kLeafWarps, kLeafBlocks<T, KC>)
         }
       continue;
     }
-    // Many pairs: lane (t, c) owns target group members t and column c; the
-    // sources are staged 32 at a time and the kernel evaluated once per pair.
+    }
+    // Many pairs: the targets in groups of G; for each group, lane (t, c)
+    // owns group member t and column c, the sources are staged 32 at a time
+    // and the kernel is evaluated once per (target, source) pair.  Groups run
+    // one after the other (a loop, not unrolled: one accumulator, little
+    // code), so the warp keeps few registers and a small instruction
+    // footprint.
     const bool col_ok = tl < G && c0 + cl < C;
-    LeafAcc<T> acc[NG];
-    // far field: phi += sum_l F[l] Sx[l1] Sy[l2] Sz[l3], 32 coefficients at
-    // a time: lanes over coefficients load the KC columns (coalesced) and
-    // form every target's basis products, then lane (t, c) sums the chunk
-    for (int l0 = 0; l0 < n3; l0 += 32) {
-      const int l = l0 + lane, mm = min(32, n3 - l0);
-      __syncwarp();
-      if (l < n3) {
-        const int l1 = l / (n * n), l2 = (l / n) % n, l3 = l % n;
+#pragma unroll 1
+    for (int g0 = 0; g0 < nt; g0 += G) {
+      const int gn = min(G, nt - g0);  // targets of this group
+      const int t = g0 + tl;           // this lane's target
+      const bool mine = col_ok && tl < gn;
+      LeafAcc<T> acc;
+      // far field: phi += sum_l F[l] Sx[l1] Sy[l2] Sz[l3], 32 coefficients at
+      // a time: lanes over coefficients load the KC columns (coalesced) and
+      // form the group's basis products, then lane (t, c) sums the chunk
+      for (int l0 = 0; l0 < n3; l0 += 32) {
+        const int l = l0 + lane, mm = min(32, n3 - l0);
+        __syncwarp();
+        if (l < n3) {
+          const int l1 = l / (n * n), l2 = (l / n) % n, l3 = l % n;
 #pragma unroll
-        for (int cc = 0; cc < KC; ++cc)
-          s_F[wl][cc * 33 + lane] = cc < kce ? F_L[((int64_t)leaf * C + c0 + cc) * n3 + l] : T(0);
-        for (int t = 0; t < nt; ++t) {
-          const T* b = s_b[wl][t];
-          s_k[wl][t][lane] = b[l1] * b[n + l2] * b[2 * n + l3];
-        }
-      }
-      __syncwarp();
-#pragma unroll
-      for (int g = 0; g < NG; ++g) {
-        const int t = g * G + tl;
-        if (col_ok && t < nt) {
-          T part = 0;
-          for (int jj = 0; jj < mm; ++jj) part = fma(s_F[wl][cl * 33 + jj], s_k[wl][t][jj], part);
-          acc[g].add(part);
-        }
-      }
-    }
-    // near field: the neighbours' sources in tiles of 32
-    int q = 0;
-    for (int v0 = 0; v0 < nsrc_total; v0 += 32) {
-      const int v = v0 + lane, m = min(32, nsrc_total - v0);
-      __syncwarp();
-      if (v < nsrc_total) {
-        while (v >= s_pre[wl][q + 1]) ++q;
-        const int j = s_nb[wl][q][0] + (v - s_pre[wl][q]);
-        RelPos<T> sp;
-        sp.set(spos[j] - c[0], spos[(int64_t)Ns + j] - c[1], spos[2 * (int64_t)Ns + j] - c[2]);
-        V4 h;
-        h.x = sp.h[0], h.y = sp.h[1], h.z = sp.h[2], h.w = 0;
-        s_sh[wl][lane] = h;
-        if constexpr (kMixed) {
-          V4 lo;
-          lo.x = sp.l[0], lo.y = sp.l[1], lo.z = sp.l[2], lo.w = 0;
-          s_sl[wl][lane] = lo;
-        }
-        const double* wj = wsorted + (int64_t)j * C + c0;
-#pragma unroll
-        for (int cc = 0; cc < KC; ++cc) s_w[wl][lane][cc] = c0 + cc < C ? (T)wj[cc] : T(0);
-      }
-      __syncwarp();
-      // kernel values: lanes over the tile's sources, one target at a time
-      if (lane < m) {
-        const V4 sh = s_sh[wl][lane];
-        const V4 sl = s_sl[wl][kMixed ? lane : 0];
-        for (int t = 0; t < nt; ++t) {
-          RelPos<T> tp;
-          const V4 th = s_th[wl][t];
-          tp.h[0] = th.x, tp.h[1] = th.y, tp.h[2] = th.z;
-          if constexpr (kMixed) {
-            const V4 tlo = s_tl[wl][t];
-            tp.l[0] = tlo.x, tp.l[1] = tlo.y, tp.l[2] = tlo.z;
+          for (int cc = 0; cc < KC; ++cc)
+            s_F[wl][cc * 33 + lane] =
+                cc < kce ? F_L[((int64_t)leaf * C + c0 + cc) * n3 + l] : T(0);
+          for (int u = 0; u < gn; ++u) {
+            const T* bb = s_b[wl][g0 + u];
+            s_k[wl][u][lane] = bb[l1] * bb[n + l2] * bb[2 * n + l3];
           }
-          T d[3];
-          tp.diff(sh, sl, d);
-          T kv = KF::template eval<T>(d[0], d[1], d[2], kp);
-          if (isinf(kv)) kv = 0;  // coincident points (include/compute.hpp:767)
-          s_k[wl][t][lane] = kv;
         }
-      }
-      __syncwarp();
-      // sums over the tile: lane (t, c)
-#pragma unroll
-      for (int g = 0; g < NG; ++g) {
-        const int t = g * G + tl;
-        if (col_ok && t < nt) {
+        __syncwarp();
+        if (mine) {
           T part = 0;
-          for (int jj = 0; jj < m; ++jj) part = fma(s_k[wl][t][jj], s_w[wl][jj][cl], part);
-          acc[g].add(part);
+          for (int jj = 0; jj < mm; ++jj) part = fma(s_F[wl][cl * 33 + jj], s_k[wl][tl][jj], part);
+          acc.add(part);
         }
       }
-    }
+      // near field: the neighbours' sources in tiles of 32
+      int q = 0;
+      for (int v0 = 0; v0 < nsrc_total; v0 += 32) {
+        const int v = v0 + lane, m = min(32, nsrc_total - v0);
+        __syncwarp();
+        if (v < nsrc_total) {
+          while (v >= s_pre[wl][q + 1]) ++q;
+          const int j = s_nb[wl][q][0] + (v - s_pre[wl][q]);
+          RelPos<T> sp;
+          sp.set(spos[j] - c[0], spos[(int64_t)Ns + j] - c[1], spos[2 * (int64_t)Ns + j] - c[2]);
+          V4 h;
+          h.x = sp.h[0], h.y = sp.h[1], h.z = sp.h[2], h.w = 0;
+          s_sh[wl][lane] = h;
+          if constexpr (kMixed) {
+            V4 lo;
+            lo.x = sp.l[0], lo.y = sp.l[1], lo.z = sp.l[2], lo.w = 0;
+            s_sl[wl][lane] = lo;
+          }
+          const double* wj = wsorted + (int64_t)j * C + c0;
 #pragma unroll
-    for (int g = 0; g < NG; ++g) {
-      const int t = g * G + tl;
-      if (col_ok && t < nt)
-        out[(int64_t)(c0 + cl) * Nf + tperm[ta + t]] += (double)acc[g].value();
+          for (int cc = 0; cc < KC; ++cc) s_w[wl][lane][cc] = c0 + cc < C ? (T)wj[cc] : T(0);
+        }
+        __syncwarp();
+        // kernel values: lanes over the tile's sources, one target at a time
+        if (lane < m) {
+          const V4 sh = s_sh[wl][lane];
+          const V4 sl = s_sl[wl][kMixed ? lane : 0];
+          for (int u = 0; u < gn; ++u) {
+            RelPos<T> tp;
+            const V4 th = s_th[wl][g0 + u];
+            tp.h[0] = th.x, tp.h[1] = th.y, tp.h[2] = th.z;
+            if constexpr (kMixed) {
+              const V4 tlo = s_tl[wl][g0 + u];
+              tp.l[0] = tlo.x, tp.l[1] = tlo.y, tp.l[2] = tlo.z;
+            }
+            T d[3];
+            tp.diff(sh, sl, d);
+            T kv = KF::template eval<T>(d[0], d[1], d[2], kp);
+            if (isinf(kv)) kv = 0;  // coincident points (include/compute.hpp:767)
+            s_k[wl][u][lane] = kv;
+          }
+        }
+        __syncwarp();
+        // sums over the tile: lane (t, c)
+        if (mine) {
+          T part = 0;
+          for (int jj = 0; jj < m; ++jj) part = fma(s_k[wl][tl][jj], s_w[wl][jj][cl], part);
+          acc.add(part);
+        }
+      }
+      if (mine) out[(int64_t)(c0 + cl) * Nf + tperm[ta + t]] += (double)acc.value();
     }
   }
 }

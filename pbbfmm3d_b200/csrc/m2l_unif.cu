@@ -78,6 +78,76 @@ int init_fft_twiddles() {
   return PBBFMM_OK;
 }
 
+// Length-9 transforms (order 5) by one radix-3 step, with l = b + 3a:
+//   forward, 5 inputs:  X[k] = U0[k%3] + w^k U1[k%3] + w^2k v2,
+//     U0[j] = v0 + v3 w^3j, U1[j] = v1 + v4 w^3j;
+//   inverse, 9 inputs:  X[t] = sum_b w^-bt V_b[t%3], V_b[j] = sum_a v[b+3a] w^-3aj,
+// for w = e^{-2 pi i / 9}; about half the multiply-adds of the direct sums.
+// (a + ib) w^j = (a c + b s) + i (b c - a s), (a + ib) w^-j = (a c - b s) + i (b c + a s).
+template <int n, typename T>
+__device__ __forceinline__ cplx_t<T> mul_w(cplx_t<T> x, int j) {
+  using W = Tw<n, T>;
+  return make_cplx<T>(fma(x.x, W::c(j), x.y * W::s(j)), fma(x.y, W::c(j), -x.x * W::s(j)));
+}
+template <int n, typename T>
+__device__ __forceinline__ cplx_t<T> mul_wc(cplx_t<T> x, int j) {
+  using W = Tw<n, T>;
+  return make_cplx<T>(fma(x.x, W::c(j), -x.y * W::s(j)), fma(x.y, W::c(j), x.x * W::s(j)));
+}
+// forward 5 -> 9, out(k, X[k]) for k = 0..8
+template <int n, typename T, class Out>
+__device__ __forceinline__ void dft_5_to_9(const cplx_t<T>* v, Out out) {
+  static_assert(2 * n - 1 == 9, "length-9 transform");
+  using W = Tw<n, T>;
+  cplx_t<T> u0[3], u1[3];
+  u0[0] = make_cplx<T>(v[0].x + v[3].x, v[0].y + v[3].y);
+  u1[0] = make_cplx<T>(v[1].x + v[4].x, v[1].y + v[4].y);
+#pragma unroll
+  for (int j = 1; j < 3; ++j) {
+    const cplx_t<T> a = mul_w<n, T>(v[3], 3 * j), b = mul_w<n, T>(v[4], 3 * j);
+    u0[j] = make_cplx<T>(v[0].x + a.x, v[0].y + a.y);
+    u1[j] = make_cplx<T>(v[1].x + b.x, v[1].y + b.y);
+  }
+#pragma unroll
+  for (int k = 0; k < 9; ++k) {
+    const cplx_t<T> a = u0[k % 3], b = u1[k % 3], c = v[2];
+    const int j1 = k, j2 = (2 * k) % 9;
+    T re = fma(c.x, W::c(j2), fma(c.y, W::s(j2), a.x));
+    re = fma(b.x, W::c(j1), fma(b.y, W::s(j1), re));
+    T im = fma(c.y, W::c(j2), fma(-c.x, W::s(j2), a.y));
+    im = fma(b.y, W::c(j1), fma(-b.x, W::s(j1), im));
+    out(k, make_cplx<T>(re, im));
+  }
+}
+// inverse 9 -> 5 at t = (a + 5) mod 9, out(a, X[t]) for a = 0..4
+template <int n, typename T, class Out>
+__device__ __forceinline__ void idft_9_to_5(const cplx_t<T>* v, Out out) {
+  static_assert(2 * n - 1 == 9, "length-9 transform");
+  using W = Tw<n, T>;
+  cplx_t<T> vb[3][3];  // [b][j]
+#pragma unroll
+  for (int b = 0; b < 3; ++b) {
+    const cplx_t<T> x0 = v[b], x1 = v[b + 3], x2 = v[b + 6];
+    vb[b][0] = make_cplx<T>(x0.x + x1.x + x2.x, x0.y + x1.y + x2.y);
+#pragma unroll
+    for (int j = 1; j < 3; ++j) {
+      const cplx_t<T> p = mul_wc<n, T>(x1, 3 * j), q = mul_wc<n, T>(x2, (6 * j) % 9);
+      vb[b][j] = make_cplx<T>(x0.x + p.x + q.x, x0.y + p.y + q.y);
+    }
+  }
+#pragma unroll
+  for (int a = 0; a < 5; ++a) {
+    const int t = (a + 5) % 9, j = t % 3;
+    const cplx_t<T> y0 = vb[0][j], y1 = vb[1][j], y2 = vb[2][j];
+    const int j1 = t, j2 = (2 * t) % 9;
+    T re = fma(y2.x, W::c(j2), fma(-y2.y, W::s(j2), y0.x));
+    re = fma(y1.x, W::c(j1), fma(-y1.y, W::s(j1), re));
+    T im = fma(y2.y, W::c(j2), fma(y2.x, W::s(j2), y0.y));
+    im = fma(y1.y, W::c(j1), fma(y1.x, W::s(j1), im));
+    out(a, make_cplx<T>(re, im));
+  }
+}
+
 // Spectra of a level are stored frequency-major: X[(k * ncells + cell) * C + col]
 // (ncells = 8^level), so that one frequency plane of a level is contiguous.
 
@@ -140,16 +210,20 @@ __global__ void k_fft_fwd(const int* __restrict__ cells, int ncl, const T* __res
 #pragma unroll
       for (int l = 0; l < n; ++l) v[l] = z[l * n];
       C2* y = Y + cc * ny + l1 * m * n + k3;
+      if constexpr (m == 9) {
+        dft_5_to_9<n, T>(v, [&](int k, C2 r) { y[k * n] = r; });
+      } else {
 #pragma unroll
-      for (int k = 0; k < m; ++k) {
-        T re = 0, im = 0;
+        for (int k = 0; k < m; ++k) {
+          T re = 0, im = 0;
 #pragma unroll
-        for (int l = 0; l < n; ++l) {
-          const T c = W::c((k * l) % m), s = W::s((k * l) % m);
-          re = fma(v[l].x, c, fma(v[l].y, s, re));
-          im = fma(v[l].y, c, fma(-v[l].x, s, im));
+          for (int l = 0; l < n; ++l) {
+            const T c = W::c((k * l) % m), s = W::s((k * l) % m);
+            re = fma(v[l].x, c, fma(v[l].y, s, re));
+            im = fma(v[l].y, c, fma(-v[l].x, s, im));
+          }
+          y[k * n] = make_cplx<T>(re, im);
         }
-        y[k * n] = make_cplx<T>(re, im);
       }
     }
     __syncthreads();
@@ -169,16 +243,21 @@ __global__ void k_fft_fwd(const int* __restrict__ cells, int ncl, const T* __res
           atomicMax(&s_amax[k23 * 8 + ((c0 + cc) & 7)], __float_as_uint(bnd));
         }
       }
+      const int64_t kstride = (int64_t)m * n * ncells * C;
+      if constexpr (m == 9) {
+        dft_5_to_9<n, T>(v, [&](int k, C2 r) { out[k * kstride] = r; });
+      } else {
 #pragma unroll
-      for (int k = 0; k < m; ++k) {
-        T re = 0, im = 0;
+        for (int k = 0; k < m; ++k) {
+          T re = 0, im = 0;
 #pragma unroll
-        for (int l = 0; l < n; ++l) {
-          const T c = W::c((k * l) % m), s = W::s((k * l) % m);
-          re = fma(v[l].x, c, fma(v[l].y, s, re));
-          im = fma(v[l].y, c, fma(-v[l].x, s, im));
+          for (int l = 0; l < n; ++l) {
+            const T c = W::c((k * l) % m), s = W::s((k * l) % m);
+            re = fma(v[l].x, c, fma(v[l].y, s, re));
+            im = fma(v[l].y, c, fma(-v[l].x, s, im));
+          }
+          out[k * kstride] = make_cplx<T>(re, im);
         }
-        out[(int64_t)k * m * n * ncells * C] = make_cplx<T>(re, im);
       }
     }
   }
@@ -225,17 +304,21 @@ __global__ void k_fft_inv(const int* __restrict__ cells, const cplx_t<T>* __rest
 #pragma unroll
       for (int k = 0; k < m; ++k) v[k] = y[k * m * n];
       C2* g = G + cc * ng + k23;
+      if constexpr (m == 9) {
+        idft_9_to_5<n, T>(v, [&](int a, C2 r) { g[a * m * n] = r; });
+      } else {
 #pragma unroll
-      for (int a = 0; a < n; ++a) {
-        const int t = (a + n) % m;
-        T re = 0, im = 0;
+        for (int a = 0; a < n; ++a) {
+          const int t = (a + n) % m;
+          T re = 0, im = 0;
 #pragma unroll
-        for (int k = 0; k < m; ++k) {
-          const T c = W::c((k * t) % m), s = W::s((k * t) % m);
-          re = fma(v[k].x, c, fma(-v[k].y, s, re));
-          im = fma(v[k].y, c, fma(v[k].x, s, im));
+          for (int k = 0; k < m; ++k) {
+            const T c = W::c((k * t) % m), s = W::s((k * t) % m);
+            re = fma(v[k].x, c, fma(-v[k].y, s, re));
+            im = fma(v[k].y, c, fma(v[k].x, s, im));
+          }
+          g[a * m * n] = make_cplx<T>(re, im);
         }
-        g[a * m * n] = make_cplx<T>(re, im);
       }
     }
     __syncthreads();
@@ -247,17 +330,21 @@ __global__ void k_fft_inv(const int* __restrict__ cells, const cplx_t<T>* __rest
 #pragma unroll
       for (int k = 0; k < m; ++k) v[k] = g[k * n];
       C2* h = H + cc * n3 + a1 * n2 + k3;
+      if constexpr (m == 9) {
+        idft_9_to_5<n, T>(v, [&](int a, C2 r) { h[a * n] = r; });
+      } else {
 #pragma unroll
-      for (int a = 0; a < n; ++a) {
-        const int t = (a + n) % m;
-        T re = 0, im = 0;
+        for (int a = 0; a < n; ++a) {
+          const int t = (a + n) % m;
+          T re = 0, im = 0;
 #pragma unroll
-        for (int k = 0; k < m; ++k) {
-          const T c = W::c((k * t) % m), s = W::s((k * t) % m);
-          re = fma(v[k].x, c, fma(-v[k].y, s, re));
-          im = fma(v[k].y, c, fma(v[k].x, s, im));
+          for (int k = 0; k < m; ++k) {
+            const T c = W::c((k * t) % m), s = W::s((k * t) % m);
+            re = fma(v[k].x, c, fma(-v[k].y, s, re));
+            im = fma(v[k].y, c, fma(v[k].x, s, im));
+          }
+          h[a * n] = make_cplx<T>(re, im);
         }
-        h[a * n] = make_cplx<T>(re, im);
       }
     }
     __syncthreads();
