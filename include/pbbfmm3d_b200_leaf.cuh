@@ -167,14 +167,27 @@ __device__ __forceinline__ void cell_center_d(uint32_t m, int l, double box, dou
 constexpr int kLeafWarps = 4;
 constexpr int kLeafCols = 8;  // columns per pass (registers)
 constexpr int kLaneLeafMin = 12;  // leaves with fewer targets take the warp-per-target path
-// resident CTAs per SM the leaf kernels are compiled for: the float32
-// one-column kernels fit 64 registers (32 warps per SM, latency hiding for
+// resident CTAs per SM the dense-leaf kernel is compiled for: the float32
+// one-column kernel fits 64 registers (32 warps per SM, latency hiding for
 // the gathers); the others keep 128
 template <typename T, int KC>
-constexpr int kLeafBlocks = sizeof(T) == 4 && KC == 1 ? 6 : 4;
+constexpr int kLeafBlocks = sizeof(T) == 4 && KC == 1 ? 8 : 4;
 // the sparse-leaf kernel: float32 at 6 CTAs per SM for any column count
 template <typename T>
 constexpr int kSparseBlocks = sizeof(T) == 4 ? 6 : 4;
+
+// pre[q] = the number of sources in neighbour slots < q (q = 0..27), from
+// lane q's count (lanes 27..31 hold 0): a warp scan.
+__device__ __forceinline__ void neighbour_prefix(int cnt, int lane, int* pre) {
+  int incl = cnt;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const int y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane < 27) pre[lane] = incl - cnt;
+  if (lane == 26) pre[27] = incl;
+}
 
 // Source coordinates relative to the target leaf's centre.  float (mixed
 // path): hi = float(d), lo = float(d - hi), so that differences of nearby
@@ -274,6 +287,7 @@ __global__ void __launch_bounds__(32 * kLeafWarps, kLeafBlocks<T, KC>)
   morton_decode((uint32_t)leaf, &ax, &ay, &az);
   const int nside = 1 << L;
   // neighbour source ranges, slot 9(x+1)+3(y+1)+(z+1)
+  int nb_cnt = 0;
   if (lane < 27) {
     const int q = lane;
     const int bx = ax + q / 9 - 1, by = ay + (q / 3) % 3 - 1, bz = az + q % 3 - 1;
@@ -285,16 +299,10 @@ __global__ void __launch_bounds__(32 * kLeafWarps, kLeafBlocks<T, KC>)
     }
     s_nb[wl][q][0] = a;
     s_nb[wl][q][1] = e;
+    nb_cnt = e - a;
   }
   __syncwarp();
-  if (lane == 0) {
-    int acc = 0;
-    for (int q = 0; q < 27; ++q) {
-      s_pre[wl][q] = acc;
-      acc += s_nb[wl][q][1] - s_nb[wl][q][0];
-    }
-    s_pre[wl][27] = acc;
-  }
+  neighbour_prefix(nb_cnt, lane, s_pre[wl]);
   __syncwarp();
   const int nsrc_total = s_pre[wl][27];
   for (int c0 = 0; c0 < C; c0 += KC) {
@@ -459,6 +467,7 @@ __global__ void __launch_bounds__(32 * kLeafWarps, kSparseBlocks<T>)
   int ax, ay, az;
   morton_decode((uint32_t)leaf, &ax, &ay, &az);
   const int nside = 1 << L;
+  int nb_cnt = 0;
   if (lane < 27) {
     const int q = lane;
     const int bx = ax + q / 9 - 1, by = ay + (q / 3) % 3 - 1, bz = az + q % 3 - 1;
@@ -470,6 +479,7 @@ __global__ void __launch_bounds__(32 * kLeafWarps, kSparseBlocks<T>)
     }
     s_nb[wl][q][0] = a;
     s_nb[wl][q][1] = e;
+    nb_cnt = e - a;
   }
   // the targets, relative to the leaf centre, and their basis values
   if (lane < nt) {
@@ -491,14 +501,7 @@ __global__ void __launch_bounds__(32 * kLeafWarps, kSparseBlocks<T>)
     s_b[wl][t][d * n + m] = basis_one<T>(n, cheb, (T)(ihalfL * (xd - c[d])), sTkz, m);
   }
   __syncwarp();
-  if (lane == 0) {
-    int acc = 0;
-    for (int q = 0; q < 27; ++q) {
-      s_pre[wl][q] = acc;
-      acc += s_nb[wl][q][1] - s_nb[wl][q][0];
-    }
-    s_pre[wl][27] = acc;
-  }
+  neighbour_prefix(nb_cnt, lane, s_pre[wl]);
   __syncwarp();
   const int nsrc_total = s_pre[wl][27];
   const int tl = lane / KC, cl = lane % KC;  // this lane's target-group member and column
@@ -510,17 +513,31 @@ __global__ void __launch_bounds__(32 * kLeafWarps, kSparseBlocks<T>)
       // coefficients), every pair's sum in each lane, one warp reduction
       // per pair at the end.
       LeafAcc<T> acc[TA][KC];
-      for (int l = lane; l < n3; l += 32) {
-        const int l1 = l / (n * n), l2 = (l / n) % n, l3 = l % n;
+      // the coefficients four per lane at a time, their loads issued together
+      for (int l0 = lane; l0 < n3; l0 += 128) {
+        T fv[4][KC];
 #pragma unroll
-        for (int t = 0; t < TA; ++t)
-          if (t < nt) {
-            const T* b = s_b[wl][t];
-            const T v = b[l1] * b[n + l2] * b[2 * n + l3];
+        for (int r = 0; r < 4; ++r) {
+          const int l = l0 + 32 * r;
 #pragma unroll
-            for (int cc = 0; cc < KC; ++cc)
-              if (cc < kce) acc[t][cc].add(F_L[((int64_t)leaf * C + c0 + cc) * n3 + l] * v);
-          }
+          for (int cc = 0; cc < KC; ++cc)
+            fv[r][cc] = (l < n3 && cc < kce) ? F_L[((int64_t)leaf * C + c0 + cc) * n3 + l] : T(0);
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const int l = l0 + 32 * r;
+          if (l >= n3) break;
+          const int l1 = l / (n * n), l2 = (l / n) % n, l3 = l % n;
+#pragma unroll
+          for (int t = 0; t < TA; ++t)
+            if (t < nt) {
+              const T* b = s_b[wl][t];
+              const T v = b[l1] * b[n + l2] * b[2 * n + l3];
+#pragma unroll
+              for (int cc = 0; cc < KC; ++cc)
+                if (cc < kce) acc[t][cc].add(fv[r][cc] * v);
+            }
+        }
       }
       int q = 0;
       for (int v = lane; v < nsrc_total; v += 32) {
@@ -700,6 +717,7 @@ __global__ void __launch_bounds__(32 * kLeafWarps)
   int ax, ay, az;
   morton_decode((uint32_t)leaf, &ax, &ay, &az);
   const int nside = 1 << L;
+  int nb_cnt = 0;
   if (lane < 27) {
     const int q = lane;
     const int bx = ax + q / 9 - 1, by = ay + (q / 3) % 3 - 1, bz = az + q % 3 - 1;
@@ -711,16 +729,10 @@ __global__ void __launch_bounds__(32 * kLeafWarps)
     }
     s_nb[wl][q][0] = a;
     s_nb[wl][q][1] = e;
+    nb_cnt = e - a;
   }
   __syncwarp();
-  if (lane == 0) {
-    int acc = 0;
-    for (int q = 0; q < 27; ++q) {
-      s_pre[wl][q] = acc;
-      acc += s_nb[wl][q][1] - s_nb[wl][q][0];
-    }
-    s_pre[wl][27] = acc;
-  }
+  neighbour_prefix(nb_cnt, lane, s_pre[wl]);
   __syncwarp();
   const int nsrc_total = s_pre[wl][27];
   const T* Sb = s_b[wl];

@@ -4,6 +4,7 @@
 #include "precompute.h"
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -177,75 +178,198 @@ Weights compute_weights(int n, int cheb) {
 // --------------------------------------------------------------------- SVD
 
 // Householder QR of a tall column-major m x n matrix (in place); returns the
-// n x n upper-triangular R (column-major).
+// n x n upper-triangular R (column-major).  Blocked: a panel of kQrPanel
+// columns is factored column by column, then applied to the trailing
+// columns at once in compact WY form, A2 -= V T^T V^T A2, with both products
+// parallel over row blocks (the matrix is streamed twice per panel instead
+// of once per column).
+constexpr int kQrPanel = 32;
 static std::vector<double> householder_r(std::vector<double>& A, int64_t m, int n) {
   std::vector<double> R((size_t)n * n, 0.0);
-  std::vector<double> v;
-  for (int j = 0; j < n; ++j) {
-    double* a = &A[(size_t)j * m];
-    double nrm = 0;
-    for (int64_t i = j; i < m; ++i) nrm += a[i] * a[i];
-    nrm = sqrt(nrm);
-    double alpha = a[j] > 0 ? -nrm : nrm;
-    v.assign(a + j, a + m);
-    v[0] -= alpha;
-    double vv = 0;
-    for (double x : v) vv += x * x;
-    R[(size_t)j * n + j] = alpha;
-    if (vv == 0) continue;
-    const double inv = 2.0 / vv;
-    parallel_for(n - j - 1, [&](int64_t c0, int64_t c1) {
-      for (int64_t c = c0; c < c1; ++c) {
-        double* b = &A[(size_t)(j + 1 + c) * m];
-        double d = 0;
-        for (int64_t i = j; i < m; ++i) d += v[i - j] * b[i];
-        d *= inv;
-        for (int64_t i = j; i < m; ++i) b[i] -= d * v[i - j];
+  std::vector<double> tau(n, 0.0);
+  constexpr int64_t kRows = 2048;  // row block of the parallel products
+  const int64_t nrb = (m + kRows - 1) / kRows;
+  for (int j0 = 0; j0 < n; j0 += kQrPanel) {
+    const int b = std::min(kQrPanel, n - j0);
+    // panel: reflector j stored in column j, rows j..m-1 (v_j[j] kept in a[j])
+    for (int j = j0; j < j0 + b; ++j) {
+      double* a = &A[(size_t)j * m];
+      double nrm2 = 0;
+      for (int64_t i = j; i < m; ++i) nrm2 += a[i] * a[i];
+      const double nrm = sqrt(nrm2);
+      const double alpha = a[j] > 0 ? -nrm : nrm;
+      const double v0 = a[j] - alpha;
+      const double vv = nrm2 - a[j] * a[j] + v0 * v0;
+      R[(size_t)j * n + j] = alpha;
+      a[j] = v0;
+      tau[j] = vv == 0 ? 0.0 : 2.0 / vv;
+      if (tau[j] == 0.0) continue;
+      const int nc = j0 + b - j - 1;  // remaining panel columns
+      parallel_for(nc, [&](int64_t c0, int64_t c1) {
+        for (int64_t c = c0; c < c1; ++c) {
+          double* bc = &A[(size_t)(j + 1 + c) * m];
+          double d = 0;
+          for (int64_t i = j; i < m; ++i) d += a[i] * bc[i];
+          d *= tau[j];
+          for (int64_t i = j; i < m; ++i) bc[i] -= d * a[i];
+        }
+      });
+    }
+    for (int j = j0; j < j0 + b; ++j)
+      for (int c = j + 1; c < j0 + b; ++c) R[(size_t)c * n + j] = A[(size_t)c * m + j];
+    const int nt = n - j0 - b;  // trailing columns
+    if (nt > 0) {
+      // T (b x b, upper triangular): H_j0 ... H_j0+b-1 = I - V T V^T
+      std::vector<double> T((size_t)b * b, 0.0), vtv((size_t)b * b, 0.0);
+      parallel_for(b, [&](int64_t k0, int64_t k1) {
+        for (int64_t k = k0; k < k1; ++k)
+          for (int l = 0; l < k; ++l) {
+            // v_l^T v_k over rows >= j0 + k (v_k is zero above its diagonal)
+            const double* vl = &A[(size_t)(j0 + l) * m];
+            const double* vk = &A[(size_t)(j0 + k) * m];
+            double d = 0;
+            for (int64_t i = j0 + k; i < m; ++i) d += vl[i] * vk[i];
+            vtv[(size_t)l * b + k] = d;
+          }
+      });
+      for (int k = 0; k < b; ++k) {
+        T[(size_t)k * b + k] = tau[j0 + k];
+        for (int r = 0; r < k; ++r) {
+          double acc = 0;
+          for (int l = r; l < k; ++l) acc += T[(size_t)l * b + r] * vtv[(size_t)l * b + k];
+          T[(size_t)k * b + r] = -tau[j0 + k] * acc;
+        }
       }
-    });
-    for (int c = j + 1; c < n; ++c) R[(size_t)c * n + j] = A[(size_t)c * m + j];
+      // W = V^T A2 (b x nt): partial sums per row block, then summed in order
+      std::vector<double> Wp((size_t)nrb * b * nt, 0.0);
+      parallel_for(nrb, [&](int64_t r0, int64_t r1) {
+        for (int64_t rb = r0; rb < r1; ++rb) {
+          const int64_t i0 = std::max<int64_t>(rb * kRows, j0), i1 = std::min(m, (rb + 1) * kRows);
+          double* W = &Wp[(size_t)rb * b * nt];
+          for (int c = 0; c < nt; ++c) {
+            const double* ac = &A[(size_t)(j0 + b + c) * m];
+            for (int k = 0; k < b; ++k) {
+              const double* vk = &A[(size_t)(j0 + k) * m];
+              const int64_t lo = std::max<int64_t>(i0, j0 + k);
+              double d = 0;
+              for (int64_t i = lo; i < i1; ++i) d += vk[i] * ac[i];
+              W[(size_t)c * b + k] = d;
+            }
+          }
+        }
+      });
+      std::vector<double> W((size_t)b * nt, 0.0), W2((size_t)b * nt, 0.0);
+      for (int64_t rb = 0; rb < nrb; ++rb)
+        for (size_t e = 0; e < W.size(); ++e) W[e] += Wp[(size_t)rb * b * nt + e];
+      // W2 = T^T W
+      for (int c = 0; c < nt; ++c)
+        for (int k = 0; k < b; ++k) {
+          double acc = 0;
+          for (int r = 0; r <= k; ++r) acc += T[(size_t)k * b + r] * W[(size_t)c * b + r];
+          W2[(size_t)c * b + k] = acc;
+        }
+      // A2 -= V W2, parallel over row blocks
+      parallel_for(nrb, [&](int64_t r0, int64_t r1) {
+        for (int64_t rb = r0; rb < r1; ++rb) {
+          const int64_t i0 = std::max<int64_t>(rb * kRows, j0), i1 = std::min(m, (rb + 1) * kRows);
+          for (int c = 0; c < nt; ++c) {
+            double* ac = &A[(size_t)(j0 + b + c) * m];
+            for (int k = 0; k < b; ++k) {
+              const double* vk = &A[(size_t)(j0 + k) * m];
+              const double w = W2[(size_t)c * b + k];
+              const int64_t lo = std::max<int64_t>(i0, j0 + k);
+              for (int64_t i = lo; i < i1; ++i) ac[i] -= vk[i] * w;
+            }
+          }
+        }
+      });
+    }
+    // the trailing columns' rows j0..j0+b-1 are final: the panel's part of R
+    for (int j = j0; j < j0 + b; ++j)
+      for (int c = j0 + b; c < n; ++c) R[(size_t)c * n + j] = A[(size_t)c * m + j];
   }
   return R;
 }
 
 // One-sided (Hestenes) Jacobi on a square column-major n x n matrix B:
 // B W = U Sigma.  Returns sigma (descending) and W (columns permuted to match).
+// Each sweep runs the n(n-1)/2 column pairs as rounds of disjoint pairs (a
+// round-robin tournament over n rounded up to even; the extra player sits
+// out), the pairs of a round spread over a fixed set of threads that meet at
+// a barrier after every round; the order of the rounds and the rotations are
+// the same on every run.
 static void jacobi_svd(std::vector<double> B, int n, std::vector<double>* sigma,
                        std::vector<double>* W) {
   std::vector<double> V((size_t)n * n, 0.0);
   for (int i = 0; i < n; ++i) V[(size_t)i * n + i] = 1.0;
-  for (int sweep = 0; sweep < 80; ++sweep) {
-    bool rotated = false;
-    for (int p = 0; p < n - 1; ++p)
-      for (int q = p + 1; q < n; ++q) {
-        double* bp = &B[(size_t)p * n];
-        double* bq = &B[(size_t)q * n];
-        double a = 0, b = 0, g = 0;
-        for (int i = 0; i < n; ++i) {
-          a += bp[i] * bp[i];
-          b += bq[i] * bq[i];
-          g += bp[i] * bq[i];
+  const int np = n + (n & 1);
+  unsigned hw = std::thread::hardware_concurrency();
+  const int nth = std::max(1, std::min<int>(hw ? (int)hw : 1, std::min(32, np / 2)));
+  // sense-reversing spin barrier
+  std::atomic<int> count(0), sense(0);
+  auto barrier = [&](int& local) {
+    local ^= 1;
+    if (count.fetch_add(1) + 1 == nth) {
+      count.store(0);
+      sense.store(local);
+    } else {
+      while (sense.load() != local) std::this_thread::yield();
+    }
+  };
+  std::atomic<int> rot_flag[2];
+  rot_flag[0].store(0);
+  rot_flag[1].store(0);
+  auto work = [&](int tid) {
+    int local = 0;
+    std::vector<int> ring(np);
+    for (int i = 0; i < np; ++i) ring[i] = i;
+    for (int sweep = 0; sweep < 80; ++sweep) {
+      std::atomic<int>& rot = rot_flag[sweep & 1];
+      for (int round = 0; round < np - 1; ++round) {
+        for (int i = tid; i < np / 2; i += nth) {
+          int p = ring[i], q = ring[np - 1 - i];
+          if (p > q) std::swap(p, q);
+          if (q >= n) continue;
+          double* bp = &B[(size_t)p * n];
+          double* bq = &B[(size_t)q * n];
+          double a = 0, b = 0, g = 0;
+          for (int k = 0; k < n; ++k) {
+            a += bp[k] * bp[k];
+            b += bq[k] * bq[k];
+            g += bp[k] * bq[k];
+          }
+          if (fabs(g) <= 1e-15 * sqrt(a * b) || g == 0) continue;
+          rot.store(1, std::memory_order_relaxed);
+          const double zeta = (b - a) / (2 * g);
+          const double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1 + zeta * zeta));
+          const double c = 1 / sqrt(1 + t * t), s = c * t;
+          for (int k = 0; k < n; ++k) {
+            const double x = bp[k], y = bq[k];
+            bp[k] = c * x - s * y;
+            bq[k] = s * x + c * y;
+          }
+          double* vp = &V[(size_t)p * n];
+          double* vq = &V[(size_t)q * n];
+          for (int k = 0; k < n; ++k) {
+            const double x = vp[k], y = vq[k];
+            vp[k] = c * x - s * y;
+            vq[k] = s * x + c * y;
+          }
         }
-        if (fabs(g) <= 1e-15 * sqrt(a * b) || g == 0) continue;
-        rotated = true;
-        double zeta = (b - a) / (2 * g);
-        double t = (zeta >= 0 ? 1.0 : -1.0) / (fabs(zeta) + sqrt(1 + zeta * zeta));
-        double c = 1 / sqrt(1 + t * t), s = c * t;
-        for (int i = 0; i < n; ++i) {
-          double x = bp[i], y = bq[i];
-          bp[i] = c * x - s * y;
-          bq[i] = s * x + c * y;
-        }
-        double* vp = &V[(size_t)p * n];
-        double* vq = &V[(size_t)q * n];
-        for (int i = 0; i < n; ++i) {
-          double x = vp[i], y = vq[i];
-          vp[i] = c * x - s * y;
-          vq[i] = s * x + c * y;
-        }
+        std::rotate(ring.begin() + 1, ring.end() - 1, ring.end());  // player 0 stays
+        barrier(local);
       }
-    if (!rotated) break;
-  }
+      const bool more = rot.load() != 0;
+      barrier(local);  // every thread has read this sweep's flag
+      if (tid == 0) rot_flag[(sweep + 1) & 1].store(0);
+      barrier(local);
+      if (!more) break;
+    }
+  };
+  std::vector<std::thread> th;
+  for (int t = 1; t < nth; ++t) th.emplace_back(work, t);
+  work(0);
+  for (auto& x : th) x.join();
   std::vector<double> sv(n);
   for (int j = 0; j < n; ++j) {
     double s = 0;
@@ -381,12 +505,16 @@ static void cheb_level(const KernelSpec& k, int n, double eps, double boxLen,
     std::vector<double> KV((size_t)n3 * s);
     for (int64_t c = c0; c < c1; ++c) {
       const double* blk = &K0[(size_t)c * n6];
-      for (int b = 0; b < s; ++b)
-        for (int i = 0; i < n3; ++i) {
-          double acc = 0;
-          for (int j = 0; j < n3; ++j) acc += blk[i + (size_t)n3 * j] * Vfull[(size_t)b * n3 + j];
-          KV[i + (size_t)n3 * b] = acc;
+      // KV = K_c V, column by column as axpys over the contiguous columns of K_c
+      for (int b = 0; b < s; ++b) {
+        double* kv = &KV[(size_t)n3 * b];
+        for (int i = 0; i < n3; ++i) kv[i] = 0;
+        for (int j = 0; j < n3; ++j) {
+          const double v = Vfull[(size_t)b * n3 + j];
+          const double* col = blk + (size_t)n3 * j;
+          for (int i = 0; i < n3; ++i) kv[i] += col[i] * v;
         }
+      }
       double* E = Eout + (size_t)c * f * s;
       for (int b = 0; b < s; ++b)
         for (int a = 0; a < f; ++a) {
