@@ -176,6 +176,40 @@ constexpr int kLeafBlocks = sizeof(T) == 4 && KC == 1 ? 8 : 4;
 template <typename T>
 constexpr int kSparseBlocks = sizeof(T) == 4 ? 6 : 4;
 
+// Packed float32 pairs (two lanes of arithmetic per instruction, sm_100):
+// a pair is a 64-bit register holding (first, second).
+__device__ __forceinline__ unsigned long long f2_pack(float a, float b) {
+  unsigned long long r;
+  asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(a), "f"(b));
+  return r;
+}
+__device__ __forceinline__ void f2_unpack(unsigned long long v, float& a, float& b) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(v));
+}
+__device__ __forceinline__ unsigned long long f2_add(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ unsigned long long f2_mul(unsigned long long a, unsigned long long b) {
+  unsigned long long r;
+  asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+  return r;
+}
+__device__ __forceinline__ unsigned long long f2_fma(unsigned long long a, unsigned long long b,
+                                                     unsigned long long c) {
+  unsigned long long r;
+  asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r) : "l"(a), "l"(b), "l"(c));
+  return r;
+}
+
+// Kernels that are functions of r^2 may provide eval_r2(r2, params); the
+// packed pair loop then forms r^2 with packed arithmetic as well.
+template <class KF, class = void>
+struct HasEvalR2 : std::false_type {};
+template <class KF>
+struct HasEvalR2<KF, decltype((void)KF::template eval_r2<float>(0.f, nullptr))> : std::true_type {};
+
 // pre[q] = the number of sources in neighbour slots < q (q = 0..27), from
 // lane q's count (lanes 27..31 hold 0): a warp scan.
 __device__ __forceinline__ void neighbour_prefix(int cnt, int lane, int* pre) {
@@ -354,6 +388,74 @@ __global__ void __launch_bounds__(32 * kLeafWarps, kLeafBlocks<T, KC>)
       }
       // near field: the 27 neighbours' source ranges, concatenated, in tiles of 32
       int q = 0;
+      if constexpr (kMixed && KC == 1) {
+        // float32, one column: two sources per step in packed f32x2
+        // arithmetic.  The tile is staged as source pairs: per pair p,
+        // (x_hi, y_hi) and (z_hi, w) of sources 2p and 2p + 1 interleaved,
+        // then (x_lo, y_lo) and z_lo; an odd tile ends with a far, weightless
+        // dummy source (finite kernel value times 0).
+        float* P01 = reinterpret_cast<float*>(&s_sh[wl][0]);  // [16][4] | [16][4]
+        float* P23 = reinterpret_cast<float*>(&s_sl[wl][0]);  // [16][4] | [16][2]
+        const unsigned long long ntxh = f2_pack(-tp.h[0], -tp.h[0]), ntyh = f2_pack(-tp.h[1], -tp.h[1]),
+                                 ntzh = f2_pack(-tp.h[2], -tp.h[2]), ntxl = f2_pack(-tp.l[0], -tp.l[0]),
+                                 ntyl = f2_pack(-tp.l[1], -tp.l[1]), ntzl = f2_pack(-tp.l[2], -tp.l[2]);
+        for (int v0 = 0; v0 < nsrc_total; v0 += 32) {
+          const int v = v0 + lane, pr = lane >> 1, e = lane & 1;
+          float xh = 1.0e3f, yh = 0.f, zh = 0.f, xl = 0.f, yl = 0.f, zl = 0.f, wv = 0.f;
+          if (v < nsrc_total) {
+            while (v >= s_pre[wl][q + 1]) ++q;
+            const int j = s_nb[wl][q][0] + (v - s_pre[wl][q]);
+            RelPos<T> sp;
+            sp.set(spos[j] - c[0], spos[(int64_t)Ns + j] - c[1], spos[2 * (int64_t)Ns + j] - c[2]);
+            xh = sp.h[0], yh = sp.h[1], zh = sp.h[2], xl = sp.l[0], yl = sp.l[1], zl = sp.l[2];
+            wv = (float)wsorted[(int64_t)j * C + c0];
+          }
+          P01[4 * pr + e] = xh;
+          P01[4 * pr + 2 + e] = yh;
+          P01[64 + 4 * pr + e] = zh;
+          P01[64 + 4 * pr + 2 + e] = wv;
+          P23[4 * pr + e] = xl;
+          P23[4 * pr + 2 + e] = yl;
+          P23[64 + 2 * pr + e] = zl;
+          __syncwarp();
+          if (active) {
+            const int np = (min(32, nsrc_total - v0) + 1) >> 1;
+            unsigned long long part2 = 0ull;  // (0.f, 0.f)
+#pragma unroll 4
+            for (int pp = 0; pp < np; ++pp) {
+              const ulonglong2 a = *reinterpret_cast<const ulonglong2*>(P01 + 4 * pp);
+              const ulonglong2 b = *reinterpret_cast<const ulonglong2*>(P01 + 64 + 4 * pp);
+              const ulonglong2 cl = *reinterpret_cast<const ulonglong2*>(P23 + 4 * pp);
+              const unsigned long long zl2 = *reinterpret_cast<const unsigned long long*>(P23 + 64 + 2 * pp);
+              const unsigned long long dx = f2_add(f2_add(a.x, ntxh), f2_add(cl.x, ntxl));
+              const unsigned long long dy = f2_add(f2_add(a.y, ntyh), f2_add(cl.y, ntyl));
+              const unsigned long long dz = f2_add(f2_add(b.x, ntzh), f2_add(zl2, ntzl));
+              float k0, k1;
+              if constexpr (HasEvalR2<KF>::value) {
+                const unsigned long long r2 = f2_fma(dz, dz, f2_fma(dy, dy, f2_mul(dx, dx)));
+                float r0, r1;
+                f2_unpack(r2, r0, r1);
+                k0 = KF::template eval_r2<float>(r0, kp);
+                k1 = KF::template eval_r2<float>(r1, kp);
+              } else {
+                float x0, x1, y0, y1, z0, z1;
+                f2_unpack(dx, x0, x1);
+                f2_unpack(dy, y0, y1);
+                f2_unpack(dz, z0, z1);
+                k0 = KF::template eval<float>(x0, y0, z0, kp);
+                k1 = KF::template eval<float>(x1, y1, z1, kp);
+              }
+              if (isinf(k0)) k0 = 0;  // coincident points (include/compute.hpp:767)
+              if (isinf(k1)) k1 = 0;
+              part2 = f2_fma(f2_pack(k0, k1), b.y, part2);
+            }
+            float p0, p1;
+            f2_unpack(part2, p0, p1);
+            acc[0].add(p0 + p1);
+          }
+          __syncwarp();
+        }
+      } else {
       for (int v0 = 0; v0 < nsrc_total; v0 += 32) {
         const int v = v0 + lane;
         if (v < nsrc_total) {
@@ -394,6 +496,7 @@ __global__ void __launch_bounds__(32 * kLeafWarps, kLeafBlocks<T, KC>)
             if (cc < cg) acc[cc].add(part[cc]);
         }
         __syncwarp();
+      }
       }
       if (active) {
         const int64_t oi = tperm[i];

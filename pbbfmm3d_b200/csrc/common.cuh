@@ -27,6 +27,10 @@ struct Kern<PBBFMM_KERNEL_LAPLACIAN> {
   __device__ static T eval(T dx, T dy, T dz, const double*) {
     return inv_sqrt(dx * dx + dy * dy + dz * dz);
   }
+  template <typename T>
+  __device__ static T eval_r2(T r2, const double*) {
+    return inv_sqrt(r2);
+  }
   // value, and g = dK/dd (the gradient with respect to the target is -g); g = 0 at d = 0
   template <typename T>
   __device__ static T grad(T dx, T dy, T dz, const double* p, T* g) {
@@ -42,6 +46,11 @@ struct Kern<PBBFMM_KERNEL_ONEOVERR2> {
   template <typename T>
   __device__ static T eval(T dx, T dy, T dz, const double*) {
     T ri = inv_sqrt(dx * dx + dy * dy + dz * dz);
+    return ri * ri;
+  }
+  template <typename T>
+  __device__ static T eval_r2(T r2, const double*) {
+    T ri = inv_sqrt(r2);
     return ri * ri;
   }
   // value, and g = dK/dd (the gradient with respect to the target is -g); g = 0 at d = 0
@@ -156,6 +165,10 @@ struct Kern<PBBFMM_KERNEL_EXPCOV> {
   __device__ static T eval(T dx, T dy, T dz, const double* p) {
     return exp(-sqrt(dx * dx + dy * dy + dz * dz) / T(p[0]));
   }
+  template <typename T>
+  __device__ static T eval_r2(T r2, const double* p) {
+    return exp(-sqrt(r2) / T(p[0]));
+  }
   // value, and g = dK/dd (the gradient with respect to the target is -g); g = 0 at d = 0
   template <typename T>
   __device__ static T grad(T dx, T dy, T dz, const double* p, T* g) {
@@ -171,6 +184,10 @@ struct Kern<PBBFMM_KERNEL_GAUSSSIGMA> {
   template <typename T>
   __device__ static T eval(T dx, T dy, T dz, const double* p) {
     return exp(-(dx * dx + dy * dy + dz * dz) / (T(2) * T(p[0]) * T(p[0])));
+  }
+  template <typename T>
+  __device__ static T eval_r2(T r2, const double* p) {
+    return exp(-r2 / (T(2) * T(p[0]) * T(p[0])));
   }
   // value, and g = dK/dd (the gradient with respect to the target is -g); g = 0 at d = 0
   template <typename T>

@@ -48,9 +48,7 @@ __global__ void __launch_bounds__(32 * L2LCfg<N>::warps)
   const T* src = Fpar + ((int64_t)par * C + col) * n3;
   for (int i = lane; i < n3; i += 32) sp[i] = src[i];
   // which children hold targets (lanes 0..8 read the 9 leaf-range bounds at
-  // once), and (float32, orders up to 5: the registers of order 6 cost more
-  // resident warps than the batched loads save) every child's current
-  // coefficients, loaded with all loads in flight before the passes
+  // once)
   int bound = 0;
   if (lane <= 8) bound = tstart[(int64_t)(par * 8 + lane) * span_child];
   unsigned present = 0;
@@ -59,61 +57,126 @@ __global__ void __launch_bounds__(32 * L2LCfg<N>::warps)
     present |= (__shfl_sync(0xffffffffu, bound, ch + 1) != __shfl_sync(0xffffffffu, bound, ch))
                    ? 1u << ch : 0u;
   constexpr int PER = (n3 + 31) / 32;
+  constexpr bool kRows = N <= (sizeof(T) == 4 ? 6 : 5);  // passes as row tasks
   constexpr bool kBatch = sizeof(T) == 4 && N <= 5;
-  T cur[kBatch ? 8 : 1][kBatch ? PER : 1];
-  if constexpr (kBatch) {
+  constexpr int TPL = (n2 + 31) / 32;                    // row tasks per lane
+  if constexpr (kRows) {
+    // Each pass as row tasks: a lane loads the N inputs of one 1-D transform
+    // once and forms its N outputs (operator rows read by broadcast).  The
+    // z pass of task r updates the child's coefficients r n .. r n + n-1,
+    // read up front for all children (kBatch) so those loads are in flight
+    // together.
+    T cur[kBatch ? 8 : 1][kBatch ? TPL : 1][kBatch ? N : 1];
+    if constexpr (kBatch) {
 #pragma unroll
-    for (int ch = 0; ch < 8; ++ch) {
-      const T* d = Fch + ((int64_t)(par * 8 + ch) * C + col) * n3;
+      for (int ch = 0; ch < 8; ++ch) {
+        const T* d = Fch + ((int64_t)(par * 8 + ch) * C + col) * n3;
 #pragma unroll
-      for (int r = 0; r < PER; ++r) {
-        const int i = lane + 32 * r;
-        cur[ch][r] = ((present >> ch) & 1) && i < n3 ? d[i] : T(0);
+        for (int t = 0; t < TPL; ++t) {
+          const int r = lane + 32 * t;
+#pragma unroll
+          for (int l3 = 0; l3 < N; ++l3)
+            cur[ch][t][l3] = ((present >> ch) & 1) && r < n2 ? d[r * N + l3] : T(0);
+        }
       }
     }
-  }
-  __syncwarp();
-#pragma unroll
-  for (int ch = 0; ch < 8; ++ch) {
-    const int cell = par * 8 + ch;
-    if (!((present >> ch) & 1)) continue;  // child without targets
-    const T* wx = sCw + (((ch >> 2) & 1) ? n2 : 0);
-    const T* wy = sCw + (((ch >> 1) & 1) ? n2 : 0);
-    const T* wz = sCw + ((ch & 1) ? n2 : 0);
-    // x: Fx[l1 n2 + l2 n + l3] = sum_k F[k n2 + l2 n + l3] wx[l1 + k n]
-    for (int i = lane; i < n3; i += 32) {
-      const int l1 = i / n2, rem = i % n2;
-      T v = 0;
-#pragma unroll
-      for (int k = 0; k < N; ++k) v += sp[k * n2 + rem] * wx[l1 + k * N];
-      b0[i] = v;
-    }
     __syncwarp();
-    // y: Fy[l1 n2 + l2 n + l3] = sum_k Fx[l1 n2 + k n + l3] wy[l2 + k n]
-    for (int i = lane; i < n3; i += 32) {
-      const int l1 = i / n2, l2 = (i / N) % N, l3 = i % N;
-      T v = 0;
 #pragma unroll
-      for (int k = 0; k < N; ++k) v += b0[l1 * n2 + k * N + l3] * wy[l2 + k * N];
-      b1[i] = v;
+    for (int ch = 0; ch < 8; ++ch) {
+      const int cell = par * 8 + ch;
+      if (!((present >> ch) & 1)) continue;  // child without targets
+      const T* wx = sCw + (((ch >> 2) & 1) ? n2 : 0);
+      const T* wy = sCw + (((ch >> 1) & 1) ? n2 : 0);
+      const T* wz = sCw + ((ch & 1) ? n2 : 0);
+      // x: Fx[l1 n2 + rem] = sum_k F[k n2 + rem] wx[l1 + k n]   (task rem)
+      for (int q = lane; q < n2; q += 32) {
+        T x[N];
+#pragma unroll
+        for (int k = 0; k < N; ++k) x[k] = sp[k * n2 + q];
+#pragma unroll
+        for (int l1 = 0; l1 < N; ++l1) {
+          T v = 0;
+#pragma unroll
+          for (int k = 0; k < N; ++k) v = fma(x[k], wx[l1 + k * N], v);
+          b0[l1 * n2 + q] = v;
+        }
+      }
+      __syncwarp();
+      // y: Fy[l1 n2 + l2 n + l3] = sum_k Fx[l1 n2 + k n + l3] wy[l2 + k n]   (task (l1, l3))
+      for (int q = lane; q < n2; q += 32) {
+        const int l1 = q / N, l3 = q % N;
+        T x[N];
+#pragma unroll
+        for (int k = 0; k < N; ++k) x[k] = b0[l1 * n2 + k * N + l3];
+#pragma unroll
+        for (int l2 = 0; l2 < N; ++l2) {
+          T v = 0;
+#pragma unroll
+          for (int k = 0; k < N; ++k) v = fma(x[k], wy[l2 + k * N], v);
+          b1[l1 * n2 + l2 * N + l3] = v;
+        }
+      }
+      __syncwarp();
+      // z: Fchild[r n + l3] += sum_k Fy[r n + k] wz[l3 + k n]   (task row r over n^2)
+      T* dst = Fch + ((int64_t)cell * C + col) * n3;
+#pragma unroll
+      for (int t = 0; t < TPL; ++t) {
+        const int r = lane + 32 * t;
+        if (r < n2) {
+          T x[N];
+#pragma unroll
+          for (int k = 0; k < N; ++k) x[k] = b1[r * N + k];
+#pragma unroll
+          for (int l3 = 0; l3 < N; ++l3) {
+            T v = 0;
+#pragma unroll
+            for (int k = 0; k < N; ++k) v = fma(x[k], wz[l3 + k * N], v);
+            if constexpr (kBatch) dst[r * N + l3] = cur[ch][t][l3] + v;
+            else dst[r * N + l3] += v;
+          }
+        }
+      }
+      __syncwarp();
     }
+  } else {
     __syncwarp();
-    // z: Fchild[l1 n + l3] += sum_k Fy[l1 n + k] wz[l3 + k n]   (l1 over n^2)
-    T* dst = Fch + ((int64_t)cell * C + col) * n3;
+    for (int ch = 0; ch < 8; ++ch) {
+      const int cell = par * 8 + ch;
+      if (!((present >> ch) & 1)) continue;  // child without targets
+      const T* wx = sCw + (((ch >> 2) & 1) ? n2 : 0);
+      const T* wy = sCw + (((ch >> 1) & 1) ? n2 : 0);
+      const T* wz = sCw + ((ch & 1) ? n2 : 0);
+      // x: Fx[l1 n2 + l2 n + l3] = sum_k F[k n2 + l2 n + l3] wx[l1 + k n]
+      for (int i = lane; i < n3; i += 32) {
+        const int l1 = i / n2, rem = i % n2;
+        T v = 0;
 #pragma unroll
-    for (int r = 0; r < PER; ++r) {
-      const int i = lane + 32 * r;
-      if (i < n3) {
+        for (int k = 0; k < N; ++k) v += sp[k * n2 + rem] * wx[l1 + k * N];
+        b0[i] = v;
+      }
+      __syncwarp();
+      // y: Fy[l1 n2 + l2 n + l3] = sum_k Fx[l1 n2 + k n + l3] wy[l2 + k n]
+      for (int i = lane; i < n3; i += 32) {
+        const int l1 = i / n2, l2 = (i / N) % N, l3 = i % N;
+        T v = 0;
+#pragma unroll
+        for (int k = 0; k < N; ++k) v += b0[l1 * n2 + k * N + l3] * wy[l2 + k * N];
+        b1[i] = v;
+      }
+      __syncwarp();
+      // z: Fchild[l1 n + l3] += sum_k Fy[l1 n + k] wz[l3 + k n]   (l1 over n^2)
+      T* dst = Fch + ((int64_t)cell * C + col) * n3;
+      for (int i = lane; i < n3; i += 32) {
         const int l1 = i / N, l3 = i % N;
         T v = 0;
 #pragma unroll
         for (int k = 0; k < N; ++k) v += b1[l1 * N + k] * wz[l3 + k * N];
-        if constexpr (kBatch) dst[i] = cur[ch][r] + v;
-        else dst[i] += v;
+        dst[i] += v;
       }
+      __syncwarp();
     }
-    __syncwarp();
   }
+  (void)PER;
 }
 
 template <typename T>

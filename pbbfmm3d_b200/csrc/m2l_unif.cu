@@ -168,21 +168,40 @@ __global__ void k_fft_fwd(const int* __restrict__ cells, int ncl, const T* __res
   extern __shared__ __align__(16) unsigned char smraw[];
   T* sm = reinterpret_cast<T*>(smraw);
   constexpr int m = 2 * n - 1, n2 = n * n, n3 = n2 * n, ny = n * m * n;
-  T* sin_ = sm + 2 * m;                         // CG * n3 real moments
-  C2* Z = (C2*)(sin_ + ((CG * n3 + 3) & ~3));  // CG * n * n * n   (l1, l2, k3)
+  const int sin_stride = (CG * n3 + 3) & ~3;
+  T* sin_buf = sm + 2 * m;                      // 2 x CG * n3 real moments (double-buffered)
+  C2* Z = (C2*)(sin_buf + 2 * sin_stride);      // CG * n * n * n   (l1, l2, k3)
   C2* Y = Z + CG * n3;                         // CG * n * m * n   (l1, k2, k3)
   unsigned* s_amax = reinterpret_cast<unsigned*>(Y + CG * ny);  // [m n][8]
   (void)twid;
   const int tid = threadIdx.x, bd = blockDim.x;
   if (amax)
     for (int i = tid; i < m * n * 8; i += bd) s_amax[i] = 0u;
+  // work units (cell, column group) of this CTA in order; each unit's moments
+  // are copied (cp.async) into the other buffer while the previous unit is
+  // transformed
+  const int ngrp = (C + CG - 1) / CG;
+  auto fetch = [&](int u, int buf) {
+    const int ci = blockIdx.x + (u / ngrp) * gridDim.x;
+    if (ci < ncl) {
+      const int c0 = (u % ngrp) * CG, cg = min(CG, C - c0);
+      const T* src = S_l + ((int64_t)cells[ci] * C + c0) * n3;
+      T* dst = sin_buf + buf * sin_stride;
+      for (int i = tid; i < cg * n3; i += bd) cp_async_elem(dst + i, src + i, true);
+    }
+    cp_async_commit();
+  };
+  int unit = 0;
+  fetch(0, 0);
   for (int ci = blockIdx.x; ci < ncl; ci += gridDim.x) {
   const int cell = cells[ci];
-  for (int c0 = 0; c0 < C; c0 += CG) {
+  for (int c0 = 0; c0 < C; c0 += CG, ++unit) {
     const int cg = min(CG, C - c0);
+    __syncthreads();  // the previous unit's readers of the other buffer are done
+    fetch(unit + 1, (unit + 1) & 1);
+    asm volatile("cp.async.wait_group 1;\n" ::: "memory");
     __syncthreads();
-    for (int i = tid; i < cg * n3; i += bd) sin_[i] = S_l[((int64_t)cell * C + c0) * n3 + i];
-    __syncthreads();
+    const T* sin_ = sin_buf + (unit & 1) * sin_stride;
     // z: Z[c][l1][l2][k3] = sum_l3 S[c][l1][l2][l3] w^(k3 l3), real input
     for (int job = tid; job < cg * n2; job += bd) {
       const T* s = sin_ + job * n;
@@ -262,6 +281,7 @@ __global__ void k_fft_fwd(const int* __restrict__ cells, int ncl, const T* __res
     }
   }
   }
+  cp_async_wait_all();  // the (empty) prefetch past the last unit
   if (amax) {
     __syncthreads();
     for (int i = tid; i < m * n * 8; i += bd)
@@ -651,7 +671,7 @@ static int run_m2l_unif_t(pbbfmm_tree* t, int C, cudaStream_t st) {
   // forward transforms of all nonempty source cells, levels 2..L
   const int fwd_col = n3 * ts + n3 * 2 * ts + n * m * n * 2 * ts;
   const int CGf = max(1, min(C, 60000 / fwd_col));
-  const size_t smem_f = (size_t)ts * (2 * m + ((CGf * n3 + 3) & ~3)) +
+  const size_t smem_f = (size_t)ts * (2 * m + 2 * ((CGf * n3 + 3) & ~3)) +
                         (size_t)2 * ts * (CGf * n3 + CGf * n * m * n) + (size_t)4 * m * n * 8;
   const int inv_col = (nk + n * m * n + n3) * 2 * ts;
   const int CGi = max(1, min(C, 60000 / inv_col));

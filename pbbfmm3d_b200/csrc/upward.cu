@@ -40,11 +40,12 @@ constexpr int p2m_warps() {
 
 // One warp per nonempty source leaf.  Lanes first evaluate the basis of up to
 // 32 points (one point each) and stage their weights, then each lane owns
-// outputs o = lane + 32 r of the (column, l1, l2, l3) block and sums over the
-// staged points in point order.  Leaves with more than 32 points accumulate
-// chunk by chunk in the output array (each output has a single owner lane).
+// tasks (column, l1, l2) and sums the N outputs l3 of a task over the staged
+// points in point order.  Leaves with more than 32 points accumulate chunk by
+// chunk in the output array (each output has a single owner lane).
 // T = float (mixed path): the basis is evaluated from float64 leaf-relative
-// coordinates and each chunk's sum is compensated (Kahan).
+// coordinates, each chunk of up to 32 points is summed in float32 and added to
+// the running value in float64.
 template <int N, typename T, int kP2MWarps = p2m_warps<N, T>()>
 __global__ void __launch_bounds__(32 * kP2MWarps)
     k_p2m(const int* __restrict__ leaves, int nleaves, const int* __restrict__ sstart,
@@ -86,19 +87,26 @@ __global__ void __launch_bounds__(32 * kP2MWarps)
           sW[wl][lane][cc] = (T)wsorted[(int64_t)(p0 + lane) * C + c0 + cc];
       }
       __syncwarp();
-      for (int o = lane; o < cg * n3; o += 32) {
-        const int cc = o / n3, l = o % n3;
-        const int l1 = l / (N * N), l2 = (l / N) % N, l3 = l % N;
-        if (kKahan) {
-          Kahan<T> acc;
-          for (int j = 0; j < cnt; ++j)
-            acc.add(sW[wl][j][cc] * sB[wl][0][l1][j] * sB[wl][1][l2][j] * sB[wl][2][l3][j]);
-          Sout[o] = (T)(p0 == a ? acc.value() : (double)Sout[o] + acc.value());
-        } else {
-          T sum = p0 == a ? T(0) : Sout[o];
-          for (int j = 0; j < cnt; ++j)
-            sum += sW[wl][j][cc] * sB[wl][0][l1][j] * sB[wl][1][l2][j] * sB[wl][2][l3][j];
-          Sout[o] = sum;
+      // lane task (column, l1, l2): the N outputs l3 = 0..N-1 at once, the
+      // weight x basis product over (l1, l2) formed once per point
+      for (int task = lane; task < cg * N * N; task += 32) {
+        const int cc = task / (N * N), l12 = task % (N * N), l1 = l12 / N, l2 = l12 % N;
+        T part[N];
+#pragma unroll
+        for (int l3 = 0; l3 < N; ++l3) part[l3] = 0;
+        for (int j = 0; j < cnt; ++j) {
+          const T t = sW[wl][j][cc] * sB[wl][0][l1][j] * sB[wl][1][l2][j];
+#pragma unroll
+          for (int l3 = 0; l3 < N; ++l3) part[l3] = fma(t, sB[wl][2][l3][j], part[l3]);
+        }
+        T* o = Sout + cc * n3 + l12 * N;
+#pragma unroll
+        for (int l3 = 0; l3 < N; ++l3) {
+          if (kKahan) {  // the chunk's float32 sum added to the float64 running value
+            o[l3] = (T)(p0 == a ? (double)part[l3] : (double)o[l3] + (double)part[l3]);
+          } else {
+            o[l3] = p0 == a ? part[l3] : o[l3] + part[l3];
+          }
         }
       }
     }
@@ -193,6 +201,81 @@ __global__ void __launch_bounds__(32 * M2MCfg<N, T>::warps)
       }
   }
   __syncwarp();
+  // Orders up to 6 (float32) or 5 (float64): each pass as row tasks, a lane
+  // loading the N inputs of one 1-D transform once and forming its N outputs
+  // (the operator rows read by broadcast).  Higher orders (registers):
+  // element tasks, one output per lane and pass.
+  if constexpr (N <= (sizeof(T) == 4 ? 6 : 5)) {
+  constexpr int TPL = (n2 + 31) / 32;  // x-pass tasks per lane
+  T acc[TPL][N];
+#pragma unroll
+  for (int t = 0; t < TPL; ++t)
+#pragma unroll
+    for (int l = 0; l < N; ++l) acc[t][l] = 0;
+  for (int ch = 0; ch < 8; ++ch) {
+    if (!((present >> ch) & 1)) continue;
+    const T* wx = sCw + (((ch >> 2) & 1) ? n2 : 0);
+    const T* wy = sCw + (((ch >> 1) & 1) ? n2 : 0);
+    const T* wz = sCw + ((ch & 1) ? n2 : 0);
+    const T* sc = sch + ch * n3;
+    // z: Sz[r n + l3] = sum_k S[r n + k] wz[l3 n + k]   (row r over n^2)
+    for (int r = lane; r < n2; r += 32) {
+      T x[N];
+#pragma unroll
+      for (int k = 0; k < N; ++k) x[k] = sc[r * N + k];
+#pragma unroll
+      for (int l3 = 0; l3 < N; ++l3) {
+        T v = 0;
+#pragma unroll
+        for (int k = 0; k < N; ++k) v = fma(x[k], wz[l3 * N + k], v);
+        b0[r * N + l3] = v;
+      }
+    }
+    __syncwarp();
+    // y: Sy[l1 n2 + l2 n + l3] = sum_k Sz[l1 n2 + k n + l3] wy[l2 n + k]   (task (l1, l3))
+    for (int q = lane; q < n2; q += 32) {
+      const int l1 = q / N, l3 = q % N;
+      T x[N];
+#pragma unroll
+      for (int k = 0; k < N; ++k) x[k] = b0[l1 * n2 + k * N + l3];
+#pragma unroll
+      for (int l2 = 0; l2 < N; ++l2) {
+        T v = 0;
+#pragma unroll
+        for (int k = 0; k < N; ++k) v = fma(x[k], wy[l2 * N + k], v);
+        b1[l1 * n2 + l2 * N + l3] = v;
+      }
+    }
+    __syncwarp();
+    // x: SS[l1 n2 + rem] += sum_k Sy[k n2 + rem] wx[l1 n + k]   (task rem)
+#pragma unroll
+    for (int t = 0; t < TPL; ++t) {
+      const int rem = lane + 32 * t;
+      if (rem < n2) {
+        T x[N];
+#pragma unroll
+        for (int k = 0; k < N; ++k) x[k] = b1[k * n2 + rem];
+#pragma unroll
+        for (int l1 = 0; l1 < N; ++l1) {
+          T v = acc[t][l1];
+#pragma unroll
+          for (int k = 0; k < N; ++k) v = fma(x[k], wx[l1 * N + k], v);
+          acc[t][l1] = v;
+        }
+      }
+    }
+    __syncwarp();
+  }
+  T* dst = Spar + ((int64_t)par * C + col) * n3;
+#pragma unroll
+  for (int t = 0; t < TPL; ++t) {
+    const int rem = lane + 32 * t;
+    if (rem < n2)
+#pragma unroll
+      for (int l1 = 0; l1 < N; ++l1) dst[l1 * n2 + rem] = acc[t][l1];
+  }
+  } else {
+  constexpr int PER = (n3 + 31) / 32;
   T acc[PER];
 #pragma unroll
   for (int r = 0; r < PER; ++r) acc[r] = 0;
@@ -239,6 +322,7 @@ __global__ void __launch_bounds__(32 * M2MCfg<N, T>::warps)
   for (int r = 0; r < PER; ++r) {
     const int i = lane + 32 * r;
     if (i < n3) dst[i] = acc[r];
+  }
   }
 }
 
