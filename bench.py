@@ -456,9 +456,9 @@ def per_step(kt, steps):
 
 # DRAM bytes per (cell, frequency, column) of the frequency-domain M2L, from
 # the ncu capture in profiles/k_m2l_unif_tc_expcov0.3_unif5_N262144_C8_L5.md
-# (the level-5 launch of k_m2l_unif_tc: 891.98 MB read + 810.80 MB written
+# (the level-5 launch of k_m2l_unif_tc: 1021.17 MB read + 815.66 MB written
 # for 32,768 cells x 405 frequencies x 8 columns)
-MAC_DRAM_BYTES_PER_UNIT = (891.978752e6 + 810.800896e6) / (32768 * 405 * 8)
+MAC_DRAM_BYTES_PER_UNIT = (1021.168e6 + 815.659e6) / (32768 * 405 * 8)
 # tensor-core MAC tiling (csrc/m2l_unif_tc.cu): 8 target lines of 16 parents
 # per CTA, 3 x 10 source lines per frequency, 6 MMAs (M = 128, K = 16) per
 # source line with N = 32 x (target lines it serves)
