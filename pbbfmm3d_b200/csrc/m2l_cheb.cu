@@ -99,17 +99,50 @@ struct TypeTiles {
 
 // M2L for one level on the CUDA cores (float64 path; also the float32 path
 // when r_f exceeds the tensor-core tile).  A CTA owns 128 (target, column)
-// rows of one child type and 128 rows of r_f; it walks the offsets that have
-// a source in the tile and, for each, r_s in chunks of 16, with the gathered
-// proxies (A, 128 x 16) and the operator (B, 128 x 16) in double-buffered
-// shared memory (cp.async, element-wise so the A tile is stored transposed).
-// Each thread accumulates an 8 x 8 block (rows ty + 16 i, columns tx + 16 j).
+// rows of one child type and 128 rows of r_f, and walks the offsets where
+// some row of the tile has a source.  Per offset only the rows with a source
+// take part: they are compacted (in tile-row order) into chunks of 16, so
+// that a tile whose targets have few sources at an offset (sparse cells at
+// the deepest levels of a clustered tree) multiplies 16-row chunks instead
+// of all 128 rows.  For each offset and r_s in steps of 16, the gathered
+// proxies of the compacted rows (A, up to 128 x 16) and the operator (B,
+// 128 x 16) are staged in double-buffered shared memory (cp.async, element-
+// wise so the A tile is stored transposed).  Each thread accumulates a
+// c x 8 block of the offset's product in registers (compacted rows ty + 16 i,
+// i < c chunks; columns tx + 16 j), then adds it into the tile's running sum
+// in shared memory under the rows' target positions.  Every row of the tile
+// appears at most once per offset, the offsets are taken in a fixed order,
+// and a block barrier separates the adds of consecutive offsets, so the
+// result is deterministic.
 constexpr int CG_M = 128, CG_N = 128, CG_K = 16, CG_THREADS = 256;
+constexpr int CG_NS = 2;           // stages: loads run one K step ahead
+constexpr int CG_SLOTS = 3;        // compacted row lists in flight (see lookup)
 constexpr int CG_APAD = CG_M + 1;  // A rows padded: conflict-free transposed stores
 
+// stages (A and B) and the running sum [CG_M][CG_N]; the float64 instance
+// takes 192 KB (two 16-deep stages next to the 128 KB running sum)
 template <typename T>
 __host__ __device__ constexpr size_t cg_smem_bytes() {
-  return sizeof(T) * 2 * CG_K * (CG_APAD + CG_N);
+  return sizeof(T) * (CG_NS * CG_K * (CG_APAD + CG_N) + (size_t)CG_M * CG_N);
+}
+
+// One K step of CG_K for the first NC chunks of compacted rows: thread
+// (tx, ty) owns compacted rows ty + 16 i and columns tx + 16 j.
+template <int NC, typename T>
+__device__ __forceinline__ void cg_step(const T* __restrict__ as, const T* __restrict__ bs, int tx,
+                                        int ty, T (&acc)[8][8]) {
+#pragma unroll
+  for (int kk = 0; kk < CG_K; ++kk) {
+    T a[NC], b[8];
+#pragma unroll
+    for (int i = 0; i < NC; ++i) a[i] = as[kk * CG_APAD + ty + 16 * i];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) b[j] = bs[kk * CG_N + tx + 16 * j];
+#pragma unroll
+    for (int i = 0; i < NC; ++i)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+  }
 }
 
 template <typename T>
@@ -118,14 +151,23 @@ __global__ void __launch_bounds__(CG_THREADS, 1)
                TypeTiles tt, int C, int lev, const int* __restrict__ sstart, int span,
                const int* __restrict__ offs, const T* __restrict__ proxy, T* __restrict__ pf) {
   extern __shared__ __align__(16) unsigned char cg_raw[];
-  T* As = reinterpret_cast<T*>(cg_raw);         // [2][CG_K][CG_APAD]
-  T* Bs = As + 2 * CG_K * CG_APAD;              // [2][CG_K][CG_N]
-  __shared__ long long s_src[2][CG_M];          // proxy row offset of each row's source, or -1
+  T* As = reinterpret_cast<T*>(cg_raw);         // [CG_NS][CG_K][CG_APAD]
+  T* Bs = As + CG_NS * CG_K * CG_APAD;          // [CG_NS][CG_K][CG_N]
+  T* Sum = Bs + CG_NS * CG_K * CG_N;            // [CG_M][CG_N] running sum by tile row
+  // Compacted rows of valid offset q, in slot q % CG_SLOTS.  The lookup of
+  // the offset that starts at iteration it + 1 runs at the top of iteration
+  // it; with one K step per offset, offset q - 2's adds end in iteration
+  // it - 1 and q - 3's in it - 2, behind iteration it - 1's block barrier:
+  // three slots never overwrite rows that a thread may still be adding.
+  __shared__ long long s_src[CG_SLOTS][CG_M];   // compacted row j: proxy row offset of its source
+  __shared__ uint8_t s_row[CG_SLOTS][CG_M];     // compacted row j: its tile row
+  __shared__ int s_wcnt[CG_SLOTS][4];           // rows with a source per lookup warp
   __shared__ int s_cell[CG_M], s_xyz[CG_M];
   __shared__ uint32_t s_valid[6];
   __shared__ int4 s_off[189];
   __shared__ int s_nvalid;
-  const int tid = threadIdx.x, tx = tid & 15, ty = tid >> 4;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int tx = tid & 15, ty = tid >> 4;
   const int n0 = blockIdx.y * CG_N;
   int type = 0, tstart = 0, tlist = 0, tcount = 0;
 #pragma unroll
@@ -149,6 +191,7 @@ __global__ void __launch_bounds__(CG_THREADS, 1)
     s_xyz[tid] = (x << 20) | (y << 10) | z;
   }
   if (tid < 6) s_valid[tid] = 0;
+  for (int i = tid; i < CG_M * CG_N; i += CG_THREADS) Sum[i] = T(0);
   __syncthreads();
   if (tid < CG_M && s_cell[tid] >= 0 && tid % C == 0) {
     const int x = s_xyz[tid] >> 20, y = (s_xyz[tid] >> 10) & 1023, z = s_xyz[tid] & 1023;
@@ -173,9 +216,12 @@ __global__ void __launch_bounds__(CG_THREADS, 1)
   const int nvalid = s_nvalid;
   const int kchunks = (rs + CG_K - 1) / CG_K;
   const int niter = nvalid * kchunks;
-  // row tid's source for valid offset q, into s_src[q & 1]
+  // The rows of the tile that have a source at valid offset q, compacted in
+  // row order into slot q % CG_SLOTS; warps 0-3 (one row per thread), with a
+  // barrier of their own between the per-warp counts and the writes.
   auto lookup = [&](int q) {
     if (tid >= CG_M) return;
+    const int sl = q % CG_SLOTS;
     long long r = -1;
     const int cell = s_cell[tid];
     if (cell >= 0) {
@@ -188,15 +234,33 @@ __global__ void __launch_bounds__(CG_THREADS, 1)
           r = ((long long)bm * C + tid % C) * rs;
       }
     }
-    s_src[q & 1][tid] = r;
+    const unsigned has = __ballot_sync(0xffffffffu, r >= 0);
+    if (lane == 0) s_wcnt[sl][warp] = __popc(has);
+    asm volatile("bar.sync 1, 128;\n" ::: "memory");
+    int base = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) base += k < warp ? s_wcnt[sl][k] : 0;
+    if (r >= 0) {
+      const int j = base + __popc(has & ((1u << lane) - 1u));
+      s_src[sl][j] = r;
+      s_row[sl][j] = (uint8_t)tid;
+    }
   };
+  auto rows_at = [&](int q) {
+    const int sl = q % CG_SLOTS;
+    return s_wcnt[sl][0] + s_wcnt[sl][1] + s_wcnt[sl][2] + s_wcnt[sl][3];
+  };
+  // iteration j (offset q = j / kchunks, K chunk j % kchunks) into stage j % CG_NS
   auto load = [&](int j) {
-    const int q = j / kchunks, k0 = (j - q * kchunks) * CG_K, st = j & 1;
+    const int q = j / kchunks, k0 = (j - q * kchunks) * CG_K, st = j % CG_NS;
+    const int m_o = rows_at(q);
+    const int nr = (m_o + 15) & ~15;  // compacted rows, whole chunks (zero-filled)
+    const long long* src = s_src[q % CG_SLOTS];
     T* as = As + st * CG_K * CG_APAD;
     T* bs = Bs + st * CG_K * CG_N;
-    for (int e = tid; e < CG_M * CG_K; e += CG_THREADS) {
+    for (int e = tid; e < nr * CG_K; e += CG_THREADS) {
       const int m = e / CG_K, kk = e - m * CG_K;
-      const long long r = s_src[q & 1][m];
+      const long long r = m < m_o ? src[m] : -1;
       const bool ok = r >= 0 && k0 + kk < rs;
       cp_async_elem(as + kk * CG_APAD + m, proxy + (ok ? r + k0 + kk : 0), ok);
     }
@@ -209,49 +273,58 @@ __global__ void __launch_bounds__(CG_THREADS, 1)
     }
     cp_async_commit();
   };
-  T acc[8][8];
+  T acc[8][8];  // the current offset's product, compacted rows ty + 16 i
 #pragma unroll
   for (int i = 0; i < 8; ++i)
 #pragma unroll
     for (int j = 0; j < 8; ++j) acc[i][j] = 0;
-  if (niter > 0) {
-    lookup(0);
-    __syncthreads();
-    load(0);
-  }
+  // prologue: the first iteration's rows and loads
+  if (niter > 0) lookup(0);
+  __syncthreads();
+  if (niter > 0) load(0);
   for (int it = 0; it < niter; ++it) {
-    // the next offset's sources, one iteration ahead (other parity buffer)
-    const int qn = (it + 1) / kchunks;
-    if (it + 1 < niter && qn != it / kchunks) lookup(qn);
+    const int q = it / kchunks;
+    // the rows of the offset that starts at iteration it + 1
+    if (it + 1 < niter && (it + 1) % kchunks == 0) lookup((it + 1) / kchunks);
     cp_async_wait_all();
     __syncthreads();
     if (it + 1 < niter) load(it + 1);
-    const T* as = As + (it & 1) * CG_K * CG_APAD;
-    const T* bs = Bs + (it & 1) * CG_K * CG_N;
+    const T* as = As + (it % CG_NS) * CG_K * CG_APAD;
+    const T* bs = Bs + (it % CG_NS) * CG_K * CG_N;
+    const int m_o = rows_at(q);
+    switch ((m_o + 15) >> 4) {  // uniform: chunks of 16 compacted rows
+      case 1: cg_step<1>(as, bs, tx, ty, acc); break;
+      case 2: cg_step<2>(as, bs, tx, ty, acc); break;
+      case 3: cg_step<3>(as, bs, tx, ty, acc); break;
+      case 4: cg_step<4>(as, bs, tx, ty, acc); break;
+      case 5: cg_step<5>(as, bs, tx, ty, acc); break;
+      case 6: cg_step<6>(as, bs, tx, ty, acc); break;
+      case 7: cg_step<7>(as, bs, tx, ty, acc); break;
+      default: cg_step<8>(as, bs, tx, ty, acc); break;
+    }
+    if ((it + 1) % kchunks == 0) {
+      // the offset is complete: add its rows into the running sum by tile row
+      const uint8_t* rows = s_row[q % CG_SLOTS];
 #pragma unroll
-    for (int kk = 0; kk < CG_K; ++kk) {
-      T a[8], b[8];
+      for (int i = 0; i < 8; ++i) {
+        const int j = ty + 16 * i;
+        if (j < m_o) {
+          T* srow = Sum + (int)rows[j] * CG_N;
 #pragma unroll
-      for (int i = 0; i < 8; ++i) a[i] = as[kk * CG_APAD + ty + 16 * i];
+          for (int c = 0; c < 8; ++c) srow[tx + 16 * c] += acc[i][c];
+        }
 #pragma unroll
-      for (int j = 0; j < 8; ++j) b[j] = bs[kk * CG_N + tx + 16 * j];
-#pragma unroll
-      for (int i = 0; i < 8; ++i)
-#pragma unroll
-        for (int j = 0; j < 8; ++j) acc[i][j] = fma(a[i], b[j], acc[i][j]);
+        for (int c = 0; c < 8; ++c) acc[i][c] = 0;
+      }
     }
   }
-#pragma unroll
-  for (int i = 0; i < 8; ++i) {
-    const int m = ty + 16 * i;
+  __syncthreads();
+  const int ncol = min(CG_N, rf - n0);
+  for (int e = tid; e < CG_M * CG_N; e += CG_THREADS) {
+    const int m = e / CG_N, n = e - m * CG_N;
     const int cell = s_cell[m];
-    if (cell < 0) continue;
-    T* dst = pf + ((int64_t)cell * C + m % C) * rf;
-#pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const int n = n0 + tx + 16 * j;
-      if (n < rf) dst[n] = acc[i][j];
-    }
+    if (cell < 0 || n >= ncol) continue;
+    pf[((int64_t)cell * C + m % C) * rf + n0 + n] = Sum[m * CG_N + n];
   }
 }
 
