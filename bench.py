@@ -560,7 +560,7 @@ def cheb_roofline(fmm, tree, wl, results, steps, local_rank):
         "algorithmic": "%.4g useful flops per step = %d M2L pairs x rf %d x rs %d x %d cols x 2"
                        % (flops, sum(pairs.values()), rf, rs, C),
         "launches_per_step": kt["m2l"][1] / steps,
-        "fp64_path": {"kernel": "k_m2l_cheb<double> (CUDA cores)",
+        "fp64_path": {"kernel": "k_m2l_cheb<double> (CUDA cores, rows compacted per offset)",
                       "achieved": flops / (ms64 * 1e-3) / 1e12, "peak": fp64_peak,
                       "frac": flops / (ms64 * 1e-3) / 1e12 / fp64_peak, "unit": "TFLOP/s"},
     }
